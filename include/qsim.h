@@ -1,0 +1,252 @@
+/*
+ * qsim.h — C ABI of libqsim.so, the B200 (sm_100a) statevector engine.
+ *
+ * Conventions
+ *   - A state is a device pointer to 2^n complex64 amplitudes (float re, float im
+ *     interleaved), 16-byte aligned.  Basis index i has qubit q at bit q
+ *     (little-endian, the Qiskit convention).
+ *   - Gate matrices are HOST pointers to complex values, row-major, re/im
+ *     interleaved.  The "*_f32" forms take complex64 (the reference's tensor
+ *     dtype); program ops (qs_op) carry complex128 so that host-side fusion runs
+ *     in FP64.
+ *   - Two-qubit matrices: index bit 0 = first listed qubit, bit 1 = second.
+ *   - Every call returns QS_OK (0) or an error code; qs_last_error() gives the
+ *     message.  No C++ exception crosses this boundary.  Calls are asynchronous
+ *     on the handle's stream except those that return host scalars.
+ *   - One handle per host thread (a handle is not internally locked).
+ *
+ * Each entry point names the reference interface it replaces
+ * (DarrellThomas/qiskit-blackwell, file:line).
+ */
+#ifndef QSIM_H
+#define QSIM_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QS_OK            0
+#define QS_ERR_INVALID   1   /* bad argument (reference: TORCH_CHECK RuntimeError) */
+#define QS_ERR_CUDA      2   /* CUDA runtime error                                  */
+#define QS_ERR_NOMEM     3   /* device allocation failed                            */
+#define QS_ERR_TIMEOUT   4   /* a bounded device-side wait gave up                  */
+#define QS_ERR_BUDGET    5   /* request exceeds the handle's memory budget          */
+
+#define QS_MAX_QUBITS    34
+#define QS_MAX_CONTROLS  7
+
+typedef struct qs_context* qs_handle_t;
+typedef struct qs_plan_s*  qs_plan_t;
+
+/* ---------------------------------------------------------------- ops ---- */
+/* Circuit operation kinds (program IR).  Qubit roles per kind:             */
+enum {
+  QS_OP_U1      = 1,  /* dense 2x2 on q[0]; m = 2x2                          */
+  QS_OP_U2      = 2,  /* dense 4x4; bit0 = q[0], bit1 = q[1]; m = 4x4         */
+  QS_OP_DIAG1   = 3,  /* diagonal; m[0..3] = d0, d1 on q[0]                   */
+  QS_OP_DIAG2   = 4,  /* diagonal; m = d[4], index = b(q[1])<<1 | b(q[0])     */
+  QS_OP_MCU1    = 5,  /* controls q[0..nq-2], target q[nq-1]; m = 2x2         */
+  QS_OP_MCU2    = 6,  /* controls q[0..nq-3], targets q[nq-2] (bit0), q[nq-1] */
+  QS_OP_MCX     = 7,  /* exact X; controls q[0..nq-2], target q[nq-1]         */
+  QS_OP_MCSWAP  = 8,  /* exact swap; controls q[0..nq-3], targets last two    */
+  QS_OP_MCPHASE = 9,  /* multiply by m[0]+i m[1] where all q[0..nq-1] are 1   */
+  QS_OP_Y       = 10, /* exact Pauli-Y on q[0]                                */
+  QS_OP_RX      = 11, /* exp(-i m[0] X/2) on q[0]; param = parameter index    */
+  QS_OP_RY      = 12, /* exp(-i m[0] Y/2) on q[0]                             */
+  QS_OP_RZ      = 13  /* exp(-i m[0] Z/2) on q[0]                             */
+};
+
+typedef struct qs_op {
+  int32_t kind;
+  int32_t nq;        /* number of entries of q[] in use                      */
+  int32_t q[8];
+  int32_t param;     /* parameter index for QS_OP_R*; -1 otherwise           */
+  int32_t flags;     /* reserved, 0                                          */
+  double  m[32];     /* up to 16 complex128 coefficients, re/im interleaved  */
+} qs_op;
+
+typedef struct qs_plan_info {
+  int32_t n_qubits;
+  int32_t tile_bits;
+  int32_t n_passes;
+  int32_t n_blocks;
+  int64_t n_ops_in;      /* ops given to the planner                        */
+  int64_t n_ops_fused;   /* device ops after FP64 1Q fusion                  */
+  double  bytes_moved;   /* HBM bytes: passes * 16 * 2^n                     */
+  double  flops;         /* FP32 flop estimate of the program                */
+} qs_plan_info;
+
+/* ------------------------------------------------------------ context ---- */
+/* Reference: blackwell_backend/simulator.py:95-116 (BlackwellSimulator
+ * __init__ loads the kernels); bwk/setup.py:20-44 (the one extension).      */
+int  qs_create(int device, qs_handle_t* out);
+int  qs_destroy(qs_handle_t h);
+/* Run subsequent work on a caller-owned cudaStream_t (e.g. torch's current
+ * stream).  NULL selects the handle's own stream.                           */
+int  qs_set_stream(qs_handle_t h, void* cuda_stream);
+void* qs_get_stream(qs_handle_t h);
+int  qs_sync(qs_handle_t h);
+const char* qs_last_error(qs_handle_t h);
+const char* qs_version(void);
+/* Tile bits used by the fused-pass planner (10..14); 0 = default (13).      */
+int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
+/* Number of kernels this handle has launched since creation.               */
+int64_t qs_launch_count(qs_handle_t h);
+
+/* ------------------------------------------------------------ states ----- */
+/* Reference: bwk/csrc/apply_diagonal_sm120.cu:109-113,210-224 (state_init) */
+int qs_state_init(qs_handle_t h, void* state, int n_qubits);
+/* |index> basis state (generalises state_init).                            */
+int qs_state_init_basis(qs_handle_t h, void* state, int n_qubits, uint64_t index);
+/* Reference: bwk/csrc/batch_sm120.cu:165-181 (state_init_batched)          */
+int qs_state_init_batched(qs_handle_t h, void* states, int n_states, int n_qubits);
+
+/* ------------------------------------------------------- single gates ---- */
+/* Reference: bwk/csrc/apply_gate_sm120.cu:65-114,269-307 (apply_gate).     */
+int qs_apply_1q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64, int target);
+/* Reference: bwk/csrc/apply_gate2q_sm120.cu:84-228,232-280 (apply_gate_2q).
+ * Unlike the reference (which always maps bit 0 to min(q0,q1)), bit 0 of the
+ * matrix index is q0 here; blackwell_kernels.apply_gate_2q sorts the qubits to
+ * keep the reference's call semantics.                                      */
+int qs_apply_2q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64, int q0, int q1);
+/* Reference: bwk/csrc/apply_diagonal_sm120.cu:43-59,118-146 (apply_diagonal) */
+int qs_apply_diag1(qs_handle_t h, void* state, int n_qubits, const float* diag_c64, int target);
+/* Reference: bwk/csrc/apply_diagonal_sm120.cu:64-83,150-175 (apply_diagonal_phase) */
+int qs_apply_phase(qs_handle_t h, void* state, int n_qubits, float phase_re, float phase_im, int target);
+/* Reference: bwk/csrc/apply_diagonal_sm120.cu:88-105,177-208 (apply_diagonal_2q);
+ * diag index = b(q1)<<1 | b(q0) with q0 < q1 as in the reference.          */
+int qs_apply_diag2(qs_handle_t h, void* state, int n_qubits, const float* diag_c64, int q0, int q1);
+/* Reference: bwk/csrc/apply_mcgate_sm120.cu:74-165 (apply_mcgate).         */
+int qs_apply_mc1q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64,
+                  const int* controls, int n_controls, int target);
+/* Reference: bwk/csrc/apply_mc2qgate_sm120.cu:88-196 (apply_mc2qgate);
+ * bit 0 of the 4x4 index = min(t0,t1) as in the reference.                  */
+int qs_apply_mc2q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64,
+                  const int* controls, int n_controls, int t0, int t1);
+/* Exact permutation / sign kernels (X, CNOT, Toffoli, SWAP, CSWAP, Z, CZ):
+ * values are moved or negated, never multiplied.  Reference: the same gates
+ * go through apply_mcgate / apply_gate_2q with 0/1 matrices
+ * (blackwell_backend/simulator.py:456-461, bwk/python/blackwell_kernels/cuquantum.py:150-171). */
+int qs_apply_mcx(qs_handle_t h, void* state, int n_qubits, const int* controls, int n_controls, int target);
+int qs_apply_mcswap(qs_handle_t h, void* state, int n_qubits, const int* controls, int n_controls, int t0, int t1);
+int qs_apply_mcz(qs_handle_t h, void* state, int n_qubits, const int* qubits, int n);
+/* Reference: bwk/csrc/apply_gate_sm120.cu:121-161,179-234,238-350
+ * (apply_gates_fused, apply_gates_reg_tiled): K 1Q gates in one launch.     */
+int qs_apply_gates_fused(qs_handle_t h, void* state, int n_qubits, const float* gates_c64,
+                         const int* targets, int n_gates);
+/* Reference: bwk/csrc/batch_sm120.cu:53-102,185-228 (apply_gate_batched):
+ * one 2x2 gate on n_states equal-width states stored back to back.          */
+int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n_qubits,
+                        const float* gate_c64, int target);
+/* Reference: bwk/csrc/batch_sm120.cu:110-161,230-257 (apply_gates_batched_fused). */
+int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int n_qubits,
+                                 const float* gates_c64, const int* targets, int n_gates);
+
+/* ---------------------------------------------------------- programs ----- */
+/* Reference: blackwell_backend/simulator.py:247-468 (_compile_circuit 6-phase
+ * fusion + _execute_compiled).  The planner fuses in FP64 on the host and cuts
+ * the circuit into tile passes; each pass streams the state once.           */
+int qs_plan_create(qs_handle_t h, int n_qubits, const qs_op* ops, int n_ops, qs_plan_t* out);
+int qs_plan_info_get(qs_plan_t plan, qs_plan_info* info);
+int qs_plan_execute(qs_handle_t h, qs_plan_t plan, void* state);
+/* state := U|0..0>; the first pass synthesises |0..0> in shared memory, so
+ * the state is written but never read. */
+int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state);
+int qs_plan_destroy(qs_plan_t plan);
+/* plan + execute in one call (the plan is freed afterwards).               */
+int qs_run_circuit(qs_handle_t h, void* state, int n_qubits, const qs_op* ops, int n_ops);
+
+/* ------------------------------------------------------- reductions ------ */
+/* All reductions accumulate in FP64 in a fixed order: results are
+ * bit-reproducible run to run and independent of batching.                 */
+/* Reference: bwk/csrc/renorm_sm120.cu:23-50 (norm_reduce)                   */
+int qs_norm2(qs_handle_t h, const void* state, int n_qubits, double* out_host);
+/* Reference: bwk/csrc/renorm_sm120.cu:54-108 (renormalize)                  */
+int qs_renorm(qs_handle_t h, void* state, int n_qubits);
+/* Reference: bwk/csrc/measure_sm120.cu:115-130,186-207 (measure_probs)     */
+int qs_probs(qs_handle_t h, const void* state, int n_qubits, float* probs_dev);
+/* Reference: bwk/csrc/measure_sm120.cu:32-107,150-184 (measure_qubit).
+ * Outcome 0 iff u < P(bit=0); the state collapses in place.                */
+int qs_measure(qs_handle_t h, void* state, int n_qubits, int target, double u, int* outcome_host);
+/* Reference: bwk/csrc/sample_sm120.cu:29-132 (sample).  shot k = smallest i
+ * with cdf[i] >= u[k] (cdf accumulated in FP64), clamped to 2^n-1.
+ * u_dev: device float64 [n_shots]; out_dev: device int64 [n_shots].         */
+int qs_sample(qs_handle_t h, const void* state, int n_qubits, const double* u_dev,
+              int64_t n_shots, int64_t* out_dev);
+/* Reference: bwk/csrc/expectation_sm120.cu:45-80,179-202 (expectation_z)    */
+int qs_expect_z(qs_handle_t h, const void* state, int n_qubits, uint64_t z_mask, double* out_host);
+/* Reference: bwk/csrc/expectation_sm120.cu:100-163,204-239 (expectation_pauli),
+ * generalised to any X/Y/Z string: term t = coef[t] * X^x Z^z with Y counted
+ * in both masks (P = i^{|x&z|} X^x Z^z).  out = sum_t coef_t <psi|P_t|psi>. */
+int qs_expect_pauli_sum(qs_handle_t h, const void* state, int n_qubits,
+                        const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
+                        int n_terms, double* out_host);
+
+/* --------------------------------------------------------- Chebyshev ----- */
+/* Reference: bwk/csrc/spmv_sm120.cu:61-142 (spmv_csr): y = a*A*x + b*y with a
+ * Kahan-compensated row sum.  row_ptr/col_idx int32, values complex64.      */
+int qs_spmv_csr(qs_handle_t h, const int32_t* row_ptr, const int32_t* col_idx, const void* values,
+                int64_t n_rows, const void* x, void* y,
+                double alpha_re, double alpha_im, double beta_re, double beta_im);
+/* Reference: bwk/csrc/chebyshev_sm120.cu:24-91,97-159                       */
+int qs_cheb_step(qs_handle_t h, const void* spmv_result, const void* t_prev, void* t_next, int64_t n);
+int qs_cheb_accum(qs_handle_t h, void* accum, const void* t_k, double c_re, double c_im, int64_t n);
+int qs_cheb_step_accum(qs_handle_t h, const void* spmv_result, const void* t_prev, void* t_next,
+                       void* accum, double c_re, double c_im, int64_t n);
+/* Reference: blackwell_backend/chebyshev.py:81-172 (chebyshev_evolve).  The
+ * whole recurrence: one fused launch per degree (SpMV + step + accumulate),
+ * no host round trip.  coeffs: host complex128 [K+1].  work: device buffer of
+ * 3 * 2^n complex64.  out receives sum_k c_k T_k(scale*H) psi.             */
+int qs_cheb_evolve(qs_handle_t h, const int32_t* row_ptr, const int32_t* col_idx, const void* values,
+                   int n_qubits, const void* psi, void* out, const double* coeffs, int K,
+                   double scale, void* work);
+
+/* ------------------------------------------------------------ batch ------ */
+/* Many independent circuits of uneven width, states packed back to back.
+ * ops for circuit c are ops[op_offsets[c] .. op_offsets[c+1]); its state
+ * starts at amplitude state_offsets[c] of `states`.  States are initialised
+ * to |0..0> by the call.  Reference precedent: bwk/csrc/qv8_sim_sm120.cu:58-151,
+ * bwk/csrc/batch_sm120.cu:53-279 (fixed widths only).                       */
+int qs_batch_run(qs_handle_t h, int n_circuits, const int32_t* widths, const int64_t* op_offsets,
+                 const qs_op* ops, void* states, const int64_t* state_offsets);
+/* Reusable form: plan once (host FP64 fusion, per-circuit passes grouped into
+ * launches by pass level and tile size), execute many times (e.g. under a
+ * CUDA graph; execution issues no host-device copies). */
+typedef struct qs_batch_plan_s* qs_batch_plan_t;
+typedef struct qs_batch_info {
+  int32_t n_circuits;
+  int32_t n_launches;
+  int64_t n_items;        /* (circuit, pass) pairs                           */
+  int32_t max_passes;
+  int32_t pad;
+  double  bytes_moved;    /* HBM bytes of all passes (first passes write only) */
+  double  flops;          /* FP32 flop estimate                              */
+} qs_batch_info;
+int qs_batch_plan_create(qs_handle_t h, int n_circuits, const int32_t* widths, const int64_t* op_offsets,
+                         const qs_op* ops, const int64_t* state_offsets, qs_batch_plan_t* out);
+int qs_batch_plan_execute(qs_handle_t h, qs_batch_plan_t plan, void* states);
+int qs_batch_plan_info_get(qs_batch_plan_t plan, qs_batch_info* info);
+int qs_batch_plan_destroy(qs_batch_plan_t plan);
+
+/* ---------------------------------------------------------- adjoint ------ */
+/* Adjoint-method gradient of E(theta) = <psi(theta)|H|psi(theta)> for a
+ * parametrised circuit (no reference counterpart; ROADMAP.md:173-175).
+ * ops carry QS_OP_RX/RY/RZ with param >= 0; params: host [n_batch][n_params]
+ * values overriding m[0]; energies_host [n_batch]; grads_host
+ * [n_batch][n_params] accumulated in FP64.  work: device buffer of
+ * 3 * 2^n complex64 per batch entry (n_batch * 3 * 2^n).                    */
+int qs_adjoint_gradient(qs_handle_t h, int n_qubits, const qs_op* ops, int n_ops, int n_params,
+                        const double* params, int n_batch,
+                        const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs, int n_terms,
+                        void* work, double* energies_host, double* grads_host);
+/* lambda = H psi for a Pauli sum (matrix-free).                             */
+int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n_qubits,
+                       const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs, int n_terms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QSIM_H */

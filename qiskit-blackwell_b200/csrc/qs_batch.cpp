@@ -1,0 +1,249 @@
+// qs_batch.cpp — many independent circuits of uneven width in few launches.
+//
+// Every circuit is planned on its own (FP64 fusion + tile passes, in
+// parallel on the host).  Pass p of every circuit that has one is then
+// grouped, by tile size, into one launch of the tile-pass kernel: a circuit
+// of <= 14 qubits is a single pass whose tile is the whole state, so it runs
+// start to finish in one CTA's shared memory; wider circuits take several
+// levels.  All device programs live in one buffer and all item tables in
+// another, both built once, so execution issues no host-device copies and can
+// be captured in a CUDA graph.
+//
+// The reference has only fixed-width batches: bwk/csrc/qv8_sim_sm120.cu:58-151
+// (8 qubits, one CTA per circuit) and bwk/csrc/batch_sm120.cu:53-279 (one
+// launch per gate over [N, 2^n]).
+#include "qs_api.h"
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <thread>
+
+struct qs_batch_plan_s {
+  int device = 0;
+  int n_circuits = 0;
+  void* d_blob = nullptr;          // all device programs
+  void* d_items = nullptr;         // all PassItem tables
+  struct Launch { int T, R; size_t item_off; int n_items; uint64_t total_tiles; };
+  std::vector<Launch> launches;
+  qs_batch_info info{};
+};
+
+namespace {
+
+void free_bplan(qs_batch_plan_s* b) {
+  if (!b) return;
+  if (b->d_blob) cudaFree(b->d_blob);
+  if (b->d_items) cudaFree(b->d_items);
+  delete b;
+}
+
+void plan_all(int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops, int tile_bits,
+              std::vector<qs_plan_s>& plans) {
+  plans.resize(nc);
+  std::vector<std::string> errs(nc);
+  unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (nc < 64) nt = 1;
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; ++t) {
+    pool.emplace_back([&, t]() {
+      for (int c = (int)t; c < nc; c += (int)nt) {
+        try {
+          const int64_t b = op_off[c], e = op_off[c + 1];
+          if (b < 0 || e < b) throw qs_error(QS_ERR_INVALID, "op_offsets must be non-decreasing");
+          qs_build_plan(widths[c], ops + b, (int)(e - b), tile_bits, &plans[c]);
+        } catch (const std::exception& ex) {
+          errs[c] = ex.what();
+        }
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  for (int c = 0; c < nc; ++c)
+    if (!errs[c].empty()) throw qs_error(QS_ERR_INVALID, "circuit " + std::to_string(c) + ": " + errs[c]);
+}
+
+}  // namespace
+
+static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
+                                    const qs_op* ops, const int64_t* state_off) {
+  QS_CHECK_ARG(nc >= 0, "n_circuits must be >= 0");
+  QS_CHECK_ARG(nc == 0 || (widths && op_off && state_off), "null batch descriptor");
+  for (int c = 0; c < nc; ++c) {
+    QS_CHECK_ARG(widths[c] >= 1 && widths[c] <= QS_MAX_QUBITS, "circuit width out of range");
+    QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
+  }
+  std::vector<qs_plan_s> plans;
+  plan_all(nc, widths, op_off, ops, h->tile_bits, plans);
+
+  auto* B = new qs_batch_plan_s();
+  B->device = h->device;
+  B->n_circuits = nc;
+  try {
+    // concatenate device programs
+    std::vector<size_t> boff(nc);
+    size_t total = 0;
+    for (int c = 0; c < nc; ++c) {
+      boff[c] = total;
+      total += (plans[c].blob.size() + 255) & ~size_t(255);
+    }
+    std::vector<char> blob(total, 0);
+    for (int c = 0; c < nc; ++c)
+      if (!plans[c].blob.empty()) std::memcpy(blob.data() + boff[c], plans[c].blob.data(), plans[c].blob.size());
+    if (total) {
+      QS_CUDA(cudaMalloc(&B->d_blob, total));
+      QS_CUDA(cudaMemcpy(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice));
+    }
+    // group (circuit, pass) items by level, then by (T, R)
+    int maxp = 0;
+    for (auto& p : plans) maxp = std::max(maxp, (int)p.pass_offsets.size());
+    std::vector<PassItem> items;
+    double bytes = 0, flops = 0;
+    for (int L = 0; L < maxp; ++L) {
+      std::map<std::pair<int, int>, std::vector<PassItem>> groups;
+      for (int c = 0; c < nc; ++c) {
+        const qs_plan_s& p = plans[c];
+        if (L >= (int)p.pass_offsets.size()) continue;
+        const int T = p.pass_T[L];
+        PassItem it{};
+        it.state_off = (uint64_t)state_off[c];
+        it.pass = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[c] + p.pass_offsets[L]);
+        it.ntiles = 1ull << (widths[c] - T);
+        it.flags = (L == 0) ? PI_FROM_ZERO : 0u;
+        groups[{T, p.pass_R[L]}].push_back(it);
+        bytes += (L == 0 ? 8.0 : 16.0) * std::ldexp(1.0, widths[c]);
+      }
+      // larger tiles first: they are the longest-running CTAs
+      for (auto g = groups.rbegin(); g != groups.rend(); ++g) {
+        qs_batch_plan_s::Launch Lc;
+        Lc.T = g->first.first;
+        Lc.R = g->first.second;
+        Lc.item_off = items.size();
+        Lc.n_items = (int)g->second.size();
+        uint64_t tb = 0;
+        for (PassItem& it : g->second) { it.tile_begin = tb; tb += it.ntiles; items.push_back(it); }
+        Lc.total_tiles = tb;
+        B->launches.push_back(Lc);
+      }
+    }
+    for (auto& p : plans) flops += p.info.flops;
+    // circuits with no ops still need |0..0>
+    for (int c = 0; c < nc; ++c) {
+      if (!plans[c].pass_offsets.empty()) continue;
+      QS_CHECK_ARG(false, "every circuit of a batch needs at least one op");
+    }
+    if (!items.empty()) {
+      QS_CUDA(cudaMalloc(&B->d_items, items.size() * sizeof(PassItem)));
+      QS_CUDA(cudaMemcpy(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice));
+    }
+    B->info.n_circuits = nc;
+    B->info.n_launches = (int32_t)B->launches.size();
+    B->info.n_items = (int64_t)items.size();
+    B->info.max_passes = maxp;
+    B->info.bytes_moved = bytes;
+    B->info.flops = flops;
+  } catch (...) {
+    free_bplan(B);
+    throw;
+  }
+  return B;
+}
+
+static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
+  for (const auto& L : B->launches) {
+    const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
+    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R);
+  }
+}
+
+extern "C" {
+
+int qs_batch_plan_create(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops,
+                         const int64_t* state_off, qs_batch_plan_t* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  *out = build_batch(h, nc, widths, op_off, ops, state_off);
+  QS_API_END(h)
+}
+
+int qs_batch_plan_execute(qs_handle_t h, qs_batch_plan_t B, void* states) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(B != nullptr, "batch plan is null");
+  QS_CHECK_ARG(B->n_circuits == 0 || (states && ((uintptr_t)states & 15u) == 0),
+               "states must be a 16-byte aligned device pointer");
+  QS_CHECK_ARG(B->device == h->device, "batch plan was built for another device");
+  run_batch(h, B, states);
+  QS_API_END(h)
+}
+
+int qs_batch_plan_info_get(qs_batch_plan_t B, qs_batch_info* info) {
+  if (!B || !info) { qs_set_tls_error("null batch plan or info"); return QS_ERR_INVALID; }
+  *info = B->info;
+  return QS_OK;
+}
+
+int qs_batch_plan_destroy(qs_batch_plan_t B) {
+  free_bplan(B);
+  return QS_OK;
+}
+
+int qs_batch_run(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops,
+                 void* states, const int64_t* state_off) {
+  QS_REQUIRE_HANDLE(h);
+  qs_batch_plan_s* B = nullptr;
+  QS_API_BEGIN
+  B = build_batch(h, nc, widths, op_off, ops, state_off);
+  run_batch(h, B, states);
+  QS_CUDA(cudaStreamSynchronize(h->stream));  // programs must outlive the launches
+  free_bplan(B);
+  B = nullptr;
+  return QS_OK;
+  }
+  catch (const qs_error& e) {
+    h->err = e.what();
+    if (B) { cudaStreamSynchronize(h->stream); free_bplan(B); }
+    return e.code;
+  }
+  catch (const std::exception& e) {
+    h->err = e.what();
+    if (B) { cudaStreamSynchronize(h->stream); free_bplan(B); }
+    return QS_ERR_INVALID;
+  }
+}
+
+// Equal-width states back to back: the plan is built once and every pass
+// covers all states in one launch (tile ids above 2^(n-T) select the state).
+int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int n, const float* gates,
+                                 const int* targets, int ngates) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(states, n);
+  QS_CHECK_ARG(n_states >= 0, "n_states must be >= 0");
+  QS_CHECK_ARG(ngates >= 0 && (ngates == 0 || (gates && targets)), "bad gates/targets");
+  std::vector<qs_op> ops(ngates);
+  for (int g = 0; g < ngates; ++g) {
+    qs_op& o = ops[g];
+    std::memset(&o, 0, sizeof(o));
+    o.kind = QS_OP_U1;
+    o.nq = 1;
+    o.q[0] = targets[g];
+    o.param = -1;
+    for (int i = 0; i < 8; ++i) o.m[i] = gates[8 * g + i];
+  }
+  if (n_states == 0 || ngates == 0) return QS_OK;
+  qs_plan_s p;
+  qs_build_plan(n, ops.data(), ngates, h->tile_bits, &p);
+  qs_plan_upload(h, &p);
+  try {
+    qs_plan_run(h, &p, states, false, (uint64_t)n_states);
+    QS_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (...) {
+    if (p.d_blob) cudaFree(p.d_blob);
+    throw;
+  }
+  if (p.d_blob) cudaFree(p.d_blob);
+  QS_API_END(h)
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// qs_context.cu — handle lifecycle, streams, scratch and error reporting.
+#include "qs_api.h"
+#include <cstring>
+
+static thread_local std::string g_tls_err;
+void qs_set_tls_error(const std::string& m) { g_tls_err = m; }
+
+void* qs_context::scratch_get(size_t bytes) {
+  if (bytes <= scratch_bytes) return scratch;
+  // Grow-only.  Work already queued on the stream may still read the old
+  // buffer, so finish it before releasing the memory.
+  if (scratch) {
+    QS_CUDA(cudaStreamSynchronize(stream));
+    QS_CUDA(cudaFree(scratch));
+    scratch = nullptr;
+    scratch_bytes = 0;
+  }
+  size_t want = bytes < (1u << 20) ? (1u << 20) : bytes;
+  QS_CUDA(cudaMalloc(&scratch, want));
+  scratch_bytes = want;
+  return scratch;
+}
+
+double* qs_context::pinned_get(size_t bytes) {
+  if (bytes <= pinned_bytes) return pinned;
+  if (pinned) {
+    QS_CUDA(cudaStreamSynchronize(stream));
+    QS_CUDA(cudaFreeHost(pinned));
+    pinned = nullptr;
+  }
+  size_t want = bytes < 4096 ? 4096 : bytes;
+  QS_CUDA(cudaMallocHost((void**)&pinned, want));
+  pinned_bytes = want;
+  return pinned;
+}
+
+void qs_after_launch(qs_context* h, const char* what) {
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw qs_error(QS_ERR_CUDA, std::string(what) + ": launch failed: " + cudaGetErrorString(e));
+}
+
+extern "C" {
+
+const char* qs_version(void) { return "qsim-b200 0.1.0 (sm_100a)"; }
+
+int qs_create(int device, qs_handle_t* out) {
+  qs_context* h = nullptr;
+  QS_API_BEGIN
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  *out = nullptr;
+  int count = 0;
+  QS_CUDA(cudaGetDeviceCount(&count));
+  QS_CHECK_ARG(device >= 0 && device < count, "device index out of range");
+  QS_CUDA(cudaSetDevice(device));
+  h = new qs_context();
+  h->device = device;
+  QS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
+  QS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+  h->stream = h->own_stream;
+  *out = h;
+  return QS_OK;
+  }
+  catch (const qs_error& e) {
+    qs_set_tls_error(e.what());
+    delete h;
+    return e.code;
+  }
+  catch (const std::exception& e) {
+    qs_set_tls_error(e.what());
+    delete h;
+    return QS_ERR_INVALID;
+  }
+}
+
+int qs_destroy(qs_handle_t h) {
+  if (!h) return QS_OK;
+  cudaSetDevice(h->device);
+  if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+  if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+  if (h->scratch) cudaFree(h->scratch);
+  if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return QS_OK;
+}
+
+int qs_set_stream(qs_handle_t h, void* s) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  QS_API_END(h)
+}
+
+void* qs_get_stream(qs_handle_t h) { return h ? (void*)h->stream : nullptr; }
+
+int qs_sync(qs_handle_t h) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  QS_API_END(h)
+}
+
+const char* qs_last_error(qs_handle_t h) {
+  if (h) return h->err.c_str();
+  return g_tls_err.c_str();
+}
+
+int qs_set_tile_bits(qs_handle_t h, int tile_bits) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  if (tile_bits == 0) tile_bits = 13;
+  QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
+  h->tile_bits = tile_bits;
+  QS_API_END(h)
+}
+
+int64_t qs_launch_count(qs_handle_t h) { return h ? h->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,499 @@
+// qs_gates.cu — one-gate-per-launch kernels (the reference's per-op API).
+//
+// Every kernel streams the state in place with 64-bit indices and grid-stride
+// loops sized to the SM count.  Wherever the touched amplitudes come in
+// adjacent pairs the kernels use 128-bit accesses (two complex64 per float4).
+// Dense gates use the compensated Dot2 evaluation (qs_common.cuh); diagonal
+// gates the compensated Kahan complex product; X/CNOT/Toffoli/SWAP/Z/CZ are
+// exact moves or negations.
+#include "qs_api.h"
+#include "qs_common.cuh"
+#include <algorithm>
+
+using namespace qs;
+
+namespace {
+
+struct G2 { float2 g[4]; };
+struct G4 { float2 g[16]; };
+struct Sorted { int pos[12]; int k; };
+
+constexpr int kThreads = 256;
+
+// ------------------------------------------------------------ init --------
+__global__ void k_state_init(float4* __restrict__ s4, uint64_t nvec, uint64_t index) {
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((index >> 1) == i) { if (index & 1) v.z = 1.f; else v.x = 1.f; }
+    s4[i] = v;
+  }
+}
+
+// states back to back, each of 2^n amplitudes: amplitude 0 of each is 1.
+__global__ void k_state_init_batched(float4* __restrict__ s4, uint64_t nvec, int n) {
+  uint64_t mask = (1ull << n) - 1ull;
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (((2 * i) & mask) == 0) v.x = 1.f;
+    s4[i] = v;
+  }
+}
+
+// ------------------------------------------------------------- 1Q ---------
+__device__ __forceinline__ void apply2(const G2& G, float2& a0, float2& a1) {
+  float2 r0[2] = {G.g[0], G.g[1]}, r1[2] = {G.g[2], G.g[3]}, v[2] = {a0, a1};
+  float2 n0 = cdot_comp<2>(r0, v);
+  float2 n1 = cdot_comp<2>(r1, v);
+  a0 = n0; a1 = n1;
+}
+
+// target 0: the pair is one float4.
+__global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G) {
+  for (uint64_t p = gtid(); p < npairs; p += gstride()) {
+    float4 v = ld4(s + 2 * p);
+    float2 a0 = lo2(v), a1 = hi2(v);
+    apply2(G, a0, a1);
+    st4(s + 2 * p, a0, a1);
+  }
+}
+
+// target t >= 1: two neighbouring pairs per thread, two float4 accesses.
+__global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G) {
+  const uint64_t st = 1ull << t;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i0 = insert_zero(2 * it, t);
+    float4 v0 = ld4(s + i0), v1 = ld4(s + i0 + st);
+    float2 a0 = lo2(v0), b0 = hi2(v0), a1 = lo2(v1), b1 = hi2(v1);
+    apply2(G, a0, a1);
+    apply2(G, b0, b1);
+    st4(s + i0, a0, b0);
+    st4(s + i0 + st, a1, b1);
+  }
+}
+
+// ------------------------------------------------------------- 2Q ---------
+__device__ __forceinline__ void apply4(const G4& G, float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 v[4] = {a0, a1, a2, a3};
+  float2 o[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    float2 row[4] = {G.g[4 * r], G.g[4 * r + 1], G.g[4 * r + 2], G.g[4 * r + 3]};
+    o[r] = cdot_comp<4>(row, v);
+  }
+  a0 = o[0]; a1 = o[1]; a2 = o[2]; a3 = o[3];
+}
+
+// lo == 0: a00,a01 adjacent and a10,a11 adjacent.
+__global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G) {
+  const uint64_t sh = 1ull << hi;
+  for (uint64_t it = gtid(); it < nquads; it += gstride()) {
+    uint64_t i00 = insert_zero(insert_zero(it, 0), hi);
+    float4 v0 = ld4(s + i00), v1 = ld4(s + i00 + sh);
+    float2 a0 = lo2(v0), a1 = hi2(v0), a2 = lo2(v1), a3 = hi2(v1);
+    apply4(G, a0, a1, a2, a3);
+    st4(s + i00, a0, a1);
+    st4(s + i00 + sh, a2, a3);
+  }
+}
+
+// lo >= 1: two neighbouring quads per thread.
+__global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi, G4 G) {
+  const uint64_t sl = 1ull << lo, sh = 1ull << hi;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i00 = insert_zero(insert_zero(2 * it, lo), hi);
+    float4 v00 = ld4(s + i00), v01 = ld4(s + i00 + sl), v10 = ld4(s + i00 + sh), v11 = ld4(s + i00 + sl + sh);
+    float2 a0 = lo2(v00), a1 = lo2(v01), a2 = lo2(v10), a3 = lo2(v11);
+    float2 b0 = hi2(v00), b1 = hi2(v01), b2 = hi2(v10), b3 = hi2(v11);
+    apply4(G, a0, a1, a2, a3);
+    apply4(G, b0, b1, b2, b3);
+    st4(s + i00, a0, b0);
+    st4(s + i00 + sl, a1, b1);
+    st4(s + i00 + sh, a2, b2);
+    st4(s + i00 + sl + sh, a3, b3);
+  }
+}
+
+// ----------------------------------------------------------- diagonal -----
+__global__ void k_diag1(float2* __restrict__ s, uint64_t nvec, int t, float2 d0, float2 d1) {
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    uint64_t idx = 2 * i;
+    float4 v = ld4(s + idx);
+    float2 e0, e1;
+    if (t == 0) { e0 = d0; e1 = d1; }
+    else { e0 = e1 = ((idx >> t) & 1) ? d1 : d0; }
+    st4(s + idx, cmul_comp(lo2(v), e0), cmul_comp(hi2(v), e1));
+  }
+}
+
+// Only amplitudes with bit t = 1 (half the traffic).
+__global__ void k_phase_t0(float2* __restrict__ s, uint64_t npairs, float2 ph) {
+  for (uint64_t p = gtid(); p < npairs; p += gstride()) {
+    uint64_t idx = 2 * p + 1;
+    s[idx] = cmul_comp(s[idx], ph);
+  }
+}
+__global__ void k_phase_tn(float2* __restrict__ s, uint64_t nitems, int t, float2 ph) {
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t idx = insert_zero(2 * it, t) | (1ull << t);
+    float4 v = ld4(s + idx);
+    st4(s + idx, cmul_comp(lo2(v), ph), cmul_comp(hi2(v), ph));
+  }
+}
+
+__global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G2 D) {
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    uint64_t idx = 2 * i;
+    float4 v = ld4(s + idx);
+    uint64_t j = idx + 1;
+    int s0 = (int)(((idx >> q1) & 1) << 1 | ((idx >> q0) & 1));
+    int s1 = (int)(((j >> q1) & 1) << 1 | ((j >> q0) & 1));
+    st4(s + idx, cmul_comp(lo2(v), D.g[s0]), cmul_comp(hi2(v), D.g[s1]));
+  }
+}
+
+// ------------------------------------------------- multi-controlled -------
+__global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t, G2 G) {
+  const uint64_t st = 1ull << t;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i0 = insert_zeros(it, P.pos, P.k) | cmask;
+    float2 a0 = s[i0], a1 = s[i0 | st];
+    apply2(G, a0, a1);
+    s[i0] = a0;
+    s[i0 | st] = a1;
+  }
+}
+
+__global__ void k_mc2q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int lo, int hi, G4 G) {
+  const uint64_t sl = 1ull << lo, sh = 1ull << hi;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i = insert_zeros(it, P.pos, P.k) | cmask;
+    float2 a0 = s[i], a1 = s[i | sl], a2 = s[i | sh], a3 = s[i | sl | sh];
+    apply4(G, a0, a1, a2, a3);
+    s[i] = a0; s[i | sl] = a1; s[i | sh] = a2; s[i | sl | sh] = a3;
+  }
+}
+
+// ---------------------------------------------------------- exact ---------
+__global__ void k_x_t0(float2* __restrict__ s, uint64_t npairs) {
+  for (uint64_t p = gtid(); p < npairs; p += gstride()) {
+    float4 v = ld4(s + 2 * p);
+    st4(s + 2 * p, hi2(v), lo2(v));
+  }
+}
+__global__ void k_x_tn(float2* __restrict__ s, uint64_t nitems, int t) {
+  const uint64_t st = 1ull << t;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i0 = insert_zero(2 * it, t);
+    float4 v0 = ld4(s + i0), v1 = ld4(s + i0 + st);
+    *reinterpret_cast<float4*>(s + i0) = v1;
+    *reinterpret_cast<float4*>(s + i0 + st) = v0;
+  }
+}
+__global__ void k_mcx(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t) {
+  const uint64_t st = 1ull << t;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i0 = insert_zeros(it, P.pos, P.k) | cmask;
+    float2 a0 = s[i0], a1 = s[i0 | st];
+    s[i0] = a1;
+    s[i0 | st] = a0;
+  }
+}
+__global__ void k_mcswap(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t0, int t1) {
+  const uint64_t s0 = 1ull << t0, s1 = 1ull << t1;
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i = insert_zeros(it, P.pos, P.k) | cmask;
+    float2 a = s[i | s0], b = s[i | s1];
+    s[i | s0] = b;
+    s[i | s1] = a;
+  }
+}
+__global__ void k_mcz(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t mask) {
+  for (uint64_t it = gtid(); it < nitems; it += gstride()) {
+    uint64_t i = insert_zeros(it, P.pos, P.k) | mask;
+    float2 a = s[i];
+    s[i] = make_float2(-a.x, -a.y);
+  }
+}
+
+// --------------------------------------------------------- host side ------
+inline float2 f2(const float* p) { return make_float2(p[0], p[1]); }
+
+G2 load_g2(const float* g) {
+  QS_CHECK_ARG(g != nullptr, "gate pointer is null");
+  G2 G;
+  for (int i = 0; i < 4; ++i) G.g[i] = f2(g + 2 * i);
+  return G;
+}
+
+G4 load_g4(const float* g) {
+  QS_CHECK_ARG(g != nullptr, "gate pointer is null");
+  G4 G;
+  for (int i = 0; i < 16; ++i) G.g[i] = f2(g + 2 * i);
+  return G;
+}
+
+// Swap the roles of matrix index bits 0 and 1 (basis order 00,01,10,11).
+G4 swap_bits(const G4& G) {
+  static const int perm[4] = {0, 2, 1, 3};
+  G4 R;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) R.g[4 * r + c] = G.g[4 * perm[r] + perm[c]];
+  return R;
+}
+
+Sorted make_sorted(const int* qs, int k) {
+  QS_CHECK_ARG(k <= 12, "too many qubits in a controlled gate");
+  Sorted P;
+  for (int i = 0; i < k; ++i) P.pos[i] = qs[i];
+  std::sort(P.pos, P.pos + k);
+  for (int i = 1; i < k; ++i) QS_CHECK_ARG(P.pos[i] != P.pos[i - 1], "duplicate qubit in gate");
+  for (int i = k; i < 12; ++i) P.pos[i] = 0;
+  P.k = k;
+  return P;
+}
+
+void check_controls(const int* controls, int nc, int n) {
+  QS_CHECK_ARG(nc >= 0 && nc <= QS_MAX_CONTROLS, "controls must have 0-7 elements");
+  QS_CHECK_ARG(nc == 0 || controls != nullptr, "controls pointer is null");
+  for (int i = 0; i < nc; ++i) qs_check_qubit(controls[i], n, "control");
+}
+
+#define LAUNCH(h, kern, items, ...)                                              \
+  do {                                                                          \
+    uint64_t _items = (items);                                                  \
+    if (_items) {                                                               \
+      kern<<<qs_blocks_for(h, _items, kThreads), kThreads, 0, h->stream>>>(__VA_ARGS__); \
+      qs_after_launch(h, #kern);                                                \
+    }                                                                           \
+  } while (0)
+
+}  // namespace
+
+// Exposed to other units (apply_gates_fused fallback and tests).
+void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs_total, int t, const G2& G);
+
+void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs, int t, const G2& G) {
+  if (t == 0) LAUNCH(h, k_1q_t0, npairs, s, npairs, G);
+  else LAUNCH(h, k_1q_tn, npairs / 2, s, npairs / 2, t, G);
+}
+
+extern "C" {
+
+int qs_state_init(qs_handle_t h, void* state, int n) {
+  return qs_state_init_basis(h, state, n, 0);
+}
+
+int qs_state_init_basis(qs_handle_t h, void* state, int n, uint64_t index) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(index < (1ull << n), "basis index out of range");
+  uint64_t nvec = (1ull << n) / 2;
+  LAUNCH(h, k_state_init, nvec, (float4*)state, nvec, index);
+  QS_API_END(h)
+}
+
+int qs_state_init_batched(qs_handle_t h, void* states, int n_states, int n) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(states, n);
+  QS_CHECK_ARG(n_states >= 0, "n_states must be >= 0");
+  uint64_t nvec = (uint64_t)n_states * ((1ull << n) / 2);
+  LAUNCH(h, k_state_init_batched, nvec, (float4*)states, nvec, n);
+  QS_API_END(h)
+}
+
+int qs_apply_1q(qs_handle_t h, void* state, int n, const float* gate, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  G2 G = load_g2(gate);
+  qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G);
+  QS_API_END(h)
+}
+
+int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n, const float* gate, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(states, n);
+  qs_check_qubit(t, n, "target");
+  QS_CHECK_ARG(n_states >= 0, "n_states must be >= 0");
+  G2 G = load_g2(gate);
+  // Pair index p ranges over n_states * 2^(n-1); inserting a zero at t < n
+  // leaves the state index in the bits above n.
+  qs_launch_1q(h, (float2*)states, (uint64_t)n_states << (n - 1), t, G);
+  QS_API_END(h)
+}
+
+int qs_apply_2q(qs_handle_t h, void* state, int n, const float* gate, int q0, int q1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(n >= 2, "a 2-qubit gate needs n >= 2");
+  qs_check_qubit(q0, n, "qubit0");
+  qs_check_qubit(q1, n, "qubit1");
+  QS_CHECK_ARG(q0 != q1, "qubit0 and qubit1 must differ");
+  G4 G = load_g4(gate);
+  int lo = q0, hi = q1;
+  if (q0 > q1) { G = swap_bits(G); lo = q1; hi = q0; }
+  uint64_t nquads = 1ull << (n - 2);
+  if (lo == 0) LAUNCH(h, k_2q_lo0, nquads, (float2*)state, nquads, hi, G);
+  else LAUNCH(h, k_2q_gen, nquads / 2, (float2*)state, nquads / 2, lo, hi, G);
+  QS_API_END(h)
+}
+
+int qs_apply_diag1(qs_handle_t h, void* state, int n, const float* diag, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  QS_CHECK_ARG(diag != nullptr, "diag pointer is null");
+  uint64_t nvec = (1ull << n) / 2;
+  LAUNCH(h, k_diag1, nvec, (float2*)state, nvec, t, f2(diag), f2(diag + 2));
+  QS_API_END(h)
+}
+
+int qs_apply_phase(qs_handle_t h, void* state, int n, float re, float im, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  float2 ph = make_float2(re, im);
+  uint64_t npairs = 1ull << (n - 1);
+  if (t == 0) LAUNCH(h, k_phase_t0, npairs, (float2*)state, npairs, ph);
+  else LAUNCH(h, k_phase_tn, npairs / 2, (float2*)state, npairs / 2, t, ph);
+  QS_API_END(h)
+}
+
+int qs_apply_diag2(qs_handle_t h, void* state, int n, const float* diag, int q0, int q1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(n >= 2, "a 2-qubit gate needs n >= 2");
+  qs_check_qubit(q0, n, "qubit0");
+  qs_check_qubit(q1, n, "qubit1");
+  QS_CHECK_ARG(q0 != q1, "qubit0 and qubit1 must differ");
+  QS_CHECK_ARG(diag != nullptr, "diag pointer is null");
+  G2 D = load_g2(diag);
+  int lo = std::min(q0, q1), hi = std::max(q0, q1);
+  uint64_t nvec = (1ull << n) / 2;
+  LAUNCH(h, k_diag2, nvec, (float2*)state, nvec, lo, hi, D);
+  QS_API_END(h)
+}
+
+int qs_apply_mc1q(qs_handle_t h, void* state, int n, const float* gate, const int* controls, int nc, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  check_controls(controls, nc, n);
+  G2 G = load_g2(gate);
+  if (nc == 0) { qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G); return QS_OK; }
+  int all[QS_MAX_CONTROLS + 1];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t, "target_qubit must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = t;
+  Sorted P = make_sorted(all, nc + 1);
+  QS_CHECK_ARG(nc + 1 <= n, "more gate qubits than state qubits");
+  uint64_t items = 1ull << (n - nc - 1);
+  LAUNCH(h, k_mc1q, items, (float2*)state, items, P, cmask, t, G);
+  QS_API_END(h)
+}
+
+int qs_apply_mc2q(qs_handle_t h, void* state, int n, const float* gate, const int* controls, int nc, int t0, int t1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t0, n, "target0");
+  qs_check_qubit(t1, n, "target1");
+  QS_CHECK_ARG(t0 != t1, "target0 and target1 must differ");
+  check_controls(controls, nc, n);
+  QS_CHECK_ARG(nc + 2 <= n, "more gate qubits than state qubits");
+  G4 G = load_g4(gate);
+  int lo = std::min(t0, t1), hi = std::max(t0, t1);
+  int all[QS_MAX_CONTROLS + 2];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t0 && controls[i] != t1, "target qubits must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = lo;
+  all[nc + 1] = hi;
+  Sorted P = make_sorted(all, nc + 2);
+  uint64_t items = 1ull << (n - nc - 2);
+  LAUNCH(h, k_mc2q, items, (float2*)state, items, P, cmask, lo, hi, G);
+  QS_API_END(h)
+}
+
+int qs_apply_mcx(qs_handle_t h, void* state, int n, const int* controls, int nc, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  check_controls(controls, nc, n);
+  QS_CHECK_ARG(nc + 1 <= n, "more gate qubits than state qubits");
+  if (nc == 0) {
+    uint64_t npairs = 1ull << (n - 1);
+    if (t == 0) LAUNCH(h, k_x_t0, npairs, (float2*)state, npairs);
+    else LAUNCH(h, k_x_tn, npairs / 2, (float2*)state, npairs / 2, t);
+    return QS_OK;
+  }
+  int all[QS_MAX_CONTROLS + 1];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t, "target_qubit must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = t;
+  Sorted P = make_sorted(all, nc + 1);
+  uint64_t items = 1ull << (n - nc - 1);
+  LAUNCH(h, k_mcx, items, (float2*)state, items, P, cmask, t);
+  QS_API_END(h)
+}
+
+int qs_apply_mcswap(qs_handle_t h, void* state, int n, const int* controls, int nc, int t0, int t1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t0, n, "target0");
+  qs_check_qubit(t1, n, "target1");
+  QS_CHECK_ARG(t0 != t1, "target0 and target1 must differ");
+  check_controls(controls, nc, n);
+  QS_CHECK_ARG(nc + 2 <= n, "more gate qubits than state qubits");
+  int all[QS_MAX_CONTROLS + 2];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t0 && controls[i] != t1, "target qubits must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = t0;
+  all[nc + 1] = t1;
+  Sorted P = make_sorted(all, nc + 2);
+  uint64_t items = 1ull << (n - nc - 2);
+  LAUNCH(h, k_mcswap, items, (float2*)state, items, P, cmask, t0, t1);
+  QS_API_END(h)
+}
+
+int qs_apply_mcz(qs_handle_t h, void* state, int n, const int* qubits, int k) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(k >= 1 && k <= QS_MAX_CONTROLS + 1 && k <= n, "mcz needs 1..8 qubits");
+  QS_CHECK_ARG(qubits != nullptr, "qubits pointer is null");
+  uint64_t mask = 0;
+  for (int i = 0; i < k; ++i) { qs_check_qubit(qubits[i], n, "mcz"); mask |= 1ull << qubits[i]; }
+  Sorted P = make_sorted(qubits, k);
+  uint64_t items = 1ull << (n - k);
+  LAUNCH(h, k_mcz, items, (float2*)state, items, P, mask);
+  QS_API_END(h)
+}
+
+}  // extern "C"

@@ -1,0 +1,152 @@
+// qs_internal.h — host-side runtime internals shared by the libqsim translation
+// units: the context (stream, scratch, error text), launch helpers and the
+// device program format produced by the planner (qs_plan.cpp) and consumed by
+// the tile-pass kernel (qs_pass.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include <complex>
+#include <stdexcept>
+#include "../../include/qsim.h"
+
+// ---------------------------------------------------------------- errors --
+struct qs_error : std::runtime_error {
+  int code;
+  qs_error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define QS_CHECK_ARG(cond, msg)                                              \
+  do { if (!(cond)) throw qs_error(QS_ERR_INVALID, (msg)); } while (0)
+
+#define QS_CUDA(expr)                                                        \
+  do {                                                                       \
+    cudaError_t _e = (expr);                                                 \
+    if (_e != cudaSuccess) {                                                 \
+      int _c = (_e == cudaErrorMemoryAllocation) ? QS_ERR_NOMEM : QS_ERR_CUDA; \
+      throw qs_error(_c, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    }                                                                        \
+  } while (0)
+
+// ------------------------------------------------------------- context ----
+struct qs_context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int tile_bits = 13;
+  int64_t launches = 0;
+
+  // grow-only device scratch (reductions, sampling partials, ...)
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // pinned host staging for scalar results
+  double* pinned = nullptr;
+  size_t pinned_bytes = 0;
+
+  void* scratch_get(size_t bytes);
+  double* pinned_get(size_t bytes);
+};
+
+// Records a launch and checks the launch status.
+void qs_after_launch(qs_context* h, const char* what);
+
+// ------------------------------------------------------- device program ---
+// A plan is a list of passes.  A pass streams every tile of the state once:
+// the tile is the set of 2^T amplitudes whose non-tile bits are fixed; it is
+// staged in shared memory, a sequence of register blocks is applied, and it
+// is written back in place.  A register block gives each thread 2^R
+// amplitudes (R <= 5 tile positions) on which its ops run in registers.
+enum DevKind : uint8_t {
+  DK_U1 = 1,     // controlled dense 2x2 on register bit t0
+  DK_U2 = 2,     // controlled dense 4x4 on register bits t0 (bit0) < t1 (bit1)
+  DK_X = 3,      // controlled exact swap across register bit t0
+  DK_SWAP = 4,   // controlled exact swap of |..01..> and |..10..> (t0 < t1)
+  DK_Y = 5,      // controlled exact Pauli-Y on t0
+  DK_NEG = 6,    // negate where all control bits are set (CZ family)
+  DK_PHASE = 7,  // multiply by c[0] where all control bits are set
+  DK_DIAG1 = 8,  // multiply by c[b(d0)]
+  DK_DIAG2 = 9,  // multiply by c[b(d1)<<1 | b(d0)]
+};
+
+// Locator of a qubit inside a block: values < 8 are register positions; values
+// >= 0x80 encode (0x80 | q), a qubit read from the amplitude's global index.
+#define DLOC_GLOBAL 0x80
+
+struct __align__(16) DevOp {
+  uint8_t kind;
+  uint8_t t0, t1;
+  uint8_t rc;        // controls among the register positions (bit mask)
+  uint8_t d0, d1;    // diagonal locators
+  uint8_t ncoef;
+  uint8_t pad0;
+  uint32_t coef;     // index of the first float2 coefficient in the pass pool
+  uint32_t pad1;
+  uint64_t gc;       // controls read from the global index (mask of qubits)
+};
+static_assert(sizeof(DevOp) == 24 || sizeof(DevOp) == 32, "DevOp layout");
+
+struct __align__(16) DevBlock {
+  int8_t pos[8];     // R tile-local positions, ascending
+  int32_t op_begin;  // index into the pass's op array
+  int32_t op_end;
+};
+
+struct __align__(16) DevPass {
+  int32_t T;         // tile bits
+  int32_t R;         // register bits per block
+  int32_t nblocks;
+  int32_t n_qubits;
+  int32_t S[16];     // tile positions (global qubit ids), ascending
+  uint32_t block_off; // byte offsets from the start of this DevPass
+  uint32_t op_off;
+  uint32_t coef_off;
+  uint32_t bytes;     // total bytes of this pass record
+};
+
+// Host-side plan.
+struct qs_plan_s {
+  int n_qubits = 0;
+  int tile_bits = 0;
+  std::vector<uint32_t> pass_offsets;   // byte offset of each DevPass in blob
+  std::vector<int> pass_T, pass_R;
+  std::vector<char> blob;               // host copy of the device program
+  void* d_blob = nullptr;               // device copy
+  int device = 0;
+  qs_plan_info info{};
+};
+
+// Planner entry (qs_plan.cpp): builds passes for one circuit.
+void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan);
+void qs_plan_upload(qs_context* h, qs_plan_s* p);
+// Runs every pass on n_states equal-width states stored back to back.
+void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states);
+
+// Tile-pass launcher (qs_pass.cu).  One item per (state, pass); the state is
+// base + state_off (in amplitudes).  PI_FROM_ZERO makes the pass start from
+// |0..0> instead of loading the tile (the state is then only written).
+#define PI_FROM_ZERO 1u
+struct __align__(16) PassItem {
+  uint64_t state_off;
+  const DevPass* pass;   // device pointer
+  uint64_t ntiles;
+  uint64_t tile_begin;   // prefix of ntiles over the item table
+  uint32_t flags;
+  uint32_t pad[3];
+};
+void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
+                           uint32_t flags = 0);
+void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
+                          int maxT, int R);
+
+// Convenience used by several units.
+inline int qs_blocks_for(qs_context* h, uint64_t items, int threads, int per_sm = 8) {
+  uint64_t b = (items + threads - 1) / threads;
+  uint64_t cap = (uint64_t)h->sm_count * per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}

@@ -1,0 +1,415 @@
+// qs_pass.cu — the fused tile-pass kernel.
+//
+// One launch applies one pass of a host-built plan (qs_plan.cpp) to one or
+// more states.  A pass is defined by a tile: T qubit positions S[0..T-1]
+// (always including the low qubits, so that a tile is a set of contiguous
+// runs of amplitudes in HBM).  Each CTA loops over tiles:
+//
+//   1. HBM -> shared memory with 16-byte cp.async (swizzled layout),
+//   2. for each register block (R <= 5 tile positions): every thread gathers
+//      the 2^R amplitudes of its group into registers, runs the block's ops
+//      there (dense 1Q/2Q, exact X/SWAP/Y/negation, phases and diagonals,
+//      with controls on any qubit), and scatters them back,
+//   3. shared memory -> HBM with 16-byte stores, in place.
+//
+// The state is therefore read and written once per pass however many gates
+// the pass holds.  Gate qubit positions are compile-time template arguments
+// (dispatched by a switch), so the amplitudes stay in registers.
+#include "qs_api.h"
+#include "qs_common.cuh"
+#include <algorithm>
+#include <map>
+
+using namespace qs;
+
+namespace {
+
+// Shared-memory swizzle: XOR bits 1..3 of the index with a fold of the higher
+// bits.  It is linear over GF(2) (phys(a^b) = phys(a)^phys(b)), keeps the
+// 16-byte pairs (2k, 2k+1) together, and spreads lanes that differ only in
+// high tile bits over different banks.
+__device__ __forceinline__ uint32_t phys(uint32_t i) {
+  return i ^ ((((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 7u) << 1);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ----------------------------------------------------- register ops -------
+template <int R, int A>
+__device__ __forceinline__ void op_u1(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
+  if constexpr (A < R) {
+    const float2 g00 = c[0], g01 = c[1], g10 = c[2], g11 = c[3];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << A)) continue;
+      const int k = j | (1 << A);
+      const bool p = gp && ((j & rc) == rc);
+      float2 a0 = v[j], a1 = v[k];
+      float2 n0 = cfma2(g00, a0, g01, a1);
+      float2 n1 = cfma2(g10, a0, g11, a1);
+      v[j] = p ? n0 : a0;
+      v[k] = p ? n1 : a1;
+    }
+  }
+}
+
+template <int R, int A, int B>
+__device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
+  if constexpr (A < B && B < R) {
+    float2 g[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) g[i] = c[i];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & ((1 << A) | (1 << B))) continue;
+      const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
+      const bool p = gp && ((j & rc) == rc);
+      float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
+      float2 n0 = cfma4(g + 0, a0, a1, a2, a3);
+      float2 n1 = cfma4(g + 4, a0, a1, a2, a3);
+      float2 n2 = cfma4(g + 8, a0, a1, a2, a3);
+      float2 n3 = cfma4(g + 12, a0, a1, a2, a3);
+      v[j] = p ? n0 : a0;
+      v[j1] = p ? n1 : a1;
+      v[j2] = p ? n2 : a2;
+      v[j3] = p ? n3 : a3;
+    }
+  }
+}
+
+template <int R, int A>
+__device__ __forceinline__ void op_x(float2 (&v)[1 << R], unsigned rc, bool gp) {
+  if constexpr (A < R) {
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << A)) continue;
+      const int k = j | (1 << A);
+      const bool p = gp && ((j & rc) == rc);
+      float2 a0 = v[j], a1 = v[k];
+      v[j] = p ? a1 : a0;
+      v[k] = p ? a0 : a1;
+    }
+  }
+}
+
+template <int R, int A>
+__device__ __forceinline__ void op_y(float2 (&v)[1 << R], unsigned rc, bool gp) {
+  if constexpr (A < R) {
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << A)) continue;
+      const int k = j | (1 << A);
+      const bool p = gp && ((j & rc) == rc);
+      float2 a0 = v[j], a1 = v[k];
+      // Y|0> = i|1>, Y|1> = -i|0>:  new0 = -i*a1, new1 = i*a0
+      float2 n0 = make_float2(a1.y, -a1.x);
+      float2 n1 = make_float2(-a0.y, a0.x);
+      v[j] = p ? n0 : a0;
+      v[k] = p ? n1 : a1;
+    }
+  }
+}
+
+template <int R, int A, int B>
+__device__ __forceinline__ void op_swap(float2 (&v)[1 << R], unsigned rc, bool gp) {
+  if constexpr (A < B && B < R) {
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & ((1 << A) | (1 << B))) continue;
+      const int ja = j | (1 << A), jb = j | (1 << B);
+      const bool p = gp && ((j & rc) == rc);
+      float2 a = v[ja], b = v[jb];
+      v[ja] = p ? b : a;
+      v[jb] = p ? a : b;
+    }
+  }
+}
+
+__device__ __forceinline__ int locbit(int d, int j, uint64_t gidx) {
+  return (d & DLOC_GLOBAL) ? (int)((gidx >> (d & 0x7f)) & 1ull) : ((j >> d) & 1);
+}
+
+#define CASES_1(F, ...)                                                          \
+  case 0: F<R, 0>(__VA_ARGS__); break;                                           \
+  case 1: F<R, 1>(__VA_ARGS__); break;                                           \
+  case 2: F<R, 2>(__VA_ARGS__); break;                                           \
+  case 3: F<R, 3>(__VA_ARGS__); break;                                           \
+  case 4: F<R, 4>(__VA_ARGS__); break;
+
+#define CASES_2(F, ...)                                                          \
+  case 0 * 8 + 1: F<R, 0, 1>(__VA_ARGS__); break;                                \
+  case 0 * 8 + 2: F<R, 0, 2>(__VA_ARGS__); break;                                \
+  case 0 * 8 + 3: F<R, 0, 3>(__VA_ARGS__); break;                                \
+  case 0 * 8 + 4: F<R, 0, 4>(__VA_ARGS__); break;                                \
+  case 1 * 8 + 2: F<R, 1, 2>(__VA_ARGS__); break;                                \
+  case 1 * 8 + 3: F<R, 1, 3>(__VA_ARGS__); break;                                \
+  case 1 * 8 + 4: F<R, 1, 4>(__VA_ARGS__); break;                                \
+  case 2 * 8 + 3: F<R, 2, 3>(__VA_ARGS__); break;                                \
+  case 2 * 8 + 4: F<R, 2, 4>(__VA_ARGS__); break;                                \
+  case 3 * 8 + 4: F<R, 3, 4>(__VA_ARGS__); break;
+
+template <int R>
+__device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __restrict__ ops, int ob, int oe,
+                                        const float2* __restrict__ coef, uint64_t gidx) {
+  for (int o = ob; o < oe; ++o) {
+    const DevOp op = ops[o];
+    const bool gp = (gidx & op.gc) == op.gc;
+    const unsigned rc = op.rc;
+    const float2* c = coef + op.coef;
+    switch (op.kind) {
+      case DK_U1:
+        switch (op.t0) { CASES_1(op_u1, v, c, rc, gp) }
+        break;
+      case DK_U2:
+        switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c, rc, gp) }
+        break;
+      case DK_X:
+        switch (op.t0) { CASES_1(op_x, v, rc, gp) }
+        break;
+      case DK_Y:
+        switch (op.t0) { CASES_1(op_y, v, rc, gp) }
+        break;
+      case DK_SWAP:
+        switch (op.t0 * 8 + op.t1) { CASES_2(op_swap, v, rc, gp) }
+        break;
+      case DK_NEG:
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j)
+          if (gp && ((j & rc) == rc)) v[j] = make_float2(-v[j].x, -v[j].y);
+        break;
+      case DK_PHASE: {
+        const float2 ph = c[0];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j)
+          if (gp && ((j & rc) == rc)) v[j] = cmul_comp(v[j], ph);
+        break;
+      }
+      case DK_DIAG1: {
+        const float2 d0 = c[0], d1 = c[1];
+        const int l0 = op.d0;
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j)
+          if (gp && ((j & rc) == rc)) v[j] = cmul_comp(v[j], locbit(l0, j, gidx) ? d1 : d0);
+        break;
+      }
+      case DK_DIAG2: {
+        const float2 d0 = c[0], d1 = c[1], d2 = c[2], d3 = c[3];
+        const int l0 = op.d0, l1 = op.d1;
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+          if (!(gp && ((j & rc) == rc))) continue;
+          const int s = (locbit(l1, j, gidx) << 1) | locbit(l0, j, gidx);
+          const float2 d = s == 0 ? d0 : s == 1 ? d1 : s == 2 ? d2 : d3;
+          v[j] = cmul_comp(v[j], d);
+        }
+        break;
+      }
+      default:
+        break;
+    }
+  }
+}
+
+// ---------------------------------------------------------- the kernel ----
+template <int R>
+__global__ void __launch_bounds__(256, 2)
+k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restrict__ items, int nitems,
+       uint64_t total_tiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);
+  __shared__ uint64_t dep_lo[128];
+  __shared__ uint64_t dep_hi[128];
+  __shared__ int s_S[16];
+
+  int cur = -1;
+  const DevPass* P = nullptr;
+  float2* state = nullptr;
+  int T = 0;
+
+  for (uint64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    // Which item owns tile t (items sorted by tile_begin).
+    int it = 0;
+    if (nitems > 1) {
+      int lo = 0, hi = nitems - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+      }
+      it = lo;
+    }
+    const PassItem I = (nitems > 1) ? items[it] : single;
+    if (it != cur) {
+      __syncthreads();  // previous tables no longer in use
+      cur = it;
+      P = I.pass;
+      state = base_state + I.state_off;
+      T = P->T;
+      if (threadIdx.x < 16) s_S[threadIdx.x] = P->S[threadIdx.x];
+      __syncthreads();
+      // dep(i) = sum_k bit_k(i) << S[k], split in two 7-bit tables.
+      for (int e = threadIdx.x; e < 256; e += blockDim.x) {
+        const int part = e >> 7, x = e & 127;
+        uint64_t d = 0;
+        for (int k = 0; k < 7; ++k) {
+          const int kk = part * 7 + k;
+          if (kk < T && ((x >> k) & 1)) d |= 1ull << s_S[kk];
+        }
+        if (part == 0) dep_lo[x] = d; else dep_hi[x] = d;
+      }
+      __syncthreads();
+    }
+    const uint64_t local = t - I.tile_begin;
+    uint64_t gbase = local;
+    for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, s_S[k]);
+
+    // 1. load the tile (pairs (2c, 2c+1) are adjacent in HBM: S[0] == 0)
+    const uint32_t npairs = 1u << (T - 1);
+    if (I.flags & PI_FROM_ZERO) {
+      // |0..0>: only the tile holding index 0 of its state has a non-zero
+      // entry (the bits above n_qubits select the state in a batch)
+      const bool first = (gbase & ((1ull << P->n_qubits) - 1ull)) == 0ull;
+      for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+        const uint32_t i = c << 1;
+        const float x = (first && i == 0) ? 1.f : 0.f;
+        *reinterpret_cast<float4*>(tile + phys(i)) = make_float4(x, 0.f, 0.f, 0.f);
+      }
+    } else {
+      for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+        const uint32_t i = c << 1;
+        const uint64_t g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];
+        cp_async16(tile + phys(i), state + g);
+      }
+      cp_async_wait_all();
+    }
+    __syncthreads();
+
+    // 2. register blocks
+    const DevBlock* blocks = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off);
+    const DevOp* ops = reinterpret_cast<const DevOp*>(reinterpret_cast<const char*>(P) + P->op_off);
+    const float2* coef = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(P) + P->coef_off);
+    const int nblocks = P->nblocks;
+    const uint32_t ngroups = 1u << (T - R);
+    for (int b = 0; b < nblocks; ++b) {
+      const DevBlock blk = blocks[b];
+      int pos[R];
+      uint32_t pp[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) { pos[k] = blk.pos[k]; pp[k] = phys(1u << pos[k]); }
+      const bool need_g = blk.pos[7] != 0;
+      for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        uint32_t base = g;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+          const uint32_t lo = base & ((1u << pos[k]) - 1u);
+          base = ((base ^ lo) << 1) | lo;
+        }
+        const uint32_t pb = phys(base);
+        const uint64_t gidx = need_g ? (gbase | dep_lo[base & 127] | dep_hi[base >> 7]) : 0ull;
+        float2 v[1 << R];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+          uint32_t a = pb;
+#pragma unroll
+          for (int k = 0; k < R; ++k) if (j & (1 << k)) a ^= pp[k];
+          v[j] = tile[a];
+        }
+        run_ops<R>(v, ops, blk.op_begin, blk.op_end, coef, gidx);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+          uint32_t a = pb;
+#pragma unroll
+          for (int k = 0; k < R; ++k) if (j & (1 << k)) a ^= pp[k];
+          tile[a] = v[j];
+        }
+      }
+      __syncthreads();
+    }
+
+    // 3. store the tile back in place
+    for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+      const uint32_t i = c << 1;
+      const uint64_t g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];
+      *reinterpret_cast<float4*>(state + g) = *reinterpret_cast<const float4*>(tile + phys(i));
+    }
+    __syncthreads();
+  }
+}
+
+struct LaunchCfg { int per_sm; };
+
+template <int R>
+LaunchCfg configure(int smem, int threads) {
+  static std::map<std::pair<int, int>, LaunchCfg> cache;
+  auto key = std::make_pair(smem, threads);
+  auto f = cache.find(key);
+  if (f != cache.end()) return f->second;
+  QS_CUDA(cudaFuncSetAttribute(k_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R>, threads, smem));
+  if (per_sm < 1) throw qs_error(QS_ERR_CUDA, "tile-pass kernel does not fit on an SM");
+  LaunchCfg c{per_sm};
+  cache[key] = c;
+  return c;
+}
+
+template <int R>
+void launch_R(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
+              uint64_t total, int maxT, int threads) {
+  const int smem = (int)(sizeof(float2) << maxT);
+  LaunchCfg c = configure<R>(smem, threads);
+  uint64_t grid = std::min<uint64_t>(total, (uint64_t)h->sm_count * c.per_sm);
+  if (grid == 0) return;
+  k_pass<R><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total);
+  qs_after_launch(h, "k_pass");
+}
+
+int threads_for(int maxT, int R) {
+  int groups = 1 << (maxT - R);
+  int t = groups < 256 ? groups : 256;
+  if (t < 32) t = 32;
+  return t;
+}
+
+void dispatch(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
+              uint64_t total, int maxT, int R) {
+  QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
+  const int threads = threads_for(maxT, R);
+  switch (R) {
+    case 1: launch_R<1>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    case 2: launch_R<2>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    case 3: launch_R<3>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    case 4: launch_R<4>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    case 5: launch_R<5>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    default: throw qs_error(QS_ERR_INVALID, "register block width must be 1..5");
+  }
+}
+
+}  // namespace
+
+// One state, one pass: the item is passed by value (no device table), so the
+// launch can be captured in a CUDA graph.
+void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
+                           uint32_t flags) {
+  PassItem it{};
+  it.state_off = 0;
+  it.pass = d_pass;
+  it.ntiles = ntiles;
+  it.tile_begin = 0;
+  it.flags = flags;
+  dispatch(h, (float2*)state, it, nullptr, 1, ntiles, T, R);
+}
+
+// Several (state, pass) items in one launch; d_items is a caller-owned device
+// table whose tile_begin fields hold the prefix sums of ntiles.
+void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
+                          int maxT, int R) {
+  if (n_items <= 0 || total_tiles == 0) return;
+  PassItem dummy{};
+  dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R);
+}

@@ -1,0 +1,576 @@
+// qs_plan.cpp — host-side circuit planner (FP64) and plan execution.
+//
+// Replaces the reference's Python compile step
+// (blackwell_backend/simulator.py:247-434, the 6-phase fusion) and dispatcher
+// (simulator.py:439-468).  Differences by design:
+//   * all matrix products run in FP64 on the host (the reference multiplies
+//     complex64 tensors on the GPU, simulator.py:339-377);
+//   * instead of one launch per fused op, the circuit is cut into tile passes
+//     (qs_pass.cu): each pass streams the state through shared memory once and
+//     applies every gate it holds in registers;
+//   * diagonal gates, phases and controls never constrain a pass: they are
+//     evaluated from the amplitude index wherever their qubits live.
+#include "qs_api.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <set>
+
+namespace {
+
+using cd = std::complex<double>;
+
+enum IKind { I_U1, I_U2, I_X, I_SWAP, I_Y, I_NEG, I_PHASE, I_DIAG1, I_DIAG2 };
+
+struct IOp {
+  int kind;
+  int tq[2] = {-1, -1};   // non-diagonal targets (bit0, bit1)
+  int ntq = 0;
+  std::vector<int> cq;    // controls (all must be 1); for PHASE/NEG: the qubits
+  int dq[2] = {-1, -1};   // diagonal qubits (DIAG1/DIAG2)
+  int ndq = 0;
+  cd m[16];
+};
+
+// ------------------------------------------------------------ normalise --
+void mat_from(const double* m, cd* out, int count) {
+  for (int i = 0; i < count; ++i) out[i] = cd(m[2 * i], m[2 * i + 1]);
+}
+
+void check_q(int q, int n) {
+  if (q < 0 || q >= n) throw qs_error(QS_ERR_INVALID, "op qubit index out of range");
+}
+
+std::vector<IOp> normalise(int n, const qs_op* ops, int nops) {
+  std::vector<IOp> out;
+  out.reserve(nops);
+  for (int i = 0; i < nops; ++i) {
+    const qs_op& o = ops[i];
+    QS_CHECK_ARG(o.nq >= 0 && o.nq <= 8, "op nq out of range");
+    for (int k = 0; k < o.nq; ++k) check_q(o.q[k], n);
+    {
+      std::set<int> u(o.q, o.q + o.nq);
+      QS_CHECK_ARG((int)u.size() == o.nq, "op has a repeated qubit");
+    }
+    IOp p;
+    switch (o.kind) {
+      case QS_OP_U1:
+        QS_CHECK_ARG(o.nq == 1, "U1 needs 1 qubit");
+        p.kind = I_U1; p.tq[0] = o.q[0]; p.ntq = 1; mat_from(o.m, p.m, 4);
+        break;
+      case QS_OP_U2:
+        QS_CHECK_ARG(o.nq == 2, "U2 needs 2 qubits");
+        p.kind = I_U2; p.tq[0] = o.q[0]; p.tq[1] = o.q[1]; p.ntq = 2; mat_from(o.m, p.m, 16);
+        break;
+      case QS_OP_DIAG1:
+        QS_CHECK_ARG(o.nq == 1, "DIAG1 needs 1 qubit");
+        p.kind = I_DIAG1; p.dq[0] = o.q[0]; p.ndq = 1; mat_from(o.m, p.m, 2);
+        break;
+      case QS_OP_DIAG2:
+        QS_CHECK_ARG(o.nq == 2, "DIAG2 needs 2 qubits");
+        p.kind = I_DIAG2; p.dq[0] = o.q[0]; p.dq[1] = o.q[1]; p.ndq = 2; mat_from(o.m, p.m, 4);
+        break;
+      case QS_OP_MCU1:
+        QS_CHECK_ARG(o.nq >= 1, "MCU1 needs a target");
+        p.kind = I_U1; p.tq[0] = o.q[o.nq - 1]; p.ntq = 1;
+        p.cq.assign(o.q, o.q + o.nq - 1); mat_from(o.m, p.m, 4);
+        break;
+      case QS_OP_MCU2:
+        QS_CHECK_ARG(o.nq >= 2, "MCU2 needs two targets");
+        p.kind = I_U2; p.tq[0] = o.q[o.nq - 2]; p.tq[1] = o.q[o.nq - 1]; p.ntq = 2;
+        p.cq.assign(o.q, o.q + o.nq - 2); mat_from(o.m, p.m, 16);
+        break;
+      case QS_OP_MCX:
+        QS_CHECK_ARG(o.nq >= 1, "MCX needs a target");
+        p.kind = I_X; p.tq[0] = o.q[o.nq - 1]; p.ntq = 1; p.cq.assign(o.q, o.q + o.nq - 1);
+        break;
+      case QS_OP_MCSWAP:
+        QS_CHECK_ARG(o.nq >= 2, "MCSWAP needs two targets");
+        p.kind = I_SWAP; p.tq[0] = o.q[o.nq - 2]; p.tq[1] = o.q[o.nq - 1]; p.ntq = 2;
+        p.cq.assign(o.q, o.q + o.nq - 2);
+        break;
+      case QS_OP_MCPHASE: {
+        QS_CHECK_ARG(o.nq >= 1, "MCPHASE needs a qubit");
+        cd ph(o.m[0], o.m[1]);
+        p.kind = (ph == cd(-1.0, 0.0)) ? I_NEG : I_PHASE;
+        p.cq.assign(o.q, o.q + o.nq);
+        p.m[0] = ph;
+        break;
+      }
+      case QS_OP_Y:
+        QS_CHECK_ARG(o.nq == 1, "Y needs 1 qubit");
+        p.kind = I_Y; p.tq[0] = o.q[0]; p.ntq = 1;
+        break;
+      case QS_OP_RX: case QS_OP_RY: case QS_OP_RZ: {
+        QS_CHECK_ARG(o.nq == 1, "rotation needs 1 qubit");
+        const double th = o.m[0], c = std::cos(th / 2), s = std::sin(th / 2);
+        if (o.kind == QS_OP_RZ) {
+          p.kind = I_DIAG1; p.dq[0] = o.q[0]; p.ndq = 1;
+          p.m[0] = std::polar(1.0, -th / 2); p.m[1] = std::polar(1.0, th / 2);
+        } else {
+          p.kind = I_U1; p.tq[0] = o.q[0]; p.ntq = 1;
+          if (o.kind == QS_OP_RX) { p.m[0] = c; p.m[1] = cd(0, -s); p.m[2] = cd(0, -s); p.m[3] = c; }
+          else { p.m[0] = c; p.m[1] = -s; p.m[2] = s; p.m[3] = c; }
+        }
+        break;
+      }
+      default:
+        throw qs_error(QS_ERR_INVALID, "unknown op kind " + std::to_string(o.kind));
+    }
+    out.push_back(std::move(p));
+  }
+  return out;
+}
+
+// ----------------------------------------------------- 1Q fusion (FP64) --
+struct M2 { cd a[4]; };
+M2 mul(const M2& A, const M2& B) {  // A*B
+  M2 C;
+  C.a[0] = A.a[0] * B.a[0] + A.a[1] * B.a[2];
+  C.a[1] = A.a[0] * B.a[1] + A.a[1] * B.a[3];
+  C.a[2] = A.a[2] * B.a[0] + A.a[3] * B.a[2];
+  C.a[3] = A.a[2] * B.a[1] + A.a[3] * B.a[3];
+  return C;
+}
+
+// Is `o` an uncontrolled single-qubit op?  Then return its 2x2 matrix.
+bool as_1q(const IOp& o, int& q, M2& M) {
+  switch (o.kind) {
+    case I_U1:
+      if (!o.cq.empty()) return false;
+      q = o.tq[0]; for (int i = 0; i < 4; ++i) M.a[i] = o.m[i]; return true;
+    case I_X:
+      if (!o.cq.empty()) return false;
+      q = o.tq[0]; M.a[0] = 0; M.a[1] = 1; M.a[2] = 1; M.a[3] = 0; return true;
+    case I_Y:
+      q = o.tq[0]; M.a[0] = 0; M.a[1] = cd(0, -1); M.a[2] = cd(0, 1); M.a[3] = 0; return true;
+    case I_DIAG1:
+      q = o.dq[0]; M.a[0] = o.m[0]; M.a[1] = 0; M.a[2] = 0; M.a[3] = o.m[1]; return true;
+    case I_NEG: case I_PHASE:
+      if (o.cq.size() != 1) return false;
+      q = o.cq[0]; M.a[0] = 1; M.a[1] = 0; M.a[2] = 0; M.a[3] = o.m[0];
+      if (o.kind == I_NEG) M.a[3] = -1.0;
+      return true;
+    default:
+      return false;
+  }
+}
+
+IOp emit_1q(int q, const M2& M, bool& keep) {
+  IOp p;
+  keep = true;
+  const bool diag = (M.a[1] == 0.0 && M.a[2] == 0.0);
+  if (diag) {
+    if (M.a[0] == 1.0 && M.a[3] == 1.0) { keep = false; return p; }
+    if (M.a[0] == 1.0) {
+      p.kind = (M.a[3] == -1.0) ? I_NEG : I_PHASE;
+      p.cq = {q};
+      p.m[0] = M.a[3];
+      return p;
+    }
+    p.kind = I_DIAG1; p.dq[0] = q; p.ndq = 1; p.m[0] = M.a[0]; p.m[1] = M.a[3];
+    return p;
+  }
+  if (M.a[0] == 0.0 && M.a[3] == 0.0 && M.a[1] == 1.0 && M.a[2] == 1.0) {
+    p.kind = I_X; p.tq[0] = q; p.ntq = 1;
+    return p;
+  }
+  p.kind = I_U1; p.tq[0] = q; p.ntq = 1;
+  for (int i = 0; i < 4; ++i) p.m[i] = M.a[i];
+  return p;
+}
+
+void qubits_of(const IOp& o, std::vector<int>& qs) {
+  qs.clear();
+  for (int i = 0; i < o.ntq; ++i) qs.push_back(o.tq[i]);
+  for (int i = 0; i < o.ndq; ++i) qs.push_back(o.dq[i]);
+  for (int c : o.cq) qs.push_back(c);
+}
+
+std::vector<IOp> fuse_1q(int n, const std::vector<IOp>& in) {
+  std::vector<IOp> out;
+  std::vector<M2> pend(n);
+  std::vector<char> has(n, 0);
+  auto flush = [&](int q) {
+    if (!has[q]) return;
+    bool keep;
+    IOp p = emit_1q(q, pend[q], keep);
+    if (keep) out.push_back(std::move(p));
+    has[q] = 0;
+  };
+  std::vector<int> qs;
+  for (const IOp& o : in) {
+    int q;
+    M2 M;
+    if (as_1q(o, q, M)) {
+      pend[q] = has[q] ? mul(M, pend[q]) : M;
+      has[q] = 1;
+      continue;
+    }
+    qubits_of(o, qs);
+    for (int x : qs) flush(x);
+    out.push_back(o);
+  }
+  for (int q = 0; q < n; ++q) flush(q);
+  return out;
+}
+
+// --------------------------------------------------------- pass split ----
+struct PassPlan {
+  int T;
+  std::vector<int> S;        // tile qubits ascending
+  std::vector<int> ops;      // indices into the fused op list, in order
+};
+
+std::vector<PassPlan> split_passes(int n, int T, const std::vector<IOp>& ops) {
+  std::vector<PassPlan> passes;
+  std::vector<int> remaining(ops.size());
+  for (size_t i = 0; i < ops.size(); ++i) remaining[i] = (int)i;
+  const int Lc = std::min(T, 4);  // low qubits always in the tile (coalescing)
+  if (T >= n) {
+    PassPlan p;
+    p.T = n;
+    for (int q = 0; q < n; ++q) p.S.push_back(q);
+    p.ops = remaining;
+    passes.push_back(std::move(p));
+    return passes;
+  }
+  std::vector<char> inS(n), bT(n), bD(n);
+  while (!remaining.empty()) {
+    std::fill(inS.begin(), inS.end(), 0);
+    std::fill(bT.begin(), bT.end(), 0);
+    std::fill(bD.begin(), bD.end(), 0);
+    int sz = 0;
+    for (int q = 0; q < Lc; ++q) { inS[q] = 1; ++sz; }
+    PassPlan p;
+    p.T = T;
+    std::vector<int> left;
+    for (int idx : remaining) {
+      const IOp& o = ops[idx];
+      bool blocked = false;
+      for (int i = 0; i < o.ntq && !blocked; ++i) blocked = bT[o.tq[i]] || bD[o.tq[i]];
+      for (int i = 0; i < o.ndq && !blocked; ++i) blocked = bT[o.dq[i]];
+      for (size_t i = 0; i < o.cq.size() && !blocked; ++i) blocked = bT[o.cq[i]];
+      if (!blocked) {
+        int need = 0;
+        for (int i = 0; i < o.ntq; ++i) need += !inS[o.tq[i]];
+        if (sz + need <= T) {
+          for (int i = 0; i < o.ntq; ++i) if (!inS[o.tq[i]]) { inS[o.tq[i]] = 1; ++sz; }
+          p.ops.push_back(idx);
+          continue;
+        }
+        blocked = true;
+      }
+      for (int i = 0; i < o.ntq; ++i) bT[o.tq[i]] = 1;
+      for (int i = 0; i < o.ndq; ++i) bD[o.dq[i]] = 1;
+      for (int c : o.cq) bD[c] = 1;
+      left.push_back(idx);
+    }
+    QS_CHECK_ARG(!p.ops.empty(), "planner made no progress (op wider than the tile?)");
+    for (int q = 0; q < n && sz < T; ++q) if (!inS[q]) { inS[q] = 1; ++sz; }
+    for (int q = 0; q < n; ++q) if (inS[q]) p.S.push_back(q);
+    passes.push_back(std::move(p));
+    remaining.swap(left);
+  }
+  return passes;
+}
+
+// ---------------------------------------------------------- encoding -----
+inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+void permute_u2_bits(cd* m) {
+  static const int perm[4] = {0, 2, 1, 3};
+  cd r[16];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) r[4 * a + b] = m[4 * perm[a] + perm[b]];
+  for (int i = 0; i < 16; ++i) m[i] = r[i];
+}
+
+void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::vector<char>& blob,
+                 uint32_t& pass_off, int& R_out, int& nblocks_out) {
+  const int T = pp.T;
+  const int R = std::min(5, T);
+  std::vector<int> tpos(n, -1);  // global qubit -> tile position
+  for (int k = 0; k < T; ++k) tpos[pp.S[k]] = k;
+
+  // Register blocks: consecutive ops whose targets fit in R tile positions.
+  struct Blk { std::vector<int> regs; std::vector<int> ops; };
+  std::vector<Blk> blks;
+  Blk cur;
+  for (int idx : pp.ops) {
+    const IOp& o = ops[idx];
+    std::vector<int> need;
+    for (int i = 0; i < o.ntq; ++i) {
+      int p = tpos[o.tq[i]];
+      if (p < 0) throw qs_error(QS_ERR_INVALID, "internal: pass target outside tile");
+      if (std::find(cur.regs.begin(), cur.regs.end(), p) == cur.regs.end()) need.push_back(p);
+    }
+    if ((int)(cur.regs.size() + need.size()) > R) {
+      blks.push_back(cur);
+      cur = Blk();
+      need.clear();
+      for (int i = 0; i < o.ntq; ++i) need.push_back(tpos[o.tq[i]]);
+    }
+    for (int p : need) cur.regs.push_back(p);
+    cur.ops.push_back(idx);
+  }
+  if (!cur.ops.empty() || blks.empty()) blks.push_back(cur);
+
+  std::vector<DevBlock> dblocks;
+  std::vector<DevOp> dops;
+  std::vector<float> coef;  // float2 pool, re/im
+  for (Blk& b : blks) {
+    // pad to R positions with the lowest unused tile positions
+    for (int p = 0; (int)b.regs.size() < R && p < T; ++p)
+      if (std::find(b.regs.begin(), b.regs.end(), p) == b.regs.end()) b.regs.push_back(p);
+    std::sort(b.regs.begin(), b.regs.end());
+    auto regidx = [&](int q) -> int {
+      int p = tpos[q];
+      if (p < 0) return -1;
+      auto it = std::find(b.regs.begin(), b.regs.end(), p);
+      return it == b.regs.end() ? -1 : (int)(it - b.regs.begin());
+    };
+    DevBlock db;
+    std::memset(&db, 0, sizeof(db));
+    for (int k = 0; k < R; ++k) db.pos[k] = (int8_t)b.regs[k];
+    db.op_begin = (int32_t)dops.size();
+    bool need_g = false;
+    for (int idx : b.ops) {
+      IOp o = ops[idx];
+      DevOp d;
+      std::memset(&d, 0, sizeof(d));
+      for (int c : o.cq) {
+        int r = regidx(c);
+        if (r >= 0) d.rc |= (uint8_t)(1u << r); else { d.gc |= 1ull << c; need_g = true; }
+      }
+      auto loc = [&](int q) -> uint8_t {
+        int r = regidx(q);
+        if (r >= 0) return (uint8_t)r;
+        need_g = true;
+        return (uint8_t)(DLOC_GLOBAL | q);
+      };
+      int ncoef = 0;
+      switch (o.kind) {
+        case I_U1: d.kind = DK_U1; d.t0 = (uint8_t)regidx(o.tq[0]); ncoef = 4; break;
+        case I_U2: {
+          int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
+          if (a > c) { std::swap(a, c); permute_u2_bits(o.m); }
+          d.kind = DK_U2; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c; ncoef = 16;
+          break;
+        }
+        case I_X: d.kind = DK_X; d.t0 = (uint8_t)regidx(o.tq[0]); break;
+        case I_Y: d.kind = DK_Y; d.t0 = (uint8_t)regidx(o.tq[0]); break;
+        case I_SWAP: {
+          int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
+          if (a > c) std::swap(a, c);
+          d.kind = DK_SWAP; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c;
+          break;
+        }
+        case I_NEG: d.kind = DK_NEG; break;
+        case I_PHASE: d.kind = DK_PHASE; ncoef = 1; break;
+        case I_DIAG1: d.kind = DK_DIAG1; d.d0 = loc(o.dq[0]); ncoef = 2; break;
+        case I_DIAG2: d.kind = DK_DIAG2; d.d0 = loc(o.dq[0]); d.d1 = loc(o.dq[1]); ncoef = 4; break;
+      }
+      d.ncoef = (uint8_t)ncoef;
+      d.coef = (uint32_t)(coef.size() / 2);
+      for (int i = 0; i < ncoef; ++i) {
+        coef.push_back((float)o.m[i].real());
+        coef.push_back((float)o.m[i].imag());
+      }
+      dops.push_back(d);
+    }
+    db.op_end = (int32_t)dops.size();
+    db.pos[7] = need_g ? 1 : 0;
+    dblocks.push_back(db);
+  }
+
+  DevPass hdr;
+  std::memset(&hdr, 0, sizeof(hdr));
+  hdr.T = T;
+  hdr.R = R;
+  hdr.nblocks = (int32_t)dblocks.size();
+  hdr.n_qubits = n;
+  for (int k = 0; k < T; ++k) hdr.S[k] = pp.S[k];
+  size_t off = align16(sizeof(DevPass));
+  hdr.block_off = (uint32_t)off;
+  off = align16(off + dblocks.size() * sizeof(DevBlock));
+  hdr.op_off = (uint32_t)off;
+  off = align16(off + dops.size() * sizeof(DevOp));
+  hdr.coef_off = (uint32_t)off;
+  off = align16(off + coef.size() * sizeof(float));
+  hdr.bytes = (uint32_t)off;
+
+  pass_off = (uint32_t)blob.size();
+  blob.resize(blob.size() + off, 0);
+  char* base = blob.data() + pass_off;
+  std::memcpy(base, &hdr, sizeof(hdr));
+  if (!dblocks.empty()) std::memcpy(base + hdr.block_off, dblocks.data(), dblocks.size() * sizeof(DevBlock));
+  if (!dops.empty()) std::memcpy(base + hdr.op_off, dops.data(), dops.size() * sizeof(DevOp));
+  if (!coef.empty()) std::memcpy(base + hdr.coef_off, coef.data(), coef.size() * sizeof(float));
+  R_out = R;
+  nblocks_out = (int)dblocks.size();
+}
+
+double op_flops(const IOp& o) {
+  switch (o.kind) {
+    case I_U1: return 16;
+    case I_U2: return 32;
+    case I_PHASE: case I_DIAG1: case I_DIAG2: return 8;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* plan) {
+  QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
+  QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
+  std::vector<IOp> norm = normalise(n, ops, nops);
+  std::vector<IOp> fused = fuse_1q(n, norm);
+  int T = n <= 14 ? n : tile_bits;
+  std::vector<PassPlan> passes = split_passes(n, T, fused);
+  plan->n_qubits = n;
+  plan->tile_bits = T;
+  plan->blob.clear();
+  plan->pass_offsets.clear();
+  plan->pass_T.clear();
+  plan->pass_R.clear();
+  int nblocks_total = 0;
+  double flops = 0;
+  for (auto& o : fused) flops += op_flops(o);
+  for (const PassPlan& pp : passes) {
+    uint32_t off;
+    int R, nb;
+    encode_pass(n, pp, fused, plan->blob, off, R, nb);
+    plan->pass_offsets.push_back(off);
+    plan->pass_T.push_back(pp.T);
+    plan->pass_R.push_back(R);
+    nblocks_total += nb;
+  }
+  qs_plan_info& I = plan->info;
+  I.n_qubits = n;
+  I.tile_bits = T;
+  I.n_passes = (int32_t)passes.size();
+  I.n_blocks = nblocks_total;
+  I.n_ops_in = nops;
+  I.n_ops_fused = (int64_t)fused.size();
+  I.bytes_moved = (double)passes.size() * 16.0 * std::ldexp(1.0, n);
+  I.flops = flops * std::ldexp(1.0, n);
+}
+
+void qs_plan_upload(qs_context* h, qs_plan_s* p) {
+  p->device = h->device;
+  if (p->blob.empty()) return;
+  QS_CUDA(cudaMalloc(&p->d_blob, p->blob.size()));
+  QS_CUDA(cudaMemcpy(p->d_blob, p->blob.data(), p->blob.size(), cudaMemcpyHostToDevice));
+}
+
+void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states) {
+  const int n = p->n_qubits;
+  if (p->pass_offsets.empty()) {
+    if (from_zero) QS_CHECK_ARG(qs_state_init_batched(h, state, (int)n_states, n) == QS_OK, h->err.c_str());
+    return;
+  }
+  for (size_t i = 0; i < p->pass_offsets.size(); ++i) {
+    const DevPass* dp = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
+    const int T = p->pass_T[i];
+    const uint32_t flags = (from_zero && i == 0) ? PI_FROM_ZERO : 0u;
+    qs_launch_pass_single(h, state, dp, T, p->pass_R[i], n_states << (n - T), flags);
+  }
+}
+
+extern "C" {
+
+int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* out) {
+  QS_REQUIRE_HANDLE(h);
+  qs_plan_s* p = nullptr;
+  QS_API_BEGIN
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  *out = nullptr;
+  p = new qs_plan_s();
+  qs_build_plan(n, ops, nops, h->tile_bits, p);
+  qs_plan_upload(h, p);
+  *out = p;
+  p = nullptr;
+  return QS_OK;
+  }
+  catch (const qs_error& e) {
+    h->err = e.what();
+    if (p) { if (p->d_blob) cudaFree(p->d_blob); delete p; }
+    return e.code;
+  }
+  catch (const std::exception& e) {
+    h->err = e.what();
+    if (p) { if (p->d_blob) cudaFree(p->d_blob); delete p; }
+    return QS_ERR_INVALID;
+  }
+}
+
+int qs_plan_info_get(qs_plan_t plan, qs_plan_info* info) {
+  if (!plan || !info) { qs_set_tls_error("null plan or info"); return QS_ERR_INVALID; }
+  *info = plan->info;
+  return QS_OK;
+}
+
+int qs_plan_execute(qs_handle_t h, qs_plan_t plan, void* state) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(plan != nullptr, "plan is null");
+  qs_check_state(state, plan->n_qubits);
+  QS_CHECK_ARG(plan->device == h->device, "plan was built for another device");
+  qs_plan_run(h, plan, state, false, 1);
+  QS_API_END(h)
+}
+
+int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(plan != nullptr, "plan is null");
+  qs_check_state(state, plan->n_qubits);
+  QS_CHECK_ARG(plan->device == h->device, "plan was built for another device");
+  qs_plan_run(h, plan, state, true, 1);
+  QS_API_END(h)
+}
+
+int qs_plan_destroy(qs_plan_t plan) {
+  if (!plan) return QS_OK;
+  if (plan->d_blob) cudaFree(plan->d_blob);
+  delete plan;
+  return QS_OK;
+}
+
+int qs_run_circuit(qs_handle_t h, void* state, int n, const qs_op* ops, int nops) {
+  qs_plan_t p = nullptr;
+  int rc = qs_plan_create(h, n, ops, nops, &p);
+  if (rc != QS_OK) return rc;
+  rc = qs_plan_execute(h, p, state);
+  // The device program must outlive the queued passes.
+  if (rc == QS_OK) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { h->err = cudaGetErrorString(e); rc = QS_ERR_CUDA; }
+  }
+  qs_plan_destroy(p);
+  return rc;
+}
+
+int qs_apply_gates_fused(qs_handle_t h, void* state, int n, const float* gates, const int* targets, int ngates) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  std::vector<qs_op> ops;
+  QS_CHECK_ARG(ngates >= 0, "n_gates must be >= 0");
+  QS_CHECK_ARG(ngates == 0 || (gates && targets), "gates/targets pointer is null");
+  ops.resize(ngates);
+  for (int g = 0; g < ngates; ++g) {
+    qs_op& o = ops[g];
+    std::memset(&o, 0, sizeof(o));
+    o.kind = QS_OP_U1;
+    o.nq = 1;
+    o.q[0] = targets[g];
+    o.param = -1;
+    for (int i = 0; i < 8; ++i) o.m[i] = gates[8 * g + i];
+  }
+  return qs_run_circuit(h, state, n, ops.data(), ngates);
+  QS_API_END(h)
+}
+
+}  // extern "C"

@@ -1,0 +1,493 @@
+// qs_reduce.cu — reductions over a state, accumulated in FP64 in a fixed
+// order (no floating-point atomics), so every result is bit-reproducible and
+// the same whether a state is processed alone or inside a batch.
+//
+// Two-stage scheme: stage 1 gives each block a fixed contiguous slice of the
+// index range (the slicing depends only on the item count); every thread sums
+// a fixed strided subset sequentially, then the block reduces in a fixed tree
+// order.  Stage 2 is one block that reduces the per-block partials in order.
+#include "qs_api.h"
+#include "qs_common.cuh"
+#include <algorithm>
+#include <cmath>
+
+using namespace qs;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 1024;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fixed-order block reduction; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = 0.0;
+  if (w == 0) {
+    v = lane < nw ? ws[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+struct Slicing { int nb; uint64_t per; };
+Slicing slice(uint64_t items) {
+  uint64_t nb = (items + 4095) / 4096;
+  if (nb > kMaxBlocks) nb = kMaxBlocks;
+  if (nb < 1) nb = 1;
+  return Slicing{(int)nb, (items + nb - 1) / nb};
+}
+
+// -------------------------------------------------------------- functors -
+// Each functor sees "items" = float4 vectors (two amplitudes).
+struct FNorm {
+  const float4* s;
+  __device__ double operator()(uint64_t i) const {
+    float4 v = s[i];
+    return (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+  }
+};
+
+struct FP0 {  // probability of bit t = 0
+  const float4* s;
+  int t;
+  __device__ double operator()(uint64_t i) const {
+    float4 v = s[i];
+    double a = (double)v.x * v.x + (double)v.y * v.y;
+    double b = (double)v.z * v.z + (double)v.w * v.w;
+    if (t == 0) return a;
+    return ((2 * i) >> t) & 1 ? 0.0 : a + b;
+  }
+};
+
+struct FZ {  // sum |a_i|^2 (-1)^popc(i & z)
+  const float4* s;
+  uint64_t z;
+  __device__ double operator()(uint64_t i) const {
+    float4 v = s[i];
+    double a = (double)v.x * v.x + (double)v.y * v.y;
+    double b = (double)v.z * v.z + (double)v.w * v.w;
+    uint64_t i0 = 2 * i;
+    double s0 = (__popcll(i0 & z) & 1) ? -a : a;
+    double s1 = (__popcll((i0 + 1) & z) & 1) ? -b : b;
+    return s0 + s1;
+  }
+};
+
+template <class F>
+__global__ void k_reduce(F f, uint64_t items, uint64_t per, double* __restrict__ partial) {
+  const uint64_t b0 = (uint64_t)blockIdx.x * per;
+  const uint64_t e = min(b0 + per, items);
+  double acc = 0.0;
+  for (uint64_t i = b0 + threadIdx.x; i < e; i += blockDim.x) acc += f(i);
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// mode 0: out[0] = sum.  mode 1: out[0] = sum, out[1] = 1/sqrt(sum) (renorm).
+__global__ void k_final(const double* __restrict__ partial, int nb, double* __restrict__ out, int mode) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += partial[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) {
+    out[0] = acc;
+    if (mode == 1) out[1] = acc > 0.0 ? 1.0 / sqrt(acc) : 0.0;
+  }
+}
+
+__global__ void k_scale(float4* __restrict__ s, uint64_t nvec, const double* __restrict__ scale) {
+  const float f = (float)scale[1];
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    float4 v = s[i];
+    s[i] = make_float4(v.x * f, v.y * f, v.z * f, v.w * f);
+  }
+}
+
+__global__ void k_probs(const float4* __restrict__ s, float2* __restrict__ p, uint64_t nvec) {
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    float4 v = s[i];
+    p[i] = make_float2(v.x * v.x + v.y * v.y, v.z * v.z + v.w * v.w);
+  }
+}
+
+// Collapse after measuring qubit t: keep amplitudes with bit t == outcome,
+// scaled by 1/sqrt(p_outcome); zero the others.  pr[0] = P(bit = 0).
+__global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double u, const double* __restrict__ pr,
+                           int* __restrict__ outcome) {
+  const double p0 = pr[0];
+  const int res = (u < p0) ? 0 : 1;
+  const double p = res == 0 ? p0 : 1.0 - p0;
+  const float f = p > 1e-30 ? (float)(1.0 / sqrt(p)) : 0.f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *outcome = res;
+  for (uint64_t i = gtid(); i < nvec; i += gstride()) {
+    float4 v = s[i];
+    const uint64_t i0 = 2 * i;
+    const int b0 = (int)((i0 >> t) & 1), b1 = (int)(((i0 + 1) >> t) & 1);
+    const float f0 = b0 == res ? f : 0.f, f1 = b1 == res ? f : 0.f;
+    s[i] = make_float4(v.x * f0, v.y * f0, v.z * f1, v.w * f1);
+  }
+}
+
+// ----------------------------------------------------------- sampling ----
+// The CDF is built in chunks of kChunk amplitudes.  A chunk is split into 32
+// contiguous segments of kSeg amplitudes, one per lane; a lane sums its
+// segment sequentially in FP64 and the warp scans the 32 segment sums in a
+// fixed shuffle order.  The same routine produces the chunk totals (pass 1)
+// and the in-chunk search (pass 3), so both see identical values.
+constexpr int kSeg = 64;
+constexpr int kChunk = 32 * kSeg;
+
+__device__ __forceinline__ double seg_sum(const float2* __restrict__ s, uint64_t start, uint64_t n) {
+  double acc = 0.0;
+  for (int k = 0; k < kSeg; ++k) {
+    uint64_t i = start + k;
+    if (i < n) { float2 a = s[i]; acc += (double)a.x * a.x + (double)a.y * a.y; }
+  }
+  return acc;
+}
+
+// inclusive warp scan in fixed order
+__device__ __forceinline__ double warp_iscan(double v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    double y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+
+// pass 1: one warp per chunk -> csum[c]
+__global__ void k_chunk_sums(const float2* __restrict__ s, uint64_t n, uint64_t nchunks, double* __restrict__ csum) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (uint64_t c = warp; c < nchunks; c += nwarps) {
+    double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
+    v = warp_iscan(v);
+    if (lane == 31) csum[c] = v;
+  }
+}
+
+// pass 2: exclusive scan of the chunk sums, one block, fixed order.
+// cbase[c] = sum_{c' < c} csum[c'];  cbase[nchunks] = total.
+__global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
+  __shared__ double ws[32];
+  __shared__ double carry;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  // each thread owns a contiguous run of `per` chunks
+  const uint64_t per = (nchunks + blockDim.x - 1) / blockDim.x;
+  const uint64_t b = (uint64_t)tid * per, e = min(b + per, nchunks);
+  double local = 0.0;
+  for (uint64_t c = b; c < e; ++c) local += csum[c];
+  // block exclusive scan of `local`
+  double inc = warp_iscan(local);
+  double exc = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) exc = 0.0;
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    double x = lane < nw ? ws[lane] : 0.0;
+    double xi = warp_iscan(x);
+    double xe = __shfl_up_sync(0xffffffffu, xi, 1);
+    if (lane == 0) xe = 0.0;
+    __syncwarp();
+    if (lane < nw) ws[lane] = xe;  // exclusive warp offsets
+    if (lane == nw - 1) carry = xi;
+  }
+  __syncthreads();
+  double run = ws[w] + exc;
+  for (uint64_t c = b; c < e; ++c) { cbase[c] = run; run += csum[c]; }
+  if (tid == 0) cbase[nchunks] = carry;
+}
+
+// pass 3: one warp per shot.  Shot value u -> smallest i with cdf[i] >= u,
+// clamped to n-1 (reference semantics: sample_sm120.cu:61-68).
+__global__ void k_sample(const float2* __restrict__ s, uint64_t n, uint64_t nchunks, const double* __restrict__ cbase,
+                         const double* __restrict__ u, int64_t nshots, int64_t* __restrict__ out) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (uint64_t k = warp; k < (uint64_t)nshots; k += nwarps) {
+    const double x = u[k];
+    // smallest chunk c with cbase[c+1] >= x
+    uint64_t lo = 0, hi = nchunks;  // search in [0, nchunks)
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (cbase[mid + 1] >= x) hi = mid; else lo = mid + 1;
+    }
+    int64_t result;
+    if (lo >= nchunks) {
+      result = (int64_t)(n - 1);
+    } else {
+      const uint64_t c = lo;
+      double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
+      double inc = warp_iscan(v);
+      const double base = cbase[c];
+      const bool hit = base + inc >= x;
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (m == 0) {
+        result = (int64_t)min((c + 1) * (uint64_t)kChunk, n) - 1;
+      } else {
+        const int L = __ffs(m) - 1;
+        // lane L walks its segment
+        int64_t r = 0;
+        if (lane == L) {
+          double run = base + (inc - v);
+          const uint64_t st = c * kChunk + (uint64_t)L * kSeg;
+          uint64_t i = st;
+          r = -1;
+          for (int q = 0; q < kSeg; ++q, ++i) {
+            if (i >= n) break;
+            float2 a = s[i];
+            run += (double)a.x * a.x + (double)a.y * a.y;
+            if (run >= x) { r = (int64_t)i; break; }
+          }
+          if (r < 0) r = (int64_t)min(st + kSeg, n) - 1;
+        }
+        result = __shfl_sync(0xffffffffu, r, L);
+      }
+    }
+    if (lane == 0) out[k] = result;
+  }
+}
+
+// ---------------------------------------------------- Pauli-sum terms ----
+// Term t: coefficient w_t = coef_t * i^{popc(x_t & z_t)} (complex), x_t, z_t.
+// (P psi)[i] = i^{|x&z|} (-1)^{popc((i^x) & z)} psi[i ^ x].
+struct Term { uint64_t x, z; double wr, wi; };
+
+__device__ __forceinline__ void term_apply(const Term& T, uint64_t i, const float2* __restrict__ s, double& re,
+                                           double& im) {
+  const uint64_t j = i ^ T.x;
+  const float2 b = s[j];
+  const double sg = (__popcll(j & T.z) & 1) ? -1.0 : 1.0;
+  re += sg * (T.wr * b.x - T.wi * b.y);
+  im += sg * (T.wr * b.y + T.wi * b.x);
+}
+
+// <psi|H|psi> partials: sum_i Re(conj(psi_i) (H psi)_i)
+__global__ void k_pauli_expect(const float2* __restrict__ s, uint64_t n, const Term* __restrict__ terms, int nterms,
+                               uint64_t per, double* __restrict__ partial) {
+  extern __shared__ Term st[];
+  for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
+  __syncthreads();
+  const uint64_t b0 = (uint64_t)blockIdx.x * per;
+  const uint64_t e = min(b0 + per, n);
+  double acc = 0.0;
+  for (uint64_t i = b0 + threadIdx.x; i < e; i += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < nterms; ++k) term_apply(st[k], i, s, re, im);
+    const float2 a = s[i];
+    acc += (double)a.x * re + (double)a.y * im;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// out = H psi (complex64), accumulated in FP64 per amplitude.
+__global__ void k_pauli_apply(const float2* __restrict__ s, float2* __restrict__ out, uint64_t n,
+                              const Term* __restrict__ terms, int nterms) {
+  extern __shared__ Term st[];
+  for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < nterms; ++k) term_apply(st[k], i, s, re, im);
+    out[i] = make_float2((float)re, (float)im);
+  }
+}
+
+}  // namespace
+
+// Builds the device term table (records of {x, z, w_re, w_im}) in scratch
+// after `offset` bytes.
+void* qs_upload_terms(qs_context* h, size_t offset, int n, const uint64_t* x, const uint64_t* z, const double* c,
+                      int nterms);
+
+void* qs_upload_terms(qs_context* h, size_t offset, int n, const uint64_t* x, const uint64_t* z, const double* c,
+                      int nterms) {
+  QS_CHECK_ARG(nterms >= 1, "need at least one Pauli term");
+  QS_CHECK_ARG(x && z && c, "term pointers are null");
+  const uint64_t lim = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+  std::vector<Term> T(nterms);
+  for (int k = 0; k < nterms; ++k) {
+    QS_CHECK_ARG((x[k] & ~lim) == 0 && (z[k] & ~lim) == 0, "Pauli mask has bits beyond n_qubits");
+    const int ny = __builtin_popcountll(x[k] & z[k]) & 3;
+    // i^ny
+    static const double pr[4] = {1, 0, -1, 0}, pi[4] = {0, 1, 0, -1};
+    T[k] = Term{x[k], z[k], c[k] * pr[ny], c[k] * pi[ny]};
+  }
+  char* base = (char*)h->scratch_get(offset + sizeof(Term) * nterms);
+  Term* d = (Term*)(base + offset);
+  // From pageable memory the copy returns once T has been staged, so the
+  // host vector may go out of scope afterwards.
+  QS_CUDA(cudaMemcpyAsync(d, T.data(), sizeof(Term) * nterms, cudaMemcpyHostToDevice, h->stream));
+  return d;
+}
+
+namespace {
+
+template <class F>
+void reduce_to(qs_context* h, F f, uint64_t items, double* d_out, int mode, double* d_partial) {
+  Slicing sl = slice(items);
+  k_reduce<F><<<sl.nb, kThreads, 0, h->stream>>>(f, items, sl.per, d_partial);
+  qs_after_launch(h, "k_reduce");
+  k_final<<<1, 1024, 0, h->stream>>>(d_partial, sl.nb, d_out, mode);
+  qs_after_launch(h, "k_final");
+}
+
+// scratch layout for reductions: [0, 16) two doubles out; [64, ...) partials
+double* red_out(qs_context* h) { return (double*)h->scratch_get(64 + 8 * kMaxBlocks); }
+double* red_part(qs_context* h) { return (double*)((char*)h->scratch_get(64 + 8 * kMaxBlocks) + 64); }
+
+double fetch_scalar(qs_context* h, const double* d) {
+  double* pin = h->pinned_get(64);
+  QS_CUDA(cudaMemcpyAsync(pin, d, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  return pin[0];
+}
+
+}  // namespace
+
+extern "C" {
+
+int qs_norm2(qs_handle_t h, const void* state, int n, double* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  double* o = red_out(h);
+  reduce_to(h, FNorm{(const float4*)state}, (1ull << n) / 2, o, 0, red_part(h));
+  *out = fetch_scalar(h, o);
+  QS_API_END(h)
+}
+
+int qs_renorm(qs_handle_t h, void* state, int n) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  double* o = red_out(h);
+  const uint64_t nvec = (1ull << n) / 2;
+  reduce_to(h, FNorm{(const float4*)state}, nvec, o, 1, red_part(h));
+  k_scale<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((float4*)state, nvec, o);
+  qs_after_launch(h, "k_scale");
+  QS_API_END(h)
+}
+
+int qs_probs(qs_handle_t h, const void* state, int n, float* probs) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(probs != nullptr && ((uintptr_t)probs & 7u) == 0, "probs must be a non-null 8-byte aligned pointer");
+  const uint64_t nvec = (1ull << n) / 2;
+  k_probs<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((const float4*)state, (float2*)probs, nvec);
+  qs_after_launch(h, "k_probs");
+  QS_API_END(h)
+}
+
+int qs_measure(qs_handle_t h, void* state, int n, int t, double u, int* outcome) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  QS_CHECK_ARG(outcome != nullptr, "outcome is null");
+  double* o = red_out(h);
+  const uint64_t nvec = (1ull << n) / 2;
+  reduce_to(h, FP0{(const float4*)state, t}, nvec, o, 0, red_part(h));
+  int* d_out = (int*)(o + 2);
+  k_collapse<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((float4*)state, nvec, t, u, o, d_out);
+  qs_after_launch(h, "k_collapse");
+  double* pin = h->pinned_get(64);
+  QS_CUDA(cudaMemcpyAsync(pin, d_out, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  *outcome = *(int*)pin;
+  QS_API_END(h)
+}
+
+int qs_expect_z(qs_handle_t h, const void* state, int n, uint64_t zmask, double* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  double* o = red_out(h);
+  reduce_to(h, FZ{(const float4*)state, zmask}, (1ull << n) / 2, o, 0, red_part(h));
+  *out = fetch_scalar(h, o);
+  QS_API_END(h)
+}
+
+int qs_expect_pauli_sum(qs_handle_t h, const void* state, int n, const uint64_t* x, const uint64_t* z,
+                        const double* c, int nterms, double* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  QS_CHECK_ARG(nterms >= 1 && nterms <= 1024, "n_terms must be in [1, 1024]");
+  const size_t toff = 64 + 8 * kMaxBlocks;
+  Term* dT = (Term*)qs_upload_terms(h, toff, n, x, z, c, nterms);
+  double* o = red_out(h);
+  double* part = red_part(h);
+  const uint64_t N = 1ull << n;
+  Slicing sl = slice(N);
+  k_pauli_expect<<<sl.nb, kThreads, sizeof(Term) * nterms, h->stream>>>((const float2*)state, N, dT, nterms, sl.per,
+                                                                        part);
+  qs_after_launch(h, "k_pauli_expect");
+  k_final<<<1, 1024, 0, h->stream>>>(part, sl.nb, o, 0);
+  qs_after_launch(h, "k_final");
+  *out = fetch_scalar(h, o);
+  QS_API_END(h)
+}
+
+int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n, const uint64_t* x, const uint64_t* z,
+                       const double* c, int nterms) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(psi, n);
+  qs_check_state(out, n);
+  QS_CHECK_ARG(psi != out, "out must not alias psi");
+  QS_CHECK_ARG(nterms >= 1 && nterms <= 1024, "n_terms must be in [1, 1024]");
+  Term* dT = (Term*)qs_upload_terms(h, 0, n, x, z, c, nterms);
+  const uint64_t N = 1ull << n;
+  k_pauli_apply<<<qs_blocks_for(h, N, kThreads), kThreads, sizeof(Term) * nterms, h->stream>>>(
+      (const float2*)psi, (float2*)out, N, dT, nterms);
+  qs_after_launch(h, "k_pauli_apply");
+  QS_API_END(h)
+}
+
+int qs_sample(qs_handle_t h, const void* state, int n, const double* u, int64_t nshots, int64_t* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(nshots >= 0, "n_shots must be >= 0");
+  if (nshots == 0) return QS_OK;
+  QS_CHECK_ARG(u != nullptr && out != nullptr, "u/out pointer is null");
+  const uint64_t N = 1ull << n;
+  const uint64_t nchunks = (N + kChunk - 1) / kChunk;
+  double* base = (double*)h->scratch_get(sizeof(double) * (2 * nchunks + 1));
+  double* csum = base;
+  double* cbase = base + nchunks;
+  const int wpb = kThreads / 32;
+  k_chunk_sums<<<qs_blocks_for(h, nchunks * 32, kThreads), kThreads, 0, h->stream>>>((const float2*)state, N,
+                                                                                     nchunks, csum);
+  qs_after_launch(h, "k_chunk_sums");
+  k_chunk_scan<<<1, 1024, 0, h->stream>>>(csum, nchunks, cbase);
+  qs_after_launch(h, "k_chunk_scan");
+  const uint64_t blocks = std::min<uint64_t>(((uint64_t)nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
+  k_sample<<<(unsigned)blocks, kThreads, 0, h->stream>>>((const float2*)state, N, nchunks, cbase, u, nshots, out);
+  qs_after_launch(h, "k_sample");
+  QS_API_END(h)
+}
+
+}  // extern "C"

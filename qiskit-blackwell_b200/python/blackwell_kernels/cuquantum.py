@@ -1,0 +1,346 @@
+"""Torch-tensor kernel API, call-compatible with the reference's
+bwk/python/blackwell_kernels/cuquantum.py (same names, argument meaning,
+in-place mutation and return values), backed by libqsim.so.
+
+Differences, by design:
+* gate matrices may live on either device; they are read on the host and
+  passed to the kernel by value (the reference reads a device tensor);
+* ``sample`` draws FP64 uniforms and searches an FP64 CDF (the reference's
+  FP32 CDF loses resolution beyond ~2^24 amplitudes, sample_sm120.cu:109-123);
+* reductions accumulate in FP64 in a fixed order (no float atomics);
+* 64-bit indexing: states up to 2^34 amplitudes.
+"""
+from __future__ import annotations
+
+import cmath
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from qsim_b200 import engine as E
+from qsim_b200.engine import _h, _ptr, check_state
+
+
+def _gate_host(gate, shape) -> np.ndarray:
+    if isinstance(gate, torch.Tensor):
+        g = gate.detach().to("cpu", torch.complex64).contiguous().numpy()
+    else:
+        g = np.asarray(gate, dtype=np.complex64)
+    if g.shape != shape:
+        raise RuntimeError(f"gate must be {'x'.join(map(str, shape))}")
+    return np.ascontiguousarray(g.view(np.float32).reshape(-1))
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _ints(x) -> np.ndarray:
+    if isinstance(x, torch.Tensor):
+        x = x.detach().cpu().numpy()
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int64).reshape(-1).astype(np.int32))
+
+
+# ------------------------------------------------------------------- gates
+def apply_gate(state: torch.Tensor, gate: torch.Tensor, target_qubit: int) -> torch.Tensor:
+    """Single-qubit gate in place (cuquantum.py:40-51)."""
+    n = check_state(state)
+    g = _gate_host(gate, (2, 2))
+    _h(state.device.index).call("qs_apply_1q", _ptr(state), n, _fp(g), int(target_qubit))
+    return state
+
+
+def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: int) -> torch.Tensor:
+    """Two-qubit gate in place (cuquantum.py:54-66).  As in the reference
+    (apply_gate2q_sm120.cu:244-247) bit 0 of the 4x4 index is min(q0, q1)."""
+    n = check_state(state)
+    if qubit0 == qubit1:
+        raise RuntimeError("qubit0 and qubit1 must differ")
+    g = _gate_host(gate, (4, 4))
+    lo, hi = min(qubit0, qubit1), max(qubit0, qubit1)
+    _h(state.device.index).call("qs_apply_2q", _ptr(state), n, _fp(g), int(lo), int(hi))
+    return state
+
+
+def apply_gates_fused(state: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
+    """K 1Q gates in one fused program (cuquantum.py:69-80)."""
+    n = check_state(state)
+    if isinstance(gates, torch.Tensor):
+        g = gates.detach().to("cpu", torch.complex64).contiguous().numpy()
+    else:
+        g = np.asarray(gates, dtype=np.complex64)
+    if g.ndim != 3 or g.shape[1:] != (2, 2):
+        raise RuntimeError("gates must be [N, 2, 2]")
+    t = _ints(targets)
+    if t.size != g.shape[0]:
+        raise RuntimeError("targets must have N entries")
+    gf = np.ascontiguousarray(g.view(np.float32).reshape(-1))
+    _h(state.device.index).call("qs_apply_gates_fused", _ptr(state), n, _fp(gf), _ip(t), int(t.size))
+    return state
+
+
+def apply_gates_reg_tiled(state: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
+    """Low-qubit fused 1Q gates (cuquantum.py:83-98); any targets are accepted
+    here, since the tile-pass engine is not limited to qubits 0-4."""
+    return apply_gates_fused(state, gates, targets)
+
+
+def apply_diagonal(state: torch.Tensor, diag: torch.Tensor, target_qubit: int) -> torch.Tensor:
+    n = check_state(state)
+    d = _gate_host(diag, (2,))
+    _h(state.device.index).call("qs_apply_diag1", _ptr(state), n, _fp(d), int(target_qubit))
+    return state
+
+
+def apply_diagonal_phase(state: torch.Tensor, phase: complex, target_qubit: int) -> torch.Tensor:
+    """Multiply the bit=1 amplitudes of target_qubit by phase (half traffic)."""
+    n = check_state(state)
+    phase = complex(phase)
+    _h(state.device.index).call("qs_apply_phase", _ptr(state), n, C.c_float(phase.real), C.c_float(phase.imag),
+                                int(target_qubit))
+    return state
+
+
+def apply_diagonal_2q(state: torch.Tensor, diag: torch.Tensor, qubit0: int, qubit1: int) -> torch.Tensor:
+    n = check_state(state)
+    d = _gate_host(diag, (4,))
+    _h(state.device.index).call("qs_apply_diag2", _ptr(state), n, _fp(d), int(qubit0), int(qubit1))
+    return state
+
+
+def state_init(n_qubits: int) -> torch.Tensor:
+    return E.state_init(n_qubits, "cuda")
+
+
+def _is_x(g: np.ndarray) -> bool:
+    return np.array_equal(g.view(np.complex64).reshape(2, 2), np.array([[0, 1], [1, 0]], dtype=np.complex64))
+
+
+def _is_swap(g: np.ndarray) -> bool:
+    return np.array_equal(g.view(np.complex64).reshape(4, 4), np.eye(4, dtype=np.complex64)[[0, 2, 1, 3]])
+
+
+def apply_mcgate(state: torch.Tensor, gate: torch.Tensor, controls, target_qubit: int) -> torch.Tensor:
+    """Multi-controlled 2x2 (cuquantum.py:297-317); an exact X moves values."""
+    n = check_state(state)
+    g = _gate_host(gate, (2, 2))
+    c = _ints(controls)
+    if c.size > 7:
+        raise RuntimeError("controls must have 0-7 elements")
+    h = _h(state.device.index)
+    if _is_x(g):
+        h.call("qs_apply_mcx", _ptr(state), n, _ip(c), int(c.size), int(target_qubit))
+    else:
+        h.call("qs_apply_mc1q", _ptr(state), n, _fp(g), _ip(c), int(c.size), int(target_qubit))
+    return state
+
+
+def apply_mc2qgate(state: torch.Tensor, gate: torch.Tensor, controls, target0: int, target1: int) -> torch.Tensor:
+    """Multi-controlled 4x4 (cuquantum.py:320-337); bit 0 = min(target0, target1)."""
+    n = check_state(state)
+    g = _gate_host(gate, (4, 4))
+    c = _ints(controls)
+    if c.size > 7:
+        raise RuntimeError("controls must have 0-7 elements")
+    h = _h(state.device.index)
+    if _is_swap(g):
+        h.call("qs_apply_mcswap", _ptr(state), n, _ip(c), int(c.size), int(target0), int(target1))
+    else:
+        h.call("qs_apply_mc2q", _ptr(state), n, _fp(g), _ip(c), int(c.size), int(target0), int(target1))
+    return state
+
+
+# ------------------------------------------------------------ reductions
+def measure_qubit(state: torch.Tensor, target_qubit: int, random_val: float) -> int:
+    return E.measure(state, target_qubit, random_val)
+
+
+def measure_probs(state: torch.Tensor) -> torch.Tensor:
+    return E.probs(state)
+
+
+def sample(state: torch.Tensor, n_shots: int) -> torch.Tensor:
+    """n_shots basis indices drawn from |state|^2 (cuquantum.py:283-294)."""
+    return E.sample(state, n_shots)
+
+
+def expectation_z(state: torch.Tensor, z_mask: int) -> float:
+    n = check_state(state)
+    out = C.c_double()
+    _h(state.device.index).call("qs_expect_z", _ptr(state), n, C.c_uint64(int(z_mask)), C.byref(out))
+    return float(out.value)
+
+
+def expectation_pauli(state: torch.Tensor, z_mask: int, xy_qubit: int, op: int) -> float:
+    """<Z-string x (X or Y on xy_qubit)> (cuquantum.py:472-487); op 0 = Z only,
+    1 = X, 2 = Y.  (libqsim also evaluates arbitrary multi-X/Y strings.)"""
+    if op not in (0, 1, 2):
+        raise RuntimeError("op must be 0=I/Z, 1=X, 2=Y")
+    if op == 0:
+        return expectation_z(state, z_mask)
+    from qsim_b200.paulis import PauliSum
+    x = 1 << int(xy_qubit)
+    z = int(z_mask) | (x if op == 2 else 0)
+    n = check_state(state)
+    return E.expect_pauli_sum(state, PauliSum([x], [z], [1.0], n))
+
+
+def renormalize(state: torch.Tensor) -> torch.Tensor:
+    return E.renormalize(state)
+
+
+# ----------------------------------------------------------------- batch
+def apply_gate_batched(states: torch.Tensor, gate: torch.Tensor, target_qubit: int) -> torch.Tensor:
+    if states.dim() != 2 or not states.is_cuda or states.dtype != torch.complex64 or not states.is_contiguous():
+        raise RuntimeError("states must be a contiguous complex64 CUDA tensor [N, 2^n]")
+    N, m = states.shape
+    n = m.bit_length() - 1
+    g = _gate_host(gate, (2, 2))
+    _h(states.device.index).call("qs_apply_1q_batched", _ptr(states), int(N), n, _fp(g), int(target_qubit))
+    return states
+
+
+def apply_gates_batched_fused(states: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
+    if states.dim() != 2 or not states.is_cuda or states.dtype != torch.complex64 or not states.is_contiguous():
+        raise RuntimeError("states must be a contiguous complex64 CUDA tensor [N, 2^n]")
+    N, m = states.shape
+    n = m.bit_length() - 1
+    g = gates.detach().to("cpu", torch.complex64).contiguous().numpy() if isinstance(gates, torch.Tensor) \
+        else np.asarray(gates, dtype=np.complex64)
+    t = _ints(targets)
+    gf = np.ascontiguousarray(g.view(np.float32).reshape(-1))
+    _h(states.device.index).call("qs_apply_gates_batched_fused", _ptr(states), int(N), n, _fp(gf), _ip(t),
+                                 int(t.size))
+    return states
+
+
+def state_init_batched(n_states: int, n_qubits: int) -> torch.Tensor:
+    s = torch.empty(int(n_states), 1 << int(n_qubits), dtype=torch.complex64, device="cuda")
+    _h(s.device.index).call("qs_state_init_batched", _ptr(s), int(n_states), int(n_qubits))
+    return s
+
+
+class CircuitGraph:
+    """CUDA-graph capture of a list of 1Q gates (cuquantum.py:101-130).  libqsim
+    launches on torch's current stream, so the capture records them."""
+
+    def __init__(self, state: torch.Tensor, gates: torch.Tensor, targets):
+        if isinstance(targets, torch.Tensor):
+            targets = targets.tolist()
+        self._gates = [_gate_host(gates[i], (2, 2)) for i in range(len(targets))]
+        self._targets = [int(t) for t in targets]
+        for g, t in zip(gates, targets):
+            apply_gate(state, g, int(t))
+        torch.cuda.synchronize()
+        self._graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self._graph):
+            for g, t in zip(gates, targets):
+                apply_gate(state, g, int(t))
+        self._state = state
+
+    def replay(self):
+        self._graph.replay()
+
+
+# ----------------------------------------------------------- Chebyshev
+def spmv_csr(row_ptr, col_idx, values, x, y, alpha_re=1.0, alpha_im=0.0, beta_re=0.0, beta_im=0.0):
+    """y = alpha*A*x + beta*y (cuquantum.py:518-531)."""
+    for t, name in ((row_ptr, "row_ptr"), (col_idx, "col_idx"), (values, "values"), (x, "x"), (y, "y")):
+        if not t.is_cuda:
+            raise RuntimeError(f"{name} must be a CUDA tensor")
+    if row_ptr.dtype != torch.int32 or col_idx.dtype != torch.int32:
+        raise RuntimeError("row_ptr/col_idx must be int32")
+    if values.dtype != torch.complex64 or x.dtype != torch.complex64 or y.dtype != torch.complex64:
+        raise RuntimeError("values, x and y must be complex64")
+    _h(x.device.index).call("qs_spmv_csr", _ptr(row_ptr), _ptr(col_idx), _ptr(values), int(row_ptr.numel() - 1),
+                            _ptr(x), _ptr(y), float(alpha_re), float(alpha_im), float(beta_re), float(beta_im))
+
+
+def chebyshev_step(spmv_result, t_prev, t_next):
+    _h(t_next.device.index).call("qs_cheb_step", _ptr(spmv_result), _ptr(t_prev), _ptr(t_next),
+                                 int(spmv_result.numel()))
+
+
+def chebyshev_accum(accum, t_k, c_re, c_im):
+    _h(accum.device.index).call("qs_cheb_accum", _ptr(accum), _ptr(t_k), float(c_re), float(c_im),
+                                int(accum.numel()))
+
+
+def chebyshev_step_accum(spmv_result, t_prev, t_next, accum, c_re, c_im):
+    _h(accum.device.index).call("qs_cheb_step_accum", _ptr(spmv_result), _ptr(t_prev), _ptr(t_next), _ptr(accum),
+                                float(c_re), float(c_im), int(accum.numel()))
+
+
+# ------------------------------------------------------ gate constructors
+def hadamard_gate(device="cuda"):
+    return torch.tensor([[1, 1], [1, -1]], dtype=torch.complex64, device=device) / (2 ** 0.5)
+
+
+def pauli_x_gate(device="cuda"):
+    return torch.tensor([[0, 1], [1, 0]], dtype=torch.complex64, device=device)
+
+
+def cnot_gate(device="cuda"):
+    """|00>->|00>, |01>->|01>, |10>->|11>, |11>->|10> (control in index bit 1)."""
+    return torch.tensor([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=torch.complex64,
+                        device=device)
+
+
+def cz_gate(device="cuda"):
+    return torch.tensor([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, -1]], dtype=torch.complex64,
+                        device=device)
+
+
+def swap_gate(device="cuda"):
+    return torch.tensor([[1, 0, 0, 0], [0, 0, 1, 0], [0, 1, 0, 0], [0, 0, 0, 1]], dtype=torch.complex64,
+                        device=device)
+
+
+def cswap_gate(device="cuda"):
+    return swap_gate(device)
+
+
+def _haar(dim, device):
+    z = torch.randn(dim, dim, dtype=torch.complex64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    return (q * (d / d.abs()).unsqueeze(0)).to(device)
+
+
+def random_unitary(device="cuda"):
+    return _haar(2, device)
+
+
+def random_unitary_4x4(device="cuda"):
+    return _haar(4, device)
+
+
+def rz_gate_diag(theta, device="cuda"):
+    return torch.tensor([cmath.exp(-1j * theta / 2), cmath.exp(1j * theta / 2)], dtype=torch.complex64,
+                        device=device)
+
+
+def phase_gate_diag(theta, device="cuda"):
+    return torch.tensor([1.0, cmath.exp(1j * theta)], dtype=torch.complex64, device=device)
+
+
+def t_gate_diag(device="cuda"):
+    return torch.tensor([1.0, cmath.exp(1j * math.pi / 4)], dtype=torch.complex64, device=device)
+
+
+def s_gate_diag(device="cuda"):
+    return torch.tensor([1.0, 1j], dtype=torch.complex64, device=device)
+
+
+def z_gate_diag(device="cuda"):
+    return torch.tensor([1.0, -1.0], dtype=torch.complex64, device=device)
+
+
+def cz_gate_diag(device="cuda"):
+    return torch.tensor([1.0, 1.0, 1.0, -1.0], dtype=torch.complex64, device=device)

@@ -1,0 +1,235 @@
+"""Torch-facing engine over the C ABI.
+
+States are ``torch.complex64`` CUDA tensors; their data pointers go straight
+to libqsim, which runs on torch's current CUDA stream.  torch is used only for
+device memory, streams and RNG here; every kernel that touches a state is in
+libqsim.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import QsBatchInfo, QsOp, QsPlanInfo
+from .circuit import OP_DTYPE
+
+
+def _h(device: int | None = None) -> _lib.Handle:
+    dev = torch.cuda.current_device() if device is None else int(device)
+    return _lib.handle(dev, torch.cuda.current_stream(dev).cuda_stream)
+
+
+def _ptr(t: torch.Tensor) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+def _ops_ptr(ops: np.ndarray):
+    if ops.dtype != OP_DTYPE or not ops.flags["C_CONTIGUOUS"]:
+        ops = np.ascontiguousarray(ops, dtype=OP_DTYPE)
+    return ops, ops.ctypes.data_as(C.POINTER(QsOp))
+
+
+def check_state(state: torch.Tensor) -> int:
+    if not isinstance(state, torch.Tensor) or not state.is_cuda:
+        raise RuntimeError("state must be CUDA")
+    if state.dtype != torch.complex64:
+        raise RuntimeError("state must be complex64")
+    if not state.is_contiguous():
+        raise RuntimeError("state must be contiguous")
+    n = state.numel()
+    if n < 2 or n & (n - 1):
+        raise RuntimeError("state size must be a power of two >= 2")
+    return n.bit_length() - 1
+
+
+def empty_state(n_qubits: int, device="cuda") -> torch.Tensor:
+    return torch.empty(1 << n_qubits, dtype=torch.complex64, device=device)
+
+
+def state_init(n_qubits: int, device="cuda") -> torch.Tensor:
+    s = empty_state(n_qubits, device)
+    _h(s.device.index).call("qs_state_init", _ptr(s), int(n_qubits))
+    return s
+
+
+class Plan:
+    """A planned circuit (host FP64 fusion + tile passes) resident on the GPU."""
+
+    def __init__(self, n_qubits: int, ops: np.ndarray, device: int | None = None):
+        self.n = int(n_qubits)
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self.ops, p = _ops_ptr(ops)
+        self._h = _h(self.device)
+        self.L = self._h.L
+        out = C.c_void_p()
+        self._h.call("qs_plan_create", self.n, p, int(len(self.ops)), C.byref(out))
+        self.ptr = out
+        info = QsPlanInfo()
+        _lib.check(self.L.qs_plan_info_get(self.ptr, C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in QsPlanInfo._fields_}
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None):
+                torch.cuda.synchronize(self.device)
+                self.L.qs_plan_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def execute(self, state: torch.Tensor) -> torch.Tensor:
+        if check_state(state) != self.n:
+            raise RuntimeError("state width does not match the plan")
+        _h(self.device).call("qs_plan_execute", self.ptr, _ptr(state))
+        return state
+
+    def execute_from_zero(self, state: torch.Tensor) -> torch.Tensor:
+        if check_state(state) != self.n:
+            raise RuntimeError("state width does not match the plan")
+        _h(self.device).call("qs_plan_execute_from_zero", self.ptr, _ptr(state))
+        return state
+
+
+class BatchPlan:
+    """Many circuits of uneven width, states packed back to back."""
+
+    def __init__(self, widths, op_offsets, ops, state_offsets, device: int | None = None):
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self.widths = np.ascontiguousarray(widths, dtype=np.int32)
+        self.op_offsets = np.ascontiguousarray(op_offsets, dtype=np.int64)
+        self.state_offsets = np.ascontiguousarray(state_offsets, dtype=np.int64)
+        self.ops, p = _ops_ptr(ops)
+        self.n_amps = int((self.state_offsets + (1 << self.widths.astype(np.int64))).max()) if len(self.widths) else 0
+        h = _h(self.device)
+        self.L = h.L
+        out = C.c_void_p()
+        h.call("qs_batch_plan_create", int(len(self.widths)),
+               self.widths.ctypes.data_as(C.POINTER(C.c_int32)),
+               self.op_offsets.ctypes.data_as(C.POINTER(C.c_int64)), p,
+               self.state_offsets.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(out))
+        self.ptr = out
+        info = QsBatchInfo()
+        _lib.check(self.L.qs_batch_plan_info_get(self.ptr, C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in QsBatchInfo._fields_}
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None):
+                torch.cuda.synchronize(self.device)
+                self.L.qs_batch_plan_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def alloc_states(self) -> torch.Tensor:
+        return torch.empty(max(self.n_amps, 2), dtype=torch.complex64, device=f"cuda:{self.device}")
+
+    def execute(self, states: torch.Tensor) -> torch.Tensor:
+        if states.numel() < self.n_amps or states.dtype != torch.complex64 or not states.is_cuda:
+            raise RuntimeError("states buffer too small or not complex64 CUDA")
+        _h(self.device).call("qs_batch_plan_execute", self.ptr, _ptr(states))
+        return states
+
+
+def run_ops(state: torch.Tensor, ops: np.ndarray) -> torch.Tensor:
+    n = check_state(state)
+    ops, p = _ops_ptr(ops)
+    _h(state.device.index).call("qs_run_circuit", _ptr(state), n, p, int(len(ops)))
+    return state
+
+
+def norm2(state: torch.Tensor) -> float:
+    n = check_state(state)
+    out = C.c_double()
+    _h(state.device.index).call("qs_norm2", _ptr(state), n, C.byref(out))
+    return out.value
+
+
+def renormalize(state: torch.Tensor) -> torch.Tensor:
+    n = check_state(state)
+    _h(state.device.index).call("qs_renorm", _ptr(state), n)
+    return state
+
+
+def probs(state: torch.Tensor) -> torch.Tensor:
+    n = check_state(state)
+    out = torch.empty(1 << n, dtype=torch.float32, device=state.device)
+    _h(state.device.index).call("qs_probs", _ptr(state), n, _ptr(out))
+    return out
+
+
+def measure(state: torch.Tensor, target: int, u: float) -> int:
+    n = check_state(state)
+    out = C.c_int()
+    _h(state.device.index).call("qs_measure", _ptr(state), n, int(target), float(u), C.byref(out))
+    return int(out.value)
+
+
+def sample_u(state: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
+    """Shots for given uniforms u (float64 CUDA): smallest i with cdf[i] >= u."""
+    n = check_state(state)
+    if u.dtype != torch.float64 or not u.is_cuda or not u.is_contiguous():
+        raise RuntimeError("u must be a contiguous float64 CUDA tensor")
+    out = torch.empty(u.numel(), dtype=torch.int64, device=state.device)
+    _h(state.device.index).call("qs_sample", _ptr(state), n, _ptr(u), int(u.numel()), _ptr(out))
+    return out
+
+
+def sample(state: torch.Tensor, shots: int, generator: torch.Generator | None = None) -> torch.Tensor:
+    u = torch.rand(int(shots), dtype=torch.float64, device=state.device, generator=generator)
+    return sample_u(state, u)
+
+
+def _masks(ps):
+    x = np.ascontiguousarray(ps.x, dtype=np.uint64)
+    z = np.ascontiguousarray(ps.z, dtype=np.uint64)
+    c = np.ascontiguousarray(ps.real_coefs(), dtype=np.float64)
+    return x, z, c
+
+
+def expect_pauli_sum(state: torch.Tensor, ps) -> float:
+    n = check_state(state)
+    x, z, c = _masks(ps)
+    out = C.c_double()
+    _h(state.device.index).call("qs_expect_pauli_sum", _ptr(state), n,
+                                x.ctypes.data_as(C.POINTER(C.c_uint64)), z.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                c.ctypes.data_as(C.POINTER(C.c_double)), int(len(c)), C.byref(out))
+    return out.value
+
+
+def apply_pauli_sum(state: torch.Tensor, ps) -> torch.Tensor:
+    n = check_state(state)
+    x, z, c = _masks(ps)
+    out = torch.empty_like(state)
+    _h(state.device.index).call("qs_apply_pauli_sum", _ptr(state), _ptr(out), n,
+                                x.ctypes.data_as(C.POINTER(C.c_uint64)), z.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                c.ctypes.data_as(C.POINTER(C.c_double)), int(len(c)))
+    return out
+
+
+def adjoint_gradient(n: int, ops: np.ndarray, n_params: int, params: np.ndarray, ps, device: int | None = None):
+    """Energies [B] and gradients [B, n_params] (FP64) for parameter vectors
+    params [B, n_params]."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, n_params) if n_params else \
+        np.zeros((int(params.shape[0]) if params.ndim else 1, 0))
+    B = params.shape[0]
+    ops, p = _ops_ptr(ops)
+    x, z, c = _masks(ps)
+    work = torch.empty(B * 3 * (1 << n), dtype=torch.complex64, device=f"cuda:{dev}")
+    e = np.zeros(B, dtype=np.float64)
+    g = np.zeros((B, max(n_params, 1)), dtype=np.float64)
+    _h(dev).call("qs_adjoint_gradient", int(n), p, int(len(ops)), int(n_params),
+                 params.ctypes.data_as(C.POINTER(C.c_double)), int(B),
+                 x.ctypes.data_as(C.POINTER(C.c_uint64)), z.ctypes.data_as(C.POINTER(C.c_uint64)),
+                 c.ctypes.data_as(C.POINTER(C.c_double)), int(len(c)), _ptr(work),
+                 e.ctypes.data_as(C.POINTER(C.c_double)), g.ctypes.data_as(C.POINTER(C.c_double)))
+    return e, g[:, :n_params]
+
+
+def launch_count(device: int | None = None) -> int:
+    return _h(device).launches()

@@ -1,0 +1,155 @@
+"""GPU parity of the batch engine, the Chebyshev evolution and the adjoint
+gradient."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import sv_oracle as O
+from qsim_b200 import engine as E
+from qsim_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_batch_uneven_widths_vs_oracle_and_alone():
+    widths, oo, ops, so = W.qv_batch(40, 4, 17, seed=11)
+    bp = E.BatchPlan(widths, oo, ops, so)
+    st = bp.alloc_states()
+    bp.execute(st)
+    torch.cuda.synchronize()
+    allv = st.cpu().numpy()
+    for c in range(len(widths)):
+        n = int(widths[c])
+        got = allv[so[c]: so[c] + (1 << n)]
+        cops = ops[oo[c]: oo[c + 1]]
+        ref = O.simulate(n, cops)
+        assert abs(1 - O.fidelity(got, ref)) <= 1e-6, (c, n)
+        # alone == in the batch, bit for bit
+        alone = E.empty_state(n)
+        E.Plan(n, cops).execute_from_zero(alone)
+        assert np.array_equal(alone.cpu().numpy(), got), (c, n)
+
+
+def test_qv8_and_qv4_match_reference_golden():
+    import blackwell_kernels as bk
+    d = np.load(os.path.join(GOLD, "qv8_ref.npz"))
+    probs = bk.qv8_simulate(torch.from_numpy(d["gate_matrices"]), torch.from_numpy(d["gate_qubits"]),
+                            d["gate_matrices"].shape[0]).cpu().numpy()
+    np.testing.assert_allclose(probs, d["probs"], atol=3e-6)
+    d = np.load(os.path.join(GOLD, "qv4_ref.npz"))
+    probs = bk.qv4_simulate_cuda(d["gate_data"], d["pair_ids"]).cpu().numpy()
+    np.testing.assert_allclose(probs, d["probs"], atol=3e-6)
+    np.testing.assert_allclose(bk.heavy_output_probability(probs), d["hop"], atol=1e-5)
+
+
+def _hams(n):
+    from qsim_b200.paulis import PauliSum
+    z = PauliSum.from_list([("I" * (n - 1) + "Z", 1.0)])
+    heis, tfim = [], []
+    for i in range(n - 1):
+        for p in "XYZ":
+            lab = ["I"] * n
+            lab[i] = lab[i + 1] = p
+            heis.append(("".join(lab), 0.5))
+        lab = ["I"] * n
+        lab[i] = lab[i + 1] = "Z"
+        tfim.append(("".join(lab), 1.0))
+    for i in range(n):
+        lab = ["I"] * n
+        lab[i] = "X"
+        tfim.append(("".join(lab), 1.0))
+    return [z, PauliSum.from_list(heis), PauliSum.from_list(tfim)]
+
+
+@pytest.mark.parametrize("n", [4, 8, 12])
+@pytest.mark.parametrize("t", [0.5, 1.0])
+def test_chebyshev_vs_expm(n, t):
+    """ab_test.py:424-466: Z, Heisenberg, TFIM vs dense scipy expm (FP64)."""
+    from blackwell_backend import BlackwellSimulator
+    sim = BlackwellSimulator()
+    for H in _hams(n):
+        sv, info = sim.run_hamiltonian(H, t, precision=1e-12)
+        ref = O.expm_evolve(H.to_dense(), O.zero_state(n), t)
+        assert abs(1 - O.fidelity(sv, ref)) <= 1e-6, info
+        assert O.max_abs_err(sv, ref) < 5e-5
+
+
+@pytest.mark.parametrize("n", [10, 14])
+def test_chebyshev_serving_hamiltonian(n):
+    import scipy.sparse as sp
+    from blackwell_backend import BlackwellSimulator
+    H = W.serving_hamiltonian(n, seed=n)
+    psi = W.product_state(n, seed=n + 1)
+    t = 3.0
+    sv, info = BlackwellSimulator().run_hamiltonian(H, t, initial_state=psi.astype(np.complex64), precision=1e-6)
+    ref = O.expm_multiply_evolve(sp.csr_matrix(H.to_dense()) if n <= 10 else _sparse(H), psi, t)
+    assert abs(1 - O.fidelity(sv, ref)) <= 1e-6, info
+
+
+def _sparse(H):
+    import scipy.sparse as sp
+    from qsim_b200.paulis import csr_from_paulis
+    rp, ci, v = csr_from_paulis(H)
+    return sp.csr_matrix((v.astype(np.complex128), ci, rp), shape=(1 << H.num_qubits,) * 2)
+
+
+def test_spmv_and_step_mirrors():
+    import blackwell_kernels as bk
+    from qsim_b200.paulis import csr_from_paulis
+    H = W.serving_hamiltonian(9, seed=1)
+    rp, ci, v = csr_from_paulis(H)
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal(512) + 1j * rng.standard_normal(512)).astype(np.complex64)
+    y0 = (rng.standard_normal(512) + 1j * rng.standard_normal(512)).astype(np.complex64)
+    X, Y = torch.from_numpy(x).cuda(), torch.from_numpy(y0).cuda()
+    bk.spmv_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).cuda(), X, Y,
+                0.7, -0.2, 0.3, 0.1)
+    A = _sparse(H)
+    want = (0.7 - 0.2j) * (A @ x.astype(np.complex128)) + (0.3 + 0.1j) * y0
+    np.testing.assert_allclose(Y.cpu().numpy(), want, atol=1e-5)
+    acc = torch.zeros_like(X)
+    nxt = torch.empty_like(X)
+    bk.chebyshev_step_accum(X, Y, nxt, acc, 0.25, -0.5)
+    t = 2 * x - Y.cpu().numpy()
+    np.testing.assert_allclose(nxt.cpu().numpy(), t, atol=1e-6)
+    np.testing.assert_allclose(acc.cpu().numpy(), (0.25 - 0.5j) * t, atol=1e-6)
+
+
+def test_adjoint_gradient_vs_fd_and_shift():
+    n = 8
+    qc, npar = W.efficient_su2(n, reps=2)
+    from qsim_b200.circuit import lower
+    ops = lower(qc)
+    ps = W.random_pauli_observable(n, 24, seed=5)
+    rng = np.random.default_rng(3)
+    P = rng.uniform(0, 2 * np.pi, (3, npar))
+    e, g = E.adjoint_gradient(n, ops, npar, P, ps)
+    x, z, c = ps.x, ps.z, ps.real_coefs()
+    for b in range(3):
+        assert abs(e[b] - O.energy(n, ops, P[b], x, z, c)) < 1e-5
+        which = list(range(0, npar, 5))
+        shift = O.grad_param_shift(n, ops, P[b], x, z, c, which)
+        np.testing.assert_allclose(g[b, which], shift, atol=1e-5)
+        fd = O.grad_central_fd(n, ops, P[b], x, z, c, which[:6], h=1e-3)
+        # central FD bias for one-parameter entry: f'(sin h/h - 1) ~ -1.7e-7 f'
+        np.testing.assert_allclose(g[b, which[:6]], fd, atol=1e-5)
+
+
+def test_autograd_function():
+    from qsim_b200.autograd import ExpectationFunction
+    n = 6
+    qc, npar = W.efficient_su2(n, reps=1)
+    from qsim_b200.circuit import lower
+    ops = lower(qc)
+    ps = W.random_pauli_observable(n, 10, seed=8)
+    theta = torch.tensor(np.random.default_rng(1).uniform(0, 6.28, (2, npar)), dtype=torch.float64,
+                         requires_grad=True)
+    E_ = ExpectationFunction.apply(theta, n, ops, ps)
+    E_.sum().backward()
+    x, z, c = ps.x, ps.z, ps.real_coefs()
+    for b in range(2):
+        shift = O.grad_param_shift(n, ops, theta[b].detach().numpy(), x, z, c, range(npar))
+        np.testing.assert_allclose(theta.grad[b].numpy(), shift, atol=1e-5)
