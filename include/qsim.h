@@ -85,7 +85,8 @@ typedef struct qs_plan_info {
 int  qs_create(int device, qs_handle_t* out);
 int  qs_destroy(qs_handle_t h);
 /* Run subsequent work on a caller-owned cudaStream_t (e.g. torch's current
- * stream).  NULL selects the handle's own stream.                           */
+ * stream), used verbatim: NULL is the legacy default stream.  A new handle
+ * starts on its own non-blocking stream (see qs_get_stream).                */
 int  qs_set_stream(qs_handle_t h, void* cuda_stream);
 void* qs_get_stream(qs_handle_t h);
 int  qs_sync(qs_handle_t h);
@@ -156,6 +157,9 @@ int qs_plan_execute(qs_handle_t h, qs_plan_t plan, void* state);
  * the state is written but never read. */
 int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state);
 int qs_plan_destroy(qs_plan_t plan);
+/* Host-only dry run of the planner (no device needed): fills `info` for the
+ * plan qs_plan_create would build with the given tile bits (0 = default). */
+int qs_plan_analyze(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_info* info);
 /* plan + execute in one call (the plan is freed afterwards).               */
 int qs_run_circuit(qs_handle_t h, void* state, int n_qubits, const qs_op* ops, int n_ops);
 

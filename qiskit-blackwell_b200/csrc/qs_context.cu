@@ -78,7 +78,7 @@ int qs_destroy(qs_handle_t h) {
   if (!h) return QS_OK;
   cudaSetDevice(h->device);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-  if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+  if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
   if (h->scratch) cudaFree(h->scratch);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -89,7 +89,8 @@ int qs_destroy(qs_handle_t h) {
 int qs_set_stream(qs_handle_t h, void* s) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
-  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  // Used verbatim: NULL is the legacy default stream (torch's default).
+  h->stream = (cudaStream_t)s;
   QS_API_END(h)
 }
 

@@ -45,6 +45,17 @@ template <int R, int A>
 __device__ __forceinline__ void op_u1(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
   if constexpr (A < R) {
     const float2 g00 = c[0], g01 = c[1], g10 = c[2], g11 = c[3];
+    if (rc == 0 && gp) {  // uncontrolled: no selects
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        if (j & (1 << A)) continue;
+        const int k = j | (1 << A);
+        const float2 a0 = v[j], a1 = v[k];
+        v[j] = cfma2(g00, a0, g01, a1);
+        v[k] = cfma2(g10, a0, g11, a1);
+      }
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & (1 << A)) continue;
@@ -65,6 +76,19 @@ __device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restr
     float2 g[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) g[i] = c[i];
+    if (rc == 0 && gp) {  // uncontrolled: no selects
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        if (j & ((1 << A) | (1 << B))) continue;
+        const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
+        const float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
+        v[j] = cfma4(g + 0, a0, a1, a2, a3);
+        v[j1] = cfma4(g + 4, a0, a1, a2, a3);
+        v[j2] = cfma4(g + 8, a0, a1, a2, a3);
+        v[j3] = cfma4(g + 12, a0, a1, a2, a3);
+      }
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & ((1 << A) | (1 << B))) continue;
@@ -217,8 +241,13 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 }
 
 // ---------------------------------------------------------- the kernel ----
+// R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs with
+// up to 168 registers, 3 CTAs per SM.  Narrower blocks use 256 threads.
+constexpr int kMaxThreads(int R) { return R == 5 ? 128 : 256; }
+constexpr int kMinBlocks(int R) { return R == 5 ? 3 : 2; }
+
 template <int R>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kMaxThreads(R), kMinBlocks(R))
 k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restrict__ items, int nitems,
        uint64_t total_tiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -243,7 +272,8 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
       }
       it = lo;
     }
-    const PassItem I = (nitems > 1) ? items[it] : single;
+    // A device table (even of one item) takes precedence over `single`.
+    const PassItem I = items ? items[it] : single;
     if (it != cur) {
       __syncthreads();  // previous tables no longer in use
       cur = it;
@@ -349,7 +379,14 @@ LaunchCfg configure(int smem, int threads) {
   auto key = std::make_pair(smem, threads);
   auto f = cache.find(key);
   if (f != cache.end()) return f->second;
-  QS_CUDA(cudaFuncSetAttribute(k_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  // The attribute is a per-function maximum: set it once to the largest tile
+  // (2^14 amplitudes) so that launches of any tile size stay valid.
+  static bool attr_set = false;
+  if (!attr_set) {
+    QS_CUDA(cudaFuncSetAttribute(k_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(float2) << 14)));
+    attr_set = true;
+  }
   int per_sm = 0;
   QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R>, threads, smem));
   if (per_sm < 1) throw qs_error(QS_ERR_CUDA, "tile-pass kernel does not fit on an SM");
@@ -370,8 +407,9 @@ void launch_R(qs_context* h, float2* base, const PassItem& single, const PassIte
 }
 
 int threads_for(int maxT, int R) {
+  const int cap = R == 5 ? 128 : 256;
   int groups = 1 << (maxT - R);
-  int t = groups < 256 ? groups : 256;
+  int t = groups < cap ? groups : cap;
   if (t < 32) t = 32;
   return t;
 }

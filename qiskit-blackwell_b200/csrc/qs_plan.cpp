@@ -506,6 +506,18 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   }
 }
 
+int qs_plan_analyze(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_info* info) {
+  qs_context* h = nullptr;
+  QS_API_BEGIN
+  QS_CHECK_ARG(info != nullptr, "info is null");
+  if (tile_bits == 0) tile_bits = 13;
+  QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
+  qs_plan_s p;
+  qs_build_plan(n, ops, nops, tile_bits, &p);
+  *info = p.info;
+  QS_API_END(h)
+}
+
 int qs_plan_info_get(qs_plan_t plan, qs_plan_info* info) {
   if (!plan || !info) { qs_set_tls_error("null plan or info"); return QS_ERR_INVALID; }
   *info = plan->info;

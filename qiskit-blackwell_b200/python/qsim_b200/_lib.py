@@ -96,6 +96,7 @@ SIGNATURES = {
     "qs_plan_execute": (_i, [_vp, _vp, _vp]),
     "qs_plan_execute_from_zero": (_i, [_vp, _vp, _vp]),
     "qs_plan_destroy": (_i, [_vp]),
+    "qs_plan_analyze": (_i, [_i, _pop, _i, _i, C.POINTER(QsPlanInfo)]),
     "qs_run_circuit": (_i, [_vp, _vp, _i, _pop, _i]),
     "qs_norm2": (_i, [_vp, _vp, _i, _pd]),
     "qs_renorm": (_i, [_vp, _vp, _i]),
