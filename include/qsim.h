@@ -172,6 +172,9 @@ int qs_norm2(qs_handle_t h, const void* state, int n_qubits, double* out_host);
 int qs_renorm(qs_handle_t h, void* state, int n_qubits);
 /* Reference: bwk/csrc/measure_sm120.cu:115-130,186-207 (measure_probs)     */
 int qs_probs(qs_handle_t h, const void* state, int n_qubits, float* probs_dev);
+/* |a_i|^2 of n_amps (even) consecutive amplitudes, e.g. equal-width states
+ * packed back to back (reference: qv8_sim_sm120.cu returns [C, 256] probs). */
+int qs_probs_n(qs_handle_t h, const void* states, int64_t n_amps, float* probs_dev);
 /* Reference: bwk/csrc/measure_sm120.cu:32-107,150-184 (measure_qubit).
  * Outcome 0 iff u < P(bit=0); the state collapses in place.                */
 int qs_measure(qs_handle_t h, void* state, int n_qubits, int target, double u, int* outcome_host);

@@ -398,6 +398,20 @@ int qs_probs(qs_handle_t h, const void* state, int n, float* probs) {
   QS_API_END(h)
 }
 
+int qs_probs_n(qs_handle_t h, const void* states, int64_t n_amps, float* probs) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(states && ((uintptr_t)states & 15u) == 0, "states must be a 16-byte aligned device pointer");
+  QS_CHECK_ARG(probs != nullptr && ((uintptr_t)probs & 7u) == 0, "probs must be a non-null 8-byte aligned pointer");
+  QS_CHECK_ARG(n_amps >= 0 && (n_amps & 1) == 0, "n_amps must be even and >= 0");
+  const uint64_t nvec = (uint64_t)n_amps / 2;
+  if (nvec) {
+    k_probs<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((const float4*)states, (float2*)probs, nvec);
+    qs_after_launch(h, "k_probs");
+  }
+  QS_API_END(h)
+}
+
 int qs_measure(qs_handle_t h, void* state, int n, int t, double u, int* outcome) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN

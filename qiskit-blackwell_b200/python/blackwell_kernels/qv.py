@@ -53,7 +53,7 @@ def _run_fixed(n: int, mats: np.ndarray, qubits: np.ndarray) -> torch.Tensor:
     bp = E.BatchPlan(widths, op_off, ops, st_off)
     states = bp.alloc_states()
     bp.execute(states)
-    return E.probs(states).reshape(C, 1 << n)
+    return E.probs_n(states, C << n).reshape(C, 1 << n)
 
 
 def qv8_simulate(gate_matrices, gate_qubits, num_circuits):

@@ -101,6 +101,7 @@ SIGNATURES = {
     "qs_norm2": (_i, [_vp, _vp, _i, _pd]),
     "qs_renorm": (_i, [_vp, _vp, _i]),
     "qs_probs": (_i, [_vp, _vp, _i, _vp]),
+    "qs_probs_n": (_i, [_vp, _vp, _i64, _vp]),
     "qs_measure": (_i, [_vp, _vp, _i, _i, _d, _pi]),
     "qs_sample": (_i, [_vp, _vp, _i, _vp, _i64, _vp]),
     "qs_expect_z": (_i, [_vp, _vp, _i, _u64, _pd]),

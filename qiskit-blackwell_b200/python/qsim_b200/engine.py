@@ -162,6 +162,15 @@ def probs(state: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def probs_n(states: torch.Tensor, n_amps: int) -> torch.Tensor:
+    """|a|^2 of the first n_amps amplitudes of a packed buffer."""
+    if states.dtype != torch.complex64 or not states.is_cuda or states.numel() < n_amps or n_amps % 2:
+        raise RuntimeError("states must be complex64 CUDA with at least n_amps (even) amplitudes")
+    out = torch.empty(int(n_amps), dtype=torch.float32, device=states.device)
+    _h(states.device.index).call("qs_probs_n", _ptr(states), int(n_amps), _ptr(out))
+    return out
+
+
 def measure(state: torch.Tensor, target: int, u: float) -> int:
     n = check_state(state)
     out = C.c_int()
