@@ -32,8 +32,8 @@ namespace {
 
 void free_bplan(qs_batch_plan_s* b) {
   if (!b) return;
-  if (b->d_blob) cudaFree(b->d_blob);
-  if (b->d_items) cudaFree(b->d_items);
+  qs_plan_free_device(b->d_blob);
+  qs_plan_free_device(b->d_items);
   delete b;
 }
 
@@ -90,8 +90,8 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     for (int c = 0; c < nc; ++c)
       if (!plans[c].blob.empty()) std::memcpy(blob.data() + boff[c], plans[c].blob.data(), plans[c].blob.size());
     if (total) {
-      QS_CUDA(cudaMalloc(&B->d_blob, total));
-      QS_CUDA(cudaMemcpy(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice));
+      QS_CUDA(cudaMallocAsync(&B->d_blob, total, h->stream));
+      QS_CUDA(cudaMemcpyAsync(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice, h->stream));
     }
     // group (circuit, pass) items by level, then by (T, R)
     int maxp = 0;
@@ -132,9 +132,12 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
       QS_CHECK_ARG(false, "every circuit of a batch needs at least one op");
     }
     if (!items.empty()) {
-      QS_CUDA(cudaMalloc(&B->d_items, items.size() * sizeof(PassItem)));
-      QS_CUDA(cudaMemcpy(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice));
+      QS_CUDA(cudaMallocAsync(&B->d_items, items.size() * sizeof(PassItem), h->stream));
+      QS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice,
+                              h->stream));
     }
+    // blob/items are host temporaries: wait for the copies before they go
+    QS_CUDA(cudaStreamSynchronize(h->stream));
     B->info.n_circuits = nc;
     B->info.n_launches = (int32_t)B->launches.size();
     B->info.n_items = (int64_t)items.size();
@@ -239,10 +242,10 @@ int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int 
     qs_plan_run(h, &p, states, false, (uint64_t)n_states);
     QS_CUDA(cudaStreamSynchronize(h->stream));
   } catch (...) {
-    if (p.d_blob) cudaFree(p.d_blob);
+    qs_plan_free_device(p.d_blob);
     throw;
   }
-  if (p.d_blob) cudaFree(p.d_blob);
+  qs_plan_free_device(p.d_blob);
   QS_API_END(h)
 }
 

@@ -167,6 +167,63 @@ __global__ void k_step_accum(const float4* __restrict__ s, const float4* __restr
   }
 }
 
+// ---- matrix-free Pauli-sum operator -------------------------------------
+// (H x)_i = sum_t w_t (-1)^{popc((i^x_t) & z_t)} x[i ^ x_t],  w_t = c_t i^{|x_t&z_t|}.
+// Terms live in shared memory; XOR with a constant maps aligned blocks onto
+// aligned blocks, so the gathers of a warp stay coalesced.
+struct __align__(16) PTerm { uint64_t x, z; float wr, wi, pad0, pad1; };
+
+__device__ __forceinline__ float2 hx_row(const PTerm* __restrict__ st, int nterms, const float2* __restrict__ x,
+                                         uint64_t i) {
+  float re = 0.f, im = 0.f;
+  for (int k = 0; k < nterms; ++k) {
+    const PTerm T = st[k];
+    const uint64_t j = i ^ T.x;
+    const float2 v = x[j];
+    const float sg = (__popcll(j & T.z) & 1) ? -1.f : 1.f;
+    const float wr = sg * T.wr, wi = sg * T.wi;
+    re = fmaf(wr, v.x, fmaf(-wi, v.y, re));
+    im = fmaf(wr, v.y, fmaf(wi, v.x, im));
+  }
+  return make_float2(re, im);
+}
+
+__global__ void k_chebp_first(const PTerm* __restrict__ terms, int nterms, uint64_t n, const float2* __restrict__ x0,
+                              float2* __restrict__ x1, float2* __restrict__ out, float scale, float2 c0, float2 c1) {
+  extern __shared__ PTerm st[];
+  for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const float2 d = hx_row(st, nterms, x0, i);
+    const float2 t = make_float2(scale * d.x, scale * d.y);
+    x1[i] = t;
+    const float2 a0 = x0[i];
+    float2 a;
+    a.x = c0.x * a0.x - c0.y * a0.y;
+    a.y = c0.x * a0.y + c0.y * a0.x;
+    a.x = fmaf(c1.x, t.x, fmaf(-c1.y, t.y, a.x));
+    a.y = fmaf(c1.x, t.y, fmaf(c1.y, t.x, a.y));
+    out[i] = a;
+  }
+}
+
+__global__ void k_chebp_fused(const PTerm* __restrict__ terms, int nterms, uint64_t n, const float2* __restrict__ xk,
+                              float2* __restrict__ xprev, float2* __restrict__ out, float two_scale, float2 c) {
+  extern __shared__ PTerm st[];
+  for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const float2 d = hx_row(st, nterms, xk, i);
+    const float2 p = xprev[i];
+    const float2 t = make_float2(fmaf(two_scale, d.x, -p.x), fmaf(two_scale, d.y, -p.y));
+    xprev[i] = t;
+    float2 a = out[i];
+    a.x = fmaf(c.x, t.x, fmaf(-c.y, t.y, a.x));
+    a.y = fmaf(c.x, t.y, fmaf(c.y, t.x, a.y));
+    out[i] = a;
+  }
+}
+
 int pick_V(int64_t nrows, const int32_t* rp_dev, qs_context* h) {
   // mean row length from the first and last row pointers
   int32_t ends[2] = {0, 0};
@@ -277,6 +334,44 @@ int qs_cheb_evolve(qs_handle_t h, const int32_t* rp, const int32_t* ci, const vo
     // x0 holds x_{k-2}, x1 holds x_{k-1}; x0 becomes x_k
     DISPATCH_V(V, k_cheb_fused, grid, rp, ci, (const float2*)val, N, x1, x0, (float2*)out, two_scale, C(k));
     qs_after_launch(h, "k_cheb_fused");
+    std::swap(x0, x1);
+  }
+  QS_API_END(h)
+}
+
+int qs_cheb_evolve_pauli(qs_handle_t h, int n, const void* psi, void* out, const uint64_t* xm, const uint64_t* zm,
+                         const double* coefs, int nterms, const double* coeffs, int K, double scale, void* work) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(psi, n);
+  qs_check_state(out, n);
+  qs_check_state(work, n);
+  QS_CHECK_ARG(xm && zm && coefs && coeffs, "null term or coefficient pointer");
+  QS_CHECK_ARG(nterms >= 1 && nterms <= 1024, "n_terms must be in [1, 1024]");
+  QS_CHECK_ARG(K >= 1, "K must be >= 1");
+  const uint64_t lim = (1ull << n) - 1ull;
+  std::vector<PTerm> T(nterms);
+  static const float pr[4] = {1.f, 0.f, -1.f, 0.f}, pim[4] = {0.f, 1.f, 0.f, -1.f};
+  for (int k = 0; k < nterms; ++k) {
+    QS_CHECK_ARG((xm[k] & ~lim) == 0 && (zm[k] & ~lim) == 0, "Pauli mask has bits beyond n_qubits");
+    const int ny = __builtin_popcountll(xm[k] & zm[k]) & 3;
+    T[k] = PTerm{xm[k], zm[k], (float)(coefs[k] * pr[ny]), (float)(coefs[k] * pim[ny]), 0.f, 0.f};
+  }
+  PTerm* dT = (PTerm*)h->scratch_get(sizeof(PTerm) * nterms);
+  QS_CUDA(cudaMemcpyAsync(dT, T.data(), sizeof(PTerm) * nterms, cudaMemcpyHostToDevice, h->stream));
+  const uint64_t N = 1ull << n;
+  float2* x0 = (float2*)work;
+  float2* x1 = x0 + N;
+  QS_CUDA(cudaMemcpyAsync(x0, psi, sizeof(float2) * N, cudaMemcpyDeviceToDevice, h->stream));
+  const unsigned grid = (unsigned)qs_blocks_for(h, N, kThreads, 8);
+  const size_t smem = sizeof(PTerm) * nterms;
+  auto C = [&](int k) { return make_float2((float)coeffs[2 * k], (float)coeffs[2 * k + 1]); };
+  k_chebp_first<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x0, x1, (float2*)out, (float)scale, C(0), C(1));
+  qs_after_launch(h, "k_chebp_first");
+  const float two_scale = (float)(2.0 * scale);
+  for (int k = 2; k <= K; ++k) {
+    k_chebp_fused<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x1, x0, (float2*)out, two_scale, C(k));
+    qs_after_launch(h, "k_chebp_fused");
     std::swap(x0, x1);
   }
   QS_API_END(h)

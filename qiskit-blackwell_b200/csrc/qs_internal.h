@@ -122,6 +122,7 @@ struct qs_plan_s {
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
 void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan);
 void qs_plan_upload(qs_context* h, qs_plan_s* p);
+void qs_plan_free_device(void* d);  // stream-ordered free (no device sync)
 // Runs every pass on n_states equal-width states stored back to back.
 void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states);
 

@@ -458,11 +458,20 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   I.flops = flops * std::ldexp(1.0, n);
 }
 
+// Stream-ordered allocation: creating or destroying a plan never
+// synchronises the device (a plain cudaFree would wait for every stream).
 void qs_plan_upload(qs_context* h, qs_plan_s* p) {
   p->device = h->device;
   if (p->blob.empty()) return;
-  QS_CUDA(cudaMalloc(&p->d_blob, p->blob.size()));
-  QS_CUDA(cudaMemcpy(p->d_blob, p->blob.data(), p->blob.size(), cudaMemcpyHostToDevice));
+  QS_CUDA(cudaMallocAsync(&p->d_blob, p->blob.size(), h->stream));
+  QS_CUDA(cudaMemcpyAsync(p->d_blob, p->blob.data(), p->blob.size(), cudaMemcpyHostToDevice, h->stream));
+  // The plan may be executed on another stream: make the program resident
+  // before returning (this waits on the handle's stream only).
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+void qs_plan_free_device(void* d) {
+  if (d) cudaFreeAsync(d, 0);
 }
 
 void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states) {
@@ -496,12 +505,12 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   }
   catch (const qs_error& e) {
     h->err = e.what();
-    if (p) { if (p->d_blob) cudaFree(p->d_blob); delete p; }
+    if (p) { qs_plan_free_device(p->d_blob); delete p; }
     return e.code;
   }
   catch (const std::exception& e) {
     h->err = e.what();
-    if (p) { if (p->d_blob) cudaFree(p->d_blob); delete p; }
+    if (p) { qs_plan_free_device(p->d_blob); delete p; }
     return QS_ERR_INVALID;
   }
 }
@@ -546,7 +555,7 @@ int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state) {
 
 int qs_plan_destroy(qs_plan_t plan) {
   if (!plan) return QS_OK;
-  if (plan->d_blob) cudaFree(plan->d_blob);
+  qs_plan_free_device(plan->d_blob);
   delete plan;
   return QS_OK;
 }

@@ -6,6 +6,6 @@ re-exported for run_hamiltonian users.
 """
 from .simulator import BlackwellSimulator, Result, counts_from_samples  # noqa: F401
 from .hamiltonian import HamiltonianCSR  # noqa: F401
-from .chebyshev import chebyshev_coefficients, chebyshev_evolve  # noqa: F401
+from .chebyshev import chebyshev_coefficients, chebyshev_evolve, chebyshev_evolve_pauli  # noqa: F401
 
 __all__ = ["BlackwellSimulator", "HamiltonianCSR", "chebyshev_coefficients", "chebyshev_evolve", "Result"]

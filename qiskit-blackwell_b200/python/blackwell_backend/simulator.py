@@ -212,23 +212,37 @@ class BlackwellSimulator:
                         "mean_s": float(np.mean(times))}
 
     # --------------------------------------------------------- Chebyshev --
-    def run_hamiltonian(self, hamiltonian, time_val, initial_state=None, precision=1e-10, shots=None):
-        """exp(-iHt)|psi> by Chebyshev expansion (simulator.py:649-723)."""
-        from .chebyshev import chebyshev_evolve
+    def run_hamiltonian(self, hamiltonian, time_val, initial_state=None, precision=1e-10, shots=None,
+                        method="csr"):
+        """exp(-iHt)|psi> by Chebyshev expansion (simulator.py:649-723).
+        method="csr" builds the CSR as the reference does; method="pauli"
+        applies H matrix-free from its Pauli masks."""
+        from .chebyshev import chebyshev_evolve, chebyshev_evolve_pauli
         from .hamiltonian import HamiltonianCSR
-        hcsr = hamiltonian if isinstance(hamiltonian, HamiltonianCSR) else \
-            HamiltonianCSR.from_sparse_pauli_op(hamiltonian, device=self.device)
+        from qsim_b200.paulis import PauliSum
+        if method == "pauli":
+            op = hamiltonian.paulis if isinstance(hamiltonian, HamiltonianCSR) else \
+                PauliSum.from_sparse_pauli_op(hamiltonian)
+            nq = op.num_qubits
+        else:
+            op = hamiltonian if isinstance(hamiltonian, HamiltonianCSR) else \
+                HamiltonianCSR.from_sparse_pauli_op(hamiltonian, device=self.device)
+            nq = op.n_qubits
         if initial_state is None:
-            state = E.state_init(hcsr.n_qubits, self.device)
+            state = E.state_init(nq, self.device)
         else:
             state = initial_state
             if not isinstance(state, torch.Tensor):
                 state = torch.as_tensor(np.asarray(state, dtype=np.complex64))
             state = state.to(self.device, torch.complex64).contiguous()
-        result_state, info = chebyshev_evolve(state, hcsr, time_val, precision=precision)
+        if method == "pauli":
+            result_state, info = chebyshev_evolve_pauli(state, op, time_val, precision=precision)
+        else:
+            result_state, info = chebyshev_evolve(state, op, time_val, precision=precision)
+        hcsr = op if method != "pauli" else None
         if shots is None:
             return result_state.cpu().numpy(), info
         samples = E.sample(result_state, shots).cpu().numpy()
         res = _make_result(counts_from_samples(samples), shots,
-                           {"name": "chebyshev_evolution", "n_qubits": hcsr.n_qubits}, info["elapsed_s"], info)
+                           {"name": "chebyshev_evolution", "n_qubits": nq}, info["elapsed_s"], info)
         return res, info

@@ -111,6 +111,7 @@ SIGNATURES = {
     "qs_cheb_accum": (_i, [_vp, _vp, _vp, _d, _d, _i64]),
     "qs_cheb_step_accum": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _i64]),
     "qs_cheb_evolve": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _pd, _i, _d, _vp]),
+    "qs_cheb_evolve_pauli": (_i, [_vp, _i, _vp, _vp, _pu64, _pu64, _pd, _i, _pd, _i, _d, _vp]),
     "qs_batch_run": (_i, [_vp, _i, _pi32, _pi64, _pop, _vp, _pi64]),
     "qs_batch_plan_create": (_i, [_vp, _i, _pi32, _pi64, _pop, _pi64, C.POINTER(_vp)]),
     "qs_batch_plan_execute": (_i, [_vp, _vp, _vp]),

@@ -18,6 +18,20 @@ from ._lib import QsBatchInfo, QsOp, QsPlanInfo
 from .circuit import OP_DTYPE
 
 
+def _record_use(plan) -> None:
+    """Remember the last launch that reads the plan's device program (an
+    event on the current stream), so destroying the plan waits for exactly
+    that work instead of the whole device."""
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(plan.device))
+    plan._uses = getattr(plan, "_uses", [])[-7:] + [ev]
+
+
+def _wait_uses(plan) -> None:
+    for ev in getattr(plan, "_uses", []):
+        ev.synchronize()
+
+
 def _h(device: int | None = None) -> _lib.Handle:
     dev = torch.cuda.current_device() if device is None else int(device)
     return _lib.handle(dev, torch.cuda.current_stream(dev).cuda_stream)
@@ -75,7 +89,7 @@ class Plan:
     def __del__(self):
         try:
             if getattr(self, "ptr", None):
-                torch.cuda.synchronize(self.device)
+                _wait_uses(self)
                 self.L.qs_plan_destroy(self.ptr)
                 self.ptr = None
         except Exception:
@@ -85,12 +99,14 @@ class Plan:
         if check_state(state) != self.n:
             raise RuntimeError("state width does not match the plan")
         _h(self.device).call("qs_plan_execute", self.ptr, _ptr(state))
+        _record_use(self)
         return state
 
     def execute_from_zero(self, state: torch.Tensor) -> torch.Tensor:
         if check_state(state) != self.n:
             raise RuntimeError("state width does not match the plan")
         _h(self.device).call("qs_plan_execute_from_zero", self.ptr, _ptr(state))
+        _record_use(self)
         return state
 
 
@@ -119,7 +135,7 @@ class BatchPlan:
     def __del__(self):
         try:
             if getattr(self, "ptr", None):
-                torch.cuda.synchronize(self.device)
+                _wait_uses(self)
                 self.L.qs_batch_plan_destroy(self.ptr)
                 self.ptr = None
         except Exception:
@@ -132,6 +148,7 @@ class BatchPlan:
         if states.numel() < self.n_amps or states.dtype != torch.complex64 or not states.is_cuda:
             raise RuntimeError("states buffer too small or not complex64 CUDA")
         _h(self.device).call("qs_batch_plan_execute", self.ptr, _ptr(states))
+        _record_use(self)
         return states
 
 

@@ -153,3 +153,47 @@ def test_autograd_function():
     for b in range(2):
         shift = O.grad_param_shift(n, ops, theta[b].detach().numpy(), x, z, c, range(npar))
         np.testing.assert_allclose(theta.grad[b].numpy(), shift, atol=1e-5)
+
+
+@pytest.mark.parametrize("n", [8, 12])
+def test_chebyshev_matrix_free_matches_expm_and_csr(n):
+    from blackwell_backend import BlackwellSimulator
+    H = W.serving_hamiltonian(n, seed=n, n_pairs=min(20, n))
+    psi = W.product_state(n, seed=3).astype(np.complex64)
+    sim = BlackwellSimulator()
+    a, info = sim.run_hamiltonian(H, 2.0, initial_state=psi, precision=1e-8, method="pauli")
+    b, _ = sim.run_hamiltonian(H, 2.0, initial_state=psi, precision=1e-8, method="csr")
+    ref = O.expm_evolve(H.to_dense(), psi.astype(np.complex128), 2.0)
+    assert abs(1 - O.fidelity(a, ref)) <= 1e-6, info
+    assert O.max_abs_err(a, ref) < 5e-5
+    assert O.max_abs_err(a, b.astype(np.complex128)) < 5e-5
+
+
+def test_server_mix_equals_alone():
+    """Requests give the same result alone and in a concurrent mix."""
+    from qsim_b200.server import CircuitRequest, EvolutionRequest, GradientRequest, Server
+    from qsim_b200.circuit import lower
+    reqs = []
+    for i, w in enumerate([10, 13, 16, 11, 18]):
+        reqs.append(CircuitRequest(n_qubits=w, ops=W.qv_ops(w, w, 100 + i), shots=512, seed=i))
+    qc, npar = W.efficient_su2(8, reps=2)
+    obs = W.random_pauli_observable(8, 20, seed=1)
+    P = np.random.default_rng(0).uniform(0, 6.28, (2, npar))
+    reqs.append(GradientRequest(n_qubits=8, ops=lower(qc), n_params=npar, params=P, observable=obs))
+    reqs.append(EvolutionRequest(hamiltonian=W.serving_hamiltonian(10, 4, 10), t=1.5,
+                                 psi0=W.product_state(10, 5), precision=1e-8))
+    alone = []
+    for r in reqs:
+        s = Server(workers=1, batch_window_s=0)
+        alone.append(s.submit(r).result(120))
+        s.close()
+    s = Server(workers=4)
+    futs = [s.submit(r) for r in reqs]
+    mixed = [f.result(120) for f in futs]
+    st = s.stats()
+    s.close()
+    for a, m in zip(alone[:5], mixed[:5]):
+        assert np.array_equal(a, m)
+    assert np.array_equal(alone[5][0], mixed[5][0]) and np.array_equal(alone[5][1], mixed[5][1])
+    assert np.array_equal(alone[6][0], mixed[6][0])
+    assert st["completed"] == len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
