@@ -192,6 +192,22 @@ int qs_expect_pauli_sum(qs_handle_t h, const void* state, int n_qubits,
                         const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
                         int n_terms, double* out_host);
 
+/* No counterpart in the reference.  Same result as qs_expect_pauli_sum, but
+ * the call allocates nothing: no cudaMalloc/cudaFree, no pinned host memory.
+ * For callers that cannot let a library allocate behind their back (a runtime
+ * that owns all device memory through its own arena and budget, or a
+ * latency-critical loop that must not pay cudaMalloc/cudaFree's implicit
+ * synchronisation).  Its scratch is a fixed static device array (~40 KiB per
+ * GPU, held until exit): at most QS_NOALLOC_MAX_TERMS terms, larger requests
+ * fail with QS_ERR_INVALID.  All calls share that array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress); make it before
+ * any stream capture begins. */
+#define QS_NOALLOC_MAX_TERMS 1024
+int qs_expect_pauli_sum_noalloc(qs_handle_t h, const void* state, int n_qubits,
+                                const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
+                                int n_terms, double* out_host);
+
 /* --------------------------------------------------------- Chebyshev ----- */
 /* Reference: bwk/csrc/spmv_sm120.cu:61-142 (spmv_csr): y = a*A*x + b*y with a
  * Kahan-compensated row sum.  row_ptr/col_idx int32, values complex64.      */

@@ -106,6 +106,7 @@ SIGNATURES = {
     "qs_sample": (_i, [_vp, _vp, _i, _vp, _i64, _vp]),
     "qs_expect_z": (_i, [_vp, _vp, _i, _u64, _pd]),
     "qs_expect_pauli_sum": (_i, [_vp, _vp, _i, _pu64, _pu64, _pd, _i, _pd]),
+    "qs_expect_pauli_sum_noalloc": (_i, [_vp, _vp, _i, _pu64, _pu64, _pd, _i, _pd]),
     "qs_spmv_csr": (_i, [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _d, _d, _d, _d]),
     "qs_cheb_step": (_i, [_vp, _vp, _vp, _vp, _i64]),
     "qs_cheb_accum": (_i, [_vp, _vp, _vp, _d, _d, _i64]),
