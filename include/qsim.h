@@ -77,6 +77,7 @@ typedef struct qs_plan_info {
   int64_t n_ops_fused;   /* device ops after FP64 1Q fusion                  */
   double  bytes_moved;   /* HBM bytes: passes * 16 * 2^n                     */
   double  flops;         /* FP32 flop estimate of the program                */
+  int64_t n_device_ops;  /* ops in the device program (after merging)       */
 } qs_plan_info;
 
 /* ------------------------------------------------------------ context ---- */

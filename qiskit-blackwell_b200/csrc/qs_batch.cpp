@@ -17,13 +17,14 @@
 #include <cstring>
 #include <map>
 #include <thread>
+#include <tuple>
 
 struct qs_batch_plan_s {
   int device = 0;
   int n_circuits = 0;
   void* d_blob = nullptr;          // all device programs
   void* d_items = nullptr;         // all PassItem tables
-  struct Launch { int T, R; size_t item_off; int n_items; uint64_t total_tiles; };
+  struct Launch { int T, R, has2, ncoef; size_t item_off; int n_items; uint64_t total_tiles; };
   std::vector<Launch> launches;
   qs_batch_info info{};
 };
@@ -99,7 +100,8 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     std::vector<PassItem> items;
     double bytes = 0, flops = 0;
     for (int L = 0; L < maxp; ++L) {
-      std::map<std::pair<int, int>, std::vector<PassItem>> groups;
+      // key: (T, R, has2); value: items and the largest coefficient pool
+      std::map<std::tuple<int, int, int>, std::pair<std::vector<PassItem>, int>> groups;
       for (int c = 0; c < nc; ++c) {
         const qs_plan_s& p = plans[c];
         if (L >= (int)p.pass_offsets.size()) continue;
@@ -109,18 +111,22 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
         it.pass = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[c] + p.pass_offsets[L]);
         it.ntiles = 1ull << (widths[c] - T);
         it.flags = (L == 0) ? PI_FROM_ZERO : 0u;
-        groups[{T, p.pass_R[L]}].push_back(it);
+        auto& g = groups[std::make_tuple(T, p.pass_R[L], p.pass_has2[L])];
+        g.first.push_back(it);
+        g.second = std::max(g.second, p.pass_ncoef[L]);
         bytes += (L == 0 ? 8.0 : 16.0) * std::ldexp(1.0, widths[c]);
       }
       // larger tiles first: they are the longest-running CTAs
       for (auto g = groups.rbegin(); g != groups.rend(); ++g) {
         qs_batch_plan_s::Launch Lc;
-        Lc.T = g->first.first;
-        Lc.R = g->first.second;
+        Lc.T = std::get<0>(g->first);
+        Lc.R = std::get<1>(g->first);
+        Lc.has2 = std::get<2>(g->first);
+        Lc.ncoef = g->second.second;
         Lc.item_off = items.size();
-        Lc.n_items = (int)g->second.size();
+        Lc.n_items = (int)g->second.first.size();
         uint64_t tb = 0;
-        for (PassItem& it : g->second) { it.tile_begin = tb; tb += it.ntiles; items.push_back(it); }
+        for (PassItem& it : g->second.first) { it.tile_begin = tb; tb += it.ntiles; items.push_back(it); }
         Lc.total_tiles = tb;
         B->launches.push_back(Lc);
       }
@@ -154,7 +160,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
 static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
-    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R);
+    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef);
   }
 }
 

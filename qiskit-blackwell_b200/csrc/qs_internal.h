@@ -70,6 +70,9 @@ enum DevKind : uint8_t {
   DK_PHASE = 7,  // multiply by c[0] where all control bits are set
   DK_DIAG1 = 8,  // multiply by c[b(d0)]
   DK_DIAG2 = 9,  // multiply by c[b(d1)<<1 | b(d0)]
+  DK_RY = 10,    // real rotation [[c, -s], [s, c]] on t0; c[0] = (c, s)
+  DK_DTAB = 11,  // merged diagonal: table over the register bits x group
+                 // factor x sign mask (layout in qs_pass.cu, encode_dtab)
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -105,6 +108,9 @@ struct __align__(16) DevPass {
   uint32_t op_off;
   uint32_t coef_off;
   uint32_t bytes;     // total bytes of this pass record
+  uint32_t ncoef;     // float2 entries in the coefficient pool
+  uint32_t has2;      // 1 if the pass holds a two-target op (U2 / SWAP)
+  uint32_t pad[2];
 };
 
 // Host-side plan.
@@ -112,7 +118,7 @@ struct qs_plan_s {
   int n_qubits = 0;
   int tile_bits = 0;
   std::vector<uint32_t> pass_offsets;   // byte offset of each DevPass in blob
-  std::vector<int> pass_T, pass_R;
+  std::vector<int> pass_T, pass_R, pass_has2, pass_ncoef;
   std::vector<char> blob;               // host copy of the device program
   void* d_blob = nullptr;               // device copy
   int device = 0;
@@ -138,10 +144,12 @@ struct __align__(16) PassItem {
   uint32_t flags;
   uint32_t pad[3];
 };
+// has2: the pass (or any item of the launch) holds a two-target op; ncoef:
+// the largest coefficient pool (float2) of the launch's passes.
 void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
-                           uint32_t flags = 0);
+                           uint32_t flags, int has2, int ncoef);
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
-                          int maxT, int R);
+                          int maxT, int R, int has2, int ncoef);
 
 // Convenience used by several units.
 inline int qs_blocks_for(qs_context* h, uint64_t items, int threads, int per_sm = 8) {

@@ -36,16 +36,29 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
+// Largest dynamic shared memory a pass launch may ask for: a 2^14-amplitude
+// tile (128 KiB) + coefficient pool + dep tables.
+constexpr int kMaxPassSmem = 200 * 1024;
+
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // ----------------------------------------------------- register ops -------
+// v[j] holds amplitude j of the thread's group (bit k of j = register
+// position k).  "gp" is the controls-read-from-the-global-index predicate,
+// "rc" the mask of controls among the register bits.
+
+// single-rounding complex product (FMA form)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -__fmul_rn(a.y, b.y)), fmaf(a.x, b.y, __fmul_rn(a.y, b.x)));
+}
+
 template <int R, int A>
 __device__ __forceinline__ void op_u1(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
   if constexpr (A < R) {
     const float2 g00 = c[0], g01 = c[1], g10 = c[2], g11 = c[3];
-    if (rc == 0 && gp) {  // uncontrolled: no selects
+    if (rc == 0 && gp) {
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) {
         if (j & (1 << A)) continue;
@@ -70,35 +83,53 @@ __device__ __forceinline__ void op_u1(float2 (&v)[1 << R], const float2* __restr
   }
 }
 
+// Real rotation [[c, -s], [s, c]]: 4 FP32 instructions per amplitude.
+template <int R, int A>
+__device__ __forceinline__ void op_ry(float2 (&v)[1 << R], float2 cs, unsigned rc, bool gp) {
+  if constexpr (A < R) {
+    const float co = cs.x, si = cs.y;
+    if (rc == 0 && gp) {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        if (j & (1 << A)) continue;
+        const int k = j | (1 << A);
+        const float2 a0 = v[j], a1 = v[k];
+        v[j] = make_float2(fmaf(co, a0.x, -__fmul_rn(si, a1.x)), fmaf(co, a0.y, -__fmul_rn(si, a1.y)));
+        v[k] = make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
+      }
+      return;
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << A)) continue;
+      const int k = j | (1 << A);
+      const bool p = gp && ((j & rc) == rc);
+      const float2 a0 = v[j], a1 = v[k];
+      const float2 n0 = make_float2(fmaf(co, a0.x, -__fmul_rn(si, a1.x)), fmaf(co, a0.y, -__fmul_rn(si, a1.y)));
+      const float2 n1 = make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
+      v[j] = p ? n0 : a0;
+      v[k] = p ? n1 : a1;
+    }
+  }
+}
+
 template <int R, int A, int B>
 __device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
   if constexpr (A < B && B < R) {
     float2 g[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) g[i] = c[i];
-    if (rc == 0 && gp) {  // uncontrolled: no selects
-#pragma unroll
-      for (int j = 0; j < (1 << R); ++j) {
-        if (j & ((1 << A) | (1 << B))) continue;
-        const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
-        const float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
-        v[j] = cfma4(g + 0, a0, a1, a2, a3);
-        v[j1] = cfma4(g + 4, a0, a1, a2, a3);
-        v[j2] = cfma4(g + 8, a0, a1, a2, a3);
-        v[j3] = cfma4(g + 12, a0, a1, a2, a3);
-      }
-      return;
-    }
+    const bool all = (rc == 0 && gp);
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & ((1 << A) | (1 << B))) continue;
       const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
-      const bool p = gp && ((j & rc) == rc);
-      float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
-      float2 n0 = cfma4(g + 0, a0, a1, a2, a3);
-      float2 n1 = cfma4(g + 4, a0, a1, a2, a3);
-      float2 n2 = cfma4(g + 8, a0, a1, a2, a3);
-      float2 n3 = cfma4(g + 12, a0, a1, a2, a3);
+      const float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
+      const float2 n0 = cfma4(g + 0, a0, a1, a2, a3);
+      const float2 n1 = cfma4(g + 4, a0, a1, a2, a3);
+      const float2 n2 = cfma4(g + 8, a0, a1, a2, a3);
+      const float2 n3 = cfma4(g + 12, a0, a1, a2, a3);
+      const bool p = all || (gp && ((j & rc) == rc));
       v[j] = p ? n0 : a0;
       v[j1] = p ? n1 : a1;
       v[j2] = p ? n2 : a2;
@@ -110,6 +141,16 @@ __device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restr
 template <int R, int A>
 __device__ __forceinline__ void op_x(float2 (&v)[1 << R], unsigned rc, bool gp) {
   if constexpr (A < R) {
+    if (rc == 0 && gp) {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        if (j & (1 << A)) continue;
+        const float2 t = v[j];
+        v[j] = v[j | (1 << A)];
+        v[j | (1 << A)] = t;
+      }
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & (1 << A)) continue;
@@ -155,8 +196,65 @@ __device__ __forceinline__ void op_swap(float2 (&v)[1 << R], unsigned rc, bool g
   }
 }
 
-__device__ __forceinline__ int locbit(int d, int j, uint64_t gidx) {
-  return (d & DLOC_GLOBAL) ? (int)((gidx >> (d & 0x7f)) & 1ull) : ((j >> d) & 1);
+__device__ __forceinline__ uint64_t bits64(float2 f) {
+  return (uint64_t)__float_as_uint(f.x) | ((uint64_t)__float_as_uint(f.y) << 32);
+}
+
+// Merged diagonal (layout written by encode_dtab in qs_plan.cpp).
+template <int R>
+__device__ __forceinline__ void op_dtab(float2 (&v)[1 << R], const DevOp& op, const float2* __restrict__ c,
+                                        uint64_t gidx) {
+  const float2* p = c;
+  const bool table = op.rc & 1;
+  const float2* T = p;
+  if (table) p += (1 << R);
+  float fr = 1.f, fi = 0.f;
+  for (int k = 0; k < op.t0; ++k) {
+    const uint64_t gm = bits64(p[0]);
+    const float2 w = p[1];
+    p += 2;
+    if ((gidx & gm) == gm) {
+      const float r = fmaf(fr, w.x, -__fmul_rn(fi, w.y));
+      fi = fmaf(fr, w.y, __fmul_rn(fi, w.x));
+      fr = r;
+    }
+  }
+  uint32_t m = 0;
+  for (int k = 0; k < op.t1; ++k) {
+    const uint32_t rm = __float_as_uint(p[0].x);
+    const uint64_t gm = bits64(p[1]);
+    p += 2;
+    if ((gidx & gm) == gm) m ^= rm;
+  }
+  const float2 f = make_float2(fr, fi);
+  if (!table && op.t0 == 0) {  // signs only (CZ runs): flip sign bits
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      const uint32_t sb = (m << (31 - j)) & 0x80000000u;
+      v[j].x = __uint_as_float(__float_as_uint(v[j].x) ^ sb);
+      v[j].y = __uint_as_float(__float_as_uint(v[j].y) ^ sb);
+    }
+  } else {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) {
+    float2 t = table ? cmul(T[j], f) : f;
+    const uint32_t sb = (m << (31 - j)) & 0x80000000u;
+    t.x = __uint_as_float(__float_as_uint(t.x) ^ sb);
+    t.y = __uint_as_float(__float_as_uint(t.y) ^ sb);
+    v[j] = cmul(v[j], t);
+  }
+  }
+  for (int k = 0; k < op.d0; ++k) {
+    const uint32_t rm = __float_as_uint(p[0].x);
+    const uint64_t gm = bits64(p[1]);
+    const float2 w = p[2];
+    p += 3;
+    if ((gidx & gm) == gm) {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j)
+        if ((rm >> j) & 1u) v[j] = cmul(v[j], w);
+    }
+  }
 }
 
 #define CASES_1(F, ...)                                                          \
@@ -178,7 +276,7 @@ __device__ __forceinline__ int locbit(int d, int j, uint64_t gidx) {
   case 2 * 8 + 4: F<R, 2, 4>(__VA_ARGS__); break;                                \
   case 3 * 8 + 4: F<R, 3, 4>(__VA_ARGS__); break;
 
-template <int R>
+template <int R, bool TWO>
 __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __restrict__ ops, int ob, int oe,
                                         const float2* __restrict__ coef, uint64_t gidx) {
   for (int o = ob; o < oe; ++o) {
@@ -190,8 +288,8 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
       case DK_U1:
         switch (op.t0) { CASES_1(op_u1, v, c, rc, gp) }
         break;
-      case DK_U2:
-        switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c, rc, gp) }
+      case DK_RY:
+        switch (op.t0) { CASES_1(op_ry, v, c[0], rc, gp) }
         break;
       case DK_X:
         switch (op.t0) { CASES_1(op_x, v, rc, gp) }
@@ -199,41 +297,19 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
       case DK_Y:
         switch (op.t0) { CASES_1(op_y, v, rc, gp) }
         break;
-      case DK_SWAP:
-        switch (op.t0 * 8 + op.t1) { CASES_2(op_swap, v, rc, gp) }
+      case DK_DTAB:
+        op_dtab<R>(v, op, c, gidx);
         break;
-      case DK_NEG:
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j)
-          if (gp && ((j & rc) == rc)) v[j] = make_float2(-v[j].x, -v[j].y);
-        break;
-      case DK_PHASE: {
-        const float2 ph = c[0];
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j)
-          if (gp && ((j & rc) == rc)) v[j] = cmul_comp(v[j], ph);
-        break;
-      }
-      case DK_DIAG1: {
-        const float2 d0 = c[0], d1 = c[1];
-        const int l0 = op.d0;
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j)
-          if (gp && ((j & rc) == rc)) v[j] = cmul_comp(v[j], locbit(l0, j, gidx) ? d1 : d0);
-        break;
-      }
-      case DK_DIAG2: {
-        const float2 d0 = c[0], d1 = c[1], d2 = c[2], d3 = c[3];
-        const int l0 = op.d0, l1 = op.d1;
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j) {
-          if (!(gp && ((j & rc) == rc))) continue;
-          const int s = (locbit(l1, j, gidx) << 1) | locbit(l0, j, gidx);
-          const float2 d = s == 0 ? d0 : s == 1 ? d1 : s == 2 ? d2 : d3;
-          v[j] = cmul_comp(v[j], d);
+      case DK_U2:
+        if constexpr (TWO) {
+          switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c, rc, gp) }
         }
         break;
-      }
+      case DK_SWAP:
+        if constexpr (TWO) {
+          switch (op.t0 * 8 + op.t1) { CASES_2(op_swap, v, rc, gp) }
+        }
+        break;
       default:
         break;
     }
@@ -241,20 +317,22 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 }
 
 // ---------------------------------------------------------- the kernel ----
-// R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs with
-// up to 168 registers, 3 CTAs per SM.  Narrower blocks use 256 threads.
+// R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs, 3 per
+// SM.  Narrower blocks use 256 threads.
 constexpr int kMaxThreads(int R) { return R == 5 ? 128 : 256; }
 constexpr int kMinBlocks(int R) { return R == 5 ? 3 : 2; }
 
-template <int R>
+// Dynamic shared memory: [tile 2^maxT float2][coefficient pool][dep tables].
+template <int R, bool TWO>
 __global__ void __launch_bounds__(kMaxThreads(R), kMinBlocks(R))
 k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restrict__ items, int nitems,
-       uint64_t total_tiles) {
+       uint64_t total_tiles, uint32_t coef_off_bytes, uint32_t dep_off_bytes) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* tile = reinterpret_cast<float2*>(smem_raw);
-  __shared__ uint64_t dep_lo[128];
-  __shared__ uint64_t dep_hi[128];
-  __shared__ int s_S[16];
+  float2* s_coef = reinterpret_cast<float2*>(smem_raw + coef_off_bytes);
+  uint64_t* dep_lo = reinterpret_cast<uint64_t*>(smem_raw + dep_off_bytes);
+  uint64_t* dep_hi = dep_lo + 128;
+  int* s_S = reinterpret_cast<int*>(dep_hi + 128);
 
   int cur = -1;
   const DevPass* P = nullptr;
@@ -281,6 +359,8 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
       state = base_state + I.state_off;
       T = P->T;
       if (threadIdx.x < 16) s_S[threadIdx.x] = P->S[threadIdx.x];
+      const float2* gcoef = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(P) + P->coef_off);
+      for (uint32_t k = threadIdx.x; k < P->ncoef; k += blockDim.x) s_coef[k] = gcoef[k];
       __syncthreads();
       // dep(i) = sum_k bit_k(i) << S[k], split in two 7-bit tables.
       for (int e = threadIdx.x; e < 256; e += blockDim.x) {
@@ -322,7 +402,6 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
     // 2. register blocks
     const DevBlock* blocks = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off);
     const DevOp* ops = reinterpret_cast<const DevOp*>(reinterpret_cast<const char*>(P) + P->op_off);
-    const float2* coef = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(P) + P->coef_off);
     const int nblocks = P->nblocks;
     const uint32_t ngroups = 1u << (T - R);
     for (int b = 0; b < nblocks; ++b) {
@@ -342,20 +421,25 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
         const uint32_t pb = phys(base);
         const uint64_t gidx = need_g ? (gbase | dep_lo[base & 127] | dep_hi[base >> 7]) : 0ull;
         float2 v[1 << R];
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j) {
+        // Gray-code walk: consecutive indices differ in one register bit
+        {
           uint32_t a = pb;
 #pragma unroll
-          for (int k = 0; k < R; ++k) if (j & (1 << k)) a ^= pp[k];
-          v[j] = tile[a];
+          for (int q = 0; q < (1 << R); ++q) {
+            const int j = q ^ (q >> 1);
+            if (q) a ^= pp[__ffs(q) - 1];
+            v[j] = tile[a];
+          }
         }
-        run_ops<R>(v, ops, blk.op_begin, blk.op_end, coef, gidx);
-#pragma unroll
-        for (int j = 0; j < (1 << R); ++j) {
+        run_ops<R, TWO>(v, ops, blk.op_begin, blk.op_end, s_coef, gidx);
+        {
           uint32_t a = pb;
 #pragma unroll
-          for (int k = 0; k < R; ++k) if (j & (1 << k)) a ^= pp[k];
-          tile[a] = v[j];
+          for (int q = 0; q < (1 << R); ++q) {
+            const int j = q ^ (q >> 1);
+            if (q) a ^= pp[__ffs(q) - 1];
+            tile[a] = v[j];
+          }
         }
       }
       __syncthreads();
@@ -373,36 +457,43 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
 
 struct LaunchCfg { int per_sm; };
 
-template <int R>
+size_t coef_bytes_for(int ncoef) { return (((size_t)ncoef * sizeof(float2)) + 15) & ~size_t(15); }
+
+template <int R, bool TWO>
 LaunchCfg configure(int smem, int threads) {
   static std::map<std::pair<int, int>, LaunchCfg> cache;
   auto key = std::make_pair(smem, threads);
   auto f = cache.find(key);
   if (f != cache.end()) return f->second;
   // The attribute is a per-function maximum: set it once to the largest tile
-  // (2^14 amplitudes) so that launches of any tile size stay valid.
+  // (2^14 amplitudes) plus the largest coefficient pool, so that launches of
+  // any size stay valid.
   static bool attr_set = false;
   if (!attr_set) {
-    QS_CUDA(cudaFuncSetAttribute(k_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(float2) << 14)));
+    QS_CUDA(cudaFuncSetAttribute(k_pass<R, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
     attr_set = true;
   }
   int per_sm = 0;
-  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R>, threads, smem));
+  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R, TWO>, threads, smem));
   if (per_sm < 1) throw qs_error(QS_ERR_CUDA, "tile-pass kernel does not fit on an SM");
   LaunchCfg c{per_sm};
   cache[key] = c;
   return c;
 }
 
-template <int R>
+template <int R, bool TWO>
 void launch_R(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
-              uint64_t total, int maxT, int threads) {
-  const int smem = (int)(sizeof(float2) << maxT);
-  LaunchCfg c = configure<R>(smem, threads);
+              uint64_t total, int maxT, int threads, int ncoef) {
+  const uint32_t tile_bytes = (uint32_t)(sizeof(float2) << maxT);
+  const uint32_t coef_off = tile_bytes;
+  const uint32_t dep_off = coef_off + (uint32_t)coef_bytes_for(ncoef);
+  const int smem = (int)(dep_off + 2 * 128 * sizeof(uint64_t) + 16 * sizeof(int));
+  QS_CHECK_ARG(smem <= kMaxPassSmem, "tile-pass program too large for shared memory (coefficient pool)");
+  LaunchCfg c = configure<R, TWO>(smem, threads);
   uint64_t grid = std::min<uint64_t>(total, (uint64_t)h->sm_count * c.per_sm);
   if (grid == 0) return;
-  k_pass<R><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total);
+  k_pass<R, TWO><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total, coef_off,
+                                                               dep_off);
   qs_after_launch(h, "k_pass");
 }
 
@@ -414,18 +505,25 @@ int threads_for(int maxT, int R) {
   return t;
 }
 
-void dispatch(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
-              uint64_t total, int maxT, int R) {
-  QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
+template <bool TWO>
+void dispatch_two(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
+                  uint64_t total, int maxT, int R, int ncoef) {
   const int threads = threads_for(maxT, R);
   switch (R) {
-    case 1: launch_R<1>(h, base, single, d_items, nitems, total, maxT, threads); break;
-    case 2: launch_R<2>(h, base, single, d_items, nitems, total, maxT, threads); break;
-    case 3: launch_R<3>(h, base, single, d_items, nitems, total, maxT, threads); break;
-    case 4: launch_R<4>(h, base, single, d_items, nitems, total, maxT, threads); break;
-    case 5: launch_R<5>(h, base, single, d_items, nitems, total, maxT, threads); break;
+    case 1: launch_R<1, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 2: launch_R<2, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 3: launch_R<3, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 4: launch_R<4, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 5: launch_R<5, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
     default: throw qs_error(QS_ERR_INVALID, "register block width must be 1..5");
   }
+}
+
+void dispatch(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
+              uint64_t total, int maxT, int R, int has2, int ncoef) {
+  QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
+  if (has2) dispatch_two<true>(h, base, single, d_items, nitems, total, maxT, R, ncoef);
+  else dispatch_two<false>(h, base, single, d_items, nitems, total, maxT, R, ncoef);
 }
 
 }  // namespace
@@ -433,21 +531,21 @@ void dispatch(qs_context* h, float2* base, const PassItem& single, const PassIte
 // One state, one pass: the item is passed by value (no device table), so the
 // launch can be captured in a CUDA graph.
 void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
-                           uint32_t flags) {
+                           uint32_t flags, int has2, int ncoef) {
   PassItem it{};
   it.state_off = 0;
   it.pass = d_pass;
   it.ntiles = ntiles;
   it.tile_begin = 0;
   it.flags = flags;
-  dispatch(h, (float2*)state, it, nullptr, 1, ntiles, T, R);
+  dispatch(h, (float2*)state, it, nullptr, 1, ntiles, T, R, has2, ncoef);
 }
 
 // Several (state, pass) items in one launch; d_items is a caller-owned device
 // table whose tile_begin fields hold the prefix sums of ntiles.
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
-                          int maxT, int R) {
+                          int maxT, int R, int has2, int ncoef) {
   if (n_items <= 0 || total_tiles == 0) return;
   PassItem dummy{};
-  dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R);
+  dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R, has2, ncoef);
 }

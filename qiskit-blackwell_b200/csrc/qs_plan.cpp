@@ -14,13 +14,17 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <set>
+#include <tuple>
 
 namespace {
 
 using cd = std::complex<double>;
 
-enum IKind { I_U1, I_U2, I_X, I_SWAP, I_Y, I_NEG, I_PHASE, I_DIAG1, I_DIAG2 };
+enum IKind { I_U1, I_U2, I_X, I_SWAP, I_Y, I_NEG, I_PHASE, I_DIAG1, I_DIAG2, I_RY };
+
+inline bool is_diag_kind(int k) { return k == I_NEG || k == I_PHASE || k == I_DIAG1 || k == I_DIAG2; }
 
 struct IOp {
   int kind;
@@ -117,6 +121,16 @@ std::vector<IOp> normalise(int n, const qs_op* ops, int nops) {
       default:
         throw qs_error(QS_ERR_INVALID, "unknown op kind " + std::to_string(o.kind));
     }
+    if (p.kind == I_U1 && !p.cq.empty() && p.m[1] == 0.0 && p.m[2] == 0.0) {
+      // controlled diagonal: phase d0 where the controls are set, times
+      // d1/d0 where controls and target are set
+      IOp a, b;
+      a.kind = I_PHASE; a.cq = p.cq; a.m[0] = p.m[0];
+      b.kind = I_PHASE; b.cq = p.cq; b.cq.push_back(p.tq[0]); b.m[0] = p.m[3] / p.m[0];
+      if (a.m[0] != 1.0) out.push_back(a);
+      if (b.m[0] != 1.0) out.push_back(b);
+      continue;
+    }
     out.push_back(std::move(p));
   }
   return out;
@@ -156,28 +170,53 @@ bool as_1q(const IOp& o, int& q, M2& M) {
   }
 }
 
-IOp emit_1q(int q, const M2& M, bool& keep) {
+IOp diag_op(int q, cd d0, cd d1) {
   IOp p;
-  keep = true;
+  if (d0 == 1.0) {
+    p.kind = (d1 == -1.0) ? I_NEG : I_PHASE;
+    p.cq = {q};
+    p.m[0] = d1;
+    return p;
+  }
+  p.kind = I_DIAG1; p.dq[0] = q; p.ndq = 1; p.m[0] = d0; p.m[1] = d1;
+  return p;
+}
+
+// Emits the fused single-qubit matrix M on q.  Dense matrices become
+// D_L * R(c, s) * D_R with R = [[c, -s], [s, c]] real (4 FMA per amplitude
+// instead of 8) and D_L, D_R diagonal; the diagonals are later merged with
+// neighbouring diagonal gates into one table op per register block.
+//   c = |M00|, s = |M10|, D_R = diag(1, r1), D_L = diag(M00/c, M10/s),
+//   r1 = -M01 / (l0 s)            (exact factorisation of a unitary M)
+void emit_1q(int q, const M2& M, std::vector<IOp>& out, bool decompose) {
   const bool diag = (M.a[1] == 0.0 && M.a[2] == 0.0);
   if (diag) {
-    if (M.a[0] == 1.0 && M.a[3] == 1.0) { keep = false; return p; }
-    if (M.a[0] == 1.0) {
-      p.kind = (M.a[3] == -1.0) ? I_NEG : I_PHASE;
-      p.cq = {q};
-      p.m[0] = M.a[3];
-      return p;
-    }
-    p.kind = I_DIAG1; p.dq[0] = q; p.ndq = 1; p.m[0] = M.a[0]; p.m[1] = M.a[3];
-    return p;
+    if (M.a[0] == 1.0 && M.a[3] == 1.0) return;
+    out.push_back(diag_op(q, M.a[0], M.a[3]));
+    return;
   }
   if (M.a[0] == 0.0 && M.a[3] == 0.0 && M.a[1] == 1.0 && M.a[2] == 1.0) {
+    IOp p;
     p.kind = I_X; p.tq[0] = q; p.ntq = 1;
-    return p;
+    out.push_back(p);
+    return;
   }
+  const double c = std::abs(M.a[0]), sn = std::abs(M.a[2]);
+  if (decompose && c > 1e-9 && sn > 1e-9) {
+    const cd l0 = M.a[0] / c, l1 = M.a[2] / sn, r1 = -M.a[1] / (l0 * sn);
+    if (r1 != 1.0) out.push_back(diag_op(q, 1.0, r1));
+    IOp r;
+    r.kind = I_RY; r.tq[0] = q; r.ntq = 1;
+    const double nrm = std::sqrt(c * c + sn * sn);
+    r.m[0] = cd(c / nrm, sn / nrm);
+    out.push_back(r);
+    if (!(l0 == 1.0 && l1 == 1.0)) out.push_back(diag_op(q, l0, l1));
+    return;
+  }
+  IOp p;
   p.kind = I_U1; p.tq[0] = q; p.ntq = 1;
   for (int i = 0; i < 4; ++i) p.m[i] = M.a[i];
-  return p;
+  out.push_back(p);
 }
 
 void qubits_of(const IOp& o, std::vector<int>& qs) {
@@ -187,15 +226,13 @@ void qubits_of(const IOp& o, std::vector<int>& qs) {
   for (int c : o.cq) qs.push_back(c);
 }
 
-std::vector<IOp> fuse_1q(int n, const std::vector<IOp>& in) {
+std::vector<IOp> fuse_1q(int n, const std::vector<IOp>& in, bool decompose) {
   std::vector<IOp> out;
   std::vector<M2> pend(n);
   std::vector<char> has(n, 0);
   auto flush = [&](int q) {
     if (!has[q]) return;
-    bool keep;
-    IOp p = emit_1q(q, pend[q], keep);
-    if (keep) out.push_back(std::move(p));
+    emit_1q(q, pend[q], out, decompose);
     has[q] = 0;
   };
   std::vector<int> qs;
@@ -212,6 +249,72 @@ std::vector<IOp> fuse_1q(int n, const std::vector<IOp>& in) {
     out.push_back(o);
   }
   for (int q = 0; q < n; ++q) flush(q);
+  return out;
+}
+
+// Reorders the op list into alternating runs: every dense op that is ready
+// (all ops it does not commute with already emitted) goes first; when none is
+// ready, every ready diagonal op is emitted as one run.  Two ops commute when
+// each shared qubit is used in a diagonal role (control, phase, diagonal) by
+// both.  In a layered circuit this yields: all rotations of a layer, then one
+// run with every diagonal between it and the next layer, which the encoder
+// merges into a single table op per register block.
+std::vector<IOp> schedule_runs(int n, const std::vector<IOp>& in) {
+  const int m = (int)in.size();
+  std::vector<std::vector<int>> succ(m);
+  std::vector<int> indeg(m, 0);
+  std::vector<int> lastT(n, -1);
+  std::vector<std::vector<int>> dset(n);
+  auto edge = [&](int a, int b) {
+    if (a < 0) return;
+    succ[a].push_back(b);
+    ++indeg[b];
+  };
+  for (int b = 0; b < m; ++b) {
+    const IOp& o = in[b];
+    uint64_t tm = 0;
+    for (int i = 0; i < o.ntq; ++i) tm |= 1ull << o.tq[i];
+    std::vector<int> qs;
+    qubits_of(o, qs);
+    std::sort(qs.begin(), qs.end());
+    qs.erase(std::unique(qs.begin(), qs.end()), qs.end());
+    for (int q : qs) {
+      if ((tm >> q) & 1ull) {
+        edge(lastT[q], b);
+        for (int d : dset[q]) edge(d, b);
+        lastT[q] = b;
+        dset[q].clear();
+      } else {
+        edge(lastT[q], b);
+        dset[q].push_back(b);
+      }
+    }
+  }
+  // duplicate edges only inflate indeg consistently (each is decremented once)
+  std::vector<IOp> out;
+  out.reserve(m);
+  std::vector<int> ready_dense, ready_diag;
+  for (int b = 0; b < m; ++b)
+    if (indeg[b] == 0) (is_diag_kind(in[b].kind) ? ready_diag : ready_dense).push_back(b);
+  auto release = [&](int b) {
+    for (int s2 : succ[b])
+      if (--indeg[s2] == 0) (is_diag_kind(in[s2].kind) ? ready_diag : ready_dense).push_back(s2);
+  };
+  while (!ready_dense.empty() || !ready_diag.empty()) {
+    if (!ready_dense.empty()) {
+      // keep program order among the ready dense ops
+      std::sort(ready_dense.begin(), ready_dense.end());
+      std::vector<int> batch;
+      batch.swap(ready_dense);
+      for (int b : batch) { out.push_back(in[b]); release(b); }
+      continue;
+    }
+    std::sort(ready_diag.begin(), ready_diag.end());
+    std::vector<int> batch;
+    batch.swap(ready_diag);
+    for (int b : batch) { out.push_back(in[b]); release(b); }
+  }
+  if ((int)out.size() != m) throw qs_error(QS_ERR_INVALID, "internal: op scheduling cycle");
   return out;
 }
 
@@ -286,14 +389,142 @@ void permute_u2_bits(cd* m) {
   for (int i = 0; i < 16; ++i) m[i] = r[i];
 }
 
+// A diagonal op as a product of "all set" terms: multiply by w where every
+// qubit of `mask` is 1 (mask 0: a constant).  DIAG1(q; d0, d1) = d0 * (d1/d0
+// on q); DIAG2 likewise with the pair term d11 d00 / (d01 d10).
+struct DTerm { uint64_t mask; cd w; };
+
+void diag_terms(const IOp& o, std::vector<DTerm>& t) {
+  switch (o.kind) {
+    case I_NEG: case I_PHASE: {
+      uint64_t m = 0;
+      for (int c : o.cq) m |= 1ull << c;
+      t.push_back({m, o.kind == I_NEG ? cd(-1.0, 0.0) : o.m[0]});
+      break;
+    }
+    case I_DIAG1: {
+      const uint64_t a = 1ull << o.dq[0];
+      t.push_back({0, o.m[0]});
+      t.push_back({a, o.m[1] / o.m[0]});
+      break;
+    }
+    case I_DIAG2: {
+      const uint64_t a = 1ull << o.dq[0], b = 1ull << o.dq[1];
+      t.push_back({0, o.m[0]});
+      t.push_back({a, o.m[1] / o.m[0]});
+      t.push_back({b, o.m[2] / o.m[0]});
+      t.push_back({a | b, o.m[3] * o.m[0] / (o.m[1] * o.m[2])});
+      break;
+    }
+    default:
+      throw qs_error(QS_ERR_INVALID, "internal: not a diagonal op");
+  }
+}
+
+// One DK_DTAB op (kernel layout, qs_pass.cu):
+//   pool: [2^R table entries (if rc & 1)]
+//         [t0 group terms:  (gmask lo, gmask hi) as raw bits, w]        2 float2 each
+//         [t1 sign terms:   (regmask32, 0), (gmask lo, gmask hi)]       2 float2 each
+//         [d0 cross terms:  (regmask32, 0), (gmask lo, gmask hi), w]    3 float2 each
+// amplitude j of a group with global index gidx is multiplied by
+//   T[j] * prod_{group terms, gidx has gmask} w * prod_{cross, j in regmask, gidx has gmask} w
+// and negated where the XOR of the active sign terms' regmasks has bit j.
+void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, int R,
+                 std::vector<DevOp>& dops, std::vector<float>& coef, bool& need_g) {
+  uint64_t rmask_all = 0;
+  for (int k = 0; k < R; ++k) rmask_all |= 1ull << regq[k];
+  const int J = 1 << R;
+  std::vector<cd> T(J, cd(1.0, 0.0));
+  std::map<uint64_t, cd> gterm;
+  std::vector<std::pair<uint32_t, uint64_t>> sterm;
+  std::vector<std::tuple<uint32_t, uint64_t, cd>> xterm;
+  auto regmask32 = [&](uint64_t m) {
+    uint32_t rm = 0;
+    for (int j = 0; j < J; ++j) {
+      bool all = true;
+      for (int k = 0; k < R; ++k)
+        if (((m >> regq[k]) & 1ull) && !((j >> k) & 1)) all = false;
+      if (all) rm |= 1u << j;
+    }
+    return rm;
+  };
+  for (const DTerm& d : terms) {
+    if (d.w == 1.0) continue;
+    const uint64_t mr = d.mask & rmask_all, mg = d.mask & ~rmask_all;
+    if (mg == 0) {
+      const uint32_t rm = regmask32(mr);
+      for (int j = 0; j < J; ++j)
+        if ((rm >> j) & 1u) T[j] *= d.w;
+    } else if (mr == 0) {
+      auto it = gterm.find(mg);
+      if (it == gterm.end()) gterm[mg] = d.w; else it->second *= d.w;
+    } else if (d.w == -1.0) {
+      sterm.push_back({regmask32(mr), mg});
+    } else {
+      xterm.emplace_back(regmask32(mr), mg, d.w);
+    }
+  }
+  std::vector<std::pair<uint64_t, cd>> gl;
+  for (auto& kv : gterm)
+    if (kv.second != 1.0) gl.push_back(kv);
+  bool table = false;
+  for (int j = 0; j < J; ++j) table |= (T[j] != 1.0);
+  if (!table && gl.empty() && sterm.empty() && xterm.empty()) return;  // identity
+  // split into several ops if a count would overflow its 8-bit field
+  size_t gi = 0, si = 0, xi = 0;
+  bool first = true;
+  do {
+    DevOp d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = DK_DTAB;
+    const size_t ng = std::min<size_t>(gl.size() - gi, 255), ns = std::min<size_t>(sterm.size() - si, 255),
+                 nx = std::min<size_t>(xterm.size() - xi, 255);
+    d.t0 = (uint8_t)ng;
+    d.t1 = (uint8_t)ns;
+    d.d0 = (uint8_t)nx;
+    d.rc = (first && table) ? 1 : 0;
+    d.coef = (uint32_t)(coef.size() / 2);
+    auto put = [&](cd v) { coef.push_back((float)v.real()); coef.push_back((float)v.imag()); };
+    auto put_bits = [&](uint32_t a, uint32_t b) {
+      float fa, fb;
+      std::memcpy(&fa, &a, 4);
+      std::memcpy(&fb, &b, 4);
+      coef.push_back(fa);
+      coef.push_back(fb);
+    };
+    if (d.rc)
+      for (int j = 0; j < J; ++j) put(T[j]);
+    for (size_t k = 0; k < ng; ++k, ++gi) {
+      put_bits((uint32_t)gl[gi].first, (uint32_t)(gl[gi].first >> 32));
+      put(gl[gi].second);
+    }
+    for (size_t k = 0; k < ns; ++k, ++si) {
+      put_bits(sterm[si].first, 0);
+      put_bits((uint32_t)sterm[si].second, (uint32_t)(sterm[si].second >> 32));
+    }
+    for (size_t k = 0; k < nx; ++k, ++xi) {
+      put_bits(std::get<0>(xterm[xi]), 0);
+      put_bits((uint32_t)std::get<1>(xterm[xi]), (uint32_t)(std::get<1>(xterm[xi]) >> 32));
+      put(std::get<2>(xterm[xi]));
+    }
+    d.ncoef = 0;
+    if (ng || ns || nx) need_g = true;
+    dops.push_back(d);
+    first = false;
+  } while (gi < gl.size() || si < sterm.size() || xi < xterm.size());
+}
+
+thread_local int g_last_devops = 0;
+
 void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::vector<char>& blob,
-                 uint32_t& pass_off, int& R_out, int& nblocks_out) {
+                 uint32_t& pass_off, int& R_out, int& nblocks_out, int& has2_out, int& ncoef_out) {
   const int T = pp.T;
   const int R = std::min(5, T);
   std::vector<int> tpos(n, -1);  // global qubit -> tile position
   for (int k = 0; k < T; ++k) tpos[pp.S[k]] = k;
 
-  // Register blocks: consecutive ops whose targets fit in R tile positions.
+  // Register blocks: consecutive ops whose targets fit in R tile positions
+  // (diagonal ops need no register position and join the current block).
   struct Blk { std::vector<int> regs; std::vector<int> ops; };
   std::vector<Blk> blks;
   Blk cur;
@@ -319,11 +550,14 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   std::vector<DevBlock> dblocks;
   std::vector<DevOp> dops;
   std::vector<float> coef;  // float2 pool, re/im
+  int has2 = 0;
   for (Blk& b : blks) {
     // pad to R positions with the lowest unused tile positions
     for (int p = 0; (int)b.regs.size() < R && p < T; ++p)
       if (std::find(b.regs.begin(), b.regs.end(), p) == b.regs.end()) b.regs.push_back(p);
     std::sort(b.regs.begin(), b.regs.end());
+    std::vector<int> regq(R);
+    for (int k = 0; k < R; ++k) regq[k] = pp.S[b.regs[k]];
     auto regidx = [&](int q) -> int {
       int p = tpos[q];
       if (p < 0) return -1;
@@ -335,27 +569,31 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
     for (int k = 0; k < R; ++k) db.pos[k] = (int8_t)b.regs[k];
     db.op_begin = (int32_t)dops.size();
     bool need_g = false;
+    std::vector<DTerm> run;  // pending diagonal run
+    auto flush_run = [&]() {
+      if (run.empty()) return;
+      encode_dtab(run, regq, R, dops, coef, need_g);
+      run.clear();
+    };
     for (int idx : b.ops) {
       IOp o = ops[idx];
+      if (is_diag_kind(o.kind)) { diag_terms(o, run); continue; }
+      flush_run();
       DevOp d;
       std::memset(&d, 0, sizeof(d));
       for (int c : o.cq) {
         int r = regidx(c);
         if (r >= 0) d.rc |= (uint8_t)(1u << r); else { d.gc |= 1ull << c; need_g = true; }
       }
-      auto loc = [&](int q) -> uint8_t {
-        int r = regidx(q);
-        if (r >= 0) return (uint8_t)r;
-        need_g = true;
-        return (uint8_t)(DLOC_GLOBAL | q);
-      };
       int ncoef = 0;
       switch (o.kind) {
         case I_U1: d.kind = DK_U1; d.t0 = (uint8_t)regidx(o.tq[0]); ncoef = 4; break;
+        case I_RY: d.kind = DK_RY; d.t0 = (uint8_t)regidx(o.tq[0]); ncoef = 1; break;
         case I_U2: {
           int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
           if (a > c) { std::swap(a, c); permute_u2_bits(o.m); }
           d.kind = DK_U2; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c; ncoef = 16;
+          has2 = 1;
           break;
         }
         case I_X: d.kind = DK_X; d.t0 = (uint8_t)regidx(o.tq[0]); break;
@@ -364,12 +602,10 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
           int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
           if (a > c) std::swap(a, c);
           d.kind = DK_SWAP; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c;
+          has2 = 1;
           break;
         }
-        case I_NEG: d.kind = DK_NEG; break;
-        case I_PHASE: d.kind = DK_PHASE; ncoef = 1; break;
-        case I_DIAG1: d.kind = DK_DIAG1; d.d0 = loc(o.dq[0]); ncoef = 2; break;
-        case I_DIAG2: d.kind = DK_DIAG2; d.d0 = loc(o.dq[0]); d.d1 = loc(o.dq[1]); ncoef = 4; break;
+        default: throw qs_error(QS_ERR_INVALID, "internal: unexpected op kind in block");
       }
       d.ncoef = (uint8_t)ncoef;
       d.coef = (uint32_t)(coef.size() / 2);
@@ -379,6 +615,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
       }
       dops.push_back(d);
     }
+    flush_run();
     db.op_end = (int32_t)dops.size();
     db.pos[7] = need_g ? 1 : 0;
     dblocks.push_back(db);
@@ -391,6 +628,8 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   hdr.nblocks = (int32_t)dblocks.size();
   hdr.n_qubits = n;
   for (int k = 0; k < T; ++k) hdr.S[k] = pp.S[k];
+  hdr.ncoef = (uint32_t)(coef.size() / 2);
+  hdr.has2 = (uint32_t)has2;
   size_t off = align16(sizeof(DevPass));
   hdr.block_off = (uint32_t)off;
   off = align16(off + dblocks.size() * sizeof(DevBlock));
@@ -408,13 +647,17 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   if (!dops.empty()) std::memcpy(base + hdr.op_off, dops.data(), dops.size() * sizeof(DevOp));
   if (!coef.empty()) std::memcpy(base + hdr.coef_off, coef.data(), coef.size() * sizeof(float));
   R_out = R;
+  g_last_devops = (int)dops.size();
   nblocks_out = (int)dblocks.size();
+  has2_out = has2;
+  ncoef_out = (int)hdr.ncoef;
 }
 
 double op_flops(const IOp& o) {
   switch (o.kind) {
     case I_U1: return 16;
     case I_U2: return 32;
+    case I_RY: return 8;
     case I_PHASE: case I_DIAG1: case I_DIAG2: return 8;
     default: return 0;
   }
@@ -426,7 +669,7 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
   std::vector<IOp> norm = normalise(n, ops, nops);
-  std::vector<IOp> fused = fuse_1q(n, norm);
+  std::vector<IOp> fused = schedule_runs(n, fuse_1q(n, norm, true));
   int T = n <= 14 ? n : tile_bits;
   std::vector<PassPlan> passes = split_passes(n, T, fused);
   plan->n_qubits = n;
@@ -435,17 +678,23 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   plan->pass_offsets.clear();
   plan->pass_T.clear();
   plan->pass_R.clear();
+  plan->pass_has2.clear();
+  plan->pass_ncoef.clear();
   int nblocks_total = 0;
+  int64_t devops_total = 0;
   double flops = 0;
   for (auto& o : fused) flops += op_flops(o);
   for (const PassPlan& pp : passes) {
     uint32_t off;
-    int R, nb;
-    encode_pass(n, pp, fused, plan->blob, off, R, nb);
+    int R, nb, h2, nc;
+    encode_pass(n, pp, fused, plan->blob, off, R, nb, h2, nc);
     plan->pass_offsets.push_back(off);
     plan->pass_T.push_back(pp.T);
     plan->pass_R.push_back(R);
+    plan->pass_has2.push_back(h2);
+    plan->pass_ncoef.push_back(nc);
     nblocks_total += nb;
+    devops_total += g_last_devops;
   }
   qs_plan_info& I = plan->info;
   I.n_qubits = n;
@@ -456,6 +705,7 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   I.n_ops_fused = (int64_t)fused.size();
   I.bytes_moved = (double)passes.size() * 16.0 * std::ldexp(1.0, n);
   I.flops = flops * std::ldexp(1.0, n);
+  I.n_device_ops = devops_total;
 }
 
 // Stream-ordered allocation: creating or destroying a plan never
@@ -484,7 +734,8 @@ void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint6
     const DevPass* dp = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
     const int T = p->pass_T[i];
     const uint32_t flags = (from_zero && i == 0) ? PI_FROM_ZERO : 0u;
-    qs_launch_pass_single(h, state, dp, T, p->pass_R[i], n_states << (n - T), flags);
+    qs_launch_pass_single(h, state, dp, T, p->pass_R[i], n_states << (n - T), flags, p->pass_has2[i],
+                          p->pass_ncoef[i]);
   }
 }
 

@@ -33,7 +33,7 @@ class QsOp(C.Structure):
 class QsPlanInfo(C.Structure):
     _fields_ = [("n_qubits", C.c_int32), ("tile_bits", C.c_int32), ("n_passes", C.c_int32),
                 ("n_blocks", C.c_int32), ("n_ops_in", C.c_int64), ("n_ops_fused", C.c_int64),
-                ("bytes_moved", C.c_double), ("flops", C.c_double)]
+                ("bytes_moved", C.c_double), ("flops", C.c_double), ("n_device_ops", C.c_int64)]
 
 
 class QsBatchInfo(C.Structure):
