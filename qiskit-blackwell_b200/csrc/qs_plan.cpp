@@ -13,6 +13,8 @@
 #include "qs_api.h"
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <set>
@@ -393,6 +395,7 @@ void permute_u2_bits(cd* m) {
 // qubit of `mask` is 1 (mask 0: a constant).  DIAG1(q; d0, d1) = d0 * (d1/d0
 // on q); DIAG2 likewise with the pair term d11 d00 / (d01 d10).
 struct DTerm { uint64_t mask; cd w; };
+thread_local int64_t g_dtab_stats[4] = {0, 0, 0, 0};  // tables, group, sign, cross terms
 
 void diag_terms(const IOp& o, std::vector<DTerm>& t) {
   switch (o.kind) {
@@ -509,6 +512,7 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
     }
     d.ncoef = 0;
     if (ng || ns || nx) need_g = true;
+    g_dtab_stats[0] += 1; g_dtab_stats[1] += (int64_t)ng; g_dtab_stats[2] += (int64_t)ns; g_dtab_stats[3] += (int64_t)nx;
     dops.push_back(d);
     first = false;
   } while (gi < gl.size() || si < sterm.size() || xi < xterm.size());
@@ -706,6 +710,11 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   I.bytes_moved = (double)passes.size() * 16.0 * std::ldexp(1.0, n);
   I.flops = flops * std::ldexp(1.0, n);
   I.n_device_ops = devops_total;
+  if (std::getenv("QSIM_PLAN_STATS"))
+    std::fprintf(stderr, "qsim plan: n=%d passes=%d blocks=%d devops=%lld dtab=%lld gterms=%lld sterms=%lld xterms=%lld\n",
+                 n, (int)passes.size(), nblocks_total, (long long)devops_total, (long long)g_dtab_stats[0],
+                 (long long)g_dtab_stats[1], (long long)g_dtab_stats[2], (long long)g_dtab_stats[3]);
+  for (auto& v : g_dtab_stats) v = 0;
 }
 
 // Stream-ordered allocation: creating or destroying a plan never
