@@ -375,6 +375,7 @@ def main():
     ap.add_argument("--circuits", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
+    ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
 
@@ -403,9 +404,10 @@ def main():
     dev = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(dev)
     dist_init(ws, "nccl")
-    if args.tile_bits:
+    if args.tile_bits or args.block_bits:
         from qsim_b200 import engine as E
         E._h(dev).call("qs_set_tile_bits", int(args.tile_bits))
+        E._h(dev).call("qs_set_block_bits", int(args.block_bits))
     res, meta = WORKLOADS[args.workload](args, dev)
     if rank == 0:
         res.update({"n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,

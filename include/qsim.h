@@ -95,6 +95,9 @@ const char* qs_last_error(qs_handle_t h);
 const char* qs_version(void);
 /* Tile bits used by the fused-pass planner (10..14); 0 = default (13).      */
 int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
+/* Register-block width used by the planner (2..5 qubits per thread group);
+ * 0 = default (5).                                                          */
+int  qs_set_block_bits(qs_handle_t h, int block_bits);
 /* Number of kernels this handle has launched since creation.               */
 int64_t qs_launch_count(qs_handle_t h);
 

@@ -39,7 +39,7 @@ void free_bplan(qs_batch_plan_s* b) {
 }
 
 void plan_all(int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops, int tile_bits,
-              std::vector<qs_plan_s>& plans) {
+              std::vector<qs_plan_s>& plans, int block_bits) {
   plans.resize(nc);
   std::vector<std::string> errs(nc);
   unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -51,7 +51,7 @@ void plan_all(int nc, const int32_t* widths, const int64_t* op_off, const qs_op*
         try {
           const int64_t b = op_off[c], e = op_off[c + 1];
           if (b < 0 || e < b) throw qs_error(QS_ERR_INVALID, "op_offsets must be non-decreasing");
-          qs_build_plan(widths[c], ops + b, (int)(e - b), tile_bits, &plans[c]);
+          qs_build_plan(widths[c], ops + b, (int)(e - b), tile_bits, &plans[c], block_bits);
         } catch (const std::exception& ex) {
           errs[c] = ex.what();
         }
@@ -74,7 +74,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
   }
   std::vector<qs_plan_s> plans;
-  plan_all(nc, widths, op_off, ops, h->tile_bits, plans);
+  plan_all(nc, widths, op_off, ops, h->tile_bits, plans, h->block_bits);
 
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
@@ -242,7 +242,7 @@ int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int 
   }
   if (n_states == 0 || ngates == 0) return QS_OK;
   qs_plan_s p;
-  qs_build_plan(n, ops.data(), ngates, h->tile_bits, &p);
+  qs_build_plan(n, ops.data(), ngates, h->tile_bits, &p, h->block_bits);
   qs_plan_upload(h, &p);
   try {
     qs_plan_run(h, &p, states, false, (uint64_t)n_states);

@@ -117,6 +117,15 @@ int qs_set_tile_bits(qs_handle_t h, int tile_bits) {
   QS_API_END(h)
 }
 
+int qs_set_block_bits(qs_handle_t h, int bb) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  if (bb == 0) bb = 5;
+  QS_CHECK_ARG(bb >= 2 && bb <= 5, "block_bits must be in [2, 5]");
+  h->block_bits = bb;
+  QS_API_END(h)
+}
+
 int64_t qs_launch_count(qs_handle_t h) { return h ? h->launches : -1; }
 
 }  // extern "C"

@@ -38,6 +38,7 @@ struct qs_context {
   cudaStream_t stream = nullptr;
   std::string err;
   int tile_bits = 13;
+  int block_bits = 5;
   int64_t launches = 0;
 
   // grow-only device scratch (reductions, sampling partials, ...)
@@ -73,6 +74,9 @@ enum DevKind : uint8_t {
   DK_RY = 10,    // real rotation [[c, -s], [s, c]] on t0; c[0] = (c, s)
   DK_DTAB = 11,  // merged diagonal: table over the register bits x group
                  // factor x sign mask (layout in qs_pass.cu, encode_dtab)
+  DK_KRY = 12,   // one real rotation per register bit (c[k] = (c, s); identity
+                 // where t0's bit k is clear), applied as a Kronecker product
+  DK_KU1 = 13,   // one dense 2x2 per register bit (c[4k..4k+3]), likewise
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -126,7 +130,7 @@ struct qs_plan_s {
 };
 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
-void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan);
+void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 5);
 void qs_plan_upload(qs_context* h, qs_plan_s* p);
 void qs_plan_free_device(void* d);  // stream-ordered free (no device sync)
 // Runs every pass on n_states equal-width states stored back to back.

@@ -196,6 +196,60 @@ __device__ __forceinline__ void op_swap(float2 (&v)[1 << R], unsigned rc, bool g
   }
 }
 
+// Kronecker layer: a rotation on every register bit set in `mask`, fully
+// unrolled at compile-time positions; one dispatch for up to R gates.
+template <int R, int K>
+__device__ __forceinline__ void kry_stage(float2 (&v)[1 << R], float2 cs) {
+  const float co = cs.x, si = cs.y;
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) {
+    if (j & (1 << K)) continue;
+    const int k = j | (1 << K);
+    const float2 a0 = v[j], a1 = v[k];
+    v[j] = make_float2(fmaf(co, a0.x, -__fmul_rn(si, a1.x)), fmaf(co, a0.y, -__fmul_rn(si, a1.y)));
+    v[k] = make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
+  }
+}
+
+template <int R, int K>
+__device__ __forceinline__ void ku1_stage(float2 (&v)[1 << R], const float2* __restrict__ c) {
+  const float2 g00 = c[0], g01 = c[1], g10 = c[2], g11 = c[3];
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) {
+    if (j & (1 << K)) continue;
+    const int k = j | (1 << K);
+    const float2 a0 = v[j], a1 = v[k];
+    v[j] = cfma2(g00, a0, g01, a1);
+    v[k] = cfma2(g10, a0, g11, a1);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void op_kry(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned mask) {
+  if (mask == (1u << R) - 1u) {  // full layer: straight-line code
+    if constexpr (R > 0) kry_stage<R, 0>(v, c[0]);
+    if constexpr (R > 1) kry_stage<R, 1>(v, c[1]);
+    if constexpr (R > 2) kry_stage<R, 2>(v, c[2]);
+    if constexpr (R > 3) kry_stage<R, 3>(v, c[3]);
+    if constexpr (R > 4) kry_stage<R, 4>(v, c[4]);
+    return;
+  }
+  if constexpr (R > 0) if (mask & 1u) kry_stage<R, 0>(v, c[0]);
+  if constexpr (R > 1) if (mask & 2u) kry_stage<R, 1>(v, c[1]);
+  if constexpr (R > 2) if (mask & 4u) kry_stage<R, 2>(v, c[2]);
+  if constexpr (R > 3) if (mask & 8u) kry_stage<R, 3>(v, c[3]);
+  if constexpr (R > 4) if (mask & 16u) kry_stage<R, 4>(v, c[4]);
+}
+
+template <int R>
+__device__ __forceinline__ void op_ku1(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned mask) {
+  if constexpr (R > 0) if (mask & 1u) ku1_stage<R, 0>(v, c + 0);
+  if constexpr (R > 1) if (mask & 2u) ku1_stage<R, 1>(v, c + 4);
+  if constexpr (R > 2) if (mask & 4u) ku1_stage<R, 2>(v, c + 8);
+  if constexpr (R > 3) if (mask & 8u) ku1_stage<R, 3>(v, c + 12);
+  if constexpr (R > 4) if (mask & 16u) ku1_stage<R, 4>(v, c + 16);
+}
+
 __device__ __forceinline__ uint64_t bits64(float2 f) {
   return (uint64_t)__float_as_uint(f.x) | ((uint64_t)__float_as_uint(f.y) << 32);
 }
@@ -300,6 +354,12 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
       case DK_DTAB:
         op_dtab<R>(v, op, c, gidx);
         break;
+      case DK_KRY:
+        op_kry<R>(v, c, op.t0);
+        break;
+      case DK_KU1:
+        op_ku1<R>(v, c, op.t0);
+        break;
       case DK_U2:
         if constexpr (TWO) {
           switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c, rc, gp) }
@@ -320,7 +380,7 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 // R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs, 3 per
 // SM.  Narrower blocks use 256 threads.
 constexpr int kMaxThreads(int R) { return R == 5 ? 128 : 256; }
-constexpr int kMinBlocks(int R) { return R == 5 ? 3 : 2; }
+constexpr int kMinBlocks(int R) { return R == 5 ? 2 : 2; }
 
 // Dynamic shared memory: [tile 2^maxT float2][coefficient pool][dep tables].
 template <int R, bool TWO>

@@ -521,9 +521,9 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
 thread_local int g_last_devops = 0;
 
 void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::vector<char>& blob,
-                 uint32_t& pass_off, int& R_out, int& nblocks_out, int& has2_out, int& ncoef_out) {
+                 uint32_t& pass_off, int& R_out, int& nblocks_out, int& has2_out, int& ncoef_out, int block_bits) {
   const int T = pp.T;
-  const int R = std::min(5, T);
+  const int R = std::min(block_bits, T);
   std::vector<int> tpos(n, -1);  // global qubit -> tile position
   for (int k = 0; k < T; ++k) tpos[pp.S[k]] = k;
 
@@ -579,9 +579,55 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
       encode_dtab(run, regq, R, dops, coef, need_g);
       run.clear();
     };
+    // pending Kronecker layer: uncontrolled 1Q rotations / dense gates on
+    // distinct register bits (they commute), emitted as one op
+    std::vector<std::pair<int, IOp>> kron;  // (register bit, op)
+    auto flush_kron = [&]() {
+      if (kron.empty()) return;
+      bool all_ry = true;
+      for (auto& kv : kron) all_ry &= (kv.second.kind == I_RY);
+      DevOp d;
+      std::memset(&d, 0, sizeof(d));
+      unsigned mask = 0;
+      for (auto& kv : kron) mask |= 1u << kv.first;
+      d.kind = all_ry ? DK_KRY : DK_KU1;
+      d.t0 = (uint8_t)mask;
+      d.coef = (uint32_t)(coef.size() / 2);
+      const int per = all_ry ? 1 : 4;
+      std::vector<cd> slots((size_t)R * per, cd(0.0, 0.0));
+      for (int k = 0; k < R; ++k) {  // identity defaults
+        if (all_ry) slots[k] = cd(1.0, 0.0);
+        else { slots[4 * k] = 1.0; slots[4 * k + 3] = 1.0; }
+      }
+      for (auto& kv : kron) {
+        const IOp& g = kv.second;
+        const int k = kv.first;
+        if (all_ry) slots[k] = g.m[0];
+        else if (g.kind == I_RY) {
+          const double c = g.m[0].real(), sn = g.m[0].imag();
+          slots[4 * k] = c; slots[4 * k + 1] = -sn; slots[4 * k + 2] = sn; slots[4 * k + 3] = c;
+        } else {
+          for (int i = 0; i < 4; ++i) slots[4 * k + i] = g.m[i];
+        }
+      }
+      for (const cd& v : slots) { coef.push_back((float)v.real()); coef.push_back((float)v.imag()); }
+      d.ncoef = (uint8_t)slots.size();
+      dops.push_back(d);
+      kron.clear();
+    };
     for (int idx : b.ops) {
       IOp o = ops[idx];
-      if (is_diag_kind(o.kind)) { diag_terms(o, run); continue; }
+      if (is_diag_kind(o.kind)) { flush_kron(); diag_terms(o, run); continue; }
+      if ((o.kind == I_RY || o.kind == I_U1) && o.cq.empty()) {
+        flush_run();
+        const int k = regidx(o.tq[0]);
+        bool clash = false;
+        for (auto& kv : kron) clash |= (kv.first == k);
+        if (clash) flush_kron();
+        kron.push_back({k, o});
+        continue;
+      }
+      flush_kron();
       flush_run();
       DevOp d;
       std::memset(&d, 0, sizeof(d));
@@ -619,6 +665,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
       }
       dops.push_back(d);
     }
+    flush_kron();
     flush_run();
     db.op_end = (int32_t)dops.size();
     db.pos[7] = need_g ? 1 : 0;
@@ -669,7 +716,7 @@ double op_flops(const IOp& o) {
 
 }  // namespace
 
-void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* plan) {
+void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* plan, int block_bits) {
   QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
   std::vector<IOp> norm = normalise(n, ops, nops);
@@ -691,7 +738,7 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   for (const PassPlan& pp : passes) {
     uint32_t off;
     int R, nb, h2, nc;
-    encode_pass(n, pp, fused, plan->blob, off, R, nb, h2, nc);
+    encode_pass(n, pp, fused, plan->blob, off, R, nb, h2, nc, block_bits);
     plan->pass_offsets.push_back(off);
     plan->pass_T.push_back(pp.T);
     plan->pass_R.push_back(R);
@@ -757,7 +804,7 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   QS_CHECK_ARG(out != nullptr, "out is null");
   *out = nullptr;
   p = new qs_plan_s();
-  qs_build_plan(n, ops, nops, h->tile_bits, p);
+  qs_build_plan(n, ops, nops, h->tile_bits, p, h->block_bits);
   qs_plan_upload(h, p);
   *out = p;
   p = nullptr;

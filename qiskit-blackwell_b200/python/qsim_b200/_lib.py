@@ -74,6 +74,7 @@ SIGNATURES = {
     "qs_last_error": (C.c_char_p, [_vp]),
     "qs_version": (C.c_char_p, []),
     "qs_set_tile_bits": (_i, [_vp, _i]),
+    "qs_set_block_bits": (_i, [_vp, _i]),
     "qs_launch_count": (_i64, [_vp]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
     "qs_state_init_basis": (_i, [_vp, _vp, _i, _u64]),
