@@ -174,7 +174,10 @@ def bench_layers32(args, dev):
         t = _cuda_time(step, stream, args.steps)
     launches = (h.launches() - l0)
     t = reduce_max(t, f"cuda:{dev}")
-    P = plan.info["n_passes"]
+    info = plan.refresh_info()
+    P = info["n_passes"]
+    kernel = ("qs_tile_pass (one NVRTC-specialised kernel per pass)" if info["n_jit_passes"] == P
+              else "k_pass (generic tile-pass interpreter)")
     algo_bytes = (8.0 + 16.0 * (P - 1)) * (1 << n)  # first pass writes only
     per_step = t / args.steps
     peak, src = measured_peaks()
@@ -205,11 +208,12 @@ def bench_layers32(args, dev):
         "ms_per_step": per_step * 1e3, "dtype": "c64 (fp32 FMA; fp64 host fusion)",
         "config": {"workload": f"layers32: {n} qubits (2^{n} complex64 = {(8 << n) >> 30} GiB), {layers} layers "
                                f"U(2)+CZ brickwork+Toffoli/5, {ngates} gates, seed 0",
-                   "passes": P, "tile_bits": plan.info["tile_bits"], "blocks": plan.info["n_blocks"],
-                   "fused_ops": plan.info["n_ops_fused"], "l2": "state 32 GiB >> 126 MB L2 (no flush needed)"},
+                   "passes": P, "tile_bits": info["tile_bits"], "blocks": info["n_blocks"],
+                   "fused_ops": info["n_ops_fused"], "specialised_passes": info["n_jit_passes"],
+                   "l2": "state 32 GiB >> 126 MB L2 (no flush needed)"},
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_pass<5>", "peak_source": src,
+                     "traffic": None, "kernel": kernel, "peak_source": src,
                      "algorithmic_bytes_per_launch": algo_bytes / P},
         "e2e": {"value": ws * ngates / te, "unit": "gates/s", "h2d_bytes_per_step": plan_bytes,
                 "d2h_bytes_per_step": shots * 8},
@@ -376,6 +380,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
     ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")
+    ap.add_argument("--jit", type=int, default=-1,
+                    help="pass specialisation: 0 off, 1 plans >= 26 qubits, 2 all (-1 = library default)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
 
@@ -404,6 +410,9 @@ def main():
     dev = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(dev)
     dist_init(ws, "nccl")
+    if args.jit >= 0:
+        from qsim_b200 import engine as E
+        E.set_jit(args.jit, 0, dev)
     if args.tile_bits or args.block_bits:
         from qsim_b200 import engine as E
         E._h(dev).call("qs_set_tile_bits", int(args.tile_bits))

@@ -78,6 +78,8 @@ typedef struct qs_plan_info {
   double  bytes_moved;   /* HBM bytes: passes * 16 * 2^n                     */
   double  flops;         /* FP32 flop estimate of the program                */
   int64_t n_device_ops;  /* ops in the device program (after merging)       */
+  int32_t n_jit_passes;  /* passes running as specialised kernels           */
+  int32_t reserved;
 } qs_plan_info;
 
 /* ------------------------------------------------------------ context ---- */
@@ -98,6 +100,14 @@ int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
 /* Register-block width used by the planner (2..5 qubits per thread group);
  * 0 = default (5).                                                          */
 int  qs_set_block_bits(qs_handle_t h, int block_bits);
+/* Pass specialisation: plans may compile each tile pass (NVRTC, at its first
+ * execution) into a kernel with its gate positions and coefficients built in;
+ * results are bit-identical to the generic pass kernel.  mode 0 = never,
+ * 1 = plans on >= min_qubits qubits (default 26; 0 keeps the current value),
+ * 2 = every plan.  The default mode comes from the QSIM_JIT environment
+ * variable (0/1/2), else 1.  No reference counterpart (the reference
+ * compiles its kernels ahead of time).                                      */
+int  qs_set_jit(qs_handle_t h, int mode, int min_qubits);
 /* Number of kernels this handle has launched since creation.               */
 int64_t qs_launch_count(qs_handle_t h);
 
@@ -164,6 +174,10 @@ int qs_plan_destroy(qs_plan_t plan);
 /* Host-only dry run of the planner (no device needed): fills `info` for the
  * plan qs_plan_create would build with the given tile bits (0 = default). */
 int qs_plan_analyze(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_info* info);
+/* Host-only check of pass specialisation (no device needed): builds the plan
+ * and compiles every pass with NVRTC without loading it.  Returns QS_OK and
+ * the pass count, or QS_ERR_INVALID with the compiler's message.            */
+int qs_plan_jit_check(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, int block_bits, int* n_passes);
 /* plan + execute in one call (the plan is freed afterwards).               */
 int qs_run_circuit(qs_handle_t h, void* state, int n_qubits, const qs_op* ops, int n_ops);
 

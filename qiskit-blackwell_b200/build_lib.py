@@ -75,7 +75,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             for f in futs:
                 f.result()
     if jobs or not os.path.exists(LIB):
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"]
+        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

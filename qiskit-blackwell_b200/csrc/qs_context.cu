@@ -56,6 +56,7 @@ int qs_create(int device, qs_handle_t* out) {
   QS_CUDA(cudaSetDevice(device));
   h = new qs_context();
   h->device = device;
+  h->jit_mode = qs_jit_env_mode();
   QS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
   QS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
@@ -123,6 +124,16 @@ int qs_set_block_bits(qs_handle_t h, int bb) {
   if (bb == 0) bb = 5;
   QS_CHECK_ARG(bb >= 2 && bb <= 5, "block_bits must be in [2, 5]");
   h->block_bits = bb;
+  QS_API_END(h)
+}
+
+int qs_set_jit(qs_handle_t h, int mode, int min_qubits) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(mode >= 0 && mode <= 2, "jit mode must be 0 (off), 1 (large plans) or 2 (every plan)");
+  QS_CHECK_ARG(min_qubits >= 0 && min_qubits <= QS_MAX_QUBITS, "min_qubits out of range");
+  h->jit_mode = mode;
+  if (min_qubits > 0) h->jit_min_qubits = min_qubits;
   QS_API_END(h)
 }
 

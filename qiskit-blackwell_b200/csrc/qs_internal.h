@@ -39,6 +39,10 @@ struct qs_context {
   std::string err;
   int tile_bits = 13;
   int block_bits = 5;
+  // Pass specialisation (qs_jit.cpp): 0 off, 1 plans on >= jit_min_qubits,
+  // 2 every plan.
+  int jit_mode = 1;
+  int jit_min_qubits = 26;
   int64_t launches = 0;
 
   // grow-only device scratch (reductions, sampling partials, ...)
@@ -118,6 +122,12 @@ struct __align__(16) DevPass {
 };
 
 // Host-side plan.
+// A tile pass compiled into a kernel of its own (qs_jit.cpp).
+struct JitPass {
+  void* fn = nullptr;  // CUfunction
+  int threads = 0, smem = 0, per_sm = 0;
+};
+
 struct qs_plan_s {
   int n_qubits = 0;
   int tile_bits = 0;
@@ -127,7 +137,18 @@ struct qs_plan_s {
   void* d_blob = nullptr;               // device copy
   int device = 0;
   qs_plan_info info{};
+  bool jit_tried = false;               // specialisation attempted
+  std::vector<JitPass> jit;             // one per pass when specialised
+  std::string jit_err;                  // why specialisation was not used
 };
+
+// Pass specialisation (qs_jit.cpp).
+int qs_jit_env_mode();                                     // QSIM_JIT (default 1)
+bool qs_jit_available(std::string* why);
+std::string qs_jit_source(const qs_plan_s* p, size_t pass);
+bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err);
+bool qs_jit_compile_only(const qs_plan_s* p, std::string& err);         // no GPU needed
+void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, uint64_t ntiles, uint32_t flags);
 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
 void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 5);

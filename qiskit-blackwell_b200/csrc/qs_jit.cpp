@@ -1,0 +1,584 @@
+// qs_jit.cpp — runtime specialisation of tile passes (NVRTC, sm_100a).
+//
+// The tile-pass interpreter (qs_pass.cu) reads its program at run time: op
+// dispatch, runtime register positions and moves between the register array
+// and temporaries cost about as many issue slots as the arithmetic itself.
+// A plan that runs on large states is instead compiled pass by pass into
+// kernels of its own: register positions, swizzled shared-memory offsets,
+// the op sequence and the coefficients (as exact hexadecimal float literals)
+// are compile-time constants, and amplitudes are renamed instead of moved.
+//
+// The generator walks the same device program (DevPass / DevBlock / DevOp /
+// coefficient pool) the interpreter executes and writes out the identical
+// sequence of IEEE operations (the same fmaf / __fmul_rn chains, the same
+// selects), so a specialised pass returns the interpreter's amplitudes bit
+// for bit.  NVRTC and the driver API are opened with dlopen at first use; if
+// either is missing or a compile fails, the plan stays on the interpreter.
+#include "qs_api.h"
+#include <cuda.h>
+#include <nvrtc.h>
+#include <dlfcn.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+// ------------------------------------------------------------ dlopen'd APIs
+struct Api {
+  bool nvrtc_ok = false, driver_ok = false;
+  std::string why_nvrtc, why_driver;
+  decltype(&nvrtcCreateProgram) CreateProgram = nullptr;
+  decltype(&nvrtcCompileProgram) CompileProgram = nullptr;
+  decltype(&nvrtcGetCUBINSize) GetCUBINSize = nullptr;
+  decltype(&nvrtcGetCUBIN) GetCUBIN = nullptr;
+  decltype(&nvrtcGetProgramLogSize) GetProgramLogSize = nullptr;
+  decltype(&nvrtcGetProgramLog) GetProgramLog = nullptr;
+  decltype(&nvrtcDestroyProgram) DestroyProgram = nullptr;
+  decltype(&cuModuleLoadData) ModuleLoadData = nullptr;
+  decltype(&cuModuleGetFunction) ModuleGetFunction = nullptr;
+  decltype(&cuFuncSetAttribute) FuncSetAttribute = nullptr;
+  decltype(&cuLaunchKernel) LaunchKernel = nullptr;
+  decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) Occupancy = nullptr;
+};
+
+Api g_api;
+std::once_flag g_api_once;
+
+template <class F>
+bool sym(void* lib, const char* name, F& f) {
+  f = reinterpret_cast<F>(dlsym(lib, name));
+  return f != nullptr;
+}
+
+// NVRTC (the compiler, usable without a GPU) and the driver API (module
+// loading and launches) are opened separately.
+void load_api() {
+  void* nv = nullptr;
+  for (const char* n : {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"}) {
+    nv = dlopen(n, RTLD_NOW | RTLD_LOCAL);
+    if (nv) break;
+  }
+  if (!nv) {
+    g_api.why_nvrtc = "libnvrtc.so.12 not found";
+  } else if (sym(nv, "nvrtcCreateProgram", g_api.CreateProgram) &&
+             sym(nv, "nvrtcCompileProgram", g_api.CompileProgram) &&
+             sym(nv, "nvrtcGetCUBINSize", g_api.GetCUBINSize) && sym(nv, "nvrtcGetCUBIN", g_api.GetCUBIN) &&
+             sym(nv, "nvrtcGetProgramLogSize", g_api.GetProgramLogSize) &&
+             sym(nv, "nvrtcGetProgramLog", g_api.GetProgramLog) &&
+             sym(nv, "nvrtcDestroyProgram", g_api.DestroyProgram)) {
+    g_api.nvrtc_ok = true;
+  } else {
+    g_api.why_nvrtc = "an NVRTC entry point is missing";
+  }
+  void* cu = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
+  if (!cu) {
+    g_api.why_driver = "libcuda.so.1 not found";
+  } else if (sym(cu, "cuModuleLoadData", g_api.ModuleLoadData) &&
+             sym(cu, "cuModuleGetFunction", g_api.ModuleGetFunction) &&
+             sym(cu, "cuFuncSetAttribute", g_api.FuncSetAttribute) &&
+             sym(cu, "cuLaunchKernel", g_api.LaunchKernel) &&
+             sym(cu, "cuOccupancyMaxActiveBlocksPerMultiprocessor", g_api.Occupancy)) {
+    g_api.driver_ok = true;
+  } else {
+    g_api.why_driver = "a CUDA driver entry point is missing";
+  }
+}
+
+// ------------------------------------------------------------ source text
+// Device helpers: the same operations, in the same order, as qs_common.cuh's
+// cfma2/cfma4 and qs_pass.cu's cmul / rotation / sign-flip code.
+const char* kPrelude = R"(typedef unsigned long long u64;
+typedef unsigned int u32;
+__device__ __forceinline__ u32 phys(u32 i) { return i ^ ((((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 7u) << 1); }
+__device__ __forceinline__ u64 ins0(u64 x, int q) { const u64 lo = x & ((1ull << q) - 1ull); return ((x ^ lo) << 1) | lo; }
+__device__ __forceinline__ u32 ins0w(u32 x, int q) { const u32 lo = x & ((1u << q) - 1u); return ((x ^ lo) << 1) | lo; }
+__device__ __forceinline__ float2 cfma2(float2 g0, float2 a0, float2 g1, float2 a1) {
+  float re = __fmul_rn(g0.x, a0.x); re = fmaf(-g0.y, a0.y, re); re = fmaf(g1.x, a1.x, re); re = fmaf(-g1.y, a1.y, re);
+  float im = __fmul_rn(g0.x, a0.y); im = fmaf(g0.y, a0.x, im); im = fmaf(g1.x, a1.y, im); im = fmaf(g1.y, a1.x, im);
+  return make_float2(re, im);
+}
+__device__ __forceinline__ float2 cfma4(float2 g0, float2 g1, float2 g2, float2 g3,
+                                        float2 a0, float2 a1, float2 a2, float2 a3) {
+  float re = __fmul_rn(g0.x, a0.x); re = fmaf(-g0.y, a0.y, re); re = fmaf(g1.x, a1.x, re); re = fmaf(-g1.y, a1.y, re);
+  re = fmaf(g2.x, a2.x, re); re = fmaf(-g2.y, a2.y, re); re = fmaf(g3.x, a3.x, re); re = fmaf(-g3.y, a3.y, re);
+  float im = __fmul_rn(g0.x, a0.y); im = fmaf(g0.y, a0.x, im); im = fmaf(g1.x, a1.y, im); im = fmaf(g1.y, a1.x, im);
+  im = fmaf(g2.x, a2.y, im); im = fmaf(g2.y, a2.x, im); im = fmaf(g3.x, a3.y, im); im = fmaf(g3.y, a3.x, im);
+  return make_float2(re, im);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -__fmul_rn(a.y, b.y)), fmaf(a.x, b.y, __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float2 ry0(float co, float si, float2 a0, float2 a1) {
+  return make_float2(fmaf(co, a0.x, -__fmul_rn(si, a1.x)), fmaf(co, a0.y, -__fmul_rn(si, a1.y)));
+}
+__device__ __forceinline__ float2 ry1(float co, float si, float2 a0, float2 a1) {
+  return make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
+}
+__device__ __forceinline__ float2 sgn(float2 t, u32 m, int j) {
+  const u32 sb = (m << (31 - j)) & 0x80000000u;
+  return make_float2(__uint_as_float(__float_as_uint(t.x) ^ sb), __uint_as_float(__float_as_uint(t.y) ^ sb));
+}
+)";
+
+// Exact float literal (hexadecimal significand).
+std::string flit(float f) {
+  if (f == 0.0f) return std::signbit(f) ? "(-0.0f)" : "0.0f";
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "(%af)", (double)f);
+  return buf;
+}
+std::string c2(float2 v) { return "make_float2(" + flit(v.x) + ", " + flit(v.y) + ")"; }
+uint64_t bits64(float2 f) {
+  uint32_t lo, hi;
+  std::memcpy(&lo, &f.x, 4);
+  std::memcpy(&hi, &f.y, 4);
+  return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+uint32_t bits32(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+std::string mask_test(uint64_t gm, bool& used) {
+  used = true;
+  return "((gidx & " + std::to_string(gm) + "ull) == " + std::to_string(gm) + "ull)";
+}
+
+// Straight-line register block: amplitude j lives in the SSA value v[j].
+struct Block {
+  std::ostringstream o;
+  std::vector<std::string> v;
+  int fresh = 0;
+  bool uses_g = false;  // an op reads the global amplitude index
+  std::string name(const char* p) { return p + std::to_string(fresh++); }
+  // v[j] := pred ? expr : v[j]   (pred "" = always)
+  void set(int j, const std::string& expr, const std::string& pred) {
+    const std::string n = name("a");
+    if (pred.empty()) o << "      const float2 " << n << " = " << expr << ";\n";
+    else o << "      const float2 " << n << " = " << pred << " ? " << expr << " : " << v[j] << ";\n";
+    v[j] = n;
+  }
+};
+
+int pass_threads(int T, int R) { return std::max(32, std::min(R == 5 ? 128 : 256, 1 << (T - R))); }
+int pass_smem(int T) { return (8 << T) + 2 * 128 * 8; }
+
+void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* coef) {
+  const int J = 1 << R;
+  std::ostringstream& o = G.o;
+  for (int oi = ob; oi < oe; ++oi) {
+    const DevOp& op = ops[oi];
+    const float2* c = coef + op.coef;
+    std::string gp;  // "" = the global-control predicate is always true
+    if (op.gc) {
+      gp = G.name("gp");
+      o << "      const bool " << gp << " = " << mask_test(op.gc, G.uses_g) << ";\n";
+    }
+    // false: a register control is unmet, the amplitudes are left unchanged
+    auto active = [&](int j) { return (j & op.rc) == op.rc; };
+    switch (op.kind) {
+      case DK_U1:
+      case DK_RY:
+      case DK_X:
+      case DK_Y: {
+        const int A = op.t0;
+        for (int j = 0; j < J; ++j) {
+          if (((j >> A) & 1) || !active(j)) continue;
+          const int k = j | (1 << A);
+          const std::string a0 = G.v[j], a1 = G.v[k];
+          if (op.kind == DK_U1) {
+            G.set(j, "cfma2(" + c2(c[0]) + ", " + a0 + ", " + c2(c[1]) + ", " + a1 + ")", gp);
+            G.set(k, "cfma2(" + c2(c[2]) + ", " + a0 + ", " + c2(c[3]) + ", " + a1 + ")", gp);
+          } else if (op.kind == DK_RY) {
+            const std::string cs = flit(c[0].x) + ", " + flit(c[0].y);
+            G.set(j, "ry0(" + cs + ", " + a0 + ", " + a1 + ")", gp);
+            G.set(k, "ry1(" + cs + ", " + a0 + ", " + a1 + ")", gp);
+          } else if (op.kind == DK_X) {
+            if (gp.empty()) {
+              G.v[j] = a1;
+              G.v[k] = a0;
+            } else {
+              G.set(j, a1, gp);
+              G.set(k, a0, gp);
+            }
+          } else {
+            G.set(j, "make_float2(" + a1 + ".y, -" + a1 + ".x)", gp);
+            G.set(k, "make_float2(-" + a0 + ".y, " + a0 + ".x)", gp);
+          }
+        }
+        break;
+      }
+      case DK_KRY:
+      case DK_KU1: {
+        for (int K = 0; K < R; ++K) {
+          if (!((op.t0 >> K) & 1)) continue;
+          for (int j = 0; j < J; ++j) {
+            if ((j >> K) & 1) continue;
+            const int k = j | (1 << K);
+            const std::string a0 = G.v[j], a1 = G.v[k];
+            if (op.kind == DK_KRY) {
+              const std::string cs = flit(c[K].x) + ", " + flit(c[K].y);
+              G.set(j, "ry0(" + cs + ", " + a0 + ", " + a1 + ")", "");
+              G.set(k, "ry1(" + cs + ", " + a0 + ", " + a1 + ")", "");
+            } else {
+              const float2* g = c + 4 * K;
+              G.set(j, "cfma2(" + c2(g[0]) + ", " + a0 + ", " + c2(g[1]) + ", " + a1 + ")", "");
+              G.set(k, "cfma2(" + c2(g[2]) + ", " + a0 + ", " + c2(g[3]) + ", " + a1 + ")", "");
+            }
+          }
+        }
+        break;
+      }
+      case DK_U2:
+      case DK_SWAP: {
+        const int A = op.t0, B = op.t1;
+        for (int j = 0; j < J; ++j) {
+          if ((j & ((1 << A) | (1 << B))) || !active(j)) continue;
+          const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
+          if (op.kind == DK_SWAP) {
+            const std::string a = G.v[j1], b = G.v[j2];
+            if (gp.empty()) {
+              G.v[j1] = b;
+              G.v[j2] = a;
+            } else {
+              G.set(j1, b, gp);
+              G.set(j2, a, gp);
+            }
+            continue;
+          }
+          const std::string args = G.v[j] + ", " + G.v[j1] + ", " + G.v[j2] + ", " + G.v[j3] + ")";
+          const int idx[4] = {j, j1, j2, j3};
+          for (int r = 0; r < 4; ++r)
+            G.set(idx[r], "cfma4(" + c2(c[4 * r]) + ", " + c2(c[4 * r + 1]) + ", " + c2(c[4 * r + 2]) + ", " +
+                              c2(c[4 * r + 3]) + ", " + args, gp);
+        }
+        break;
+      }
+      case DK_DTAB: {
+        // Layout (encode_dtab in qs_plan.cpp): [2^R table if rc&1]
+        // [t0 group factors: mask, w][t1 sign terms: regmask, mask]
+        // [d0 cross terms: regmask, mask, w].
+        const bool table = op.rc & 1;
+        const float2* p = c;
+        const float2* Tt = p;
+        if (table) p += J;
+        const std::string f = G.name("f"), m = G.name("m");
+        o << "      float " << f << "r = 1.f, " << f << "i = 0.f; u32 " << m << " = 0u;\n";
+        for (int k = 0; k < op.t0; ++k, p += 2) {
+          const std::string wx = flit(p[1].x), wy = flit(p[1].y);
+          o << "      if " << mask_test(bits64(p[0]), G.uses_g) << " { const float r_ = fmaf(" << f << "r, " << wx
+            << ", -__fmul_rn(" << f << "i, " << wy << ")); " << f << "i = fmaf(" << f << "r, " << wy
+            << ", __fmul_rn(" << f << "i, " << wx << ")); " << f << "r = r_; }\n";
+        }
+        for (int k = 0; k < op.t1; ++k, p += 2)
+          o << "      if " << mask_test(bits64(p[1]), G.uses_g) << " " << m << " ^= " << bits32(p[0].x) << "u;\n";
+        if (!table && op.t0 == 0) {
+          for (int j = 0; j < J; ++j) G.set(j, "sgn(" + G.v[j] + ", " + m + ", " + std::to_string(j) + ")", "");
+        } else {
+          const std::string fv = "make_float2(" + f + "r, " + f + "i)";
+          for (int j = 0; j < J; ++j) {
+            const std::string t = table ? "cmul(" + c2(Tt[j]) + ", " + fv + ")" : fv;
+            G.set(j, "cmul(" + G.v[j] + ", sgn(" + t + ", " + m + ", " + std::to_string(j) + "))", "");
+          }
+        }
+        for (int k = 0; k < op.d0; ++k, p += 3) {
+          const uint32_t rm = bits32(p[0].x);
+          const std::string xp = G.name("xp");
+          o << "      const bool " << xp << " = " << mask_test(bits64(p[1]), G.uses_g) << ";\n";
+          for (int j = 0; j < J; ++j)
+            if ((rm >> j) & 1u) G.set(j, "cmul(" + G.v[j] + ", " + c2(p[2]) + ")", xp);
+        }
+        break;
+      }
+      default:
+        throw qs_error(QS_ERR_INVALID, "tile-pass specialisation: unknown device op");
+    }
+  }
+}
+
+// One register block as a device function of its own: the whole kernel as
+// one function makes the compiler's cost grow faster than linearly with the
+// number of blocks (a deep QV pass holds 30+ blocks).
+std::string gen_block_fn(int b, const DevBlock& B, int T, int R, int threads, const DevOp* ops, const float2* coef,
+                         bool inline_fn) {
+  const uint32_t ngroups = 1u << (T - R);
+  const int J = 1 << R;
+  auto physh = [](uint32_t i) { return i ^ ((((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 7u) << 1); };
+  std::vector<uint32_t> off(J);
+  for (int j = 0; j < J; ++j) {
+    uint32_t x = 0;
+    for (int k = 0; k < R; ++k)
+      if ((j >> k) & 1) x |= 1u << B.pos[k];
+    off[j] = physh(x);  // phys is linear over GF(2): phys(base|x) = phys(base)^phys(x)
+  }
+  Block G;
+  G.v.resize(J);
+  for (int j = 0; j < J; ++j) G.v[j] = "v" + std::to_string(j);
+  gen_block(G, R, ops, B.op_begin, B.op_end, coef);
+  std::ostringstream o;
+  o << "__device__ " << (inline_fn ? "__forceinline__" : "__noinline__") << " void blk" << b << "(u64 gbase) {\n";
+  o << "  float2* tile = reinterpret_cast<float2*>(smem);\n";
+  if (G.uses_g) {
+    o << "  const u64* dep_lo = reinterpret_cast<const u64*>(smem + " << (8 << T) << ");\n";
+    o << "  const u64* dep_hi = dep_lo + 128;\n";
+  }
+  o << "  #pragma unroll 1\n";
+  o << "  for (u32 g = threadIdx.x; g < " << ngroups << "u; g += " << threads << "u) {\n";
+  o << "      u32 base = g;\n";
+  for (int k = 0; k < R; ++k) o << "      base = ins0w(base, " << (int)B.pos[k] << ");\n";
+  o << "      const u32 pb = phys(base);\n";
+  if (G.uses_g) {
+    // the interpreter evaluates global controls against 0 when the block
+    // was encoded without them (pos[7] == 0)
+    if (B.pos[7] != 0) o << "      const u64 gidx = gbase | dep_lo[base & 127] | dep_hi[base >> 7];\n";
+    else o << "      const u64 gidx = 0ull;\n";
+  }
+  for (int j = 0; j < J; ++j) o << "      const float2 v" << j << " = tile[pb ^ " << off[j] << "u];\n";
+  o << G.o.str();
+  for (int j = 0; j < J; ++j) o << "      tile[pb ^ " << off[j] << "u] = " << G.v[j] << ";\n";
+  o << "  }\n}\n";
+  return o.str();
+}
+
+std::string gen_pass(const DevPass& P, const DevBlock* blocks, const DevOp* ops, const float2* coef, int min_blocks) {
+  const int T = P.T, R = P.R;
+  const int threads = pass_threads(T, R);
+  const bool inline_blocks = P.nblocks <= 4;
+  std::ostringstream s;
+  s << kPrelude;
+  s << "extern __shared__ __align__(16) unsigned char smem[];\n";
+  // dep(i) = sum_k bit_k(i) << S[k], split in two 7-bit tables (host-computed).
+  s << "__device__ const u64 kDep[256] = {";
+  for (int e = 0; e < 256; ++e) {
+    const int part = e >> 7, x = e & 127;
+    uint64_t d = 0;
+    for (int k = 0; k < 7; ++k) {
+      const int kk = part * 7 + k;
+      if (kk < T && ((x >> k) & 1)) d |= 1ull << P.S[kk];
+    }
+    s << (e ? "," : "") << d << "ull";
+  }
+  s << "};\n";
+  for (int b = 0; b < P.nblocks; ++b) s << gen_block_fn(b, blocks[b], T, R, threads, ops, coef, inline_blocks);
+  s << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << min_blocks
+    << ") qs_tile_pass(float2* __restrict__ state, u64 ntiles, u32 flags, u64 nmask) {\n";
+  s << "  float2* tile = reinterpret_cast<float2*>(smem);\n";
+  s << "  u64* dep_lo = reinterpret_cast<u64*>(smem + " << (8 << T) << ");\n";
+  s << "  const u64* dep_hi = dep_lo + 128;\n";
+  s << "  for (int e = threadIdx.x; e < 256; e += " << threads << ") dep_lo[e] = kDep[e];\n";
+  s << "  __syncthreads();\n";
+  s << "  for (u64 t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
+  s << "    u64 gbase = t;\n";
+  for (int k = 0; k < T; ++k) s << "    gbase = ins0(gbase, " << P.S[k] << ");\n";
+  const uint32_t npairs = 1u << (T - 1);
+  s << "    if (flags & 1u) {\n"
+       "      const bool first = (gbase & nmask) == 0ull;\n"
+       "      for (u32 c = threadIdx.x; c < "
+    << npairs << "u; c += " << threads
+    << "u) {\n"
+       "        const u32 i = c << 1;\n"
+       "        const float x = (first && i == 0) ? 1.f : 0.f;\n"
+       "        *reinterpret_cast<float4*>(tile + phys(i)) = make_float4(x, 0.f, 0.f, 0.f);\n"
+       "      }\n"
+       "    } else {\n"
+       "      for (u32 c = threadIdx.x; c < "
+    << npairs << "u; c += " << threads
+    << "u) {\n"
+       "        const u32 i = c << 1;\n"
+       "        const u64 g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];\n"
+       "        const u32 d = (u32)__cvta_generic_to_shared(tile + phys(i));\n"
+       "        asm volatile(\"cp.async.cg.shared.global [%0], [%1], 16;\\n\" :: \"r\"(d), \"l\"(state + g) : \"memory\");\n"
+       "      }\n"
+       "      asm volatile(\"cp.async.commit_group;\\ncp.async.wait_group 0;\\n\" ::: \"memory\");\n"
+       "    }\n"
+       "    __syncthreads();\n";
+  for (int b = 0; b < P.nblocks; ++b) s << "    blk" << b << "(gbase);\n    __syncthreads();\n";
+  s << "    for (u32 c = threadIdx.x; c < " << npairs << "u; c += " << threads
+    << "u) {\n"
+       "      const u32 i = c << 1;\n"
+       "      const u64 g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];\n"
+       "      *reinterpret_cast<float4*>(state + g) = *reinterpret_cast<const float4*>(tile + phys(i));\n"
+       "    }\n"
+       "    __syncthreads();\n"
+       "  }\n"
+       "}\n";
+  return s.str();
+}
+
+uint64_t fnv1a(const std::string& s) {
+  uint64_t h = 1469598103934665603ull;
+  for (unsigned char ch : s) {
+    h ^= ch;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Compiled passes, per device, keyed by a hash of their source (plans of the
+// same circuit share kernels; modules live until the process exits).
+std::mutex g_cache_mu;
+std::unordered_map<uint64_t, std::pair<std::string, JitPass>> g_cache[64];
+
+bool nvrtc_compile(const std::string& src, std::string& cubin, std::string& err) {
+  nvrtcProgram prog = nullptr;
+  if (g_api.CreateProgram(&prog, src.c_str(), "qs_tile_pass.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+    err = "nvrtcCreateProgram failed";
+    return false;
+  }
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=true", "-default-device"};
+  const nvrtcResult rc = g_api.CompileProgram(prog, 4, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t n = 0;
+    g_api.GetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    if (n) g_api.GetProgramLog(prog, &log[0]);
+    err = "NVRTC: " + log.substr(0, 600);
+    g_api.DestroyProgram(&prog);
+    return false;
+  }
+  size_t nb = 0;
+  g_api.GetCUBINSize(prog, &nb);
+  cubin.assign(nb, '\0');
+  g_api.GetCUBIN(prog, &cubin[0]);
+  g_api.DestroyProgram(&prog);
+  return true;
+}
+
+// CTAs per SM that the tile's shared memory allows (228 KiB per SM, 1 KiB
+// reserved per CTA), used as the register-allocation hint.
+int blocks_by_smem(int smem) { return std::max(1, std::min(4, (228 * 1024) / (smem + 1024))); }
+
+}  // namespace
+
+int qs_jit_env_mode() {
+  const char* e = std::getenv("QSIM_JIT");
+  if (!e || !*e) return 1;
+  return std::max(0, std::min(2, std::atoi(e)));
+}
+
+bool qs_jit_available(std::string* why) {
+  std::call_once(g_api_once, load_api);
+  if (why) *why = !g_api.nvrtc_ok ? g_api.why_nvrtc : g_api.why_driver;
+  return g_api.nvrtc_ok && g_api.driver_ok;
+}
+
+// Host-only check: generates and compiles (without loading) every pass.
+bool qs_jit_compile_only(const qs_plan_s* p, std::string& err) {
+  std::call_once(g_api_once, load_api);
+  if (!g_api.nvrtc_ok) {
+    err = g_api.why_nvrtc;
+    return false;
+  }
+  const char* dump = std::getenv("QSIM_JIT_DUMP");  // directory for the generated sources
+  for (size_t i = 0; i < p->pass_offsets.size(); ++i) {
+    const std::string src = qs_jit_source(p, i);
+    if (dump && *dump) {
+      const std::string fn = std::string(dump) + "/pass" + std::to_string(i) + ".cu";
+      if (FILE* f = std::fopen(fn.c_str(), "w")) {
+        std::fwrite(src.data(), 1, src.size(), f);
+        std::fclose(f);
+      }
+    }
+    std::string cubin;
+    if (!nvrtc_compile(src, cubin, err)) return false;
+  }
+  return true;
+}
+
+std::string qs_jit_source(const qs_plan_s* p, size_t i) {
+  const char* base = p->blob.data() + p->pass_offsets[i];
+  const DevPass& P = *reinterpret_cast<const DevPass*>(base);
+  return gen_pass(P, reinterpret_cast<const DevBlock*>(base + P.block_off),
+                  reinterpret_cast<const DevOp*>(base + P.op_off), reinterpret_cast<const float2*>(base + P.coef_off),
+                  blocks_by_smem(pass_smem(P.T)));
+}
+
+// Compiles every pass of the plan: sources are generated and compiled on up
+// to 16 host threads; modules are loaded on the calling thread, which holds
+// the CUDA context.  On failure the plan keeps running on the interpreter and
+// `err` says why.
+bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err) {
+  if (!qs_jit_available(&err)) return false;
+  QS_CHECK_ARG(h->device >= 0 && h->device < 64, "device index out of range");
+  const size_t np = p->pass_offsets.size();
+  std::vector<std::string> srcs(np), cubins(np), errs(np);
+  std::vector<uint64_t> keys(np);
+  std::vector<JitPass> out(np);
+  std::vector<size_t> todo;
+  for (size_t i = 0; i < np; ++i) {
+    srcs[i] = qs_jit_source(p, i);
+    keys[i] = fnv1a(srcs[i]);
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_cache[h->device].find(keys[i]);
+    if (it != g_cache[h->device].end() && it->second.first == srcs[i]) out[i] = it->second.second;
+    else todo.push_back(i);
+  }
+  if (!todo.empty()) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min<unsigned>(std::min(16u, hw), (unsigned)todo.size());
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+      pool.emplace_back([&, t]() {
+        for (size_t k = t; k < todo.size(); k += nt) {
+          const size_t i = todo[k];
+          if (!nvrtc_compile(srcs[i], cubins[i], errs[i]) && errs[i].empty()) errs[i] = "compile failed";
+        }
+      });
+    for (auto& th : pool) th.join();
+    for (size_t i : todo)
+      if (cubins[i].empty()) {
+        err = errs[i];
+        return false;
+      }
+    // The runtime's primary context must be current on this thread.
+    QS_CUDA(cudaSetDevice(h->device));
+    QS_CUDA(cudaFree(nullptr));
+    for (size_t i : todo) {
+      const DevPass& P = *reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i]);
+      CUmodule mod = nullptr;
+      CUfunction fn = nullptr;
+      if (g_api.ModuleLoadData(&mod, cubins[i].data()) != CUDA_SUCCESS ||
+          g_api.ModuleGetFunction(&fn, mod, "qs_tile_pass") != CUDA_SUCCESS) {
+        err = "loading a specialised tile pass failed";
+        return false;
+      }
+      JitPass K;
+      K.fn = fn;
+      K.threads = pass_threads(P.T, P.R);
+      K.smem = pass_smem(P.T);
+      if (g_api.FuncSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, K.smem) != CUDA_SUCCESS ||
+          g_api.Occupancy(&K.per_sm, fn, K.threads, (size_t)K.smem) != CUDA_SUCCESS || K.per_sm < 1) {
+        err = "a specialised tile pass does not fit on an SM";
+        return false;
+      }
+      out[i] = K;
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      g_cache[h->device][keys[i]] = {srcs[i], K};
+    }
+  }
+  p->jit = out;
+  return true;
+}
+
+void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t i, void* state, uint64_t ntiles, uint32_t flags) {
+  const JitPass& K = p->jit[i];
+  float2* st = static_cast<float2*>(state);
+  uint64_t nt = ntiles;
+  uint32_t fl = flags;
+  uint64_t nmask = (1ull << p->n_qubits) - 1ull;
+  void* args[] = {&st, &nt, &fl, &nmask};
+  const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)h->sm_count * (uint64_t)K.per_sm);
+  if (grid == 0) return;
+  const CUresult rc = g_api.LaunchKernel((CUfunction)K.fn, (unsigned)grid, 1, 1, (unsigned)K.threads, 1, 1,
+                                         (unsigned)K.smem, (CUstream)h->stream, args, nullptr);
+  if (rc != CUDA_SUCCESS)
+    throw qs_error(QS_ERR_CUDA, "launch of a specialised tile pass failed (CUresult " + std::to_string((int)rc) + ")");
+  qs_after_launch(h, "qs_tile_pass");
+}

@@ -786,10 +786,29 @@ void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint6
     if (from_zero) QS_CHECK_ARG(qs_state_init_batched(h, state, (int)n_states, n) == QS_OK, h->err.c_str());
     return;
   }
+  // Specialise the passes at the first execution that asks for it (the
+  // compiled kernels are cached by source, so rebuilding a plan of the same
+  // circuit costs only the source generation).
+  const bool want_jit = h->jit_mode == 2 || (h->jit_mode == 1 && n >= h->jit_min_qubits);
+  if (want_jit && !p->jit_tried) {
+    p->jit_tried = true;
+    std::string why;
+    if (!qs_jit_compile_plan(h, p, why)) {
+      p->jit.clear();
+      p->jit_err = why;
+      if (std::getenv("QSIM_JIT_VERBOSE")) std::fprintf(stderr, "qsim: pass specialisation off: %s\n", why.c_str());
+    }
+    p->info.n_jit_passes = (int32_t)p->jit.size();
+  }
+  const bool use_jit = want_jit && p->jit.size() == p->pass_offsets.size();
   for (size_t i = 0; i < p->pass_offsets.size(); ++i) {
-    const DevPass* dp = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
     const int T = p->pass_T[i];
     const uint32_t flags = (from_zero && i == 0) ? PI_FROM_ZERO : 0u;
+    if (use_jit) {
+      qs_jit_launch(h, p, i, state, n_states << (n - T), flags);
+      continue;
+    }
+    const DevPass* dp = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
     qs_launch_pass_single(h, state, dp, T, p->pass_R[i], n_states << (n - T), flags, p->pass_has2[i],
                           p->pass_ncoef[i]);
   }
@@ -831,6 +850,21 @@ int qs_plan_analyze(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_in
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p);
   *info = p.info;
+  QS_API_END(h)
+}
+
+int qs_plan_jit_check(int n, const qs_op* ops, int nops, int tile_bits, int block_bits, int* n_passes) {
+  qs_context* h = nullptr;
+  QS_API_BEGIN
+  if (tile_bits == 0) tile_bits = 13;
+  if (block_bits == 0) block_bits = 5;
+  QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
+  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
+  qs_plan_s p;
+  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits);
+  std::string err;
+  if (!qs_jit_compile_only(&p, err)) throw qs_error(QS_ERR_INVALID, "pass specialisation: " + err);
+  if (n_passes) *n_passes = (int)p.pass_offsets.size();
   QS_API_END(h)
 }
 

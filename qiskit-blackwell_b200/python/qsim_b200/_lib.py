@@ -33,7 +33,8 @@ class QsOp(C.Structure):
 class QsPlanInfo(C.Structure):
     _fields_ = [("n_qubits", C.c_int32), ("tile_bits", C.c_int32), ("n_passes", C.c_int32),
                 ("n_blocks", C.c_int32), ("n_ops_in", C.c_int64), ("n_ops_fused", C.c_int64),
-                ("bytes_moved", C.c_double), ("flops", C.c_double), ("n_device_ops", C.c_int64)]
+                ("bytes_moved", C.c_double), ("flops", C.c_double), ("n_device_ops", C.c_int64),
+                ("n_jit_passes", C.c_int32), ("reserved", C.c_int32)]
 
 
 class QsBatchInfo(C.Structure):
@@ -75,6 +76,7 @@ SIGNATURES = {
     "qs_version": (C.c_char_p, []),
     "qs_set_tile_bits": (_i, [_vp, _i]),
     "qs_set_block_bits": (_i, [_vp, _i]),
+    "qs_set_jit": (_i, [_vp, _i, _i]),
     "qs_launch_count": (_i64, [_vp]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
     "qs_state_init_basis": (_i, [_vp, _vp, _i, _u64]),
@@ -98,6 +100,7 @@ SIGNATURES = {
     "qs_plan_execute_from_zero": (_i, [_vp, _vp, _vp]),
     "qs_plan_destroy": (_i, [_vp]),
     "qs_plan_analyze": (_i, [_i, _pop, _i, _i, C.POINTER(QsPlanInfo)]),
+    "qs_plan_jit_check": (_i, [_i, _pop, _i, _i, _i, C.POINTER(C.c_int)]),
     "qs_run_circuit": (_i, [_vp, _vp, _i, _pop, _i]),
     "qs_norm2": (_i, [_vp, _vp, _i, _pd]),
     "qs_renorm": (_i, [_vp, _vp, _i]),

@@ -37,6 +37,12 @@ def _h(device: int | None = None) -> _lib.Handle:
     return _lib.handle(dev, torch.cuda.current_stream(dev).cuda_stream)
 
 
+def set_jit(mode: int, min_qubits: int = 0, device: int | None = None) -> None:
+    """Pass specialisation for plans executed by this thread's handle:
+    0 = never, 1 = plans on >= min_qubits qubits, 2 = every plan."""
+    _h(device).call("qs_set_jit", int(mode), int(min_qubits))
+
+
 def _ptr(t: torch.Tensor) -> C.c_void_p:
     return C.c_void_p(t.data_ptr())
 
@@ -82,9 +88,14 @@ class Plan:
         out = C.c_void_p()
         self._h.call("qs_plan_create", self.n, p, int(len(self.ops)), C.byref(out))
         self.ptr = out
+        self.info = self.refresh_info()
+
+    def refresh_info(self) -> dict:
+        """Planner statistics; n_jit_passes is set at the first execution."""
         info = QsPlanInfo()
         _lib.check(self.L.qs_plan_info_get(self.ptr, C.byref(info)))
         self.info = {k: getattr(info, k) for k, _ in QsPlanInfo._fields_}
+        return self.info
 
     def __del__(self):
         try:

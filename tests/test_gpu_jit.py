@@ -1,0 +1,91 @@
+"""Specialised tile passes (NVRTC) against the generic pass kernel and the
+FP64 oracle: the specialised kernels must return the interpreter's
+amplitudes bit for bit, for every device-op kind, tile width and
+register-block width, from a given state and from |0..0>."""
+import numpy as np
+import pytest
+import torch
+
+import sv_oracle as O
+from qsim_b200 import engine as E
+from qsim_b200 import workloads as W
+from test_oracle_golden import _random_ops
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(n, ops, mode, psi0=None, tile_bits=0, block_bits=0):
+    h = E._h()
+    h.call("qs_set_tile_bits", tile_bits)
+    h.call("qs_set_block_bits", block_bits)
+    E.set_jit(mode)
+    try:
+        plan = E.Plan(n, ops)
+        s = E.empty_state(n)
+        if psi0 is None:
+            plan.execute_from_zero(s)
+        else:
+            s.copy_(torch.from_numpy(psi0))
+            plan.execute(s)
+        torch.cuda.synchronize()
+        return s.cpu().numpy(), plan.refresh_info()
+    finally:
+        E.set_jit(1)
+        h.call("qs_set_tile_bits", 0)
+        h.call("qs_set_block_bits", 0)
+
+
+def _same_bits(a, b):
+    return np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("n,tile_bits,block_bits", [(6, 10, 5), (13, 10, 4), (15, 12, 3), (17, 13, 5),
+                                                    (18, 14, 5), (17, 10, 2)])
+def test_random_all_kinds_bit_identical(n, tile_bits, block_bits):
+    rng = np.random.default_rng(5000 + n)
+    ops = _random_ops(n, 100, rng)
+    psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi0 = (psi0 / np.linalg.norm(psi0)).astype(np.complex64)
+    ref, info0 = _run(n, ops, 0, psi0, tile_bits, block_bits)
+    got, info2 = _run(n, ops, 2, psi0, tile_bits, block_bits)
+    assert info0["n_jit_passes"] == 0
+    assert info2["n_jit_passes"] == info2["n_passes"] >= 1
+    assert _same_bits(ref, got)
+    exact = O.simulate(n, ops, psi0.astype(np.complex128))
+    assert abs(1 - O.fidelity(got, exact)) <= 1e-6
+
+
+@pytest.mark.parametrize("tile_bits,block_bits", [(10, 5), (13, 4), (13, 5)])
+def test_layers_from_zero_bit_identical(tile_bits, block_bits):
+    ops = W.layers_ops(20, 8, seed=3)
+    ref, _ = _run(20, ops, 0, None, tile_bits, block_bits)
+    got, info = _run(20, ops, 2, None, tile_bits, block_bits)
+    assert info["n_jit_passes"] == info["n_passes"] > 1
+    assert _same_bits(ref, got)
+    assert abs(1 - O.fidelity(got, O.simulate(20, ops))) <= 1e-6
+
+
+def test_qv_bit_identical():
+    ops = W.qv_ops(14, 14, 7)
+    ref, _ = _run(14, ops, 0)
+    got, info = _run(14, ops, 2)
+    assert info["n_jit_passes"] == info["n_passes"]
+    assert _same_bits(ref, got)
+
+
+def test_auto_mode_threshold():
+    """Mode 1 specialises only plans at or above the qubit threshold."""
+    ops = W.layers_ops(16, 2, seed=1)
+    E.set_jit(1, 17)
+    try:
+        plan = E.Plan(16, ops)
+        plan.execute_from_zero(E.empty_state(16))
+        torch.cuda.synchronize()
+        assert plan.refresh_info()["n_jit_passes"] == 0
+        E.set_jit(1, 16)
+        plan2 = E.Plan(16, ops)
+        plan2.execute_from_zero(E.empty_state(16))
+        torch.cuda.synchronize()
+        assert plan2.refresh_info()["n_jit_passes"] == plan2.info["n_passes"]
+    finally:
+        E.set_jit(1, 26)
