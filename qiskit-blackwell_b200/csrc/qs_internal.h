@@ -78,9 +78,14 @@ enum DevKind : uint8_t {
   DK_RY = 10,    // real rotation [[c, -s], [s, c]] on t0; c[0] = (c, s)
   DK_DTAB = 11,  // merged diagonal: table over the register bits x group
                  // factor x sign mask (layout in qs_pass.cu, encode_dtab)
-  DK_KRY = 12,   // one real rotation per register bit (c[k] = (c, s); identity
-                 // where t0's bit k is clear), applied as a Kronecker product
+  DK_KRY = 12,   // one scaled real rotation per register bit set in t0, applied
+                 // as a Kronecker product; c[k] = (t, form):
+                 //   form 0: (a0, a1) <- (a0 - t a1, a1 + t a0)   [rotation / c]
+                 //   form 1: (a0, a1) <- (t a0 - a1, a0 + t a1)   [rotation / s]
+                 // (one FMA per component); the dropped positive factor (c or
+                 // s) is folded into a later table op or DK_SCALE of the pass
   DK_KU1 = 13,   // one dense 2x2 per register bit (c[4k..4k+3]), likewise
+  DK_SCALE = 14, // multiply every amplitude by the real c[0].x
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values

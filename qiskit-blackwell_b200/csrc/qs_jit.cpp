@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <sstream>
 #include <thread>
@@ -121,9 +122,17 @@ __device__ __forceinline__ float2 ry0(float co, float si, float2 a0, float2 a1) 
 __device__ __forceinline__ float2 ry1(float co, float si, float2 a0, float2 a1) {
   return make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
 }
-__device__ __forceinline__ float2 sgn(float2 t, u32 m, int j) {
-  const u32 sb = (m << (31 - j)) & 0x80000000u;
-  return make_float2(__uint_as_float(__float_as_uint(t.x) ^ sb), __uint_as_float(__float_as_uint(t.y) ^ sb));
+// Scaled rotations (DK_KRY) as packed FP32x2 FMAs: one instruction per
+// output amplitude, lane results identical to the scalar fmaf.
+__device__ __forceinline__ float2 rta0(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(-t, -t), a1, a0); }
+__device__ __forceinline__ float2 rta1(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(t, t), a0, a1); }
+__device__ __forceinline__ float2 rtb0(float t, float2 a0, float2 a1) {
+  return __ffma2_rn(make_float2(t, t), a0, make_float2(-a1.x, -a1.y));
+}
+__device__ __forceinline__ float2 rtb1(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(t, t), a1, a0); }
+__device__ __forceinline__ float2 scl(float2 a, float f) { return make_float2(__fmul_rn(a.x, f), __fmul_rn(a.y, f)); }
+__device__ __forceinline__ float2 sgnw(float2 t, u32 w) {
+  return make_float2(__uint_as_float(__float_as_uint(t.x) ^ w), __uint_as_float(__float_as_uint(t.y) ^ w));
 }
 )";
 
@@ -167,7 +176,15 @@ struct Block {
   }
 };
 
-int pass_threads(int T, int R) { return std::max(32, std::min(R == 5 ? 128 : 256, 1 << (T - R))); }
+// Threads per CTA: one register group per thread, at most 128 for R = 5
+// blocks (QSIM_JIT_THREADS = 256 allows 256) and 256 otherwise.
+int pass_threads(int T, int R) {
+  static const int cap5 = [] {
+    const char* e = std::getenv("QSIM_JIT_THREADS");
+    return (e && std::atoi(e) == 256) ? 256 : 128;
+  }();
+  return std::max(32, std::min(R == 5 ? cap5 : 256, 1 << (T - R)));
+}
 int pass_smem(int T) { return (8 << T) + 2 * 128 * 8; }
 
 void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* coef) {
@@ -223,10 +240,11 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
             if ((j >> K) & 1) continue;
             const int k = j | (1 << K);
             const std::string a0 = G.v[j], a1 = G.v[k];
-            if (op.kind == DK_KRY) {
-              const std::string cs = flit(c[K].x) + ", " + flit(c[K].y);
-              G.set(j, "ry0(" + cs + ", " + a0 + ", " + a1 + ")", "");
-              G.set(k, "ry1(" + cs + ", " + a0 + ", " + a1 + ")", "");
+            if (op.kind == DK_KRY) {  // scaled rotation, form c[K].y (see DK_KRY)
+              const std::string t = flit(c[K].x) + ", " + a0 + ", " + a1 + ")";
+              const bool fb = c[K].y != 0.f;
+              G.set(j, (fb ? "rtb0(" : "rta0(") + t, "");
+              G.set(k, (fb ? "rtb1(" : "rta1(") + t, "");
             } else {
               const float2* g = c + 4 * K;
               G.set(j, "cfma2(" + c2(g[0]) + ", " + a0 + ", " + c2(g[1]) + ", " + a1 + ")", "");
@@ -236,6 +254,9 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         }
         break;
       }
+      case DK_SCALE:
+        for (int j = 0; j < J; ++j) G.set(j, "scl(" + G.v[j] + ", " + flit(c[0].x) + ")", "");
+        break;
       case DK_U2:
       case DK_SWAP: {
         const int A = op.t0, B = op.t1;
@@ -269,23 +290,73 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         const float2* p = c;
         const float2* Tt = p;
         if (table) p += J;
-        const std::string f = G.name("f"), m = G.name("m");
-        o << "      float " << f << "r = 1.f, " << f << "i = 0.f; u32 " << m << " = 0u;\n";
+        const std::string f = G.name("f");
+        if (op.t0) o << "      float " << f << "r = 1.f, " << f << "i = 0.f;\n";
         for (int k = 0; k < op.t0; ++k, p += 2) {
           const std::string wx = flit(p[1].x), wy = flit(p[1].y);
           o << "      if " << mask_test(bits64(p[0]), G.uses_g) << " { const float r_ = fmaf(" << f << "r, " << wx
             << ", -__fmul_rn(" << f << "i, " << wy << ")); " << f << "i = fmaf(" << f << "r, " << wy
             << ", __fmul_rn(" << f << "i, " << wx << ")); " << f << "r = r_; }\n";
         }
-        for (int k = 0; k < op.t1; ++k, p += 2)
-          o << "      if " << mask_test(bits64(p[1]), G.uses_g) << " " << m << " ^= " << bits32(p[0].x) << "u;\n";
+        // Sign terms: amplitude j is negated by the XOR of the predicates of
+        // the terms whose register mask holds j.  Each distinct set of terms
+        // gets one sign word per group; the word is XORed into the group
+        // factor (or the table entry, or the amplitude) - the same bits the
+        // generic kernel produces with its per-group mask.
+        std::vector<uint32_t> rms;
+        std::vector<std::string> sb;
+        for (int k = 0; k < op.t1; ++k, p += 2) {
+          rms.push_back(bits32(p[0].x));
+          sb.push_back(G.name("sb"));
+          o << "      const u32 " << sb.back() << " = " << mask_test(bits64(p[1]), G.uses_g)
+            << " ? 0x80000000u : 0u;\n";
+        }
+        std::map<uint32_t, std::string> word;  // term subset -> sign word
+        auto subset = [&](int j) {
+          uint32_t sub = 0;
+          for (size_t k = 0; k < rms.size(); ++k)
+            if ((rms[k] >> j) & 1u) sub |= 1u << k;
+          return sub;
+        };
+        auto sign_word = [&](uint32_t sub) -> std::string {
+          auto it = word.find(sub);
+          if (it != word.end()) return it->second;
+          std::string e;
+          for (size_t k = 0; k < rms.size(); ++k)
+            if ((sub >> k) & 1u) e += (e.empty() ? "" : " ^ ") + sb[k];
+          const std::string w = G.name("sw");
+          o << "      const u32 " << w << " = " << e << ";\n";
+          word[sub] = w;
+          return w;
+        };
         if (!table && op.t0 == 0) {
-          for (int j = 0; j < J; ++j) G.set(j, "sgn(" + G.v[j] + ", " + m + ", " + std::to_string(j) + ")", "");
+          for (int j = 0; j < J; ++j) {
+            const uint32_t sub = subset(j);
+            if (sub) G.set(j, "sgnw(" + G.v[j] + ", " + sign_word(sub) + ")", "");
+          }
+        } else if (op.t0 == 0) {  // table only: the group factor is exactly 1
+          for (int j = 0; j < J; ++j) {
+            const uint32_t sub = subset(j);
+            const std::string t = sub ? "sgnw(" + c2(Tt[j]) + ", " + sign_word(sub) + ")" : c2(Tt[j]);
+            G.set(j, "cmul(" + G.v[j] + ", " + t + ")", "");
+          }
         } else {
           const std::string fv = "make_float2(" + f + "r, " + f + "i)";
+          std::map<uint32_t, std::string> fs;  // term subset -> sign-adjusted group factor
           for (int j = 0; j < J; ++j) {
-            const std::string t = table ? "cmul(" + c2(Tt[j]) + ", " + fv + ")" : fv;
-            G.set(j, "cmul(" + G.v[j] + ", sgn(" + t + ", " + m + ", " + std::to_string(j) + "))", "");
+            const uint32_t sub = subset(j);
+            std::string fj = fv;
+            if (sub) {
+              auto it = fs.find(sub);
+              if (it == fs.end()) {
+                const std::string w = sign_word(sub), n = G.name("fs");
+                o << "      const float2 " << n << " = sgnw(" << fv << ", " << w << ");\n";
+                it = fs.emplace(sub, n).first;
+              }
+              fj = it->second;
+            }
+            const std::string t = table ? "cmul(" + c2(Tt[j]) + ", " + fj + ")" : fj;
+            G.set(j, "cmul(" + G.v[j] + ", " + t + ")", "");
           }
         }
         for (int k = 0; k < op.d0; ++k, p += 3) {
@@ -340,9 +411,27 @@ std::string gen_block_fn(int b, const DevBlock& B, int T, int R, int threads, co
     if (B.pos[7] != 0) o << "      const u64 gidx = gbase | dep_lo[base & 127] | dep_hi[base >> 7];\n";
     else o << "      const u64 gidx = 0ull;\n";
   }
-  for (int j = 0; j < J; ++j) o << "      const float2 v" << j << " = tile[pb ^ " << off[j] << "u];\n";
+  // Address of amplitude j: pb ^ off[j] = (pb ^ lo) + hi with lo = off[j] & 15
+  // and hi = off[j] - lo, because pb is zero at the register bits (the
+  // swizzle only rewrites bits 1..3).  The XOR then depends on at most 16
+  // distinct lo values per group and hi becomes the load's immediate offset.
+  std::map<uint32_t, std::string> lo_addr;
+  auto addr = [&](int j) {
+    const uint32_t lo = off[j] & 15u, hi = off[j] & ~15u;
+    auto it = lo_addr.find(lo);
+    if (it == lo_addr.end()) {
+      const std::string n = "pa" + std::to_string(lo);
+      o << "      const u32 " << n << " = pb ^ " << lo << "u;\n";
+      it = lo_addr.emplace(lo, n).first;
+    }
+    return it->second + " + " + std::to_string(hi) + "u";
+  };
+  for (int j = 0; j < J; ++j) {
+    const std::string a = addr(j);
+    o << "      const float2 v" << j << " = tile[" << a << "];\n";
+  }
   o << G.o.str();
-  for (int j = 0; j < J; ++j) o << "      tile[pb ^ " << off[j] << "u] = " << G.v[j] << ";\n";
+  for (int j = 0; j < J; ++j) o << "      tile[" << addr(j) << "] = " << G.v[j] << ";\n";
   o << "  }\n}\n";
   return o.str();
 }
@@ -451,9 +540,14 @@ bool nvrtc_compile(const std::string& src, std::string& cubin, std::string& err)
   return true;
 }
 
-// CTAs per SM that the tile's shared memory allows (228 KiB per SM, 1 KiB
-// reserved per CTA), used as the register-allocation hint.
-int blocks_by_smem(int smem) { return std::max(1, std::min(4, (228 * 1024) / (smem + 1024))); }
+// Register-allocation hint: the CTAs per SM that the tile's shared memory
+// allows (228 KiB per SM, 1 KiB reserved per CTA), capped so that a thread
+// keeps at least 128 registers.
+int min_blocks_for(int smem, int threads) {
+  const int by_smem = (228 * 1024) / (smem + 1024);
+  const int by_regs = 65536 / (threads * 128);
+  return std::max(1, std::min(std::min(4, by_smem), by_regs));
+}
 
 }  // namespace
 
@@ -497,7 +591,7 @@ std::string qs_jit_source(const qs_plan_s* p, size_t i) {
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
   return gen_pass(P, reinterpret_cast<const DevBlock*>(base + P.block_off),
                   reinterpret_cast<const DevOp*>(base + P.op_off), reinterpret_cast<const float2*>(base + P.coef_off),
-                  blocks_by_smem(pass_smem(P.T)));
+                  min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R)));
 }
 
 // Compiles every pass of the plan: sources are generated and compiled on up

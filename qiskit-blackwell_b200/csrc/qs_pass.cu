@@ -196,18 +196,31 @@ __device__ __forceinline__ void op_swap(float2 (&v)[1 << R], unsigned rc, bool g
   }
 }
 
-// Kronecker layer: a rotation on every register bit set in `mask`, fully
-// unrolled at compile-time positions; one dispatch for up to R gates.
+// Kronecker layer: a scaled rotation on every register bit set in `mask`
+// (c[k] = (t, form), see DK_KRY), fully unrolled at compile-time positions;
+// one dispatch for up to R gates, one FMA per output component.
 template <int R, int K>
-__device__ __forceinline__ void kry_stage(float2 (&v)[1 << R], float2 cs) {
-  const float co = cs.x, si = cs.y;
+__device__ __forceinline__ void kry_stage(float2 (&v)[1 << R], float2 tf) {
+  // packed FP32x2 FMAs; each lane is the scalar fmaf of the same operands
+  const float2 tt = make_float2(tf.x, tf.x), nt = make_float2(-tf.x, -tf.x);
+  if (tf.y == 0.f) {
 #pragma unroll
-  for (int j = 0; j < (1 << R); ++j) {
-    if (j & (1 << K)) continue;
-    const int k = j | (1 << K);
-    const float2 a0 = v[j], a1 = v[k];
-    v[j] = make_float2(fmaf(co, a0.x, -__fmul_rn(si, a1.x)), fmaf(co, a0.y, -__fmul_rn(si, a1.y)));
-    v[k] = make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << K)) continue;
+      const int k = j | (1 << K);
+      const float2 a0 = v[j], a1 = v[k];
+      v[j] = __ffma2_rn(nt, a1, a0);
+      v[k] = __ffma2_rn(tt, a0, a1);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << K)) continue;
+      const int k = j | (1 << K);
+      const float2 a0 = v[j], a1 = v[k];
+      v[j] = __ffma2_rn(tt, a0, make_float2(-a1.x, -a1.y));
+      v[k] = __ffma2_rn(tt, a1, a0);
+    }
   }
 }
 
@@ -226,19 +239,17 @@ __device__ __forceinline__ void ku1_stage(float2 (&v)[1 << R], const float2* __r
 
 template <int R>
 __device__ __forceinline__ void op_kry(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned mask) {
-  if (mask == (1u << R) - 1u) {  // full layer: straight-line code
-    if constexpr (R > 0) kry_stage<R, 0>(v, c[0]);
-    if constexpr (R > 1) kry_stage<R, 1>(v, c[1]);
-    if constexpr (R > 2) kry_stage<R, 2>(v, c[2]);
-    if constexpr (R > 3) kry_stage<R, 3>(v, c[3]);
-    if constexpr (R > 4) kry_stage<R, 4>(v, c[4]);
-    return;
-  }
   if constexpr (R > 0) if (mask & 1u) kry_stage<R, 0>(v, c[0]);
   if constexpr (R > 1) if (mask & 2u) kry_stage<R, 1>(v, c[1]);
   if constexpr (R > 2) if (mask & 4u) kry_stage<R, 2>(v, c[2]);
   if constexpr (R > 3) if (mask & 8u) kry_stage<R, 3>(v, c[3]);
   if constexpr (R > 4) if (mask & 16u) kry_stage<R, 4>(v, c[4]);
+}
+
+template <int R>
+__device__ __forceinline__ void op_scale(float2 (&v)[1 << R], float f) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) v[j] = make_float2(__fmul_rn(v[j].x, f), __fmul_rn(v[j].y, f));
 }
 
 template <int R>
@@ -288,15 +299,21 @@ __device__ __forceinline__ void op_dtab(float2 (&v)[1 << R], const DevOp& op, co
       v[j].x = __uint_as_float(__float_as_uint(v[j].x) ^ sb);
       v[j].y = __uint_as_float(__float_as_uint(v[j].y) ^ sb);
     }
-  } else {
+  } else if (op.t0 == 0) {  // table only: the group factor is exactly 1
 #pragma unroll
-  for (int j = 0; j < (1 << R); ++j) {
-    float2 t = table ? cmul(T[j], f) : f;
-    const uint32_t sb = (m << (31 - j)) & 0x80000000u;
-    t.x = __uint_as_float(__float_as_uint(t.x) ^ sb);
-    t.y = __uint_as_float(__float_as_uint(t.y) ^ sb);
-    v[j] = cmul(v[j], t);
-  }
+    for (int j = 0; j < (1 << R); ++j) {
+      const uint32_t sb = (m << (31 - j)) & 0x80000000u;
+      const float2 t = make_float2(__uint_as_float(__float_as_uint(T[j].x) ^ sb),
+                                   __uint_as_float(__float_as_uint(T[j].y) ^ sb));
+      v[j] = cmul(v[j], t);
+    }
+  } else {  // the sign goes onto the group factor, before the table product
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      const uint32_t sb = (m << (31 - j)) & 0x80000000u;
+      const float2 fs = make_float2(__uint_as_float(__float_as_uint(f.x) ^ sb), __uint_as_float(__float_as_uint(f.y) ^ sb));
+      v[j] = cmul(v[j], table ? cmul(T[j], fs) : fs);
+    }
   }
   for (int k = 0; k < op.d0; ++k) {
     const uint32_t rm = __float_as_uint(p[0].x);
@@ -359,6 +376,9 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
         break;
       case DK_KU1:
         op_ku1<R>(v, c, op.t0);
+        break;
+      case DK_SCALE:
+        op_scale<R>(v, c[0].x);
         break;
       case DK_U2:
         if constexpr (TWO) {

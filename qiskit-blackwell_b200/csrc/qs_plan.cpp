@@ -432,8 +432,10 @@ void diag_terms(const IOp& o, std::vector<DTerm>& t) {
 // amplitude j of a group with global index gidx is multiplied by
 //   T[j] * prod_{group terms, gidx has gmask} w * prod_{cross, j in regmask, gidx has gmask} w
 // and negated where the XOR of the active sign terms' regmasks has bit j.
+// `scale` is the pass's pending real factor (dropped by scaled rotations); it
+// is folded into the table when the op has one (FP64, rounded once).
 void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, int R,
-                 std::vector<DevOp>& dops, std::vector<float>& coef, bool& need_g) {
+                 std::vector<DevOp>& dops, std::vector<float>& coef, bool& need_g, double& scale) {
   uint64_t rmask_all = 0;
   for (int k = 0; k < R; ++k) rmask_all |= 1ull << regq[k];
   const int J = 1 << R;
@@ -473,6 +475,10 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
   bool table = false;
   for (int j = 0; j < J; ++j) table |= (T[j] != 1.0);
   if (!table && gl.empty() && sterm.empty() && xterm.empty()) return;  // identity
+  if (table && scale != 1.0) {
+    for (int j = 0; j < J; ++j) T[j] *= scale;
+    scale = 1.0;
+  }
   // split into several ops if a count would overflow its 8-bit field
   size_t gi = 0, si = 0, xi = 0;
   bool first = true;
@@ -555,6 +561,18 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   std::vector<DevOp> dops;
   std::vector<float> coef;  // float2 pool, re/im
   int has2 = 0;
+  double pend_scale = 1.0;  // product of the factors dropped by scaled rotations
+  auto emit_scale = [&]() {
+    DevOp d;
+    std::memset(&d, 0, sizeof(d));
+    d.kind = DK_SCALE;
+    d.ncoef = 1;
+    d.coef = (uint32_t)(coef.size() / 2);
+    coef.push_back((float)pend_scale);
+    coef.push_back(0.f);
+    dops.push_back(d);
+    pend_scale = 1.0;
+  };
   for (Blk& b : blks) {
     // pad to R positions with the lowest unused tile positions
     for (int p = 0; (int)b.regs.size() < R && p < T; ++p)
@@ -576,7 +594,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
     std::vector<DTerm> run;  // pending diagonal run
     auto flush_run = [&]() {
       if (run.empty()) return;
-      encode_dtab(run, regq, R, dops, coef, need_g);
+      encode_dtab(run, regq, R, dops, coef, need_g, pend_scale);
       run.clear();
     };
     // pending Kronecker layer: uncontrolled 1Q rotations / dense gates on
@@ -584,35 +602,38 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
     std::vector<std::pair<int, IOp>> kron;  // (register bit, op)
     auto flush_kron = [&]() {
       if (kron.empty()) return;
-      bool all_ry = true;
-      for (auto& kv : kron) all_ry &= (kv.second.kind == I_RY);
-      DevOp d;
-      std::memset(&d, 0, sizeof(d));
-      unsigned mask = 0;
-      for (auto& kv : kron) mask |= 1u << kv.first;
-      d.kind = all_ry ? DK_KRY : DK_KU1;
-      d.t0 = (uint8_t)mask;
-      d.coef = (uint32_t)(coef.size() / 2);
-      const int per = all_ry ? 1 : 4;
-      std::vector<cd> slots((size_t)R * per, cd(0.0, 0.0));
-      for (int k = 0; k < R; ++k) {  // identity defaults
-        if (all_ry) slots[k] = cd(1.0, 0.0);
-        else { slots[4 * k] = 1.0; slots[4 * k + 3] = 1.0; }
-      }
+      // rotations -> one DK_KRY (scaled form), dense 2x2s -> one DK_KU1;
+      // they act on distinct register bits, so their order is free
+      unsigned rmask = 0, umask = 0;
+      std::vector<cd> rslot((size_t)R, cd(0.0, 0.0)), uslot((size_t)R * 4, cd(0.0, 0.0));
+      for (int k = 0; k < R; ++k) { uslot[4 * k] = 1.0; uslot[4 * k + 3] = 1.0; }
       for (auto& kv : kron) {
         const IOp& g = kv.second;
         const int k = kv.first;
-        if (all_ry) slots[k] = g.m[0];
-        else if (g.kind == I_RY) {
-          const double c = g.m[0].real(), sn = g.m[0].imag();
-          slots[4 * k] = c; slots[4 * k + 1] = -sn; slots[4 * k + 2] = sn; slots[4 * k + 3] = c;
+        if (g.kind == I_RY) {
+          const double c = g.m[0].real(), sn = g.m[0].imag();  // both > 0
+          if (c >= sn) { rslot[k] = cd(sn / c, 0.0); pend_scale *= c; }
+          else { rslot[k] = cd(c / sn, 1.0); pend_scale *= sn; }
+          rmask |= 1u << k;
         } else {
-          for (int i = 0; i < 4; ++i) slots[4 * k + i] = g.m[i];
+          for (int i = 0; i < 4; ++i) uslot[4 * k + i] = g.m[i];
+          umask |= 1u << k;
         }
       }
-      for (const cd& v : slots) { coef.push_back((float)v.real()); coef.push_back((float)v.imag()); }
-      d.ncoef = (uint8_t)slots.size();
-      dops.push_back(d);
+      auto put_op = [&](DevKind kind, unsigned mask, const std::vector<cd>& slots) {
+        DevOp d;
+        std::memset(&d, 0, sizeof(d));
+        d.kind = kind;
+        d.t0 = (uint8_t)mask;
+        d.coef = (uint32_t)(coef.size() / 2);
+        for (const cd& v : slots) { coef.push_back((float)v.real()); coef.push_back((float)v.imag()); }
+        d.ncoef = (uint8_t)slots.size();
+        dops.push_back(d);
+      };
+      if (rmask) put_op(DK_KRY, rmask, rslot);
+      if (umask) put_op(DK_KU1, umask, uslot);
+      // keep intermediate amplitudes far from the FP32 range limits
+      if (pend_scale < 0x1p-40) emit_scale();
       kron.clear();
     };
     for (int idx : b.ops) {
@@ -667,6 +688,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
     }
     flush_kron();
     flush_run();
+    if (&b == &blks.back() && pend_scale != 1.0) emit_scale();  // every amplitude gets it once
     db.op_end = (int32_t)dops.size();
     db.pos[7] = need_g ? 1 : 0;
     dblocks.push_back(db);
@@ -708,7 +730,7 @@ double op_flops(const IOp& o) {
   switch (o.kind) {
     case I_U1: return 16;
     case I_U2: return 32;
-    case I_RY: return 8;
+    case I_RY: return o.cq.empty() ? 4 : 8;
     case I_PHASE: case I_DIAG1: case I_DIAG2: return 8;
     default: return 0;
   }
@@ -850,6 +872,22 @@ int qs_plan_analyze(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_in
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p);
   *info = p.info;
+  QS_API_END(h)
+}
+
+int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_bits, void* out, size_t cap,
+                    size_t* needed) {
+  qs_context* h = nullptr;
+  QS_API_BEGIN
+  QS_CHECK_ARG(needed != nullptr, "needed is null");
+  if (tile_bits == 0) tile_bits = 13;
+  if (block_bits == 0) block_bits = 5;
+  QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
+  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
+  qs_plan_s p;
+  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits);
+  *needed = p.blob.size();
+  if (out && cap >= p.blob.size() && !p.blob.empty()) std::memcpy(out, p.blob.data(), p.blob.size());
   QS_API_END(h)
 }
 
