@@ -326,7 +326,183 @@ def bench_qv12(args, dev):
             "clocks": clk.summary(), "gpu_launches": args.steps}, {"unit": "circuits/s"}
 
 
-WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12}
+class ServingMix:
+    """The serving request mix, seeded: 50% Quantum-Volume circuits (widths
+    10-28, depth = width, 1024 shots), 25% ansatz energy+gradient requests
+    (EfficientSU2, 4 reps, 12-22 qubits, 256-term observable), 25% Chebyshev
+    evolutions (ring ZZ + X field + 20 random XX+YY pairs, 12-22 qubits,
+    t ~ U[0.5, 10], seeded product state, precision 1e-6).  Observables,
+    Hamiltonians and product states are drawn once per width."""
+
+    def __init__(self, n_req: int, seed: int):
+        import numpy as np
+        self.rng = np.random.default_rng(seed)
+        r = self.rng
+        self.specs = []
+        for i in range(n_req):
+            u = r.random()
+            if u < 0.5:
+                self.specs.append(("qv", int(r.integers(10, 29)), 1_000_000 + i))
+            elif u < 0.75:
+                self.specs.append(("grad", int(r.integers(12, 23)), 2_000_000 + i))
+            else:
+                self.specs.append(("evo", int(r.integers(12, 23)), 3_000_000 + i, float(r.uniform(0.5, 10.0))))
+        self._cache = {}
+
+    def _per_width(self, kind, w):
+        from qsim_b200 import workloads as W
+        from qsim_b200.circuit import lower
+        key = (kind, w)
+        if key not in self._cache:
+            if kind == "grad":
+                qc, npar = W.efficient_su2(w, reps=4)
+                self._cache[key] = (lower(qc), npar, W.random_pauli_observable(w, 256, seed=w))
+            else:
+                self._cache[key] = (W.serving_hamiltonian(w, seed=w), W.product_state(w, seed=w))
+        return self._cache[key]
+
+    def request(self, i):
+        import numpy as np
+        from qsim_b200 import workloads as W
+        from qsim_b200.server import CircuitRequest, EvolutionRequest, GradientRequest
+        sp = self.specs[i]
+        if sp[0] == "qv":
+            return CircuitRequest(n_qubits=sp[1], ops=W.qv_ops(sp[1], sp[1], sp[2]), shots=1024, seed=sp[2])
+        if sp[0] == "grad":
+            ops, npar, obs = self._per_width("grad", sp[1])
+            p = np.random.default_rng(sp[2]).uniform(0, 2 * math.pi, (1, npar))
+            return GradientRequest(n_qubits=sp[1], ops=ops, n_params=npar, params=p, observable=obs)
+        ham, psi0 = self._per_width("evo", sp[1])
+        return EvolutionRequest(hamiltonian=ham, t=sp[3], psi0=psi0, precision=1e-6)
+
+    @staticmethod
+    def host_bytes(req):
+        import numpy as np
+        b = int(np.asarray(getattr(req, "ops", np.zeros(0))).nbytes)
+        if getattr(req, "psi0", None) is not None:
+            b += int(np.asarray(req.psi0).size) * 8
+        return b
+
+
+def run_serial(mix, reqs, dev):
+    """The plain path, one request after the other on one stream: a plan per
+    circuit + sampling, adjoint gradient, Chebyshev evolution."""
+    import numpy as np
+    import torch
+    from blackwell_backend.chebyshev import chebyshev_evolve_pauli
+    from qsim_b200 import engine as E
+    from qsim_b200.server import CircuitRequest, GradientRequest
+    for r in reqs:
+        if isinstance(r, CircuitRequest):
+            p = E.Plan(r.n_qubits, r.ops, dev)
+            st = E.empty_state(r.n_qubits, f"cuda:{dev}")
+            p.execute_from_zero(st)
+            g = torch.Generator(device=f"cuda:{dev}")
+            g.manual_seed(int(r.seed))
+            E.sample(st, r.shots, generator=g).cpu()
+            del p, st
+        elif isinstance(r, GradientRequest):
+            E.adjoint_gradient(r.n_qubits, r.ops, r.n_params, np.asarray(r.params), r.observable, dev)
+        else:
+            psi = torch.as_tensor(np.asarray(r.psi0, dtype=np.complex64)).to(f"cuda:{dev}")
+            out, _ = chebyshev_evolve_pauli(psi, r.hamiltonian, r.t, precision=r.precision)
+            out.cpu()
+
+
+def bench_serving(args, dev):
+    """Poisson request streams at each rate of the sweep, served by the
+    continuous-batching server (150 GB budget); the same request sequence is
+    replayed at every rate.  value = served requests/s at the highest rate
+    (the server saturated); p50/p99 per rate; the same requests run one by one
+    on the plain path give the serial comparison."""
+    import numpy as np
+    import torch
+    from qsim_b200 import engine as E
+    from qsim_b200.server import CircuitRequest, Server
+    rates = [float(x) for x in args.rates.split(",")]
+    n_req = args.requests
+    mix = ServingMix(n_req, seed=4)
+    reqs = [mix.request(i) for i in range(n_req)]
+    gaps = np.random.default_rng(5).exponential(1.0, n_req)
+    unit_arrivals = np.cumsum(gaps) - gaps[0]
+    h2d = sum(ServingMix.host_bytes(r) for r in reqs)
+    d2h = sum((r.shots * 8 if isinstance(r, CircuitRequest) else 8 << getattr(r, "n_qubits", 0))
+              for r in reqs)
+    # warm-up: one request of each kind and width class through the server
+    srv = Server(device=dev, workers=args.workers)
+    warm = [mix.request(i) for i in range(min(n_req, 3 * max(1, args.warmup)))]
+    for f in [srv.submit(r) for r in warm]:
+        f.result(600)
+    srv.close()
+    torch.cuda.synchronize()
+    sweep = []
+    stream = torch.cuda.current_stream(dev)
+    L = E._h(dev).L
+    with ClockSampler(dev) as clk:
+        for lam in rates:
+            arrivals = unit_arrivals / lam
+            srv = Server(device=dev, workers=args.workers)
+            futs = [None] * n_req
+            lr0 = int(L.qs_launch_count(None))
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            barrier()
+            ev0.record(stream)
+            t0 = time.perf_counter()
+            for i, r in enumerate(reqs):
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                futs[i] = srv.submit(r)
+            for f in futs:
+                f.result(1800)
+            torch.cuda.synchronize()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            makespan = ev0.elapsed_time(ev1) / 1000.0
+            st = srv.stats()
+            srv.close()
+            lat = np.array(srv.latencies)
+            kinds = np.array([sp[0] for sp in mix.specs])
+            qv_n = int((kinds == "qv").sum())
+            sweep.append({"rate_rps": lam, "served_rps": n_req / makespan, "qv_circuits_per_s": qv_n / makespan,
+                          "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                          "makespan_s": makespan, "offered_s": float(arrivals[-1]),
+                          "gpu_launches": int(L.qs_launch_count(None)) - lr0})
+    # serial plain execution of the same requests
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    run_serial(mix, reqs, dev)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_serial = ev0.elapsed_time(ev1) / 1000.0
+    top = sweep[-1]
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    top_mk = reduce_max(top["makespan_s"], f"cuda:{dev}")
+    res = {
+        "metric": METRIC, "value": ws * n_req / top_mk, "unit": "requests/s",
+        "ms_per_step": top_mk * 1e3, "dtype": "c64 state (fp32 FMA), fp64 reductions",
+        "config": {"workload": f"serving: {n_req} seeded requests (50% QV 10-28q 1024 shots, 25% EfficientSU2 "
+                               f"energy+gradient 12-22q, 25% Chebyshev evolution 12-22q), Poisson arrivals "
+                               f"replayed at each rate; 150 GB budget, {args.workers} worker streams",
+                   "rates_rps": rates, "step": "one replay of the request sequence at the highest rate",
+                   "l2": "states up to 2 GiB each; no flush"},
+        "sweep": sweep,
+        "served_circuits_per_s": ws * top["qv_circuits_per_s"],
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "serial_plain": {"value": n_req / t_serial, "unit": "requests/s", "seconds": t_serial,
+                         "speedup": t_serial / top["makespan_s"]},
+        "e2e": {"value": ws * n_req / top_mk, "unit": "requests/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "note": "host request -> admission -> device -> host result; the value itself is end to end"},
+        "gpu_launches": top["gpu_launches"],
+        "clocks": clk.summary(),
+    }
+    return res, {"unit": "requests/s"}
+
+
+WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving}
 
 
 # --------------------------------------------------------- CPU baseline
@@ -377,11 +553,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--qubits", type=int, default=32)
     ap.add_argument("--circuits", type=int, default=4096)
+    ap.add_argument("--requests", type=int, default=200, help="serving: requests per rate")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serving: Poisson rates (req/s)")
+    ap.add_argument("--workers", type=int, default=4, help="serving: worker streams")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
     ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")
     ap.add_argument("--jit", type=int, default=-1,
-                    help="pass specialisation: 0 off, 1 plans >= 26 qubits, 2 all (-1 = library default)")
+                    help="pass specialisation: 0 off, 1 tiered (background compile, plans >= 24 qubits), "
+                         "2 before first execution (-1 = 2 for layers32, else the library default)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
 
@@ -410,6 +590,8 @@ def main():
     dev = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(dev)
     dist_init(ws, "nccl")
+    if args.jit < 0 and args.workload == "layers32":
+        args.jit = 2   # specialise every pass before the timed region
     if args.jit >= 0:
         from qsim_b200 import engine as E
         E.set_jit(args.jit, 0, dev)

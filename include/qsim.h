@@ -100,15 +100,23 @@ int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
 /* Register-block width used by the planner (2..5 qubits per thread group);
  * 0 = default (5).                                                          */
 int  qs_set_block_bits(qs_handle_t h, int block_bits);
-/* Pass specialisation: plans may compile each tile pass (NVRTC, at its first
- * execution) into a kernel with its gate positions and coefficients built in;
- * results are bit-identical to the generic pass kernel.  mode 0 = never,
- * 1 = plans on >= min_qubits qubits (default 26; 0 keeps the current value),
- * 2 = every plan.  The default mode comes from the QSIM_JIT environment
- * variable (0/1/2), else 1.  No reference counterpart (the reference
- * compiles its kernels ahead of time).                                      */
+/* Pass specialisation: a plan's tile passes may be compiled (NVRTC) into
+ * kernels with their gate positions and coefficients built in; results are
+ * bit-identical to the generic pass kernel.  Compiled kernels are cached per
+ * device by source, so new plans of a known circuit use them at once.
+ *   mode 0 = never;
+ *   mode 1 = tiered: a plan on >= min_qubits qubits (default 24; 0 keeps the
+ *            current value) uses cached kernels from its first execution;
+ *            at its second execution (the plan is being reused) the missing
+ *            passes go to one background compiler thread, and the plan runs
+ *            on the generic kernel until they are ready;
+ *   mode 2 = every plan is compiled before its first execution.
+ * The default mode comes from the QSIM_JIT environment variable (0/1/2),
+ * else 1.  No reference counterpart (the reference compiles its kernels
+ * ahead of time).                                                           */
 int  qs_set_jit(qs_handle_t h, int mode, int min_qubits);
-/* Number of kernels this handle has launched since creation.               */
+/* Number of kernels this handle has launched since creation; h = NULL gives
+ * the count over every handle of the process.                               */
 int64_t qs_launch_count(qs_handle_t h);
 
 /* ------------------------------------------------------------ states ----- */

@@ -1,5 +1,6 @@
 // qs_context.cu — handle lifecycle, streams, scratch and error reporting.
 #include "qs_api.h"
+#include <atomic>
 #include <cstring>
 
 static thread_local std::string g_tls_err;
@@ -34,8 +35,11 @@ double* qs_context::pinned_get(size_t bytes) {
   return pinned;
 }
 
+static std::atomic<int64_t> g_launches{0};  // every handle of the process
+
 void qs_after_launch(qs_context* h, const char* what) {
   h->launches++;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     throw qs_error(QS_ERR_CUDA, std::string(what) + ": launch failed: " + cudaGetErrorString(e));
@@ -137,6 +141,6 @@ int qs_set_jit(qs_handle_t h, int mode, int min_qubits) {
   QS_API_END(h)
 }
 
-int64_t qs_launch_count(qs_handle_t h) { return h ? h->launches : -1; }
+int64_t qs_launch_count(qs_handle_t h) { return h ? h->launches : g_launches.load(); }
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <memory>
 #include <string>
 #include <vector>
 #include <complex>
@@ -42,7 +43,7 @@ struct qs_context {
   // Pass specialisation (qs_jit.cpp): 0 off, 1 plans on >= jit_min_qubits,
   // 2 every plan.
   int jit_mode = 1;
-  int jit_min_qubits = 26;
+  int jit_min_qubits = 24;
   int64_t launches = 0;
 
   // grow-only device scratch (reductions, sampling partials, ...)
@@ -128,6 +129,7 @@ struct __align__(16) DevPass {
 
 // Host-side plan.
 // A tile pass compiled into a kernel of its own (qs_jit.cpp).
+struct JitJob;
 struct JitPass {
   void* fn = nullptr;  // CUfunction
   int threads = 0, smem = 0, per_sm = 0;
@@ -144,6 +146,8 @@ struct qs_plan_s {
   qs_plan_info info{};
   bool jit_tried = false;               // specialisation attempted
   std::vector<JitPass> jit;             // one per pass when specialised
+  std::shared_ptr<JitJob> jit_job;      // sources awaiting / in background compile
+  bool jit_queued = false;              // jit_job handed to the background compiler
   std::string jit_err;                  // why specialisation was not used
 };
 
@@ -151,7 +155,8 @@ struct qs_plan_s {
 int qs_jit_env_mode();                                     // QSIM_JIT (default 1)
 bool qs_jit_available(std::string* why);
 std::string qs_jit_source(const qs_plan_s* p, size_t pass);
-bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err);
+bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err);  // synchronous
+void qs_jit_tiered(qs_context* h, qs_plan_s* p);                         // tiered (background)
 bool qs_jit_compile_only(const qs_plan_s* p, std::string& err);         // no GPU needed
 void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, uint64_t ntiles, uint32_t flags);
 

@@ -24,6 +24,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <thread>
@@ -49,7 +53,7 @@ struct Api {
   decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) Occupancy = nullptr;
 };
 
-Api g_api;
+Api& g_api = *new Api;  // never destroyed (background compiles may outlive main)
 std::once_flag g_api_once;
 
 template <class F>
@@ -511,9 +515,17 @@ uint64_t fnv1a(const std::string& s) {
 }
 
 // Compiled passes, per device, keyed by a hash of their source (plans of the
-// same circuit share kernels; modules live until the process exits).
-std::mutex g_cache_mu;
-std::unordered_map<uint64_t, std::pair<std::string, JitPass>> g_cache[64];
+// same circuit share kernels; modules live until the process exits).  Heap
+// objects that are never destroyed: a background compile may still be running
+// while static destructors run at exit.
+struct Cache {
+  std::mutex mu;
+  std::unordered_map<uint64_t, std::pair<std::string, JitPass>> map[64];
+};
+Cache& cache() {
+  static Cache* c = new Cache;
+  return *c;
+}
 
 bool nvrtc_compile(const std::string& src, std::string& cubin, std::string& err) {
   nvrtcProgram prog = nullptr;
@@ -594,71 +606,198 @@ std::string qs_jit_source(const qs_plan_s* p, size_t i) {
                   min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R)));
 }
 
-// Compiles every pass of the plan: sources are generated and compiled on up
-// to 16 host threads; modules are loaded on the calling thread, which holds
-// the CUDA context.  On failure the plan keeps running on the interpreter and
-// `err` says why.
+// A specialisation job: the plan's pass sources, the kernels found in the
+// cache and the ones still to compile.  Shared by the plan and, for tiered
+// compilation, the background thread that compiles it.
+struct JitJob {
+  int device = 0;
+  std::vector<std::string> srcs;
+  std::vector<uint64_t> keys;
+  std::vector<int> T, R;
+  std::vector<JitPass> out;
+  std::vector<size_t> todo;  // passes not in the cache
+  std::string err;
+  std::atomic<int> state{0};  // 0 pending, 1 ready, 2 failed
+};
+
+namespace {
+
+std::shared_ptr<JitJob> make_job(const qs_plan_s* p, int device) {
+  auto J = std::make_shared<JitJob>();
+  J->device = device;
+  const size_t np = p->pass_offsets.size();
+  J->srcs.resize(np);
+  J->keys.resize(np);
+  J->out.resize(np);
+  for (size_t i = 0; i < np; ++i) {
+    const DevPass& P = *reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i]);
+    J->T.push_back(P.T);
+    J->R.push_back(P.R);
+    J->srcs[i] = qs_jit_source(p, i);
+    J->keys[i] = fnv1a(J->srcs[i]);
+  }
+  Cache& C = cache();
+  std::lock_guard<std::mutex> lk(C.mu);
+  for (size_t i = 0; i < np; ++i) {
+    auto it = C.map[device].find(J->keys[i]);
+    if (it != C.map[device].end() && it->second.first == J->srcs[i]) J->out[i] = it->second.second;
+    else J->todo.push_back(i);
+  }
+  if (J->todo.empty()) J->state = 1;
+  return J;
+}
+
+// Compiles the missing passes on up to `max_threads` host threads, then loads
+// them (on this thread, with the device's primary context current).
+void run_job(JitJob& J, unsigned max_threads) {
+  const size_t nt_all = J.todo.size();
+  std::vector<std::string> cubins(J.srcs.size()), errs(J.srcs.size());
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = std::max(1u, std::min<unsigned>(std::min(max_threads, hw), (unsigned)nt_all));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; ++t)
+    pool.emplace_back([&, t]() {
+      for (size_t k = t; k < nt_all; k += nt) {
+        const size_t i = J.todo[k];
+        if (!nvrtc_compile(J.srcs[i], cubins[i], errs[i]) && errs[i].empty()) errs[i] = "compile failed";
+      }
+    });
+  for (auto& th : pool) th.join();
+  for (size_t i : J.todo)
+    if (cubins[i].empty()) {
+      J.err = errs[i];
+      J.state = 2;
+      return;
+    }
+  if (cudaSetDevice(J.device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+    J.err = "cannot make the device current for module loading";
+    J.state = 2;
+    return;
+  }
+  Cache& C = cache();
+  for (size_t i : J.todo) {
+    CUmodule mod = nullptr;
+    CUfunction fn = nullptr;
+    if (g_api.ModuleLoadData(&mod, cubins[i].data()) != CUDA_SUCCESS ||
+        g_api.ModuleGetFunction(&fn, mod, "qs_tile_pass") != CUDA_SUCCESS) {
+      J.err = "loading a specialised tile pass failed";
+      J.state = 2;
+      return;
+    }
+    JitPass K;
+    K.fn = fn;
+    K.threads = pass_threads(J.T[i], J.R[i]);
+    K.smem = pass_smem(J.T[i]);
+    if (g_api.FuncSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, K.smem) != CUDA_SUCCESS ||
+        g_api.Occupancy(&K.per_sm, fn, K.threads, (size_t)K.smem) != CUDA_SUCCESS || K.per_sm < 1) {
+      J.err = "a specialised tile pass does not fit on an SM";
+      J.state = 2;
+      return;
+    }
+    J.out[i] = K;
+    std::lock_guard<std::mutex> lk(C.mu);
+    C.map[J.device][J.keys[i]] = {J.srcs[i], K};
+  }
+  J.state = 1;
+}
+
+// One background thread compiles queued jobs in arrival order (each with up
+// to 8 NVRTC threads), so that many large plans in flight never start more
+// compiles than that.  Jobs whose plan has been destroyed are skipped.  At
+// exit the thread finishes the job in hand and stops.
+struct Background {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::weak_ptr<JitJob>> queue;
+  std::thread worker;
+  bool stop = false;
+};
+Background& background() {
+  static Background* b = new Background;
+  return *b;
+}
+void background_loop() {
+  Background& B = background();
+  for (;;) {
+    std::shared_ptr<JitJob> J;
+    {
+      std::unique_lock<std::mutex> lk(B.mu);
+      B.cv.wait(lk, [&] { return B.stop || !B.queue.empty(); });
+      if (B.stop) return;
+      J = B.queue.front().lock();
+      B.queue.pop_front();
+    }
+    if (J && J->state.load() == 0) run_job(*J, 8);
+  }
+}
+void stop_background() {
+  Background& B = background();
+  {
+    std::lock_guard<std::mutex> lk(B.mu);
+    B.stop = true;
+  }
+  B.cv.notify_all();
+  if (B.worker.joinable()) B.worker.join();
+}
+void enqueue(const std::shared_ptr<JitJob>& J) {
+  Background& B = background();
+  std::lock_guard<std::mutex> lk(B.mu);
+  if (B.stop) return;
+  if (!B.worker.joinable()) {
+    B.worker = std::thread(background_loop);
+    std::atexit(stop_background);
+  }
+  B.queue.push_back(J);
+  B.cv.notify_one();
+}
+
+}  // namespace
+
+// Synchronous specialisation: every pass compiled (or found in the cache)
+// before returning.  On failure the plan keeps running on the generic kernel
+// and `err` says why.
 bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err) {
   if (!qs_jit_available(&err)) return false;
   QS_CHECK_ARG(h->device >= 0 && h->device < 64, "device index out of range");
-  const size_t np = p->pass_offsets.size();
-  std::vector<std::string> srcs(np), cubins(np), errs(np);
-  std::vector<uint64_t> keys(np);
-  std::vector<JitPass> out(np);
-  std::vector<size_t> todo;
-  for (size_t i = 0; i < np; ++i) {
-    srcs[i] = qs_jit_source(p, i);
-    keys[i] = fnv1a(srcs[i]);
-    std::lock_guard<std::mutex> lk(g_cache_mu);
-    auto it = g_cache[h->device].find(keys[i]);
-    if (it != g_cache[h->device].end() && it->second.first == srcs[i]) out[i] = it->second.second;
-    else todo.push_back(i);
+  auto J = make_job(p, h->device);
+  if (J->state == 0) run_job(*J, 16);
+  if (J->state != 1) {
+    err = J->err;
+    return false;
   }
-  if (!todo.empty()) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned nt = std::min<unsigned>(std::min(16u, hw), (unsigned)todo.size());
-    std::vector<std::thread> pool;
-    for (unsigned t = 0; t < nt; ++t)
-      pool.emplace_back([&, t]() {
-        for (size_t k = t; k < todo.size(); k += nt) {
-          const size_t i = todo[k];
-          if (!nvrtc_compile(srcs[i], cubins[i], errs[i]) && errs[i].empty()) errs[i] = "compile failed";
-        }
-      });
-    for (auto& th : pool) th.join();
-    for (size_t i : todo)
-      if (cubins[i].empty()) {
-        err = errs[i];
-        return false;
-      }
-    // The runtime's primary context must be current on this thread.
-    QS_CUDA(cudaSetDevice(h->device));
-    QS_CUDA(cudaFree(nullptr));
-    for (size_t i : todo) {
-      const DevPass& P = *reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i]);
-      CUmodule mod = nullptr;
-      CUfunction fn = nullptr;
-      if (g_api.ModuleLoadData(&mod, cubins[i].data()) != CUDA_SUCCESS ||
-          g_api.ModuleGetFunction(&fn, mod, "qs_tile_pass") != CUDA_SUCCESS) {
-        err = "loading a specialised tile pass failed";
-        return false;
-      }
-      JitPass K;
-      K.fn = fn;
-      K.threads = pass_threads(P.T, P.R);
-      K.smem = pass_smem(P.T);
-      if (g_api.FuncSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, K.smem) != CUDA_SUCCESS ||
-          g_api.Occupancy(&K.per_sm, fn, K.threads, (size_t)K.smem) != CUDA_SUCCESS || K.per_sm < 1) {
-        err = "a specialised tile pass does not fit on an SM";
-        return false;
-      }
-      out[i] = K;
-      std::lock_guard<std::mutex> lk(g_cache_mu);
-      g_cache[h->device][keys[i]] = {srcs[i], K};
-    }
-  }
-  p->jit = out;
+  p->jit = J->out;
   return true;
+}
+
+// Tiered specialisation.  First execution: the pass sources are generated and
+// looked up in the kernel cache; a full hit specialises the plan at once.
+// Second execution (the plan is being reused): the missing passes are queued
+// for the background compiler.  Later executions switch over once it is done.
+void qs_jit_tiered(qs_context* h, qs_plan_s* p) {
+  if (!p->jit.empty()) return;
+  if (!p->jit_tried) {
+    p->jit_tried = true;
+    std::string why;
+    if (!qs_jit_available(&why)) {
+      p->jit_err = why;
+      return;
+    }
+    QS_CHECK_ARG(h->device >= 0 && h->device < 64, "device index out of range");
+    auto J = make_job(p, h->device);
+    if (J->state == 1) p->jit = J->out;
+    else p->jit_job = J;
+    return;
+  }
+  if (!p->jit_job) return;
+  if (!p->jit_queued) {
+    p->jit_queued = true;
+    enqueue(p->jit_job);
+    return;
+  }
+  const int st = p->jit_job->state.load();
+  if (st == 1) p->jit = p->jit_job->out;
+  if (st == 2) p->jit_err = p->jit_job->err;
+  if (st != 0) p->jit_job.reset();
 }
 
 void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t i, void* state, uint64_t ntiles, uint32_t flags) {

@@ -808,21 +808,26 @@ void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint6
     if (from_zero) QS_CHECK_ARG(qs_state_init_batched(h, state, (int)n_states, n) == QS_OK, h->err.c_str());
     return;
   }
-  // Specialise the passes at the first execution that asks for it (the
-  // compiled kernels are cached by source, so rebuilding a plan of the same
-  // circuit costs only the source generation).
-  const bool want_jit = h->jit_mode == 2 || (h->jit_mode == 1 && n >= h->jit_min_qubits);
-  if (want_jit && !p->jit_tried) {
+  // Pass specialisation.  Mode 2 compiles every pass before the first
+  // execution.  Mode 1 (tiered, plans on >= jit_min_qubits qubits) uses
+  // cached kernels from the first execution, queues a background compile at
+  // the second (the plan is being reused) and switches over when it is done.
+  if (h->jit_mode == 2 && !p->jit_tried) {
     p->jit_tried = true;
     std::string why;
     if (!qs_jit_compile_plan(h, p, why)) {
       p->jit.clear();
       p->jit_err = why;
-      if (std::getenv("QSIM_JIT_VERBOSE")) std::fprintf(stderr, "qsim: pass specialisation off: %s\n", why.c_str());
     }
-    p->info.n_jit_passes = (int32_t)p->jit.size();
+  } else if (h->jit_mode == 1 && n >= h->jit_min_qubits) {
+    qs_jit_tiered(h, p);
   }
-  const bool use_jit = want_jit && p->jit.size() == p->pass_offsets.size();
+  if (!p->jit_err.empty() && std::getenv("QSIM_JIT_VERBOSE")) {
+    std::fprintf(stderr, "qsim: pass specialisation off: %s\n", p->jit_err.c_str());
+    p->jit_err.clear();
+  }
+  p->info.n_jit_passes = (int32_t)p->jit.size();
+  const bool use_jit = h->jit_mode != 0 && p->jit.size() == p->pass_offsets.size();
   for (size_t i = 0; i < p->pass_offsets.size(); ++i) {
     const int T = p->pass_T[i];
     const uint32_t flags = (from_zero && i == 0) ? PI_FROM_ZERO : 0u;
