@@ -188,10 +188,11 @@ int qs_plan_analyze(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs
 int qs_plan_jit_check(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, int block_bits, int* n_passes);
 /* Host-only: the device program (passes back to back, each starting with its
  * pass header) the planner emits for these ops, copied to `out` when `cap`
- * is large enough; `*needed` = its size in bytes.  For inspection and tests
- * of the planner; no reference counterpart.                                 */
-int qs_plan_program(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, int block_bits, void* out,
-                    size_t cap, size_t* needed);
+ * is large enough; `*needed` = its size in bytes.  `specialised` != 0 plans
+ * for specialised passes (dense two-qubit gates split into their Cartan
+ * form).  For inspection and tests of the planner; no reference counterpart. */
+int qs_plan_program(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, int block_bits, int specialised,
+                    void* out, size_t cap, size_t* needed);
 /* plan + execute in one call (the plan is freed afterwards).               */
 int qs_run_circuit(qs_handle_t h, void* state, int n_qubits, const qs_op* ops, int n_ops);
 

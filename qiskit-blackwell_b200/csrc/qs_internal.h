@@ -87,6 +87,10 @@ enum DevKind : uint8_t {
                  // s) is folded into a later table op or DK_SCALE of the pass
   DK_KU1 = 13,   // one dense 2x2 per register bit (c[4k..4k+3]), likewise
   DK_SCALE = 14, // multiply every amplitude by the real c[0].x
+  DK_XRY = 15,   // parity rotation on register bits t0 < t1: the pairs
+                 // (x, y) = (|t0=0 t1=0>, |11>) use c[0] = (t, form), the
+                 // pairs (|t0=0 t1=1>, |t0=1 t1=0>) use c[1]; each pair as in
+                 // DK_KRY (the dropped factors are already in the next diagonal)
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -161,7 +165,10 @@ bool qs_jit_compile_only(const qs_plan_s* p, std::string& err);         // no GP
 void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, uint64_t ntiles, uint32_t flags);
 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
-void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 5);
+// `specialised`: the plan will run as specialised passes (enables the Cartan
+// split of dense two-qubit gates, which only pays off there).
+void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 5,
+                   bool specialised = false);
 void qs_plan_upload(qs_context* h, qs_plan_s* p);
 void qs_plan_free_device(void* d);  // stream-ordered free (no device sync)
 // Runs every pass on n_states equal-width states stored back to back.

@@ -261,6 +261,19 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
       case DK_SCALE:
         for (int j = 0; j < J; ++j) G.set(j, "scl(" + G.v[j] + ", " + flit(c[0].x) + ")", "");
         break;
+      case DK_XRY: {  // parity rotation: pairs (j, j ^ (A|B)), coefficients by bit B
+        const int A = op.t0, B = op.t1;
+        for (int j = 0; j < J; ++j) {
+          if ((j >> A) & 1) continue;
+          const int k = j ^ ((1 << A) | (1 << B));
+          const float2 tf = ((j >> B) & 1) ? c[1] : c[0];
+          const std::string t = flit(tf.x) + ", " + G.v[j] + ", " + G.v[k] + ")";
+          const bool fb = tf.y != 0.f;
+          G.set(j, (fb ? "rtb0(" : "rta0(") + t, "");
+          G.set(k, (fb ? "rtb1(" : "rta1(") + t, "");
+        }
+        break;
+      }
       case DK_U2:
       case DK_SWAP: {
         const int A = op.t0, B = op.t1;

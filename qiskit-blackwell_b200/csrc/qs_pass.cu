@@ -246,6 +246,30 @@ __device__ __forceinline__ void op_kry(float2 (&v)[1 << R], const float2* __rest
   if constexpr (R > 4) if (mask & 16u) kry_stage<R, 4>(v, c[4]);
 }
 
+// Parity rotation (DK_XRY) on register bits A < B: pairs j (bit A clear) and
+// j ^ (A|B), with the even-parity (bit B clear) or odd-parity coefficients.
+template <int R, int A, int B>
+__device__ __forceinline__ void op_xry(float2 (&v)[1 << R], const float2* __restrict__ c) {
+  if constexpr (A < B && B < R) {
+    const float2 ce = c[0], co = c[1];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << A)) continue;
+      const int k = j ^ ((1 << A) | (1 << B));
+      const float2 tf = (j & (1 << B)) ? co : ce;
+      const float2 tt = make_float2(tf.x, tf.x), nt = make_float2(-tf.x, -tf.x);
+      const float2 a0 = v[j], a1 = v[k];
+      if (tf.y == 0.f) {
+        v[j] = __ffma2_rn(nt, a1, a0);
+        v[k] = __ffma2_rn(tt, a0, a1);
+      } else {
+        v[j] = __ffma2_rn(tt, a0, make_float2(-a1.x, -a1.y));
+        v[k] = __ffma2_rn(tt, a1, a0);
+      }
+    }
+  }
+}
+
 template <int R>
 __device__ __forceinline__ void op_scale(float2 (&v)[1 << R], float f) {
 #pragma unroll
@@ -388,6 +412,11 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
       case DK_SWAP:
         if constexpr (TWO) {
           switch (op.t0 * 8 + op.t1) { CASES_2(op_swap, v, rc, gp) }
+        }
+        break;
+      case DK_XRY:
+        if constexpr (TWO) {
+          switch (op.t0 * 8 + op.t1) { CASES_2(op_xry, v, c) }
         }
         break;
       default:

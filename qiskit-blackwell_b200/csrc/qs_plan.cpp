@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <set>
 #include <tuple>
@@ -24,7 +25,7 @@ namespace {
 
 using cd = std::complex<double>;
 
-enum IKind { I_U1, I_U2, I_X, I_SWAP, I_Y, I_NEG, I_PHASE, I_DIAG1, I_DIAG2, I_RY };
+enum IKind { I_U1, I_U2, I_X, I_SWAP, I_Y, I_NEG, I_PHASE, I_DIAG1, I_DIAG2, I_RY, I_XRY };
 
 inline bool is_diag_kind(int k) { return k == I_NEG || k == I_PHASE || k == I_DIAG1 || k == I_DIAG2; }
 
@@ -134,6 +135,370 @@ std::vector<IOp> normalise(int n, const qs_op* ops, int nops) {
       continue;
     }
     out.push_back(std::move(p));
+  }
+  return out;
+}
+
+// --------------------------------------- two-qubit Cartan split (FP64) --
+// A dense U(4) costs 16 FMA per amplitude.  Its Cartan (KAK) form
+//   U = (A1 (x) A0) . N . (B1 (x) B0),   N = exp(i(a XX + b YY + c ZZ))
+// replaces it by four single-qubit gates, which fuse with their neighbours,
+// and N, which only mixes |00> with |11> and |01> with |10>: a real rotation
+// in each of the two subspaces (one FMA per amplitude component in scaled
+// form) between two-qubit diagonals that merge into the diagonal tables.
+// Method (Kraus & Cirac, PRA 63, 062309; Vatan & Williams, PRA 69, 032315):
+// in the magic basis Q local gates are real orthogonal and N is diagonal,
+// so with V = Q^dag U' Q (U' = U / det(U)^(1/4)) the symmetric unitary
+// V^T V = O D O^T has a real orthogonal eigenbasis O, V = K1 D^(1/2) O^T with
+// K1 real orthogonal, and A = Q K1 Q^dag, N = Q D^(1/2) Q^dag, B = Q O^T Q^dag.
+// Every result is recomposed and compared with U; any failure keeps U dense.
+namespace kak {
+
+using C4 = std::array<cd, 16>;  // row-major 4x4, index = bit0 + 2 bit1
+
+C4 mul(const C4& A, const C4& B) {
+  C4 R{};
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      cd s = 0;
+      for (int k = 0; k < 4; ++k) s += A[4 * i + k] * B[4 * k + j];
+      R[4 * i + j] = s;
+    }
+  return R;
+}
+C4 dag(const C4& A) {
+  C4 R{};
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) R[4 * i + j] = std::conj(A[4 * j + i]);
+  return R;
+}
+C4 transpose(const C4& A) {
+  C4 R{};
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) R[4 * i + j] = A[4 * j + i];
+  return R;
+}
+double dist(const C4& A, const C4& B) {
+  double m = 0;
+  for (int i = 0; i < 16; ++i) m = std::max(m, std::abs(A[i] - B[i]));
+  return m;
+}
+
+// Magic basis: columns (|00>+|11>)/sqrt2, i(|00>-|11>)/sqrt2,
+// i(|01>+|10>)/sqrt2, (|01>-|10>)/sqrt2.
+const C4& magic() {
+  static const C4 Q = [] {
+    const double r = 1.0 / std::sqrt(2.0);
+    const cd I(0, 1);
+    C4 q{};
+    q[4 * 0 + 0] = r;  q[4 * 3 + 0] = r;
+    q[4 * 0 + 1] = I * r; q[4 * 3 + 1] = -I * r;
+    q[4 * 1 + 2] = I * r; q[4 * 2 + 2] = I * r;
+    q[4 * 1 + 3] = r;  q[4 * 2 + 3] = -r;
+    return q;
+  }();
+  return Q;
+}
+
+// Cyclic Jacobi eigen-decomposition of a real symmetric 4x4 (A = V diag V^T).
+void jacobi4(double A[4][4], double V[4][4]) {
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0;
+    for (int p = 0; p < 4; ++p)
+      for (int q = p + 1; q < 4; ++q) off += A[p][q] * A[p][q];
+    if (off < 1e-30) return;
+    for (int p = 0; p < 4; ++p)
+      for (int q = p + 1; q < 4; ++q) {
+        if (std::abs(A[p][q]) < 1e-300) continue;
+        const double th = (A[q][q] - A[p][p]) / (2 * A[p][q]);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (std::abs(th) + std::sqrt(th * th + 1));
+        const double c = 1 / std::sqrt(t * t + 1), s = t * c;
+        for (int k = 0; k < 4; ++k) {  // A <- J^T A J
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 4; ++k) {
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 4; ++k) {
+          const double vkp = V[k][p], vkq = V[k][q];
+          V[k][p] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+// L = X (x) Y (X on bit 1, Y on bit 0) -> X, Y; false if L is not a product.
+bool split_local(const C4& L, cd X[4], cd Y[4]) {
+  int bi = 0, bj = 0;
+  double best = -1;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) {
+      double nrm = 0;
+      for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) nrm += std::norm(L[4 * (2 * i + k) + (2 * j + l)]);
+      if (nrm > best) { best = nrm; bi = i; bj = j; }
+    }
+  // Y = block (bi, bj) scaled to a unitary; X[i][j] = <block(i,j), Y>/2
+  const double sc = std::sqrt(best / 2.0);
+  if (sc < 1e-6) return false;
+  for (int k = 0; k < 2; ++k)
+    for (int l = 0; l < 2; ++l) Y[2 * k + l] = L[4 * (2 * bi + k) + (2 * bj + l)] / sc;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) {
+      cd s = 0;
+      for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) s += std::conj(Y[2 * k + l]) * L[4 * (2 * i + k) + (2 * j + l)];
+      X[2 * i + j] = s / 2.0;
+    }
+  C4 R{};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) R[4 * (2 * i + k) + (2 * j + l)] = X[2 * i + j] * Y[2 * k + l];
+  return dist(R, L) < 1e-10;
+}
+
+C4 kron(const cd X[4], const cd Y[4]) {
+  C4 R{};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) R[4 * (2 * i + k) + (2 * j + l)] = X[2 * i + j] * Y[2 * k + l];
+  return R;
+}
+
+// U = (A1 (x) A0) N (B1 (x) B0) with N in span{I, XX, YY, ZZ}; false when the
+// split does not reproduce U to 1e-10.
+bool decompose(const cd* Uin, cd A0[4], cd A1[4], cd B0[4], cd B1[4], C4& N) {
+  C4 U;
+  for (int i = 0; i < 16; ++i) U[i] = Uin[i];
+  // det(U) by Gaussian elimination with partial pivoting
+  C4 T = U;
+  cd det = 1;
+  for (int c = 0; c < 4; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::abs(T[4 * r + c]) > std::abs(T[4 * p + c])) p = r;
+    if (std::abs(T[4 * p + c]) < 1e-12) return false;
+    if (p != c) {
+      for (int k = 0; k < 4; ++k) std::swap(T[4 * p + k], T[4 * c + k]);
+      det = -det;
+    }
+    det *= T[4 * c + c];
+    for (int r = c + 1; r < 4; ++r) {
+      const cd f = T[4 * r + c] / T[4 * c + c];
+      for (int k = c; k < 4; ++k) T[4 * r + k] -= f * T[4 * c + k];
+    }
+  }
+  const cd root = std::pow(det, 0.25);
+  C4 Us;
+  for (int i = 0; i < 16; ++i) Us[i] = U[i] / root;
+  const C4& Q = magic();
+  const C4 V = mul(dag(Q), mul(Us, Q));
+  const C4 P = mul(transpose(V), V);
+  double O[4][4];
+  bool ok = false;
+  for (double r : {0.5772156649015329, 1.4142135623730951, 2.718281828459045, 0.3183098861837907}) {
+    double A[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) A[i][j] = P[4 * i + j].real() + r * P[4 * i + j].imag();
+    jacobi4(A, O);
+    // O^T P O must be diagonal
+    ok = true;
+    for (int i = 0; i < 4 && ok; ++i)
+      for (int j = 0; j < 4 && ok; ++j) {
+        if (i == j) continue;
+        cd s = 0;
+        for (int k = 0; k < 4; ++k)
+          for (int l = 0; l < 4; ++l) s += O[k][i] * P[4 * k + l] * O[l][j];
+        if (std::abs(s) > 1e-9) ok = false;
+      }
+    if (ok) break;
+  }
+  if (!ok) return false;
+  // det(O) = +1
+  {
+    double M[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) M[i][j] = O[i][j];
+    double d = 1;
+    for (int c = 0; c < 4; ++c) {
+      int p = c;
+      for (int r = c + 1; r < 4; ++r)
+        if (std::abs(M[r][c]) > std::abs(M[p][c])) p = r;
+      if (p != c) { for (int k = 0; k < 4; ++k) std::swap(M[p][k], M[c][k]); d = -d; }
+      d *= M[c][c];
+      if (std::abs(M[c][c]) < 1e-300) return false;
+      for (int r = c + 1; r < 4; ++r) {
+        const double f = M[r][c] / M[c][c];
+        for (int k = c; k < 4; ++k) M[r][k] -= f * M[c][k];
+      }
+    }
+    if (d < 0)
+      for (int i = 0; i < 4; ++i) O[i][0] = -O[i][0];
+  }
+  cd dh[4];  // square roots of the eigenvalues of P
+  for (int i = 0; i < 4; ++i) {
+    cd s = 0;
+    for (int k = 0; k < 4; ++k)
+      for (int l = 0; l < 4; ++l) s += O[k][i] * P[4 * k + l] * O[l][i];
+    dh[i] = std::sqrt(s);
+  }
+  auto build_k1 = [&](C4& K1) {
+    C4 VO{};
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) {
+        cd s = 0;
+        for (int k = 0; k < 4; ++k) s += V[4 * i + k] * O[k][j];
+        VO[4 * i + j] = s / dh[j];
+      }
+    K1 = VO;
+  };
+  C4 K1;
+  build_k1(K1);
+  // K1 is real orthogonal; make det(K1) = +1 by flipping one square root
+  {
+    double M[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) M[i][j] = K1[4 * i + j].real();
+    double d = 1;
+    for (int c = 0; c < 4; ++c) {
+      int p = c;
+      for (int r = c + 1; r < 4; ++r)
+        if (std::abs(M[r][c]) > std::abs(M[p][c])) p = r;
+      if (p != c) { for (int k = 0; k < 4; ++k) std::swap(M[p][k], M[c][k]); d = -d; }
+      d *= M[c][c];
+      if (std::abs(M[c][c]) < 1e-300) return false;
+      for (int r = c + 1; r < 4; ++r) {
+        const double f = M[r][c] / M[c][c];
+        for (int k = c; k < 4; ++k) M[r][k] -= f * M[c][k];
+      }
+    }
+    if (d < 0) {
+      dh[0] = -dh[0];
+      build_k1(K1);
+    }
+  }
+  C4 Dh{}, OT{};
+  for (int i = 0; i < 4; ++i) Dh[4 * i + i] = dh[i];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) OT[4 * i + j] = O[j][i];
+  const C4 La = mul(Q, mul(K1, dag(Q)));
+  const C4 Lb = mul(Q, mul(OT, dag(Q)));
+  N = mul(Q, mul(Dh, dag(Q)));
+  if (!split_local(La, A1, A0) || !split_local(Lb, B1, B0)) return false;
+  // N only couples |00>-|11> and |01>-|10>
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      const bool coupled = (i == j) || (i ^ j) == 3;
+      if (!coupled && std::abs(N[4 * i + j]) > 1e-10) return false;
+    }
+  // global phase onto A0, then check the recomposition
+  C4 R = mul(kron(A1, A0), mul(N, kron(B1, B0)));
+  cd z = 0;
+  for (int i = 0; i < 16; ++i) z += std::conj(R[i]) * U[i];
+  z /= 4.0;
+  if (std::abs(std::abs(z) - 1.0) > 1e-9) return false;
+  for (int i = 0; i < 4; ++i) A0[i] *= z;
+  R = mul(kron(A1, A0), mul(N, kron(B1, B0)));
+  return dist(R, U) < 1e-10;
+}
+
+}  // namespace kak
+
+// The Cartan split trades one dense op for several cheap ones: a win in
+// specialised passes, a loss in the generic kernel, whose cost is per op.  The
+// caller says whether the plan will be specialised; QSIM_KAK=0/1 overrides.
+bool kak_enabled(bool specialised) {
+  const char* e = std::getenv("QSIM_KAK");
+  const int env = (e && *e) ? (e[0] == '0' ? 0 : 1) : -1;
+  return env < 0 ? specialised : env == 1;
+}
+
+// 2x2 unitary V on (x, y) = diag(l0, l1) . [[c, -s], [s, c]] . diag(1, r1)
+// with c, s >= 0 (the single-qubit factorisation of emit_1q).
+void split_2x2(const cd V[4], cd& l0, cd& l1, double& c, double& s, cd& r1) {
+  c = std::abs(V[0]);
+  s = std::abs(V[2]);
+  const double nrm = std::sqrt(c * c + s * s);
+  if (s <= 1e-12 * nrm) {         // diagonal
+    l0 = V[0]; l1 = V[3]; c = 1; s = 0; r1 = 1;
+  } else if (c <= 1e-12 * nrm) {  // anti-diagonal
+    l0 = 1; l1 = V[2]; c = 0; s = 1; r1 = -V[1];
+  } else {
+    l0 = V[0] / c; l1 = V[2] / s; r1 = -V[1] / (l0 * s);
+    c /= nrm; s /= nrm;
+  }
+}
+
+void permute_u2_bits(cd* m);
+
+// Replaces uncontrolled dense two-qubit gates by their Cartan form (see
+// namespace kak): B0, B1, diag, parity rotation (I_XRY), diag, A0, A1.
+std::vector<IOp> kak_expand(const std::vector<IOp>& in, bool specialised) {
+  if (!kak_enabled(specialised)) return in;
+  std::vector<IOp> out;
+  out.reserve(in.size() * 4);
+  for (const IOp& o : in) {
+    if (o.kind != I_U2 || !o.cq.empty()) { out.push_back(o); continue; }
+    IOp u = o;
+    if (u.tq[0] > u.tq[1]) {  // bit0 = the lower qubit
+      std::swap(u.tq[0], u.tq[1]);
+      permute_u2_bits(u.m);
+    }
+    cd A0[4], A1[4], B0[4], B1[4];
+    kak::C4 N;
+    if (!kak::decompose(u.m, A0, A1, B0, B1, N)) { out.push_back(o); continue; }
+    const int qa = u.tq[0], qb = u.tq[1];
+    // subspaces of N: even (x, y) = (|00>, |11>) = indices (0, 3);
+    // odd (x, y) = (qa=0 qb=1, qa=1 qb=0) = indices (2, 1)
+    const cd Ve[4] = {N[0], N[3], N[12], N[15]};
+    const cd Vo[4] = {N[10], N[9], N[6], N[5]};
+    cd le0, le1, re1, lo0, lo1, ro1;
+    double ce, se, co, so;
+    split_2x2(Ve, le0, le1, ce, se, re1);
+    split_2x2(Vo, lo0, lo1, co, so, ro1);
+    auto one = [&](int q, const cd* M) {
+      IOp g;
+      g.kind = I_U1; g.tq[0] = q; g.ntq = 1;
+      for (int i = 0; i < 4; ++i) g.m[i] = M[i];
+      out.push_back(g);
+    };
+    auto diag2 = [&](cd d0, cd d1, cd d2, cd d3) {  // index = bit(qa) + 2 bit(qb)
+      IOp g;
+      g.kind = I_DIAG2; g.dq[0] = qa; g.dq[1] = qb; g.ndq = 2;
+      g.m[0] = d0; g.m[1] = d1; g.m[2] = d2; g.m[3] = d3;
+      out.push_back(g);
+    };
+    one(qa, B0);
+    one(qb, B1);
+    if (se == 0.0 && so == 0.0) {  // N is diagonal
+      diag2(le0, lo1 * ro1, lo0, le1 * re1);
+    } else {
+      diag2(1.0, ro1, 1.0, re1);
+      // scaled rotation per subspace: (t, form) and the dropped factor
+      auto scaled = [](double c, double s, double& t, double& form, double& f) {
+        if (c >= s) { t = s / c; form = 0; f = c; } else { t = c / s; form = 1; f = s; }
+      };
+      double te, fe_form, fe, to, fo_form, fo;
+      scaled(ce, se, te, fe_form, fe);
+      scaled(co, so, to, fo_form, fo);
+      IOp x;
+      x.kind = I_XRY; x.tq[0] = qa; x.tq[1] = qb; x.ntq = 2;
+      x.m[0] = cd(te, fe_form);
+      x.m[1] = cd(to, fo_form);
+      out.push_back(x);
+      diag2(le0 * fe, lo1 * fo, lo0 * fo, le1 * fe);
+    }
+    one(qa, A0);
+    one(qb, A1);
   }
   return out;
 }
@@ -533,29 +898,87 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   std::vector<int> tpos(n, -1);  // global qubit -> tile position
   for (int k = 0; k < T; ++k) tpos[pp.S[k]] = k;
 
-  // Register blocks: consecutive ops whose targets fit in R tile positions
-  // (diagonal ops need no register position and join the current block).
+  // Register blocks.  The pass's ops form a dependency graph (two ops depend
+  // on each other when they share a qubit, unless both are diagonal).  Each
+  // block starts empty and repeatedly takes, in circuit order, every ready
+  // op that fits: diagonal ops always (they need no register position),
+  // others when their targets fit in R tile positions with the block's.  A
+  // block thus follows the light cone of its qubits instead of cutting the
+  // op list into consecutive runs.
   struct Blk { std::vector<int> regs; std::vector<int> ops; };
   std::vector<Blk> blks;
-  Blk cur;
-  for (int idx : pp.ops) {
-    const IOp& o = ops[idx];
-    std::vector<int> need;
-    for (int i = 0; i < o.ntq; ++i) {
-      int p = tpos[o.tq[i]];
-      if (p < 0) throw qs_error(QS_ERR_INVALID, "internal: pass target outside tile");
-      if (std::find(cur.regs.begin(), cur.regs.end(), p) == cur.regs.end()) need.push_back(p);
+  {
+    const int m = (int)pp.ops.size();
+    std::vector<std::vector<int>> succ(m);
+    std::vector<int> indeg(m, 0);
+    std::vector<uint64_t> qmask(m, 0);
+    std::vector<char> diag(m, 0);
+    std::vector<int> qs;
+    for (int i = 0; i < m; ++i) {
+      const IOp& o = ops[pp.ops[i]];
+      qubits_of(o, qs);
+      for (int q : qs) qmask[i] |= 1ull << q;
+      diag[i] = is_diag_kind(o.kind);
+      for (int k = 0; k < o.ntq; ++k)
+        if (tpos[o.tq[k]] < 0) throw qs_error(QS_ERR_INVALID, "internal: pass target outside tile");
     }
-    if ((int)(cur.regs.size() + need.size()) > R) {
+    // last op seen on each qubit, split into the trailing diagonal group and
+    // the last non-diagonal op, so edges stay O(ops * qubits)
+    std::vector<int> last_nd(64, -1);
+    std::vector<std::vector<int>> diag_since(64);
+    for (int i = 0; i < m; ++i) {
+      std::vector<int> preds;
+      for (int q = 0; q < 64; ++q) {
+        if (!((qmask[i] >> q) & 1ull)) continue;
+        if (diag[i]) {
+          if (last_nd[q] >= 0) preds.push_back(last_nd[q]);
+        } else {
+          if (last_nd[q] >= 0) preds.push_back(last_nd[q]);
+          for (int d : diag_since[q]) preds.push_back(d);
+        }
+      }
+      std::sort(preds.begin(), preds.end());
+      preds.erase(std::unique(preds.begin(), preds.end()), preds.end());
+      for (int pi : preds) { succ[pi].push_back(i); ++indeg[i]; }
+      for (int q = 0; q < 64; ++q) {
+        if (!((qmask[i] >> q) & 1ull)) continue;
+        if (diag[i]) diag_since[q].push_back(i);
+        else { last_nd[q] = i; diag_since[q].clear(); }
+      }
+    }
+    std::set<int> ready;
+    for (int i = 0; i < m; ++i)
+      if (indeg[i] == 0) ready.insert(i);
+    int placed = 0;
+    while (placed < m) {
+      Blk cur;
+      bool took = true;
+      while (took) {
+        took = false;
+        for (auto it = ready.begin(); it != ready.end(); ++it) {
+          const int i = *it;
+          const IOp& o = ops[pp.ops[i]];
+          std::vector<int> need;
+          for (int k = 0; k < o.ntq; ++k) {
+            const int p = tpos[o.tq[k]];
+            if (std::find(cur.regs.begin(), cur.regs.end(), p) == cur.regs.end()) need.push_back(p);
+          }
+          if ((int)(cur.regs.size() + need.size()) > R) continue;
+          for (int p : need) cur.regs.push_back(p);
+          cur.ops.push_back(pp.ops[i]);
+          ready.erase(it);
+          ++placed;
+          for (int sidx : succ[i])
+            if (--indeg[sidx] == 0) ready.insert(sidx);
+          took = true;
+          break;  // rescan from the earliest ready op
+        }
+      }
+      if (cur.ops.empty()) throw qs_error(QS_ERR_INVALID, "internal: no op fits an empty register block");
       blks.push_back(cur);
-      cur = Blk();
-      need.clear();
-      for (int i = 0; i < o.ntq; ++i) need.push_back(tpos[o.tq[i]]);
     }
-    for (int p : need) cur.regs.push_back(p);
-    cur.ops.push_back(idx);
+    if (blks.empty()) blks.push_back(Blk());
   }
-  if (!cur.ops.empty() || blks.empty()) blks.push_back(cur);
 
   std::vector<DevBlock> dblocks;
   std::vector<DevOp> dops;
@@ -676,6 +1099,13 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
           has2 = 1;
           break;
         }
+        case I_XRY: {  // tq[0] < tq[1], and register order follows qubit order
+          const int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
+          if (a >= c) throw qs_error(QS_ERR_INVALID, "internal: parity rotation bits out of order");
+          d.kind = DK_XRY; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c; ncoef = 2;
+          has2 = 1;
+          break;
+        }
         default: throw qs_error(QS_ERR_INVALID, "internal: unexpected op kind in block");
       }
       d.ncoef = (uint8_t)ncoef;
@@ -730,6 +1160,7 @@ double op_flops(const IOp& o) {
   switch (o.kind) {
     case I_U1: return 16;
     case I_U2: return 32;
+    case I_XRY: return 4;
     case I_RY: return o.cq.empty() ? 4 : 8;
     case I_PHASE: case I_DIAG1: case I_DIAG2: return 8;
     default: return 0;
@@ -738,10 +1169,11 @@ double op_flops(const IOp& o) {
 
 }  // namespace
 
-void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* plan, int block_bits) {
+void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* plan, int block_bits,
+                   bool specialised) {
   QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
-  std::vector<IOp> norm = normalise(n, ops, nops);
+  std::vector<IOp> norm = kak_expand(normalise(n, ops, nops), specialised);
   std::vector<IOp> fused = schedule_runs(n, fuse_1q(n, norm, true));
   int T = n <= 14 ? n : tile_bits;
   std::vector<PassPlan> passes = split_passes(n, T, fused);
@@ -850,7 +1282,7 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   QS_CHECK_ARG(out != nullptr, "out is null");
   *out = nullptr;
   p = new qs_plan_s();
-  qs_build_plan(n, ops, nops, h->tile_bits, p, h->block_bits);
+  qs_build_plan(n, ops, nops, h->tile_bits, p, h->block_bits, h->jit_mode == 2);
   qs_plan_upload(h, p);
   *out = p;
   p = nullptr;
@@ -880,8 +1312,8 @@ int qs_plan_analyze(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_in
   QS_API_END(h)
 }
 
-int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_bits, void* out, size_t cap,
-                    size_t* needed) {
+int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_bits, int specialised, void* out,
+                    size_t cap, size_t* needed) {
   qs_context* h = nullptr;
   QS_API_BEGIN
   QS_CHECK_ARG(needed != nullptr, "needed is null");
@@ -890,7 +1322,7 @@ int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
   QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
   qs_plan_s p;
-  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits);
+  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, specialised != 0);
   *needed = p.blob.size();
   if (out && cap >= p.blob.size() && !p.blob.empty()) std::memcpy(out, p.blob.data(), p.blob.size());
   QS_API_END(h)
@@ -904,7 +1336,7 @@ int qs_plan_jit_check(int n, const qs_op* ops, int nops, int tile_bits, int bloc
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
   QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
   qs_plan_s p;
-  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits);
+  qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, true);
   std::string err;
   if (!qs_jit_compile_only(&p, err)) throw qs_error(QS_ERR_INVALID, "pass specialisation: " + err);
   if (n_passes) *n_passes = (int)p.pass_offsets.size();

@@ -30,17 +30,18 @@ OP_DT = np.dtype({"names": ["kind", "t0", "t1", "rc", "d0", "d1", "ncoef", "pad0
 assert PASS_DT.itemsize == 112 and BLOCK_DT.itemsize == 16
 
 DK_U1, DK_U2, DK_X, DK_SWAP, DK_Y = 1, 2, 3, 4, 5
-DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE = 10, 11, 12, 13, 14
+DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE, DK_XRY = 10, 11, 12, 13, 14, 15
 
 
-def program(n, ops, tile_bits=0, block_bits=0) -> bytes:
+def program(n, ops, tile_bits=0, block_bits=0, specialised=False) -> bytes:
     L = _lib.load()
     ops = np.ascontiguousarray(ops)
     p = ops.ctypes.data_as(C.POINTER(_lib.QsOp))
     need = C.c_size_t(0)
-    _lib.check(L.qs_plan_program(n, p, len(ops), tile_bits, block_bits, None, 0, C.byref(need)))
+    sp = int(bool(specialised))
+    _lib.check(L.qs_plan_program(n, p, len(ops), tile_bits, block_bits, sp, None, 0, C.byref(need)))
     buf = (C.c_char * max(1, need.value))()
-    _lib.check(L.qs_plan_program(n, p, len(ops), tile_bits, block_bits, buf, need.value, C.byref(need)))
+    _lib.check(L.qs_plan_program(n, p, len(ops), tile_bits, block_bits, sp, buf, need.value, C.byref(need)))
     return bytes(buf)[: need.value]
 
 
@@ -148,6 +149,20 @@ def _apply(psi, o, cf, raw, regq, R, idx, gidx, jreg):
         return psi
     if kind == DK_SCALE:
         return psi * float(raw[2 * c0])
+    if kind == DK_XRY:
+        qa, qb = regq[int(o["t0"])], regq[int(o["t1"])]
+        ma, mb = np.uint64(1 << qa), np.uint64(1 << qb)
+        for par in (0, 1):   # 0: (|00>, |11>), 1: (|qa=0 qb=1>, |qa=1 qb=0>)
+            x = idx[((idx & ma) == 0) & (((idx & mb) != 0) == bool(par))]
+            y = x ^ (ma | mb)
+            x, y = x.astype(np.int64), y.astype(np.int64)
+            t, form = float(raw[2 * (c0 + par)]), float(raw[2 * (c0 + par) + 1])
+            a0, a1 = psi[x].copy(), psi[y].copy()
+            if form == 0.0:
+                psi[x], psi[y] = a0 - t * a1, a1 + t * a0
+            else:
+                psi[x], psi[y] = t * a0 - a1, a0 + t * a1
+        return psi
     if kind in (DK_U2, DK_SWAP):
         qa, qb = regq[int(o["t0"])], regq[int(o["t1"])]
         ma, mb = np.uint64(1 << qa), np.uint64(1 << qb)

@@ -41,9 +41,12 @@ def _same_bits(a, b):
     return np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+@pytest.mark.parametrize("kak", ["0", "1"])
 @pytest.mark.parametrize("n,tile_bits,block_bits", [(6, 10, 5), (13, 10, 4), (15, 12, 3), (17, 13, 5),
                                                     (18, 14, 5), (17, 10, 2)])
-def test_random_all_kinds_bit_identical(n, tile_bits, block_bits):
+def test_random_all_kinds_bit_identical(n, tile_bits, block_bits, kak, monkeypatch):
+    # the same plan (Cartan split of dense 2Q gates forced on or off) on both kernels
+    monkeypatch.setenv("QSIM_KAK", kak)
     rng = np.random.default_rng(5000 + n)
     ops = _random_ops(n, 100, rng)
     psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
@@ -67,12 +70,15 @@ def test_layers_from_zero_bit_identical(tile_bits, block_bits):
     assert abs(1 - O.fidelity(got, O.simulate(20, ops))) <= 1e-6
 
 
-def test_qv_bit_identical():
+@pytest.mark.parametrize("kak", ["0", "1"])
+def test_qv_bit_identical(kak, monkeypatch):
+    monkeypatch.setenv("QSIM_KAK", kak)
     ops = W.qv_ops(14, 14, 7)
     ref, _ = _run(14, ops, 0)
     got, info = _run(14, ops, 2)
     assert info["n_jit_passes"] == info["n_passes"]
     assert _same_bits(ref, got)
+    assert abs(1 - O.fidelity(got, O.simulate(14, ops))) <= 1e-6
 
 
 def test_tiered_mode_switches_over_and_matches():

@@ -13,8 +13,8 @@ from qsim_b200 import workloads as W
 from test_oracle_golden import _random_ops
 
 
-def _check(n, ops, tile_bits, block_bits, psi0=None):
-    blob = PE.program(n, ops, tile_bits, block_bits)
+def _check(n, ops, tile_bits, block_bits, psi0=None, specialised=False):
+    blob = PE.program(n, ops, tile_bits, block_bits, specialised)
     if psi0 is None:
         psi0 = np.zeros(1 << n, complex)
         psi0[0] = 1
@@ -25,13 +25,14 @@ def _check(n, ops, tile_bits, block_bits, psi0=None):
     return len(PE.decode(blob))
 
 
+@pytest.mark.parametrize("specialised", [False, True])
 @pytest.mark.parametrize("n,tile_bits,block_bits", [(3, 10, 5), (6, 10, 5), (10, 10, 4), (12, 10, 3),
                                                     (13, 10, 5), (12, 10, 2), (13, 11, 5)])
-def test_random_all_kinds(n, tile_bits, block_bits):
+def test_random_all_kinds(n, tile_bits, block_bits, specialised):
     rng = np.random.default_rng(7000 + n)
     ops = _random_ops(n, 100, rng)
     psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
-    _check(n, ops, tile_bits, block_bits, psi0 / np.linalg.norm(psi0))
+    _check(n, ops, tile_bits, block_bits, psi0 / np.linalg.norm(psi0), specialised)
 
 
 @pytest.mark.parametrize("tile_bits,block_bits", [(10, 5), (12, 4), (11, 3)])
@@ -39,8 +40,9 @@ def test_layered_brickwork_multipass(tile_bits, block_bits):
     assert _check(16, W.layers_ops(16, 8, seed=3), tile_bits, block_bits) > 1
 
 
-def test_qv():
-    _check(12, W.qv_ops(12, 12, 0), 10, 5)
+@pytest.mark.parametrize("specialised", [False, True])
+def test_qv(specialised):
+    _check(12, W.qv_ops(12, 12, 0), 10, 5, specialised=specialised)
 
 
 def test_scale_folding_long_rotation_chain():
@@ -55,3 +57,42 @@ def test_scale_folding_long_rotation_chain():
         r["q"][0] = k % n
         r["m"][0] = rng.uniform(0.3, 2.8)
     _check(n, recs, 10, 5)
+
+
+def _u2_record(m, q0, q1):
+    from qsim_b200.circuit import OP_DTYPE
+    r = np.zeros(1, dtype=OP_DTYPE)
+    r["kind"], r["nq"], r["param"] = 2, 2, -1
+    r["q"][0, 0], r["q"][0, 1] = q0, q1
+    flat = np.asarray(m, dtype=np.complex128).reshape(-1)
+    r["m"][0, :32:2] = flat.real
+    r["m"][0, 1:32:2] = flat.imag
+    return r
+
+
+def test_cartan_split_special_two_qubit_gates():
+    """Dense 4x4 gates with degenerate Cartan forms (product, diagonal, CNOT,
+    SWAP, iSWAP, sqrt(SWAP), identity) and random ones, on both qubit orders."""
+    rng = np.random.default_rng(21)
+    I2 = np.eye(2)
+    X = np.array([[0, 1], [1, 0]])
+    H = np.array([[1, 1], [1, -1]]) / np.sqrt(2)
+    cnot = np.array([[1, 0, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0], [0, 1, 0, 0]])
+    swap = np.eye(4)[[0, 2, 1, 3]]
+    iswap = np.array([[1, 0, 0, 0], [0, 0, 1j, 0], [0, 1j, 0, 0], [0, 0, 0, 1]])
+    sq = np.array([[1, 0, 0, 0], [0, (1 + 1j) / 2, (1 - 1j) / 2, 0], [0, (1 - 1j) / 2, (1 + 1j) / 2, 0], [0, 0, 0, 1]])
+    mats = [np.eye(4), np.kron(H, X), np.diag(np.exp(1j * rng.uniform(0, 6, 4))), cnot, swap, iswap, sq,
+            np.kron(I2, H) @ cnot]
+    mats += [W.G.haar_unitary(rng, 4) for _ in range(6)]
+    n = 6
+    recs = []
+    for k, m in enumerate(mats):
+        q0, q1 = (k % n, (k * 3 + 1) % n) if k % 2 else ((k * 3 + 1) % n, k % n)
+        if q0 == q1:
+            q1 = (q0 + 1) % n
+        recs.append(_u2_record(m, q0, q1))
+        recs.append(_u2_record(W.G.haar_unitary(rng, 4), (q0 + 2) % n, (q1 + 3) % n)
+                    if (q0 + 2) % n != (q1 + 3) % n else _u2_record(np.eye(4), 0, 1))
+    ops = np.concatenate(recs)
+    psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    _check(n, ops, 10, 5, psi0 / np.linalg.norm(psi0), specialised=True)
