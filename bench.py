@@ -7,8 +7,16 @@ Workloads (--workload):
             state resident in HBM; e2e = gates/s of the public call path
             (host op list -> plan upload -> passes -> 1024 shots -> host).
   qv_batch  4096 Quantum-Volume circuits, widths uniform in [10, 20], depth =
-            width, per-circuit seeds; value = circuits/s of the batch engine.
+            width, per-circuit seeds; value = circuits/s of the batch engine,
+            beside one plan per circuit on the same GPU.
   qv12      one 12-qubit, depth-12 QV circuit; value = circuits/s.
+  adjoint   20-qubit EfficientSU2 (4 reps, 200 parameters), 256-term
+            observable, batch 64; value = gradients/s, with the energy-only
+            forward timed for the gradient/forward ratio.
+  serving   seeded Poisson request streams (QV circuits with shots, ansatz
+            gradients, Chebyshev evolutions) at rates 50..2000 req/s through
+            the continuous-batching server; value = served requests/s at the
+            highest rate, p50/p99 per rate, serial plain execution beside it.
 
 --impl reference times the CPU implementation of the same workload: the FP64
 statevector restatement (oracle/sv64.c, OpenMP on all host cores) on a
@@ -213,7 +221,12 @@ def bench_layers32(args, dev):
                    "l2": "state 32 GiB >> 126 MB L2 (no flush needed)"},
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": kernel, "peak_source": src,
+                     # dram read+write per launch from the ncu capture of the
+                     # same kernel at 26 qubits (537.0 + 478.6 MB), scaled by
+                     # the amplitudes per launch (traffic grows in proportion)
+                     "traffic": (537.0e6 + 478.6e6) * 2.0 ** (n - 26) if n >= 26 else None,
+                     "traffic_source": "ncu dram__bytes_read/write.sum, 26-qubit capture scaled by 2^(n-26)",
+                     "kernel": kernel, "peak_source": src,
                      "algorithmic_bytes_per_launch": algo_bytes / P},
         "e2e": {"value": ws * ngates / te, "unit": "gates/s", "h2d_bytes_per_step": plan_bytes,
                 "d2h_bytes_per_step": shots * 8},
@@ -502,7 +515,72 @@ def bench_serving(args, dev):
     return res, {"unit": "requests/s"}
 
 
-WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving}
+def bench_adjoint(args, dev):
+    """Energy and full gradient of a 20-qubit EfficientSU2 ansatz (4 reps,
+    200 parameters) for a batch of 64 parameter vectors, observable = 256
+    random Pauli strings of weight 1-4.  value = gradient evaluations
+    (parameter vectors) per second through the adjoint kernels; the forward
+    (energies only: batched circuits + <H>) is timed on the same batch for the
+    backward/forward ratio."""
+    import numpy as np
+    import torch
+    from qsim_b200 import engine as E
+    from qsim_b200 import workloads as W
+    from qsim_b200.circuit import lower
+    n, B = args.qubits if args.qubits != 32 else 20, 64
+    qc, npar = W.efficient_su2(n, reps=4)
+    ops = lower(qc)
+    obs = W.random_pauli_observable(n, 256, seed=3)
+    params = np.random.default_rng(8).uniform(0, 2 * math.pi, (B, npar))
+    stream = torch.cuda.current_stream(dev)
+    pidx = ops["param"].astype(np.int64)
+
+    def forward():
+        bound = np.concatenate([ops] * B)
+        for b in range(B):
+            blk = bound[b * len(ops):(b + 1) * len(ops)]
+            sel = pidx >= 0
+            blk["m"][sel, 0] = params[b, pidx[sel]]
+        widths = np.full(B, n, dtype=np.int32)
+        oo = np.arange(B + 1, dtype=np.int64) * len(ops)
+        so = np.arange(B, dtype=np.int64) << n
+        bp = E.BatchPlan(widths, oo, bound, so, dev)
+        st = bp.alloc_states()
+        bp.execute(st)
+        return [E.expect_pauli_sum(st[b << n:(b + 1) << n], obs) for b in range(B)]
+
+    def gradient():
+        return E.adjoint_gradient(n, ops, npar, params, obs, dev)
+
+    for _ in range(args.warmup):
+        forward()
+        gradient()
+    h = E._h(dev)
+    with ClockSampler(dev) as clk:
+        t_f = _cuda_time(forward, stream, args.steps) / args.steps
+        l0 = h.launches()
+        t_g = _cuda_time(gradient, stream, args.steps) / args.steps
+        launches = h.launches() - l0
+    t_f, t_g = reduce_max(t_f, f"cuda:{dev}"), reduce_max(t_g, f"cuda:{dev}")
+    e_f = np.array(forward())
+    e_g, g = gradient()
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    amp = B << n
+    return {"metric": METRIC, "value": ws * B / t_g, "unit": "gradients/s", "ms_per_step": t_g * 1e3,
+            "dtype": "c64 state, fp64 gradient accumulation",
+            "config": {"workload": f"adjoint: EfficientSU2 {n} qubits, 4 reps, {npar} params, 256-term observable, "
+                                   f"batch {B}", "l2": f"{amp * 8 >> 20} MiB of states per batch > L2"},
+            "forward_ms": t_f * 1e3, "gradient_over_forward": t_g / t_f,
+            "energy_agreement": float(np.max(np.abs(e_f - e_g))),
+            "e2e": {"value": ws * B / t_g, "unit": "gradients/s", "h2d_bytes_per_step": int(params.nbytes + ops.nbytes),
+                    "d2h_bytes_per_step": int(g.nbytes + e_g.nbytes),
+                    "note": "host parameters in, host FP64 gradients out, every step"},
+            "gpu_launches": int(launches // max(1, args.steps)) * args.steps, "clocks": clk.summary()}, \
+        {"unit": "gradients/s"}
+
+
+WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
+             "adjoint": bench_adjoint}
 
 
 # --------------------------------------------------------- CPU baseline
