@@ -237,6 +237,7 @@ def bench_layers32(args, dev):
 
 
 def bench_qv_batch(args, dev):
+    import ctypes as ct
     import numpy as np
     import torch
     from qsim_b200 import engine as E
@@ -273,11 +274,27 @@ def bench_qv_batch(args, dev):
     ev1.record(stream)
     torch.cuda.synchronize()
     t_plain = ev0.elapsed_time(ev1) / 1000.0
-    # weight the sample to the full width distribution
-    per_width = {}
-    for (w, _), c in zip(plans, idx):
-        per_width.setdefault(w, []).append(c)
     plain_cps = len(idx) / t_plain
+    # the reference's plain path: one launch per gate (state init + every
+    # U(4) through qs_apply_2q), on the same sample of circuits
+    hdl = E._h(dev)
+    mats = [[np.ascontiguousarray(np.asarray(r["m"][:32], dtype=np.float32)) for r in ops[oo[c]:oo[c + 1]]]
+            for c in idx]
+
+    def per_gate():
+        for (w, _), b, c, ms in zip(plans, bufs, idx, mats):
+            hdl.call("qs_state_init", ct.c_void_p(b.data_ptr()), int(w))
+            for r, m in zip(ops[oo[c]:oo[c + 1]], ms):
+                hdl.call("qs_apply_2q", ct.c_void_p(b.data_ptr()), int(w),
+                         m.ctypes.data_as(ct.POINTER(ct.c_float)), int(r["q"][0]), int(r["q"][1]))
+
+    per_gate()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    per_gate()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    pergate_cps = len(idx) / (ev0.elapsed_time(ev1) / 1000.0)
     # e2e: host ops -> batch plan (FP64 fusion, H2D) -> run -> probabilities of
     # circuit 0 back to the host, every step
     ops_host = np.ascontiguousarray(ops)
@@ -305,10 +322,14 @@ def bench_qv_batch(args, dev):
                    "launches_per_step": bp.info["n_launches"], "items": bp.info["n_items"],
                    "max_passes": bp.info["max_passes"], "l2": "6.2 GB of states >> L2"},
         "per_circuit_launches": {"value": plain_cps, "unit": "circuits/s",
-                                 "sample": f"{len(idx)} random circuits of the batch, one plan per circuit"},
+                                 "sample": f"{len(idx)} random circuits of the batch, one fused plan per circuit"},
+        "per_gate_launches": {"value": pergate_cps, "unit": "circuits/s",
+                              "sample": f"the same {len(idx)} circuits, one launch per gate (the reference's "
+                                        f"dispatch: state init + qs_apply_2q per U(4))"},
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_pass<5>", "peak_source": src},
+                     "traffic": None, "kernel": "k_pass<R> (generic tile-pass kernel, batched items)",
+                     "peak_source": src},
         "e2e": {"value": ws * C / te, "unit": "circuits/s", "h2d_bytes_per_step": int(ops.nbytes),
                 "d2h_bytes_per_step": 8 << int(widths[0])},
         "gpu_launches": int(launches // max(1, args.steps)) * args.steps,

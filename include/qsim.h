@@ -98,7 +98,8 @@ const char* qs_version(void);
 /* Tile bits used by the fused-pass planner (10..14); 0 = default (13).      */
 int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
 /* Register-block width used by the planner (2..5 qubits per thread group);
- * 0 = default (5).                                                          */
+ * 0 = automatic (5 for plans compiled into specialised passes, 4 for the
+ * generic pass kernel, batches included).                                   */
 int  qs_set_block_bits(qs_handle_t h, int block_bits);
 /* Pass specialisation: a plan's tile passes may be compiled (NVRTC) into
  * kernels with their gate positions and coefficients built in; results are

@@ -125,8 +125,7 @@ int qs_set_tile_bits(qs_handle_t h, int tile_bits) {
 int qs_set_block_bits(qs_handle_t h, int bb) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
-  if (bb == 0) bb = 5;
-  QS_CHECK_ARG(bb >= 2 && bb <= 5, "block_bits must be in [2, 5]");
+  QS_CHECK_ARG(bb == 0 || (bb >= 2 && bb <= 5), "block_bits must be 0 (auto) or in [2, 5]");
   h->block_bits = bb;
   QS_API_END(h)
 }

@@ -39,7 +39,7 @@ struct qs_context {
   cudaStream_t stream = nullptr;
   std::string err;
   int tile_bits = 13;
-  int block_bits = 5;
+  int block_bits = 0;   // 0: 5 for specialised plans, 4 for the generic kernel
   // Pass specialisation (qs_jit.cpp): 0 off, 1 plans on >= jit_min_qubits,
   // 2 every plan.
   int jit_mode = 1;
@@ -68,7 +68,7 @@ void qs_after_launch(qs_context* h, const char* what);
 // amplitudes (R <= 5 tile positions) on which its ops run in registers.
 enum DevKind : uint8_t {
   DK_U1 = 1,     // controlled dense 2x2 on register bit t0
-  DK_U2 = 2,     // controlled dense 4x4 on register bits t0 (bit0) < t1 (bit1)
+  DK_U2 = 2,     // dense 4x4 on register bits t0 (bit0) < t1 (bit1), no controls
   DK_X = 3,      // controlled exact swap across register bit t0
   DK_SWAP = 4,   // controlled exact swap of |..01..> and |..10..> (t0 < t1)
   DK_Y = 5,      // controlled exact Pauli-Y on t0
@@ -91,6 +91,7 @@ enum DevKind : uint8_t {
                  // (x, y) = (|t0=0 t1=0>, |11>) use c[0] = (t, form), the
                  // pairs (|t0=0 t1=1>, |t0=1 t1=0>) use c[1]; each pair as in
                  // DK_KRY (the dropped factors are already in the next diagonal)
+  DK_CU2 = 16,   // DK_U2 with controls (rc on register bits, gc on the index)
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -167,7 +168,7 @@ void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
 // `specialised`: the plan will run as specialised passes (enables the Cartan
 // split of dense two-qubit gates, which only pays off there).
-void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 5,
+void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 0,
                    bool specialised = false);
 void qs_plan_upload(qs_context* h, qs_plan_s* p);
 void qs_plan_free_device(void* d);  // stream-ordered free (no device sync)

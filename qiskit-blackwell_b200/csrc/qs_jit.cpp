@@ -275,6 +275,7 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         break;
       }
       case DK_U2:
+      case DK_CU2:
       case DK_SWAP: {
         const int A = op.t0, B = op.t1;
         for (int j = 0; j < J; ++j) {

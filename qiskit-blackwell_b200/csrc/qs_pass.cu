@@ -113,13 +113,33 @@ __device__ __forceinline__ void op_ry(float2 (&v)[1 << R], float2 cs, unsigned r
   }
 }
 
+// Uncontrolled dense 4x4 (DK_U2): no predication.
 template <int R, int A, int B>
-__device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
+__device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restrict__ c) {
   if constexpr (A < B && B < R) {
     float2 g[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) g[i] = c[i];
-    const bool all = (rc == 0 && gp);
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & ((1 << A) | (1 << B))) continue;
+      const int j1 = j | (1 << A), j2 = j | (1 << B), j3 = j1 | (1 << B);
+      const float2 a0 = v[j], a1 = v[j1], a2 = v[j2], a3 = v[j3];
+      v[j] = cfma4(g + 0, a0, a1, a2, a3);
+      v[j1] = cfma4(g + 4, a0, a1, a2, a3);
+      v[j2] = cfma4(g + 8, a0, a1, a2, a3);
+      v[j3] = cfma4(g + 12, a0, a1, a2, a3);
+    }
+  }
+}
+
+// Controlled dense 4x4 (DK_CU2): each quad is updated where its controls hold.
+template <int R, int A, int B>
+__device__ __forceinline__ void op_cu2(float2 (&v)[1 << R], const float2* __restrict__ c, unsigned rc, bool gp) {
+  if constexpr (A < B && B < R) {
+    float2 g[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) g[i] = c[i];
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & ((1 << A) | (1 << B))) continue;
@@ -129,7 +149,7 @@ __device__ __forceinline__ void op_u2(float2 (&v)[1 << R], const float2* __restr
       const float2 n1 = cfma4(g + 4, a0, a1, a2, a3);
       const float2 n2 = cfma4(g + 8, a0, a1, a2, a3);
       const float2 n3 = cfma4(g + 12, a0, a1, a2, a3);
-      const bool p = all || (gp && ((j & rc) == rc));
+      const bool p = gp && ((j & rc) == rc);
       v[j] = p ? n0 : a0;
       v[j1] = p ? n1 : a1;
       v[j2] = p ? n2 : a2;
@@ -406,7 +426,12 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
         break;
       case DK_U2:
         if constexpr (TWO) {
-          switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c, rc, gp) }
+          switch (op.t0 * 8 + op.t1) { CASES_2(op_u2, v, c) }
+        }
+        break;
+      case DK_CU2:
+        if constexpr (TWO) {
+          switch (op.t0 * 8 + op.t1) { CASES_2(op_cu2, v, c, rc, gp) }
         }
         break;
       case DK_SWAP:

@@ -1086,7 +1086,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
         case I_U2: {
           int a = regidx(o.tq[0]), c = regidx(o.tq[1]);
           if (a > c) { std::swap(a, c); permute_u2_bits(o.m); }
-          d.kind = DK_U2; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c; ncoef = 16;
+          d.kind = (d.rc || d.gc) ? DK_CU2 : DK_U2; d.t0 = (uint8_t)a; d.t1 = (uint8_t)c; ncoef = 16;
           has2 = 1;
           break;
         }
@@ -1173,6 +1173,10 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
                    bool specialised) {
   QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
+  // register blocks: 5 qubits for specialised passes, 4 for the generic kernel
+  // (fewer registers, higher occupancy: measured faster there)
+  if (block_bits == 0) block_bits = specialised ? 5 : 4;
+  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
   std::vector<IOp> norm = kak_expand(normalise(n, ops, nops), specialised);
   std::vector<IOp> fused = schedule_runs(n, fuse_1q(n, norm, true));
   int T = n <= 14 ? n : tile_bits;
@@ -1318,9 +1322,8 @@ int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_
   QS_API_BEGIN
   QS_CHECK_ARG(needed != nullptr, "needed is null");
   if (tile_bits == 0) tile_bits = 13;
-  if (block_bits == 0) block_bits = 5;
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
-  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
+  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 5 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 5]");
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, specialised != 0);
   *needed = p.blob.size();
@@ -1332,9 +1335,8 @@ int qs_plan_jit_check(int n, const qs_op* ops, int nops, int tile_bits, int bloc
   qs_context* h = nullptr;
   QS_API_BEGIN
   if (tile_bits == 0) tile_bits = 13;
-  if (block_bits == 0) block_bits = 5;
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
-  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
+  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 5 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 5]");
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, true);
   std::string err;

@@ -30,7 +30,7 @@ OP_DT = np.dtype({"names": ["kind", "t0", "t1", "rc", "d0", "d1", "ncoef", "pad0
 assert PASS_DT.itemsize == 112 and BLOCK_DT.itemsize == 16
 
 DK_U1, DK_U2, DK_X, DK_SWAP, DK_Y = 1, 2, 3, 4, 5
-DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE, DK_XRY = 10, 11, 12, 13, 14, 15
+DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE, DK_XRY, DK_CU2 = 10, 11, 12, 13, 14, 15, 16
 
 
 def program(n, ops, tile_bits=0, block_bits=0, specialised=False) -> bytes:
@@ -163,7 +163,7 @@ def _apply(psi, o, cf, raw, regq, R, idx, gidx, jreg):
             else:
                 psi[x], psi[y] = t * a0 - a1, a0 + t * a1
         return psi
-    if kind in (DK_U2, DK_SWAP):
+    if kind in (DK_U2, DK_CU2, DK_SWAP):
         qa, qb = regq[int(o["t0"])], regq[int(o["t1"])]
         ma, mb = np.uint64(1 << qa), np.uint64(1 << qb)
         base = idx[((idx & ma) == 0) & ((idx & mb) == 0)]

@@ -74,8 +74,8 @@ def test_layers_from_zero_bit_identical(tile_bits, block_bits):
 def test_qv_bit_identical(kak, monkeypatch):
     monkeypatch.setenv("QSIM_KAK", kak)
     ops = W.qv_ops(14, 14, 7)
-    ref, _ = _run(14, ops, 0)
-    got, info = _run(14, ops, 2)
+    ref, _ = _run(14, ops, 0, None, 0, 5)    # same register-block width on both kernels
+    got, info = _run(14, ops, 2, None, 0, 5)
     assert info["n_jit_passes"] == info["n_passes"]
     assert _same_bits(ref, got)
     assert abs(1 - O.fidelity(got, O.simulate(14, ops))) <= 1e-6
