@@ -125,7 +125,7 @@ int qs_set_tile_bits(qs_handle_t h, int tile_bits) {
 int qs_set_block_bits(qs_handle_t h, int bb) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
-  QS_CHECK_ARG(bb == 0 || (bb >= 2 && bb <= 5), "block_bits must be 0 (auto) or in [2, 5]");
+  QS_CHECK_ARG(bb == 0 || (bb >= 2 && bb <= 6), "block_bits must be 0 (auto) or in [2, 6] (6: specialised plans only)");
   h->block_bits = bb;
   QS_API_END(h)
 }

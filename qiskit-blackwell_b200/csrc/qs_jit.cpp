@@ -134,6 +134,11 @@ __device__ __forceinline__ float2 rtb0(float t, float2 a0, float2 a1) {
   return __ffma2_rn(make_float2(t, t), a0, make_float2(-a1.x, -a1.y));
 }
 __device__ __forceinline__ float2 rtb1(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(t, t), a1, a0); }
+// The same four updates as two scalar FMAs (identical results lane by lane).
+__device__ __forceinline__ float2 sta0(float t, float2 a0, float2 a1) { return make_float2(fmaf(-t, a1.x, a0.x), fmaf(-t, a1.y, a0.y)); }
+__device__ __forceinline__ float2 sta1(float t, float2 a0, float2 a1) { return make_float2(fmaf(t, a0.x, a1.x), fmaf(t, a0.y, a1.y)); }
+__device__ __forceinline__ float2 stb0(float t, float2 a0, float2 a1) { return make_float2(fmaf(t, a0.x, -a1.x), fmaf(t, a0.y, -a1.y)); }
+__device__ __forceinline__ float2 stb1(float t, float2 a0, float2 a1) { return make_float2(fmaf(t, a1.x, a0.x), fmaf(t, a1.y, a0.y)); }
 __device__ __forceinline__ float2 scl(float2 a, float f) { return make_float2(__fmul_rn(a.x, f), __fmul_rn(a.y, f)); }
 __device__ __forceinline__ float2 sgnw(float2 t, u32 w) {
   return make_float2(__uint_as_float(__float_as_uint(t.x) ^ w), __uint_as_float(__float_as_uint(t.y) ^ w));
@@ -182,12 +187,31 @@ struct Block {
 
 // Threads per CTA: one register group per thread, at most 128 for R = 5
 // blocks (QSIM_JIT_THREADS = 256 allows 256) and 256 otherwise.
+// Rotation pairs emitted as packed FP32x2 FMAs, except every `n`-th pair as
+// two scalar FMAs (QSIM_JIT_SCALAR_EVERY = n; 0 = all packed): a tuning knob
+// for the balance between the FMA sub-pipes.  Results are identical.
+int scalar_every() {
+  static const int n = [] {
+    const char* e = std::getenv("QSIM_JIT_SCALAR_EVERY");
+    return e ? std::max(0, std::atoi(e)) : 0;
+  }();
+  return n;
+}
+std::string rot_fn(bool form_b, bool second, int pair_index) {
+  const int n = scalar_every();
+  const bool scalar = n > 0 && (pair_index % n) == 0;
+  std::string f = scalar ? "st" : "rt";
+  f += form_b ? "b" : "a";
+  f += second ? "1(" : "0(";
+  return f;
+}
+
 int pass_threads(int T, int R) {
   static const int cap5 = [] {
     const char* e = std::getenv("QSIM_JIT_THREADS");
     return (e && std::atoi(e) == 256) ? 256 : 128;
   }();
-  return std::max(32, std::min(R == 5 ? cap5 : 256, 1 << (T - R)));
+  return std::max(32, std::min(R >= 5 ? cap5 : 256, 1 << (T - R)));
 }
 int pass_smem(int T) { return (8 << T) + 2 * 128 * 8; }
 
@@ -240,15 +264,17 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
       case DK_KU1: {
         for (int K = 0; K < R; ++K) {
           if (!((op.t0 >> K) & 1)) continue;
+          int pair = 0;
           for (int j = 0; j < J; ++j) {
             if ((j >> K) & 1) continue;
+            ++pair;
             const int k = j | (1 << K);
             const std::string a0 = G.v[j], a1 = G.v[k];
             if (op.kind == DK_KRY) {  // scaled rotation, form c[K].y (see DK_KRY)
               const std::string t = flit(c[K].x) + ", " + a0 + ", " + a1 + ")";
               const bool fb = c[K].y != 0.f;
-              G.set(j, (fb ? "rtb0(" : "rta0(") + t, "");
-              G.set(k, (fb ? "rtb1(" : "rta1(") + t, "");
+              G.set(j, rot_fn(fb, false, pair) + t, "");
+              G.set(k, rot_fn(fb, true, pair) + t, "");
             } else {
               const float2* g = c + 4 * K;
               G.set(j, "cfma2(" + c2(g[0]) + ", " + a0 + ", " + c2(g[1]) + ", " + a1 + ")", "");
@@ -263,14 +289,16 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         break;
       case DK_XRY: {  // parity rotation: pairs (j, j ^ (A|B)), coefficients by bit B
         const int A = op.t0, B = op.t1;
+        int pair = 0;
         for (int j = 0; j < J; ++j) {
           if ((j >> A) & 1) continue;
+          ++pair;
           const int k = j ^ ((1 << A) | (1 << B));
           const float2 tf = ((j >> B) & 1) ? c[1] : c[0];
           const std::string t = flit(tf.x) + ", " + G.v[j] + ", " + G.v[k] + ")";
           const bool fb = tf.y != 0.f;
-          G.set(j, (fb ? "rtb0(" : "rta0(") + t, "");
-          G.set(k, (fb ? "rtb1(" : "rta1(") + t, "");
+          G.set(j, rot_fn(fb, false, pair) + t, "");
+          G.set(k, rot_fn(fb, true, pair) + t, "");
         }
         break;
       }
@@ -321,27 +349,28 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         // gets one sign word per group; the word is XORed into the group
         // factor (or the table entry, or the amplitude) - the same bits the
         // generic kernel produces with its per-group mask.
-        std::vector<uint32_t> rms;
+        std::vector<uint64_t> rms;
         std::vector<std::string> sb;
         for (int k = 0; k < op.t1; ++k, p += 2) {
-          rms.push_back(bits32(p[0].x));
+          rms.push_back(bits64(p[0]));
           sb.push_back(G.name("sb"));
           o << "      const u32 " << sb.back() << " = " << mask_test(bits64(p[1]), G.uses_g)
             << " ? 0x80000000u : 0u;\n";
         }
-        std::map<uint32_t, std::string> word;  // term subset -> sign word
+        if (rms.size() > 64) throw qs_error(QS_ERR_INVALID, "tile-pass specialisation: too many sign terms");
+        std::map<uint64_t, std::string> word;  // term subset -> sign word
         auto subset = [&](int j) {
-          uint32_t sub = 0;
+          uint64_t sub = 0;
           for (size_t k = 0; k < rms.size(); ++k)
-            if ((rms[k] >> j) & 1u) sub |= 1u << k;
+            if ((rms[k] >> j) & 1ull) sub |= 1ull << k;
           return sub;
         };
-        auto sign_word = [&](uint32_t sub) -> std::string {
+        auto sign_word = [&](uint64_t sub) -> std::string {
           auto it = word.find(sub);
           if (it != word.end()) return it->second;
           std::string e;
           for (size_t k = 0; k < rms.size(); ++k)
-            if ((sub >> k) & 1u) e += (e.empty() ? "" : " ^ ") + sb[k];
+            if ((sub >> k) & 1ull) e += (e.empty() ? "" : " ^ ") + sb[k];
           const std::string w = G.name("sw");
           o << "      const u32 " << w << " = " << e << ";\n";
           word[sub] = w;
@@ -349,20 +378,20 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
         };
         if (!table && op.t0 == 0) {
           for (int j = 0; j < J; ++j) {
-            const uint32_t sub = subset(j);
+            const uint64_t sub = subset(j);
             if (sub) G.set(j, "sgnw(" + G.v[j] + ", " + sign_word(sub) + ")", "");
           }
         } else if (op.t0 == 0) {  // table only: the group factor is exactly 1
           for (int j = 0; j < J; ++j) {
-            const uint32_t sub = subset(j);
+            const uint64_t sub = subset(j);
             const std::string t = sub ? "sgnw(" + c2(Tt[j]) + ", " + sign_word(sub) + ")" : c2(Tt[j]);
             G.set(j, "cmul(" + G.v[j] + ", " + t + ")", "");
           }
         } else {
           const std::string fv = "make_float2(" + f + "r, " + f + "i)";
-          std::map<uint32_t, std::string> fs;  // term subset -> sign-adjusted group factor
+          std::map<uint64_t, std::string> fs;  // term subset -> sign-adjusted group factor
           for (int j = 0; j < J; ++j) {
-            const uint32_t sub = subset(j);
+            const uint64_t sub = subset(j);
             std::string fj = fv;
             if (sub) {
               auto it = fs.find(sub);
@@ -378,11 +407,11 @@ void gen_block(Block& G, int R, const DevOp* ops, int ob, int oe, const float2* 
           }
         }
         for (int k = 0; k < op.d0; ++k, p += 3) {
-          const uint32_t rm = bits32(p[0].x);
+          const uint64_t rm = bits64(p[0]);
           const std::string xp = G.name("xp");
           o << "      const bool " << xp << " = " << mask_test(bits64(p[1]), G.uses_g) << ";\n";
           for (int j = 0; j < J; ++j)
-            if ((rm >> j) & 1u) G.set(j, "cmul(" + G.v[j] + ", " + c2(p[2]) + ")", xp);
+            if ((rm >> j) & 1ull) G.set(j, "cmul(" + G.v[j] + ", " + c2(p[2]) + ")", xp);
         }
         break;
       }
@@ -569,9 +598,9 @@ bool nvrtc_compile(const std::string& src, std::string& cubin, std::string& err)
 // Register-allocation hint: the CTAs per SM that the tile's shared memory
 // allows (228 KiB per SM, 1 KiB reserved per CTA), capped so that a thread
 // keeps at least 128 registers.
-int min_blocks_for(int smem, int threads) {
+int min_blocks_for(int smem, int threads, int R) {
   const int by_smem = (228 * 1024) / (smem + 1024);
-  const int by_regs = 65536 / (threads * 128);
+  const int by_regs = 65536 / (threads * (R >= 6 ? 192 : 128));
   return std::max(1, std::min(std::min(4, by_smem), by_regs));
 }
 
@@ -617,7 +646,7 @@ std::string qs_jit_source(const qs_plan_s* p, size_t i) {
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
   return gen_pass(P, reinterpret_cast<const DevBlock*>(base + P.block_off),
                   reinterpret_cast<const DevOp*>(base + P.op_off), reinterpret_cast<const float2*>(base + P.coef_off),
-                  min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R)));
+                  min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R), P.R));
 }
 
 // A specialisation job: the plan's pass sources, the kernels found in the

@@ -792,8 +792,10 @@ void diag_terms(const IOp& o, std::vector<DTerm>& t) {
 // One DK_DTAB op (kernel layout, qs_pass.cu):
 //   pool: [2^R table entries (if rc & 1)]
 //         [t0 group terms:  (gmask lo, gmask hi) as raw bits, w]        2 float2 each
-//         [t1 sign terms:   (regmask32, 0), (gmask lo, gmask hi)]       2 float2 each
-//         [d0 cross terms:  (regmask32, 0), (gmask lo, gmask hi), w]    3 float2 each
+//         [t1 sign terms:   (regmask lo, hi), (gmask lo, gmask hi)]     2 float2 each
+//         [d0 cross terms:  (regmask lo, hi), (gmask lo, gmask hi), w]  3 float2 each
+// (regmask: bit j = register index j is affected; the high word is only
+// non-zero for 6-qubit register blocks, which only specialised passes use)
 // amplitude j of a group with global index gidx is multiplied by
 //   T[j] * prod_{group terms, gidx has gmask} w * prod_{cross, j in regmask, gidx has gmask} w
 // and negated where the XOR of the active sign terms' regmasks has bit j.
@@ -806,15 +808,15 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
   const int J = 1 << R;
   std::vector<cd> T(J, cd(1.0, 0.0));
   std::map<uint64_t, cd> gterm;
-  std::vector<std::pair<uint32_t, uint64_t>> sterm;
-  std::vector<std::tuple<uint32_t, uint64_t, cd>> xterm;
-  auto regmask32 = [&](uint64_t m) {
-    uint32_t rm = 0;
+  std::vector<std::pair<uint64_t, uint64_t>> sterm;
+  std::vector<std::tuple<uint64_t, uint64_t, cd>> xterm;
+  auto regmask = [&](uint64_t m) {
+    uint64_t rm = 0;
     for (int j = 0; j < J; ++j) {
       bool all = true;
       for (int k = 0; k < R; ++k)
         if (((m >> regq[k]) & 1ull) && !((j >> k) & 1)) all = false;
-      if (all) rm |= 1u << j;
+      if (all) rm |= 1ull << j;
     }
     return rm;
   };
@@ -822,16 +824,16 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
     if (d.w == 1.0) continue;
     const uint64_t mr = d.mask & rmask_all, mg = d.mask & ~rmask_all;
     if (mg == 0) {
-      const uint32_t rm = regmask32(mr);
+      const uint64_t rm = regmask(mr);
       for (int j = 0; j < J; ++j)
-        if ((rm >> j) & 1u) T[j] *= d.w;
+        if ((rm >> j) & 1ull) T[j] *= d.w;
     } else if (mr == 0) {
       auto it = gterm.find(mg);
       if (it == gterm.end()) gterm[mg] = d.w; else it->second *= d.w;
     } else if (d.w == -1.0) {
-      sterm.push_back({regmask32(mr), mg});
+      sterm.push_back({regmask(mr), mg});
     } else {
-      xterm.emplace_back(regmask32(mr), mg, d.w);
+      xterm.emplace_back(regmask(mr), mg, d.w);
     }
   }
   std::vector<std::pair<uint64_t, cd>> gl;
@@ -873,11 +875,11 @@ void encode_dtab(const std::vector<DTerm>& terms, const std::vector<int>& regq, 
       put(gl[gi].second);
     }
     for (size_t k = 0; k < ns; ++k, ++si) {
-      put_bits(sterm[si].first, 0);
+      put_bits((uint32_t)sterm[si].first, (uint32_t)(sterm[si].first >> 32));
       put_bits((uint32_t)sterm[si].second, (uint32_t)(sterm[si].second >> 32));
     }
     for (size_t k = 0; k < nx; ++k, ++xi) {
-      put_bits(std::get<0>(xterm[xi]), 0);
+      put_bits((uint32_t)std::get<0>(xterm[xi]), (uint32_t)(std::get<0>(xterm[xi]) >> 32));
       put_bits((uint32_t)std::get<1>(xterm[xi]), (uint32_t)(std::get<1>(xterm[xi]) >> 32));
       put(std::get<2>(xterm[xi]));
     }
@@ -1176,7 +1178,8 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   // register blocks: 5 qubits for specialised passes, 4 for the generic kernel
   // (fewer registers, higher occupancy: measured faster there)
   if (block_bits == 0) block_bits = specialised ? 5 : 4;
-  QS_CHECK_ARG(block_bits >= 2 && block_bits <= 5, "block_bits must be in [2, 5]");
+  QS_CHECK_ARG(block_bits >= 2 && block_bits <= (specialised ? 6 : 5),
+               "block_bits must be in [2, 5] (6 only for specialised passes)");
   std::vector<IOp> norm = kak_expand(normalise(n, ops, nops), specialised);
   std::vector<IOp> fused = schedule_runs(n, fuse_1q(n, norm, true));
   int T = n <= 14 ? n : tile_bits;
@@ -1323,7 +1326,7 @@ int qs_plan_program(int n, const qs_op* ops, int nops, int tile_bits, int block_
   QS_CHECK_ARG(needed != nullptr, "needed is null");
   if (tile_bits == 0) tile_bits = 13;
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
-  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 5 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 5]");
+  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 6 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 6]");
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, specialised != 0);
   *needed = p.blob.size();
@@ -1336,7 +1339,7 @@ int qs_plan_jit_check(int n, const qs_op* ops, int nops, int tile_bits, int bloc
   QS_API_BEGIN
   if (tile_bits == 0) tile_bits = 13;
   QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
-  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 5 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 5]");
+  QS_CHECK_ARG(block_bits >= 0 && block_bits <= 6 && block_bits != 1, "block_bits must be 0 (auto) or in [2, 6]");
   qs_plan_s p;
   qs_build_plan(n, ops, nops, tile_bits, &p, block_bits, true);
   std::string err;

@@ -192,21 +192,23 @@ def _apply(psi, o, cf, raw, regq, R, idx, gidx, jreg):
             gm = np.uint64(lo | (hi << 32))
             t = np.where((gidx & gm) == gm, t * cf[k + 1], t)
             k += 2
-        m = np.zeros(psi.shape, dtype=np.int64)
+        m = np.zeros(psi.shape, dtype=np.uint64)
         for _ in range(int(o["t1"])):
-            rm, _z = _bits(raw, k)
+            rlo, rhi = _bits(raw, k)
+            rm = rlo | (rhi << 32)
             lo, hi = _bits(raw, k + 1)
             gm = np.uint64(lo | (hi << 32))
-            m = np.where((gidx & gm) == gm, m ^ rm, m)
+            m = np.where((gidx & gm) == gm, m ^ np.uint64(rm), m)
             k += 2
-        sign = np.where((m >> jreg) & 1, -1.0, 1.0)
+        sign = np.where((m >> jreg.astype(np.uint64)) & np.uint64(1), -1.0, 1.0)
         psi = psi * t * sign
         for _ in range(int(o["d0"])):
-            rm, _z = _bits(raw, k)
+            rlo, rhi = _bits(raw, k)
+            rm = rlo | (rhi << 32)
             lo, hi = _bits(raw, k + 1)
             gm = np.uint64(lo | (hi << 32))
             w = cf[k + 2]
-            hit = ((gidx & gm) == gm) & (((rm >> jreg) & 1) == 1)
+            hit = ((gidx & gm) == gm) & (((np.uint64(rm) >> jreg.astype(np.uint64)) & np.uint64(1)) == 1)
             psi = np.where(hit, psi * w, psi)
             k += 3
         return psi

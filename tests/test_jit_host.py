@@ -35,7 +35,8 @@ def jit_check(L, n, ops, tile_bits=0, block_bits=0):
     return npass.value
 
 
-@pytest.mark.parametrize("n,tile_bits,block_bits", [(6, 10, 5), (13, 10, 4), (15, 12, 3), (17, 13, 5), (17, 10, 2)])
+@pytest.mark.parametrize("n,tile_bits,block_bits", [(6, 10, 5), (13, 10, 4), (15, 12, 3), (17, 13, 5), (17, 10, 2),
+                                                    (16, 12, 6)])
 def test_random_all_kinds_compile(L, n, tile_bits, block_bits):
     rng = np.random.default_rng(4000 + n)
     ops = _random_ops(n, 80, rng)

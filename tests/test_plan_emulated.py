@@ -96,3 +96,13 @@ def test_cartan_split_special_two_qubit_gates():
     ops = np.concatenate(recs)
     psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
     _check(n, ops, 10, 5, psi0 / np.linalg.norm(psi0), specialised=True)
+
+
+@pytest.mark.parametrize("n,tile_bits", [(14, 10), (16, 12)])
+def test_six_qubit_register_blocks(n, tile_bits):
+    """Specialised plans may use 6-qubit register blocks (64-bit register
+    masks in the diagonal tables)."""
+    rng = np.random.default_rng(9100 + n)
+    ops = np.concatenate([W.layers_ops(n, 6, seed=5), _random_ops(n, 60, rng)])
+    psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    _check(n, ops, tile_bits, 6, psi0 / np.linalg.norm(psi0), specialised=True)
