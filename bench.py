@@ -244,6 +244,9 @@ def bench_qv_batch(args, dev):
     from qsim_b200 import workloads as W
     C = args.circuits
     widths, oo, ops, so = W.qv_batch(C, 10, 20, seed=1)
+    t_tune = time.perf_counter()
+    tuned = E.autotune_batch(widths, oo, ops, dev)   # shared by the batch and the per-circuit plans
+    t_tune = time.perf_counter() - t_tune
     bp = E.BatchPlan(widths, oo, ops, so, dev)
     states = bp.alloc_states()
     stream = torch.cuda.current_stream(dev)
@@ -320,6 +323,8 @@ def bench_qv_batch(args, dev):
         "dtype": "c64 (fp32 FMA; fp64 host fusion)",
         "config": {"workload": f"qv_batch: {C} QV circuits, widths U[10,20], depth=width, seeds 1e6*1+i",
                    "launches_per_step": bp.info["n_launches"], "items": bp.info["n_items"],
+                   "autotuned_tile_block_bits": {str(k): list(v) for k, v in tuned.items()},
+                   "autotune_seconds": t_tune, "cuda_graph": "captured at the 2nd execution, replayed",
                    "max_passes": bp.info["max_passes"], "l2": "6.2 GB of states >> L2"},
         "per_circuit_launches": {"value": plain_cps, "unit": "circuits/s",
                                  "sample": f"{len(idx)} random circuits of the batch, one fused plan per circuit"},

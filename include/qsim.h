@@ -95,7 +95,8 @@ void* qs_get_stream(qs_handle_t h);
 int  qs_sync(qs_handle_t h);
 const char* qs_last_error(qs_handle_t h);
 const char* qs_version(void);
-/* Tile bits used by the fused-pass planner (10..14); 0 = default (13).      */
+/* Tile bits used by the fused-pass planner (10..14); 0 = automatic (the
+ * autotuned value for the width, else 13).                                  */
 int  qs_set_tile_bits(qs_handle_t h, int tile_bits);
 /* Register-block width used by the planner (2..5 qubits per thread group);
  * 0 = automatic (5 for plans compiled into specialised passes, 4 for the
@@ -295,6 +296,20 @@ int qs_batch_plan_create(qs_handle_t h, int n_circuits, const int32_t* widths, c
 int qs_batch_plan_execute(qs_handle_t h, qs_batch_plan_t plan, void* states);
 int qs_batch_plan_info_get(qs_batch_plan_t plan, qs_batch_info* info);
 int qs_batch_plan_destroy(qs_batch_plan_t plan);
+/* Autotuner for the generic pass kernel (no reference counterpart): for each
+ * distinct width 10..24 of the batch, times every tile width (12..14; the
+ * whole state up to 14 qubits) and register-block width (2..5) on the first
+ * circuit of that width and records the fastest per (device, width).  Every
+ * later generic plan on that device and width (batches, single circuits,
+ * the adjoint forward pass) uses the entry while the handle's tile and block
+ * bits are 0 (automatic), so a circuit gives the same bits alone and in a
+ * batch.  Synchronises the handle's stream.                                 */
+int qs_autotune_batch(qs_handle_t h, int n_circuits, const int32_t* widths, const int64_t* op_offsets,
+                      const qs_op* ops);
+/* The tuned (tile bits, block bits) for a width; QS_ERR_INVALID if none.    */
+int qs_autotune_get(int device, int width, int* tile_bits, int* block_bits);
+/* Forget the tuned entries of a device (device < 0: all devices).           */
+int qs_autotune_clear(int device);
 
 /* ---------------------------------------------------------- adjoint ------ */
 /* Adjoint-method gradient of E(theta) = <psi(theta)|H|psi(theta)> for a

@@ -13,6 +13,7 @@
 // (8 qubits, one CTA per circuit) and bwk/csrc/batch_sm120.cu:53-279 (one
 // launch per gate over [N, 2^n]).
 #include "qs_api.h"
+#include <cstdlib>
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -27,19 +28,25 @@ struct qs_batch_plan_s {
   struct Launch { int T, R, has2, ncoef; size_t item_off; int n_items; uint64_t total_tiles; };
   std::vector<Launch> launches;
   qs_batch_info info{};
+  // CUDA graph of the launch sequence, captured at the second execution on
+  // the same states buffer and replayed afterwards
+  int executions = 0;
+  cudaGraphExec_t graph = nullptr;
+  void* graph_states = nullptr;
 };
 
 namespace {
 
 void free_bplan(qs_batch_plan_s* b) {
   if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
   qs_plan_free_device(b->d_blob);
   qs_plan_free_device(b->d_items);
   delete b;
 }
 
-void plan_all(int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops, int tile_bits,
-              std::vector<qs_plan_s>& plans, int block_bits) {
+void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops,
+              std::vector<qs_plan_s>& plans) {
   plans.resize(nc);
   std::vector<std::string> errs(nc);
   unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -51,7 +58,9 @@ void plan_all(int nc, const int32_t* widths, const int64_t* op_off, const qs_op*
         try {
           const int64_t b = op_off[c], e = op_off[c + 1];
           if (b < 0 || e < b) throw qs_error(QS_ERR_INVALID, "op_offsets must be non-decreasing");
-          qs_build_plan(widths[c], ops + b, (int)(e - b), tile_bits, &plans[c], block_bits);
+          int tb = 0, bb = 0;
+          qs_plan_shape(h, widths[c], false, tb, bb);
+          qs_build_plan(widths[c], ops + b, (int)(e - b), tb, &plans[c], bb);
         } catch (const std::exception& ex) {
           errs[c] = ex.what();
         }
@@ -74,7 +83,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
   }
   std::vector<qs_plan_s> plans;
-  plan_all(nc, widths, op_off, ops, h->tile_bits, plans, h->block_bits);
+  plan_all(h, nc, widths, op_off, ops, plans);
 
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
@@ -164,6 +173,60 @@ static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
   }
 }
 
+static bool graphs_enabled() {
+  const char* e = std::getenv("QSIM_GRAPHS");
+  return !(e && e[0] == '0');
+}
+
+// Executes a reusable batch plan.  The first execution launches directly
+// (and configures the kernels); the second captures the launch sequence into
+// a CUDA graph (on the handle's own stream, since the caller's may be the
+// legacy stream, which cannot capture), and every execution on the same
+// states buffer then replays it on the caller's stream.  Nothing is captured
+// while the caller's stream is itself capturing.
+static void run_batch_graphed(qs_context* h, qs_batch_plan_s* B, void* states) {
+  ++B->executions;
+  if (!graphs_enabled() || B->executions < 2 || B->launches.empty() || !h->own_stream) {
+    run_batch(h, B, states);
+    return;
+  }
+  if (h->stream) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QS_CUDA(cudaStreamIsCapturing(h->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      run_batch(h, B, states);
+      return;
+    }
+  }
+  if (!B->graph || B->graph_states != states) {
+    if (B->graph) {
+      QS_CUDA(cudaGraphExecDestroy(B->graph));
+      B->graph = nullptr;
+    }
+    cudaStream_t caller = h->stream;
+    QS_CUDA(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    h->stream = h->own_stream;
+    try {
+      run_batch(h, B, states);
+    } catch (...) {
+      h->stream = caller;
+      cudaStreamEndCapture(h->own_stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    h->stream = caller;
+    QS_CUDA(cudaStreamEndCapture(h->own_stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw qs_error(QS_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+    B->graph_states = states;
+    qs_count_launches(h, -(int64_t)B->launches.size());  // captured, not launched
+  }
+  QS_CUDA(cudaGraphLaunch(B->graph, h->stream));
+  qs_count_launches(h, (int64_t)B->launches.size());
+}
+
 extern "C" {
 
 int qs_batch_plan_create(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops,
@@ -182,7 +245,7 @@ int qs_batch_plan_execute(qs_handle_t h, qs_batch_plan_t B, void* states) {
   QS_CHECK_ARG(B->n_circuits == 0 || (states && ((uintptr_t)states & 15u) == 0),
                "states must be a 16-byte aligned device pointer");
   QS_CHECK_ARG(B->device == h->device, "batch plan was built for another device");
-  run_batch(h, B, states);
+  run_batch_graphed(h, B, states);
   QS_API_END(h)
 }
 
@@ -242,7 +305,9 @@ int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int 
   }
   if (n_states == 0 || ngates == 0) return QS_OK;
   qs_plan_s p;
-  qs_build_plan(n, ops.data(), ngates, h->tile_bits, &p, h->block_bits);
+  int tb = 0, bb = 0;
+  qs_plan_shape(h, n, false, tb, bb);
+  qs_build_plan(n, ops.data(), ngates, tb, &p, bb);
   qs_plan_upload(h, &p);
   try {
     qs_plan_run(h, &p, states, false, (uint64_t)n_states);

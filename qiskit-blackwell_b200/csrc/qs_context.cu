@@ -37,6 +37,11 @@ double* qs_context::pinned_get(size_t bytes) {
 
 static std::atomic<int64_t> g_launches{0};  // every handle of the process
 
+void qs_count_launches(qs_context* h, int64_t delta) {
+  h->launches += delta;
+  g_launches.fetch_add(delta, std::memory_order_relaxed);
+}
+
 void qs_after_launch(qs_context* h, const char* what) {
   h->launches++;
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -116,8 +121,7 @@ const char* qs_last_error(qs_handle_t h) {
 int qs_set_tile_bits(qs_handle_t h, int tile_bits) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
-  if (tile_bits == 0) tile_bits = 13;
-  QS_CHECK_ARG(tile_bits >= 10 && tile_bits <= 14, "tile_bits must be in [10, 14]");
+  QS_CHECK_ARG(tile_bits == 0 || (tile_bits >= 10 && tile_bits <= 14), "tile_bits must be 0 (auto) or in [10, 14]");
   h->tile_bits = tile_bits;
   QS_API_END(h)
 }

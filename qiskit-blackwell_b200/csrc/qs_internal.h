@@ -38,7 +38,7 @@ struct qs_context {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  int tile_bits = 13;
+  int tile_bits = 0;    // 0: 13, or the autotuned value for the width
   int block_bits = 0;   // 0: 5 for specialised plans, 4 for the generic kernel
   // Pass specialisation (qs_jit.cpp): 0 off, 1 plans on >= jit_min_qubits,
   // 2 every plan.
@@ -59,6 +59,8 @@ struct qs_context {
 
 // Records a launch and checks the launch status.
 void qs_after_launch(qs_context* h, const char* what);
+// Adjusts the launch counters (kernels replayed from, or captured into, a graph).
+void qs_count_launches(qs_context* h, int64_t delta);
 
 // ------------------------------------------------------- device program ---
 // A plan is a list of passes.  A pass streams every tile of the state once:
@@ -164,6 +166,11 @@ bool qs_jit_compile_plan(qs_context* h, qs_plan_s* p, std::string& err);  // syn
 void qs_jit_tiered(qs_context* h, qs_plan_s* p);                         // tiered (background)
 bool qs_jit_compile_only(const qs_plan_s* p, std::string& err);         // no GPU needed
 void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, uint64_t ntiles, uint32_t flags);
+
+// Tile and register-block widths for a plan on n qubits: explicit handle
+// settings win; otherwise the autotuned entry for (device, n) when the plan
+// runs on the generic kernel (qs_tune.cpp); otherwise 13 and 5 / 4.
+void qs_plan_shape(const qs_context* h, int n, bool specialised, int& tile_bits, int& block_bits);
 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
 // `specialised`: the plan will run as specialised passes (enables the Cartan

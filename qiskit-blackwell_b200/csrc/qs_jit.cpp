@@ -654,7 +654,8 @@ std::string qs_jit_source(const qs_plan_s* p, size_t i) {
 // compilation, the background thread that compiles it.
 struct JitJob {
   int device = 0;
-  std::vector<std::string> srcs;
+  std::vector<std::string> srcs;   // generated sources (passes to compile only)
+  std::vector<std::string> progs;  // cache keys: program bytes + generator knobs
   std::vector<uint64_t> keys;
   std::vector<int> T, R;
   std::vector<JitPass> out;
@@ -665,27 +666,42 @@ struct JitJob {
 
 namespace {
 
+// Cache key of a pass: its device-program bytes (header, blocks, ops,
+// coefficients) plus the generator's tuning knobs; the source is generated
+// only for passes not in the cache.
+std::string pass_key(const qs_plan_s* p, size_t i) {
+  const char* base = p->blob.data() + p->pass_offsets[i];
+  const DevPass& P = *reinterpret_cast<const DevPass*>(base);
+  std::string k(base, base + P.bytes);
+  k += "|t" + std::to_string(pass_threads(P.T, P.R)) + "|s" + std::to_string(scalar_every());
+  return k;
+}
+
 std::shared_ptr<JitJob> make_job(const qs_plan_s* p, int device) {
   auto J = std::make_shared<JitJob>();
   J->device = device;
   const size_t np = p->pass_offsets.size();
   J->srcs.resize(np);
+  J->progs.resize(np);
   J->keys.resize(np);
   J->out.resize(np);
   for (size_t i = 0; i < np; ++i) {
     const DevPass& P = *reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i]);
     J->T.push_back(P.T);
     J->R.push_back(P.R);
-    J->srcs[i] = qs_jit_source(p, i);
-    J->keys[i] = fnv1a(J->srcs[i]);
+    J->progs[i] = pass_key(p, i);
+    J->keys[i] = fnv1a(J->progs[i]);
   }
-  Cache& C = cache();
-  std::lock_guard<std::mutex> lk(C.mu);
-  for (size_t i = 0; i < np; ++i) {
-    auto it = C.map[device].find(J->keys[i]);
-    if (it != C.map[device].end() && it->second.first == J->srcs[i]) J->out[i] = it->second.second;
-    else J->todo.push_back(i);
+  {
+    Cache& C = cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    for (size_t i = 0; i < np; ++i) {
+      auto it = C.map[device].find(J->keys[i]);
+      if (it != C.map[device].end() && it->second.first == J->progs[i]) J->out[i] = it->second.second;
+      else J->todo.push_back(i);
+    }
   }
+  for (size_t i : J->todo) J->srcs[i] = qs_jit_source(p, i);
   if (J->todo.empty()) J->state = 1;
   return J;
 }
@@ -739,7 +755,7 @@ void run_job(JitJob& J, unsigned max_threads) {
     }
     J.out[i] = K;
     std::lock_guard<std::mutex> lk(C.mu);
-    C.map[J.device][J.keys[i]] = {J.srcs[i], K};
+    C.map[J.device][J.keys[i]] = {J.progs[i], K};
   }
   J.state = 1;
 }

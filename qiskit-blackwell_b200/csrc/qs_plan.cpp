@@ -1177,6 +1177,7 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops != nullptr), "ops pointer is null");
   // register blocks: 5 qubits for specialised passes, 4 for the generic kernel
   // (fewer registers, higher occupancy: measured faster there)
+  if (tile_bits == 0) tile_bits = 13;
   if (block_bits == 0) block_bits = specialised ? 5 : 4;
   QS_CHECK_ARG(block_bits >= 2 && block_bits <= (specialised ? 6 : 5),
                "block_bits must be in [2, 5] (6 only for specialised passes)");
@@ -1289,7 +1290,9 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   QS_CHECK_ARG(out != nullptr, "out is null");
   *out = nullptr;
   p = new qs_plan_s();
-  qs_build_plan(n, ops, nops, h->tile_bits, p, h->block_bits, h->jit_mode == 2);
+  int tb = 0, bb = 0;
+  qs_plan_shape(h, n, h->jit_mode == 2, tb, bb);
+  qs_build_plan(n, ops, nops, tb, p, bb, h->jit_mode == 2);
   qs_plan_upload(h, p);
   *out = p;
   p = nullptr;

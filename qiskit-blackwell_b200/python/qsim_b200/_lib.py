@@ -101,6 +101,9 @@ SIGNATURES = {
     "qs_plan_destroy": (_i, [_vp]),
     "qs_plan_analyze": (_i, [_i, _pop, _i, _i, C.POINTER(QsPlanInfo)]),
     "qs_plan_jit_check": (_i, [_i, _pop, _i, _i, _i, C.POINTER(C.c_int)]),
+    "qs_autotune_batch": (_i, [_vp, _i, _vp, _vp, _pop]),
+    "qs_autotune_get": (_i, [_i, _i, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "qs_autotune_clear": (_i, [_i]),
     "qs_plan_program": (_i, [_i, _pop, _i, _i, _i, _i, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "qs_run_circuit": (_i, [_vp, _vp, _i, _pop, _i]),
     "qs_norm2": (_i, [_vp, _vp, _i, _pd]),

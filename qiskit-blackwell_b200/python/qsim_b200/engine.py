@@ -37,6 +37,28 @@ def _h(device: int | None = None) -> _lib.Handle:
     return _lib.handle(dev, torch.cuda.current_stream(dev).cuda_stream)
 
 
+def autotune_batch(widths, op_offsets, ops, device: int | None = None) -> dict:
+    """Tunes tile and register-block widths per circuit width on the given
+    circuits (one sample per width); returns {width: (tile_bits, block_bits)}."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    widths = np.ascontiguousarray(widths, dtype=np.int32)
+    op_offsets = np.ascontiguousarray(op_offsets, dtype=np.int64)
+    ops, p = _ops_ptr(ops)
+    h = _h(dev)
+    h.call("qs_autotune_batch", int(len(widths)), C.c_void_p(widths.ctypes.data),
+           C.c_void_p(op_offsets.ctypes.data), p)
+    out = {}
+    tb, bb = C.c_int(0), C.c_int(0)
+    for w in sorted(set(int(x) for x in widths)):
+        if h.L.qs_autotune_get(dev, w, C.byref(tb), C.byref(bb)) == 0:
+            out[w] = (tb.value, bb.value)
+    return out
+
+
+def autotune_clear(device: int | None = None) -> None:
+    _lib.load().qs_autotune_clear(-1 if device is None else int(device))
+
+
 def set_jit(mode: int, min_qubits: int = 0, device: int | None = None) -> None:
     """Pass specialisation for plans executed by this thread's handle:
     0 = never, 1 = plans on >= min_qubits qubits, 2 = every plan."""

@@ -197,3 +197,50 @@ def test_server_mix_equals_alone():
     assert np.array_equal(alone[5][0], mixed[5][0]) and np.array_equal(alone[5][1], mixed[5][1])
     assert np.array_equal(alone[6][0], mixed[6][0])
     assert st["completed"] == len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_batch_plan_graph_replay():
+    """A reusable batch plan is captured into a CUDA graph at its second
+    execution and replayed afterwards; every execution gives the same bits,
+    also after switching to another states buffer (re-capture)."""
+    widths, oo, ops, so = W.qv_batch(24, 6, 16, seed=21)
+    bp = E.BatchPlan(widths, oo, ops, so)
+    a = bp.alloc_states()
+    b = bp.alloc_states()
+    runs = []
+    for buf in (a, a, a, b, b, a):
+        buf.zero_()
+        bp.execute(buf)
+        torch.cuda.synchronize()
+        runs.append(buf.cpu().numpy().copy())
+    for r in runs[1:]:
+        assert np.array_equal(runs[0], r)
+    c = 3
+    n = int(widths[c])
+    ref = O.simulate(n, ops[oo[c]: oo[c + 1]])
+    assert abs(1 - O.fidelity(runs[-1][so[c]: so[c] + (1 << n)], ref)) <= 1e-6
+
+
+def test_autotune_widths_then_alone_equals_batch():
+    """The autotuner records one (tile, block) shape per width; batches and
+    single-circuit plans then share it, so results agree bit for bit."""
+    widths, oo, ops, so = W.qv_batch(30, 10, 17, seed=31)
+    try:
+        table = E.autotune_batch(widths, oo, ops)
+        assert set(table) == {int(w) for w in widths}
+        for w, (tb, bb) in table.items():
+            assert 2 <= bb <= 5 and (w <= 14 or 12 <= tb <= 14)
+        bp = E.BatchPlan(widths, oo, ops, so)
+        st = bp.alloc_states()
+        bp.execute(st)
+        torch.cuda.synchronize()
+        allv = st.cpu().numpy()
+        for c in range(0, len(widths), 3):
+            n = int(widths[c])
+            got = allv[so[c]: so[c] + (1 << n)]
+            assert abs(1 - O.fidelity(got, O.simulate(n, ops[oo[c]: oo[c + 1]]))) <= 1e-6
+            alone = E.empty_state(n)
+            E.Plan(n, ops[oo[c]: oo[c + 1]]).execute_from_zero(alone)
+            assert np.array_equal(alone.cpu().numpy(), got), (c, n)
+    finally:
+        E.autotune_clear()
