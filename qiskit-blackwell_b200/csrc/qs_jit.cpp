@@ -641,13 +641,15 @@ bool qs_jit_compile_only(const qs_plan_s* p, std::string& err) {
   return true;
 }
 
-std::string qs_jit_source(const qs_plan_s* p, size_t i) {
-  const char* base = p->blob.data() + p->pass_offsets[i];
+// Source of one pass from its device-program bytes (header first).
+static std::string pass_source(const char* base) {
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
   return gen_pass(P, reinterpret_cast<const DevBlock*>(base + P.block_off),
                   reinterpret_cast<const DevOp*>(base + P.op_off), reinterpret_cast<const float2*>(base + P.coef_off),
                   min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R), P.R));
 }
+
+std::string qs_jit_source(const qs_plan_s* p, size_t i) { return pass_source(p->blob.data() + p->pass_offsets[i]); }
 
 // A specialisation job: the plan's pass sources, the kernels found in the
 // cache and the ones still to compile.  Shared by the plan and, for tiered
@@ -701,7 +703,7 @@ std::shared_ptr<JitJob> make_job(const qs_plan_s* p, int device) {
       else J->todo.push_back(i);
     }
   }
-  for (size_t i : J->todo) J->srcs[i] = qs_jit_source(p, i);
+  // sources are generated by run_job, from the program bytes held in progs
   if (J->todo.empty()) J->state = 1;
   return J;
 }
@@ -710,6 +712,8 @@ std::shared_ptr<JitJob> make_job(const qs_plan_s* p, int device) {
 // them (on this thread, with the device's primary context current).
 void run_job(JitJob& J, unsigned max_threads) {
   const size_t nt_all = J.todo.size();
+  for (size_t i : J.todo)
+    if (J.srcs[i].empty()) J.srcs[i] = pass_source(J.progs[i].data());
   std::vector<std::string> cubins(J.srcs.size()), errs(J.srcs.size());
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const unsigned nt = std::max(1u, std::min<unsigned>(std::min(max_threads, hw), (unsigned)nt_all));
