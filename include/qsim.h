@@ -128,6 +128,16 @@ int qs_state_init(qs_handle_t h, void* state, int n_qubits);
 int qs_state_init_basis(qs_handle_t h, void* state, int n_qubits, uint64_t index);
 /* Reference: bwk/csrc/batch_sm120.cu:165-181 (state_init_batched)          */
 int qs_state_init_batched(qs_handle_t h, void* states, int n_states, int n_qubits);
+/* State buffers for callers without their own allocator (the reference's
+ * states are torch tensors, `torch::zeros` in apply_diagonal_sm120.cu:
+ * 210-224): 2^n complex64 from the stream-ordered pool of the handle's
+ * stream (256-byte aligned; QS_ERR_NOMEM when HBM is short), freed in stream
+ * order.  The copies are synchronous (they return when the data is there).
+ * Any other 16-byte aligned device buffer of 2^n complex64 is a valid state. */
+int qs_state_alloc(qs_handle_t h, int n_qubits, void** state_out);
+int qs_state_free(qs_handle_t h, void* state);
+int qs_state_copy_to_host(qs_handle_t h, const void* state, int n_qubits, void* host_c64);
+int qs_state_copy_from_host(qs_handle_t h, void* state, int n_qubits, const void* host_c64);
 
 /* ------------------------------------------------------- single gates ---- */
 /* Reference: bwk/csrc/apply_gate_sm120.cu:65-114,269-307 (apply_gate).     */

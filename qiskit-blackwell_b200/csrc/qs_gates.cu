@@ -293,6 +293,49 @@ int qs_state_init_basis(qs_handle_t h, void* state, int n, uint64_t index) {
   QS_API_END(h)
 }
 
+int qs_state_alloc(qs_handle_t h, int n, void** out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(out != nullptr, "out is null");
+  *out = nullptr;
+  QS_CHECK_ARG(n >= 1 && n <= QS_MAX_QUBITS, "n_qubits out of range [1, 34]");
+  void* p = nullptr;
+  const cudaError_t e = cudaMallocAsync(&p, (size_t)8 << n, h->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw qs_error(QS_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
+  }
+  *out = p;
+  QS_API_END(h)
+}
+
+int qs_state_free(qs_handle_t h, void* state) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  if (state) QS_CUDA(cudaFreeAsync(state, h->stream));
+  QS_API_END(h)
+}
+
+int qs_state_copy_to_host(qs_handle_t h, const void* state, int n, void* host) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(host != nullptr, "host buffer is null");
+  QS_CUDA(cudaMemcpyAsync(host, state, (size_t)8 << n, cudaMemcpyDeviceToHost, h->stream));
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  QS_API_END(h)
+}
+
+int qs_state_copy_from_host(qs_handle_t h, void* state, int n, const void* host) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(host != nullptr, "host buffer is null");
+  QS_CUDA(cudaMemcpyAsync(state, host, (size_t)8 << n, cudaMemcpyHostToDevice, h->stream));
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  QS_API_END(h)
+}
+
 int qs_state_init_batched(qs_handle_t h, void* states, int n_states, int n) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN

@@ -79,6 +79,10 @@ SIGNATURES = {
     "qs_set_jit": (_i, [_vp, _i, _i]),
     "qs_launch_count": (_i64, [_vp]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
+    "qs_state_alloc": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
+    "qs_state_free": (_i, [_vp, _vp]),
+    "qs_state_copy_to_host": (_i, [_vp, _vp, _i, _vp]),
+    "qs_state_copy_from_host": (_i, [_vp, _vp, _i, _vp]),
     "qs_state_init_basis": (_i, [_vp, _vp, _i, _u64]),
     "qs_state_init_batched": (_i, [_vp, _vp, _i, _i]),
     "qs_apply_1q": (_i, [_vp, _vp, _i, _pf, _i]),
