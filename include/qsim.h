@@ -34,6 +34,7 @@ extern "C" {
 #define QS_ERR_NOMEM     3   /* device allocation failed                            */
 #define QS_ERR_TIMEOUT   4   /* a bounded device-side wait gave up                  */
 #define QS_ERR_BUDGET    5   /* request exceeds the handle's memory budget          */
+#define QS_ERR_CANCELLED 6   /* a server request was cancelled before it ran        */
 
 #define QS_MAX_QUBITS    34
 #define QS_MAX_CONTROLS  7
@@ -190,6 +191,8 @@ int qs_plan_execute(qs_handle_t h, qs_plan_t plan, void* state);
 /* state := U|0..0>; the first pass synthesises |0..0> in shared memory, so
  * the state is written but never read. */
 int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state);
+/* The device program is freed in order after the work queued on the stream
+ * the plan last ran on (destroy the plan before destroying that stream).   */
 int qs_plan_destroy(qs_plan_t plan);
 /* Host-only dry run of the planner (no device needed): fills `info` for the
  * plan qs_plan_create would build with the given tile bits (0 = default). */
@@ -332,6 +335,50 @@ int qs_adjoint_gradient(qs_handle_t h, int n_qubits, const qs_op* ops, int n_ops
                         const double* params, int n_batch,
                         const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs, int n_terms,
                         void* work, double* energies_host, double* grads_host);
+/* ------------------------------------------------------------ serving ---- */
+/* Native continuous-batching server (no reference counterpart).  Requests
+ * are submitted from any thread and get an id; a scheduler admits them in
+ * arrival order against `budget_bytes` of HBM (each request counts the device
+ * bytes it will hold), batches admitted circuits into one batch plan, and
+ * `n_workers` worker threads, each with its own handle and stream, run the
+ * items concurrently.  Results are the same alone and in a mix.  Errors:
+ * too large for the budget -> QS_ERR_BUDGET at submit; deadline (seconds,
+ * 0 = none) passed while queued -> QS_ERR_TIMEOUT; cancelled while queued or
+ * at shutdown -> QS_ERR_CANCELLED; a failed item fails only its requests.  */
+typedef struct qs_server_s* qs_server_t;
+typedef struct qs_server_stats {
+  int64_t submitted, completed, failed, queued;
+  double  p50_ms, p99_ms;        /* latency (arrival -> result) of completed requests */
+  double  throughput_rps;        /* completed / (last completion - first arrival)    */
+  int64_t budget_bytes, free_bytes;
+} qs_server_stats;
+int qs_server_create(int device, int64_t budget_bytes, int n_workers, qs_server_t* out);
+/* Cancels queued requests, lets admitted ones finish, joins the threads.    */
+int qs_server_destroy(qs_server_t server);
+/* Circuit -> `shots` samples (basis indices) drawn with uniforms from `seed`. */
+int qs_server_submit_circuit(qs_server_t server, int n_qubits, const qs_op* ops, int n_ops, int64_t shots,
+                             uint64_t seed, double deadline_s, int64_t* id_out);
+/* Energy and adjoint gradient (as qs_adjoint_gradient) for n_batch vectors. */
+int qs_server_submit_gradient(qs_server_t server, int n_qubits, const qs_op* ops, int n_ops, int n_params,
+                              const double* params, int n_batch, const uint64_t* x_masks, const uint64_t* z_masks,
+                              const double* coefs, int n_terms, double deadline_s, int64_t* id_out);
+/* Chebyshev evolution (as qs_cheb_evolve_pauli) of a host complex64 psi0;
+ * cheb_coeffs: K+1 complex FP64 coefficients.                               */
+int qs_server_submit_evolution(qs_server_t server, int n_qubits, const void* psi0_host, const uint64_t* x_masks,
+                               const uint64_t* z_masks, const double* coefs, int n_terms, const double* cheb_coeffs,
+                               int K, double scale, double deadline_s, int64_t* id_out);
+/* Waits for a request (timeout_s < 0: forever; QS_ERR_TIMEOUT if not done);
+ * *status_out = the request's own status.                                   */
+int qs_server_wait(qs_server_t server, int64_t id, double timeout_s, int* status_out);
+int qs_server_cancel(qs_server_t server, int64_t id);
+const char* qs_server_request_error(qs_server_t server, int64_t id);
+int qs_server_result_samples(qs_server_t server, int64_t id, int64_t* out, int64_t n_shots);
+int qs_server_result_gradient(qs_server_t server, int64_t id, double* energies, double* grads);
+int qs_server_result_state(qs_server_t server, int64_t id, void* out_host_c64);
+/* Forgets a finished request and its results.                               */
+int qs_server_release(qs_server_t server, int64_t id);
+int qs_server_stats_get(qs_server_t server, qs_server_stats* out);
+
 /* lambda = H psi for a Pauli sum (matrix-free).                             */
 int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n_qubits,
                        const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs, int n_terms);

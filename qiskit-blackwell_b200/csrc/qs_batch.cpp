@@ -31,6 +31,7 @@ struct qs_batch_plan_s {
   // CUDA graph of the launch sequence, captured at the second execution on
   // the same states buffer and replayed afterwards
   int executions = 0;
+  cudaStream_t stream = nullptr;   // stream of the last upload/execution
   cudaGraphExec_t graph = nullptr;
   void* graph_states = nullptr;
 };
@@ -40,8 +41,8 @@ namespace {
 void free_bplan(qs_batch_plan_s* b) {
   if (!b) return;
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  qs_plan_free_device(b->d_blob);
-  qs_plan_free_device(b->d_items);
+  qs_plan_free_device(b->d_blob, b->stream);
+  qs_plan_free_device(b->d_items, b->stream);
   delete b;
 }
 
@@ -88,6 +89,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
   B->n_circuits = nc;
+  B->stream = h->stream;
   try {
     // concatenate device programs
     std::vector<size_t> boff(nc);
@@ -186,6 +188,7 @@ static bool graphs_enabled() {
 // while the caller's stream is itself capturing.
 static void run_batch_graphed(qs_context* h, qs_batch_plan_s* B, void* states) {
   ++B->executions;
+  B->stream = h->stream;
   if (!graphs_enabled() || B->executions < 2 || B->launches.empty() || !h->own_stream) {
     run_batch(h, B, states);
     return;
@@ -313,10 +316,10 @@ int qs_apply_gates_batched_fused(qs_handle_t h, void* states, int n_states, int 
     qs_plan_run(h, &p, states, false, (uint64_t)n_states);
     QS_CUDA(cudaStreamSynchronize(h->stream));
   } catch (...) {
-    qs_plan_free_device(p.d_blob);
+    qs_plan_free_device(p.d_blob, h->stream);
     throw;
   }
-  qs_plan_free_device(p.d_blob);
+  qs_plan_free_device(p.d_blob, h->stream);
   QS_API_END(h)
 }
 

@@ -151,6 +151,7 @@ struct qs_plan_s {
   void* d_blob = nullptr;               // device copy
   int device = 0;
   qs_plan_info info{};
+  cudaStream_t stream = nullptr;        // stream of the last upload/execution
   bool jit_tried = false;               // specialisation attempted
   std::vector<JitPass> jit;             // one per pass when specialised
   std::shared_ptr<JitJob> jit_job;      // sources awaiting / in background compile
@@ -178,7 +179,9 @@ void qs_plan_shape(const qs_context* h, int n, bool specialised, int& tile_bits,
 void qs_build_plan(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, qs_plan_s* plan, int block_bits = 0,
                    bool specialised = false);
 void qs_plan_upload(qs_context* h, qs_plan_s* p);
-void qs_plan_free_device(void* d);  // stream-ordered free (no device sync)
+// Stream-ordered free after the work queued on `stream` (the stream the
+// program last ran on; no device-wide synchronisation).
+void qs_plan_free_device(void* d, cudaStream_t stream);
 // Runs every pass on n_states equal-width states stored back to back.
 void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states);
 

@@ -1236,14 +1236,16 @@ void qs_plan_upload(qs_context* h, qs_plan_s* p) {
   // The plan may be executed on another stream: make the program resident
   // before returning (this waits on the handle's stream only).
   QS_CUDA(cudaStreamSynchronize(h->stream));
+  p->stream = h->stream;
 }
 
-void qs_plan_free_device(void* d) {
-  if (d) cudaFreeAsync(d, 0);
+void qs_plan_free_device(void* d, cudaStream_t stream) {
+  if (d) cudaFreeAsync(d, stream);
 }
 
 void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states) {
   const int n = p->n_qubits;
+  p->stream = h->stream;
   if (p->pass_offsets.empty()) {
     if (from_zero) QS_CHECK_ARG(qs_state_init_batched(h, state, (int)n_states, n) == QS_OK, h->err.c_str());
     return;
@@ -1300,12 +1302,12 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   }
   catch (const qs_error& e) {
     h->err = e.what();
-    if (p) { qs_plan_free_device(p->d_blob); delete p; }
+    if (p) { qs_plan_free_device(p->d_blob, h->stream); delete p; }
     return e.code;
   }
   catch (const std::exception& e) {
     h->err = e.what();
-    if (p) { qs_plan_free_device(p->d_blob); delete p; }
+    if (p) { qs_plan_free_device(p->d_blob, h->stream); delete p; }
     return QS_ERR_INVALID;
   }
 }
@@ -1379,7 +1381,7 @@ int qs_plan_execute_from_zero(qs_handle_t h, qs_plan_t plan, void* state) {
 
 int qs_plan_destroy(qs_plan_t plan) {
   if (!plan) return QS_OK;
-  qs_plan_free_device(plan->d_blob);
+  qs_plan_free_device(plan->d_blob, plan->stream);
   delete plan;
   return QS_OK;
 }

@@ -110,10 +110,10 @@ int qs_autotune_batch(qs_handle_t h, int nc, const int32_t* widths, const int64_
       try {
         ms = time_plan(h, &plan, scratch, w >= kFillBits ? 1ull : (1ull << (kFillBits - w)));
       } catch (...) {
-        qs_plan_free_device(plan.d_blob);
+        qs_plan_free_device(plan.d_blob, h->stream);
         throw;
       }
-      qs_plan_free_device(plan.d_blob);
+      qs_plan_free_device(plan.d_blob, h->stream);
       if (ms < best_ms) { best_ms = ms; best = s; }
     }
     std::lock_guard<std::mutex> lk(g_tune_mu);

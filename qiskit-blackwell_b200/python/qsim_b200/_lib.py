@@ -42,6 +42,12 @@ class QsBatchInfo(C.Structure):
                 ("max_passes", C.c_int32), ("pad", C.c_int32), ("bytes_moved", C.c_double), ("flops", C.c_double)]
 
 
+class QsServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("throughput_rps", C.c_double),
+                ("budget_bytes", C.c_int64), ("free_bytes", C.c_int64)]
+
+
 class QsimError(RuntimeError):
     """Raised when a libqsim call returns a non-zero status (the reference
     raises RuntimeError from TORCH_CHECK for the same conditions)."""
@@ -108,6 +114,20 @@ SIGNATURES = {
     "qs_autotune_batch": (_i, [_vp, _i, _vp, _vp, _pop]),
     "qs_autotune_get": (_i, [_i, _i, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qs_autotune_clear": (_i, [_i]),
+    "qs_server_create": (_i, [_i, C.c_int64, _i, C.POINTER(C.c_void_p)]),
+    "qs_server_destroy": (_i, [_vp]),
+    "qs_server_submit_circuit": (_i, [_vp, _i, _pop, _i, C.c_int64, C.c_uint64, _d, C.POINTER(C.c_int64)]),
+    "qs_server_submit_gradient": (_i, [_vp, _i, _pop, _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d,
+                                       C.POINTER(C.c_int64)]),
+    "qs_server_submit_evolution": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _i, _d, _d, C.POINTER(C.c_int64)]),
+    "qs_server_wait": (_i, [_vp, C.c_int64, _d, C.POINTER(C.c_int)]),
+    "qs_server_cancel": (_i, [_vp, C.c_int64]),
+    "qs_server_request_error": (C.c_char_p, [_vp, C.c_int64]),
+    "qs_server_result_samples": (_i, [_vp, C.c_int64, _vp, C.c_int64]),
+    "qs_server_result_gradient": (_i, [_vp, C.c_int64, _vp, _vp]),
+    "qs_server_result_state": (_i, [_vp, C.c_int64, _vp]),
+    "qs_server_release": (_i, [_vp, C.c_int64]),
+    "qs_server_stats_get": (_i, [_vp, C.POINTER(QsServerStats)]),
     "qs_plan_program": (_i, [_i, _pop, _i, _i, _i, _i, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "qs_run_circuit": (_i, [_vp, _vp, _i, _pop, _i]),
     "qs_norm2": (_i, [_vp, _vp, _i, _pd]),

@@ -26,6 +26,7 @@ a worker (e.g. a failed allocation) fails only the requests of that batch.
 """
 from __future__ import annotations
 
+import ctypes as C
 import itertools
 import queue
 import threading
@@ -35,6 +36,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 import torch
+
+from . import _lib
 
 
 class AdmissionError(RuntimeError):
@@ -297,3 +300,137 @@ class Server:
             psi = torch.as_tensor(np.asarray(r.psi0, dtype=np.complex64)).to(f"cuda:{self.device}")
         out, info = chebyshev_evolve_pauli(psi, r.hamiltonian, r.t, precision=r.precision)
         return out.cpu().numpy(), info
+
+
+# ---------------------------------------------------------------- native
+class _NativeFuture:
+    """Result handle of a NativeServer request."""
+
+    def __init__(self, srv, rid: int, req):
+        self._srv, self.rid, self._req = srv, rid, req
+        self._value = None
+        self._done = False
+
+    def done(self) -> bool:
+        st = C.c_int(0)
+        return self._srv.L.qs_server_wait(self._srv.ptr, self.rid, 0.0, C.byref(st)) == 0
+
+    def result(self, timeout: float | None = None):
+        if self._done:
+            return self._value
+        L, p = self._srv.L, self._srv.ptr
+        st = C.c_int(0)
+        rc = L.qs_server_wait(p, self.rid, -1.0 if timeout is None else float(timeout), C.byref(st))
+        if rc != 0:
+            raise TimeoutError(f"request {self.rid} not finished within {timeout} s")
+        if st.value != 0:
+            msg = (L.qs_server_request_error(p, self.rid) or b"").decode()
+            L.qs_server_release(p, self.rid)
+            self._done = True
+            if st.value == 5:
+                raise AdmissionError(msg)
+            if st.value == 4:
+                raise DeadlineExceeded(msg)
+            if st.value == 6:
+                raise Cancelled(msg)
+            raise RuntimeError(f"request failed ({st.value}): {msg}")
+        r = self._req
+        if isinstance(r, CircuitRequest):
+            out = np.empty(int(r.shots), dtype=np.int64)
+            _lib.check(L.qs_server_result_samples(p, self.rid, out.ctypes.data_as(C.c_void_p), int(r.shots)))
+            self._value = out
+        elif isinstance(r, GradientRequest):
+            P = np.asarray(r.params).reshape(-1, max(r.n_params, 1))
+            e = np.zeros(P.shape[0])
+            g = np.zeros((P.shape[0], r.n_params))
+            _lib.check(L.qs_server_result_gradient(p, self.rid, e.ctypes.data_as(C.c_void_p),
+                                                   g.ctypes.data_as(C.c_void_p)))
+            self._value = (e, g)
+        else:
+            out = np.empty(1 << r.hamiltonian.num_qubits, dtype=np.complex64)
+            _lib.check(L.qs_server_result_state(p, self.rid, out.ctypes.data_as(C.c_void_p)))
+            self._value = (out, self._info)
+        L.qs_server_release(p, self.rid)
+        self._done = True
+        return self._value
+
+
+class NativeServer:
+    """The same request types served by the C++ runtime (qs_server_* in the C
+    ABI): scheduling, admission, batching and the worker threads are native;
+    this class only marshals requests and results.  Sampling uniforms come
+    from each circuit request's seed (splitmix64), so results are identical
+    alone and in a mix (they differ from the Python Server's torch RNG)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 150 * 10 ** 9, workers: int = 4):
+        self.L = _lib.load()
+        out = C.c_void_p()
+        _lib.check(self.L.qs_server_create(int(device), int(budget_bytes), int(workers), C.byref(out)))
+        self.ptr = out
+
+    def submit(self, req) -> _NativeFuture:
+        L, p = self.L, self.ptr
+        rid = C.c_int64(0)
+        dl = float(req.deadline_s or 0.0)
+        if isinstance(req, CircuitRequest):
+            ops = np.ascontiguousarray(req.ops)
+            rc = L.qs_server_submit_circuit(p, int(req.n_qubits), ops.ctypes.data_as(C.POINTER(_lib.QsOp)),
+                                            int(len(ops)), int(req.shots), int(req.seed) & (2 ** 64 - 1), dl,
+                                            C.byref(rid))
+            fut = _NativeFuture(self, rid.value, req)
+        elif isinstance(req, GradientRequest):
+            ops = np.ascontiguousarray(req.ops)
+            P = np.ascontiguousarray(np.asarray(req.params, dtype=np.float64).reshape(-1, max(req.n_params, 1)))
+            x = np.ascontiguousarray(req.observable.x, dtype=np.uint64)
+            z = np.ascontiguousarray(req.observable.z, dtype=np.uint64)
+            c = np.ascontiguousarray(req.observable.real_coefs(), dtype=np.float64)
+            rc = L.qs_server_submit_gradient(p, int(req.n_qubits), ops.ctypes.data_as(C.POINTER(_lib.QsOp)),
+                                             int(len(ops)), int(req.n_params), P.ctypes.data_as(C.c_void_p),
+                                             int(P.shape[0]), x.ctypes.data_as(C.c_void_p),
+                                             z.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p),
+                                             int(len(c)), dl, C.byref(rid))
+            fut = _NativeFuture(self, rid.value, req)
+        else:
+            from blackwell_backend.chebyshev import chebyshev_coefficients
+            H = req.hamiltonian
+            n = H.num_qubits
+            psi = np.ascontiguousarray(np.asarray(req.psi0, dtype=np.complex64) if req.psi0 is not None
+                                       else np.eye(1, 1 << n, dtype=np.complex64)[0])
+            bound = H.spectral_bound()
+            coeffs, K, tail = chebyshev_coefficients(req.t, bound, req.precision)
+            cbuf = np.ascontiguousarray(np.stack([coeffs.real, coeffs.imag], axis=-1).reshape(-1), dtype=np.float64)
+            x = np.ascontiguousarray(H.x, dtype=np.uint64)
+            z = np.ascontiguousarray(H.z, dtype=np.uint64)
+            c = np.ascontiguousarray(H.real_coefs(), dtype=np.float64)
+            rc = L.qs_server_submit_evolution(p, n, psi.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p),
+                                              z.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p),
+                                              int(len(c)), cbuf.ctypes.data_as(C.c_void_p), int(K),
+                                              float(1.0 / bound), dl, C.byref(rid))
+            fut = _NativeFuture(self, rid.value, req)
+            fut._info = {"engine": "chebyshev-b200-pauli", "chebyshev_degree": K, "spectral_bound": bound,
+                         "truncation_error_bound": tail}
+        if rc != 0:
+            msg = (L.qs_last_error(None) or b"").decode()
+            f = Future()
+            f.set_exception(AdmissionError(msg) if rc == 5 else RuntimeError(f"submit failed ({rc}): {msg}"))
+            return f
+        return fut
+
+    def cancel(self, fut) -> bool:
+        return isinstance(fut, _NativeFuture) and self.L.qs_server_cancel(self.ptr, fut.rid) == 0
+
+    def stats(self) -> dict:
+        s = _lib.QsServerStats()
+        _lib.check(self.L.qs_server_stats_get(self.ptr, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.QsServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.L.qs_server_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
