@@ -457,7 +457,8 @@ def bench_serving(args, dev):
     import numpy as np
     import torch
     from qsim_b200 import engine as E
-    from qsim_b200.server import CircuitRequest, Server
+    from qsim_b200.server import CircuitRequest, NativeServer, Server
+    make_server = NativeServer if args.server == "native" else Server
     rates = [float(x) for x in args.rates.split(",")]
     n_req = args.requests
     mix = ServingMix(n_req, seed=4)
@@ -468,7 +469,7 @@ def bench_serving(args, dev):
     d2h = sum((r.shots * 8 if isinstance(r, CircuitRequest) else 8 << getattr(r, "n_qubits", 0))
               for r in reqs)
     # warm-up: one request of each kind and width class through the server
-    srv = Server(device=dev, workers=args.workers)
+    srv = make_server(device=dev, workers=args.workers)
     warm = [mix.request(i) for i in range(min(n_req, 3 * max(1, args.warmup)))]
     for f in [srv.submit(r) for r in warm]:
         f.result(600)
@@ -480,7 +481,7 @@ def bench_serving(args, dev):
     with ClockSampler(dev) as clk:
         for lam in rates:
             arrivals = unit_arrivals / lam
-            srv = Server(device=dev, workers=args.workers)
+            srv = make_server(device=dev, workers=args.workers)
             futs = [None] * n_req
             lr0 = int(L.qs_launch_count(None))
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -501,11 +502,10 @@ def bench_serving(args, dev):
             makespan = ev0.elapsed_time(ev1) / 1000.0
             st = srv.stats()
             srv.close()
-            lat = np.array(srv.latencies)
             kinds = np.array([sp[0] for sp in mix.specs])
             qv_n = int((kinds == "qv").sum())
             sweep.append({"rate_rps": lam, "served_rps": n_req / makespan, "qv_circuits_per_s": qv_n / makespan,
-                          "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                          "p50_ms": float(st["p50_ms"]), "p99_ms": float(st["p99_ms"]),
                           "makespan_s": makespan, "offered_s": float(arrivals[-1]),
                           "gpu_launches": int(L.qs_launch_count(None)) - lr0})
     # serial plain execution of the same requests
@@ -524,7 +524,8 @@ def bench_serving(args, dev):
         "ms_per_step": top_mk * 1e3, "dtype": "c64 state (fp32 FMA), fp64 reductions",
         "config": {"workload": f"serving: {n_req} seeded requests (50% QV 10-28q 1024 shots, 25% EfficientSU2 "
                                f"energy+gradient 12-22q, 25% Chebyshev evolution 12-22q), Poisson arrivals "
-                               f"replayed at each rate; 150 GB budget, {args.workers} worker streams",
+                               f"replayed at each rate; 150 GB budget, {args.workers} worker streams, "
+                               f"{args.server} server",
                    "rates_rps": rates, "step": "one replay of the request sequence at the highest rate",
                    "l2": "states up to 2 GiB each; no flush"},
         "sweep": sweep,
@@ -660,6 +661,8 @@ def main():
     ap.add_argument("--requests", type=int, default=200, help="serving: requests per rate")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serving: Poisson rates (req/s)")
     ap.add_argument("--workers", type=int, default=4, help="serving: worker streams")
+    ap.add_argument("--server", default="native", choices=["native", "python"],
+                    help="serving: the C++ runtime (qs_server_*) or the Python one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
     ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")

@@ -106,6 +106,8 @@ void check(qs_handle_t h, int rc) {
 
 }  // namespace
 
+constexpr int64_t kBatchAmps = int64_t(1) << 26;
+
 struct qs_server_s {
   int device = 0;
   int64_t budget = 0, free_bytes = 0;
@@ -147,6 +149,7 @@ struct qs_server_s {
       if (stop) return;
       const double t = now_s();
       std::vector<ReqP> circuits;
+      int64_t batch_amps = 0;
       std::deque<ReqP> keep;
       while (!queue.empty()) {
         ReqP r = queue.front();
@@ -162,11 +165,21 @@ struct qs_server_s {
         free_bytes -= (int64_t)r->need;
         r->state = S_RUNNING;
         if (r->kind == K_CIRCUIT) {
-          circuits.push_back(r);
-          if ((int)circuits.size() == max_batch) {
+          // a batch holds at most 2^26 amplitudes (or max_batch circuits), so
+          // several batches run on several workers at once; a circuit that
+          // large fills the GPU by itself and goes alone
+          const int64_t amps = int64_t(1) << r->n;
+          if (amps >= kBatchAmps) {
+            work.push_back({r});
+            continue;
+          }
+          if (batch_amps + amps > kBatchAmps || (int)circuits.size() == max_batch) {
             work.push_back(std::move(circuits));
             circuits.clear();
+            batch_amps = 0;
           }
+          circuits.push_back(r);
+          batch_amps += amps;
         } else {
           work.push_back({r});
         }

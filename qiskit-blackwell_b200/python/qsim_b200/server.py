@@ -105,6 +105,8 @@ class _Job:
 
 
 class Server:
+    BATCH_AMPS = 1 << 26
+
     def __init__(self, device: int = 0, budget_bytes: int = 150 * 10 ** 9, workers: int = 4,
                  max_batch_circuits: int = 4096, batch_window_s: float = 0.0005, execute=None):
         """execute(kind, jobs) -> results overrides the GPU executor (host-side
@@ -201,9 +203,24 @@ class Server:
                 if not admitted:
                     self._lock.wait(0.002)
                     continue
-            circuits = [j for j in admitted if isinstance(j.req, CircuitRequest)]
-            for k in range(0, len(circuits), self.max_batch):
-                self._work.put(("circuits", circuits[k:k + self.max_batch]))
+            # a batch holds at most 2^26 amplitudes (or max_batch circuits) so
+            # several batches run on several workers at once; a circuit that
+            # large fills the GPU by itself and goes alone
+            batch, amps = [], 0
+            for j in admitted:
+                if not isinstance(j.req, CircuitRequest):
+                    continue
+                a = 1 << j.req.n_qubits
+                if a >= self.BATCH_AMPS:
+                    self._work.put(("circuits", [j]))
+                    continue
+                if batch and (amps + a > self.BATCH_AMPS or len(batch) == self.max_batch):
+                    self._work.put(("circuits", batch))
+                    batch, amps = [], 0
+                batch.append(j)
+                amps += a
+            if batch:
+                self._work.put(("circuits", batch))
             for j in admitted:
                 if isinstance(j.req, GradientRequest):
                     self._work.put(("gradient", [j]))
