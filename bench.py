@@ -606,8 +606,42 @@ def bench_adjoint(args, dev):
         {"unit": "gradients/s"}
 
 
+def bench_qv_plain(args, dev):
+    """One Quantum-Volume circuit of --qubits qubits (depth = width, seed
+    1000) on the plain per-circuit path: one plan, executed from |0> each
+    step (specialisation as --jit says).  value = circuits/s."""
+    import torch
+    from qsim_b200 import engine as E
+    from qsim_b200 import workloads as W
+    n = args.qubits if args.qubits != 32 else 24
+    ops = W.qv_ops(n, n, 1000)
+    plan = E.Plan(n, ops, dev)
+    state = E.empty_state(n, f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    h = E._h(dev)
+    step = lambda: plan.execute_from_zero(state)
+    for _ in range(args.warmup):
+        step()
+    l0 = h.launches()
+    with ClockSampler(dev) as clk:
+        t = _cuda_time(step, stream, args.steps)
+    launches = h.launches() - l0
+    t = reduce_max(t, f"cuda:{dev}")
+    per_step = t / args.steps
+    info = plan.refresh_info()
+    peak, src = measured_peaks()
+    algo = (8.0 + 16.0 * (info["n_passes"] - 1)) * (1 << n)
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"metric": METRIC, "value": ws / per_step, "unit": "circuits/s", "ms_per_step": per_step * 1e3,
+            "dtype": "c64", "config": {"workload": f"qv_plain: {n} qubits, depth {n}, seed 1000",
+                                       "passes": info["n_passes"], "specialised_passes": info["n_jit_passes"]},
+            "roofline": {"bound": "hbm", "achieved": algo / per_step / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / per_step / 1e9 / peak, "traffic": None, "peak_source": src},
+            "clocks": clk.summary(), "gpu_launches": launches}, {"unit": "circuits/s"}
+
+
 WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
-             "adjoint": bench_adjoint}
+             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain}
 
 
 # --------------------------------------------------------- CPU baseline
