@@ -72,9 +72,16 @@ def _make_result(counts, shots, header, elapsed, metadata=None):
         return Result("blackwell_simulator", "0.1.0", "", "", True, [exp], elapsed)
 
 
-def counts_from_samples(samples: np.ndarray) -> dict:
-    """{hex(index): count} as the reference builds it (simulator.py:579-586)."""
-    vals, cnt = np.unique(np.asarray(samples, dtype=np.int64), return_counts=True)
+def counts_from_samples(samples) -> dict:
+    """{hex(index): count} as the reference builds it (simulator.py:579-586).
+    A device tensor is histogrammed on the device and only the distinct
+    outcomes and their counts are copied back (the reference loops over every
+    shot in Python)."""
+    if isinstance(samples, torch.Tensor) and samples.is_cuda:
+        vals, cnt = torch.unique(samples, return_counts=True)
+        vals, cnt = vals.cpu().numpy(), cnt.cpu().numpy()
+    else:
+        vals, cnt = np.unique(np.asarray(samples, dtype=np.int64), return_counts=True)
     return {hex(int(v)): int(c) for v, c in zip(vals, cnt)}
 
 
@@ -187,7 +194,7 @@ class BlackwellSimulator:
             np.random.seed(seed)
         clean = self._strip_measurements(circuit)
         state, _, elapsed = self._execute_circuit(clean)
-        samples = E.sample(state, shots).cpu().numpy()
+        samples = E.sample(state, shots)            # stays on the device
         n = clean.num_qubits
         return _make_result(counts_from_samples(samples), shots, {"name": clean.name, "n_qubits": n}, elapsed)
 
@@ -242,7 +249,7 @@ class BlackwellSimulator:
         hcsr = op if method != "pauli" else None
         if shots is None:
             return result_state.cpu().numpy(), info
-        samples = E.sample(result_state, shots).cpu().numpy()
+        samples = E.sample(result_state, shots)      # histogrammed on the device
         res = _make_result(counts_from_samples(samples), shots,
                            {"name": "chebyshev_evolution", "n_qubits": nq}, info["elapsed_s"], info)
         return res, info
