@@ -243,6 +243,28 @@ def sample(state: torch.Tensor, shots: int, generator: torch.Generator | None = 
     return sample_u(state, u)
 
 
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def seed_uniforms(seed: int, count: int) -> np.ndarray:
+    """The native server's per-request uniforms: splitmix64 (Steele, Lea and
+    Flood, 2014) from `seed`, top 53 bits scaled to [0, 1).  Sampling with
+    these gives the same shots as a NativeServer request with that seed."""
+    i = np.arange(1, int(count) + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(int(seed) & (2 ** 64 - 1)) + i * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def sample_seeded(state: torch.Tensor, shots: int, seed: int) -> torch.Tensor:
+    """Shots drawn with seed_uniforms(seed, shots) (device tensor)."""
+    u = torch.from_numpy(seed_uniforms(seed, shots)).to(state.device, non_blocking=False)
+    return sample_u(state, u)
+
+
 def _masks(ps):
     x = np.ascontiguousarray(ps.x, dtype=np.uint64)
     z = np.ascontiguousarray(ps.z, dtype=np.uint64)
