@@ -57,7 +57,12 @@ enum {
   QS_OP_Y       = 10, /* exact Pauli-Y on q[0]                                */
   QS_OP_RX      = 11, /* exp(-i m[0] X/2) on q[0]; param = parameter index    */
   QS_OP_RY      = 12, /* exp(-i m[0] Y/2) on q[0]                             */
-  QS_OP_RZ      = 13  /* exp(-i m[0] Z/2) on q[0]                             */
+  QS_OP_RZ      = 13, /* exp(-i m[0] Z/2) on q[0]                             */
+  /* Stochastic noise channels on q[0], parameter m[0]; only
+   * qs_noise_trajectories accepts them (a unitary program rejects them).   */
+  QS_OP_DEPOLARIZE = 20, /* I w.p. 1-p, else X, Y, Z w.p. p/3 each          */
+  QS_OP_AMP_DAMP   = 21, /* Kraus E0 = [[1,0],[0,sqrt(1-g)]], E1 = [[0,sqrt(g)],[0,0]] */
+  QS_OP_DEPHASE    = 22  /* Kraus E0 = [[1,0],[0,sqrt(1-l)]], E1 = [[0,0],[0,sqrt(l)]] */
 };
 
 typedef struct qs_op {
@@ -382,6 +387,42 @@ int qs_server_stats_get(qs_server_t server, qs_server_stats* out);
 /* lambda = H psi for a Pauli sum (matrix-free).                             */
 int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n_qubits,
                        const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs, int n_terms);
+
+/* ------------------------------------------------------------ noise ------ */
+/* Stochastic channels on one state (reference: bwk/csrc/noise_sm120.cu:238-373,
+ * bound as apply_depolarizing / apply_amplitude_damping / apply_dephasing in
+ * bwk/python/blackwell_kernels/cuquantum.py:352-411).  u is the caller's
+ * uniform in [0, 1).  Depolarizing: [0, 1-p) identity, then X, Y, Z in
+ * thirds of p (branch 0..3), chosen on the host.  Damping and dephasing pick
+ * the jump branch (1) when u < p1 = g * P(q=1) (FP64 fixed-order reduction,
+ * decided on the device) and renormalise the kept branch exactly.  When
+ * branch_host is non-null the call waits for the branch and stores it;
+ * with NULL nothing waits (the reference always synchronises).
+ * Differs from the reference: its damping jump kernel keeps the |0>
+ * amplitudes (noise_sm120.cu:200-204), which is not E1 and leaves the state
+ * unnormalised; here the jump branch is E1 exactly.                         */
+int qs_apply_depolarizing(qs_handle_t h, void* state, int n_qubits, int target, double p, double u,
+                          int32_t* branch_host);
+int qs_apply_amplitude_damping(qs_handle_t h, void* state, int n_qubits, int target, double gamma, double u,
+                               int32_t* branch_host);
+int qs_apply_dephasing(qs_handle_t h, void* state, int n_qubits, int target, double lambda, double u,
+                       int32_t* branch_host);
+/* Batched noise trajectories (no reference counterpart; the reference
+ * applies one channel per call with a host round trip each): n_traj
+ * independent runs of one circuit whose ops may include QS_OP_DEPOLARIZE,
+ * QS_OP_AMP_DAMP and QS_OP_DEPHASE.  Trajectory t draws one uniform per
+ * noise op, in program order, from seeds[t] (splitmix64, top 53 bits, as
+ * the serving runtime's sampling).  Depolarizing draws are resolved on the
+ * host into exact Paulis that the planner fuses with the circuit; damping
+ * and dephasing are decided on the device.  Up to 14 qubits each trajectory
+ * runs start to finish in one CTA's shared memory (all trajectories in one
+ * launch per program level); wider states run the unitary segments as batch
+ * launches and each state-dependent channel as two launches over all
+ * trajectories.  states: device [n_traj][2^n] complex64, written from
+ * |0..0>.  branches_host (optional): [n_traj][n_noise] uint8, the branch of
+ * every noise op (depolarizing 0..3, damping/dephasing 0/1).               */
+int qs_noise_trajectories(qs_handle_t h, int n_qubits, const qs_op* ops, int n_ops, int n_traj,
+                          const uint64_t* seeds, void* states, uint8_t* branches_host);
 
 #ifdef __cplusplus
 }

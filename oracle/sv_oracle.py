@@ -234,3 +234,140 @@ def grad_param_shift(n, ops, params_row, x, z, c, which):
         tm[p] -= math.pi / 2
         out.append(0.5 * (energy(n, ops, tp, x, z, c) - energy(n, ops, tm, x, z, c)))
     return np.array(out)
+
+
+# ------------------------------------------------------------ noise channels
+# Restatement of the reference's stochastic channels (bwk/csrc/noise_sm120.cu)
+# for checking the trajectory runner.  Parity for this part is unpinned: the
+# reference has no tests or fixtures for its noise kernels, so the checks
+# rest on this restatement and on channel-level properties (trajectory
+# averages against the Kraus-sum density matrix).
+DEPOLARIZE, AMP_DAMP, DEPHASE = 20, 21, 22
+
+
+def seed_uniforms(seed: int, count: int) -> np.ndarray:
+    """splitmix64 from `seed`, top 53 bits -> [0, 1) (pure-Python loop)."""
+    m = (1 << 64) - 1
+    x, out = int(seed) & m, []
+    for _ in range(int(count)):
+        x = (x + 0x9E3779B97F4A7C15) & m
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        z ^= z >> 31
+        out.append((z >> 11) * 2.0 ** -53)
+    return np.array(out, dtype=np.float64)
+
+
+def depol_branch(p: float, u: float) -> int:
+    """noise_sm120.cu:262-289: [0, 1-p) identity, then X, Y, Z in thirds of p."""
+    if u < 1.0 - p:
+        return 0
+    r, third = u - (1.0 - p), p / 3.0
+    if r < third:
+        return 1
+    if r < 2.0 * third:
+        return 2
+    return 3
+
+
+def apply_channel_np(psi: np.ndarray, n: int, kind: int, q: int, g: float, u: float):
+    """One channel on an FP64 state: (new state, branch, |u - p1|).
+    Depolarizing: Pauli by depol_branch.  Damping / dephasing: jump when
+    u < p1 = g P(q=1) (noise_sm120.cu:116-147, 296-312), Kraus operator of the
+    branch, renormalised.  The damping jump is E1 = [[0, sqrt g], [0, 0]]."""
+    psi = np.array(psi, dtype=np.complex128, copy=True)
+    idx = np.arange(1 << n, dtype=np.int64)
+    one = ((idx >> q) & 1) == 1
+    if kind == DEPOLARIZE:
+        b = depol_branch(g, u)
+        P = [None, [[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]]][b]
+        if P is not None:
+            psi = _apply_k(psi, n, [q], np.array(P, dtype=complex))
+        return psi, b, math.inf
+    S1 = float(np.sum(np.abs(psi[one]) ** 2))
+    S0 = float(np.sum(np.abs(psi[~one]) ** 2))
+    p1 = g * S1 / (S0 + S1)
+    keep = S0 + (1.0 - g) * S1
+    jump = S1 > 0.0 and (u < p1 or not keep > 0.0)
+    if not jump:
+        psi[~one] /= math.sqrt(keep)
+        psi[one] *= math.sqrt(1.0 - g) / math.sqrt(keep)
+    elif kind == AMP_DAMP:
+        psi[~one] = psi[one] / math.sqrt(S1)
+        psi[one] = 0
+    else:
+        psi[~one] = 0
+        psi[one] /= math.sqrt(S1)
+    return psi, int(jump), abs(u - p1)
+
+
+def noise_trajectory(n: int, ops, seed: int):
+    """One trajectory of a circuit with channel ops: (FP64 state, branches,
+    smallest |u - p1| over the state-dependent channels)."""
+    recs = _ops(ops)
+    nn = int(sum(1 for r in recs if int(r["kind"]) in (DEPOLARIZE, AMP_DAMP, DEPHASE)))
+    u = seed_uniforms(seed, nn)
+    psi = zero_state(n)
+    br, margin, k, pending = [], math.inf, 0, []
+    for r in recs:
+        kind = int(r["kind"])
+        if kind in (DEPOLARIZE, AMP_DAMP, DEPHASE):
+            if pending:
+                psi = apply_ops_np(psi, n, np.array(pending, dtype=OP_DTYPE))
+                pending = []
+            psi, b, mg = apply_channel_np(psi, n, kind, int(r["q"][0]), float(r["m"][0]), float(u[k]))
+            br.append(b)
+            margin = min(margin, mg)
+            k += 1
+        else:
+            pending.append(r)
+    if pending:
+        psi = apply_ops_np(psi, n, np.array(pending, dtype=OP_DTYPE))
+    return psi, np.array(br, dtype=np.uint8), margin
+
+
+def kraus_density(n: int, ops) -> np.ndarray:
+    """Exact density matrix of the channel circuit (Kraus sums, FP64; n <= 6)."""
+    recs = _ops(ops)
+    N = 1 << n
+    rho = np.zeros((N, N), dtype=np.complex128)
+    rho[0, 0] = 1
+    eye = np.eye(N, dtype=complex)
+    for r in recs:
+        kind, q = int(r["kind"]), int(r["q"][0])
+        if kind in (DEPOLARIZE, AMP_DAMP, DEPHASE):
+            g = float(r["m"][0])
+            if kind == DEPOLARIZE:
+                Ks = [math.sqrt(1 - g) * np.eye(2)] + [math.sqrt(g / 3) * np.array(P, dtype=complex) for P in
+                                                       ([[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]])]
+            elif kind == AMP_DAMP:
+                Ks = [np.array([[1, 0], [0, math.sqrt(1 - g)]]), np.array([[0, math.sqrt(g)], [0, 0]])]
+            else:
+                Ks = [np.array([[1, 0], [0, math.sqrt(1 - g)]]), np.array([[0, 0], [0, math.sqrt(g)]])]
+            new = np.zeros_like(rho)
+            for K in Ks:
+                Kf = np.stack([_apply_k(eye[:, j].copy(), n, [q], np.asarray(K, dtype=complex)) for j in range(N)],
+                              axis=1)
+                new += Kf @ rho @ Kf.conj().T
+            rho = new
+        else:
+            U = np.stack([apply_ops_np(eye[:, j], n, np.array([r], dtype=OP_DTYPE)) for j in range(N)], axis=1)
+            rho = U @ rho @ U.conj().T
+    return rho
+
+
+def reference_amp_damp_jump(psi: np.ndarray, n: int, q: int, g: float) -> np.ndarray:
+    """The reference's damping jump kernel as written (noise_sm120.cu:183-205,
+    renorm 1/sqrt(p1) with p1 = g P(q=1), noise_sm120.cu:358-365): it keeps
+    a0 * renorm in the |0> amplitudes, so the result is not E1|psi>/|E1 psi|."""
+    psi = np.array(psi, dtype=np.complex128, copy=True)
+    idx = np.arange(1 << n, dtype=np.int64)
+    one = ((idx >> q) & 1) == 1
+    p1 = g * float(np.sum(np.abs(psi[one]) ** 2))
+    renorm = 1.0 / math.sqrt(p1)
+    i1 = idx[one]
+    i0 = i1 & ~(1 << q)
+    psi[i0] = psi[i0] * renorm + psi[i1] * math.sqrt(g) * renorm
+    psi[i1] = 0
+    return psi

@@ -75,37 +75,35 @@ void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t*
 
 }  // namespace
 
-static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
-                                    const qs_op* ops, const int64_t* state_off) {
-  QS_CHECK_ARG(nc >= 0, "n_circuits must be >= 0");
-  QS_CHECK_ARG(nc == 0 || (widths && op_off && state_off), "null batch descriptor");
-  for (int c = 0; c < nc; ++c) {
-    QS_CHECK_ARG(widths[c] >= 1 && widths[c] <= QS_MAX_QUBITS, "circuit width out of range");
-    QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
-  }
-  std::vector<qs_plan_s> plans;
-  plan_all(h, nc, widths, op_off, ops, plans);
-
+// Uploads every plan into one device buffer and groups the (unit, pass)
+// items by pass level, then by (T, R, has2), into launches.  Units that
+// share a plan share its device program.
+qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
+                                      const std::vector<BatchUnit>& units, bool from_zero) {
+  const int np = (int)plans.size();
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
-  B->n_circuits = nc;
+  B->n_circuits = (int)units.size();
   B->stream = h->stream;
   try {
     // concatenate device programs
-    std::vector<size_t> boff(nc);
+    std::vector<size_t> boff(np);
     size_t total = 0;
-    for (int c = 0; c < nc; ++c) {
+    for (int c = 0; c < np; ++c) {
       boff[c] = total;
       total += (plans[c].blob.size() + 255) & ~size_t(255);
     }
     std::vector<char> blob(total, 0);
-    for (int c = 0; c < nc; ++c)
+    for (int c = 0; c < np; ++c)
       if (!plans[c].blob.empty()) std::memcpy(blob.data() + boff[c], plans[c].blob.data(), plans[c].blob.size());
     if (total) {
       QS_CUDA(cudaMallocAsync(&B->d_blob, total, h->stream));
       QS_CUDA(cudaMemcpyAsync(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice, h->stream));
     }
-    // group (circuit, pass) items by level, then by (T, R)
+    for (const BatchUnit& u : units) {
+      QS_CHECK_ARG(u.plan >= 0 && u.plan < np, "internal: unit plan index out of range");
+      QS_CHECK_ARG(!plans[u.plan].pass_offsets.empty(), "every circuit of a batch needs at least one op");
+    }
     int maxp = 0;
     for (auto& p : plans) maxp = std::max(maxp, (int)p.pass_offsets.size());
     std::vector<PassItem> items;
@@ -113,19 +111,22 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     for (int L = 0; L < maxp; ++L) {
       // key: (T, R, has2); value: items and the largest coefficient pool
       std::map<std::tuple<int, int, int>, std::pair<std::vector<PassItem>, int>> groups;
-      for (int c = 0; c < nc; ++c) {
-        const qs_plan_s& p = plans[c];
+      for (const BatchUnit& u : units) {
+        const qs_plan_s& p = plans[u.plan];
         if (L >= (int)p.pass_offsets.size()) continue;
         const int T = p.pass_T[L];
         PassItem it{};
-        it.state_off = (uint64_t)state_off[c];
-        it.pass = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[c] + p.pass_offsets[L]);
-        it.ntiles = 1ull << (widths[c] - T);
-        it.flags = (L == 0) ? PI_FROM_ZERO : 0u;
+        it.state_off = u.state_off;
+        it.pass = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[u.plan] +
+                                                   p.pass_offsets[L]);
+        it.ntiles = 1ull << (p.n_qubits - T);
+        it.flags = (L == 0 && from_zero) ? PI_FROM_ZERO : 0u;
+        it.noise_u = u.noise_u;
+        it.noise_branch = u.noise_branch;
         auto& g = groups[std::make_tuple(T, p.pass_R[L], p.pass_has2[L])];
         g.first.push_back(it);
         g.second = std::max(g.second, p.pass_ncoef[L]);
-        bytes += (L == 0 ? 8.0 : 16.0) * std::ldexp(1.0, widths[c]);
+        bytes += ((L == 0 && from_zero) ? 8.0 : 16.0) * std::ldexp(1.0, p.n_qubits);
       }
       // larger tiles first: they are the longest-running CTAs
       for (auto g = groups.rbegin(); g != groups.rend(); ++g) {
@@ -142,12 +143,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
         B->launches.push_back(Lc);
       }
     }
-    for (auto& p : plans) flops += p.info.flops;
-    // circuits with no ops still need |0..0>
-    for (int c = 0; c < nc; ++c) {
-      if (!plans[c].pass_offsets.empty()) continue;
-      QS_CHECK_ARG(false, "every circuit of a batch needs at least one op");
-    }
+    for (const BatchUnit& u : units) flops += plans[u.plan].info.flops;
     if (!items.empty()) {
       QS_CUDA(cudaMallocAsync(&B->d_items, items.size() * sizeof(PassItem), h->stream));
       QS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice,
@@ -155,7 +151,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
     }
     // blob/items are host temporaries: wait for the copies before they go
     QS_CUDA(cudaStreamSynchronize(h->stream));
-    B->info.n_circuits = nc;
+    B->info.n_circuits = (int32_t)units.size();
     B->info.n_launches = (int32_t)B->launches.size();
     B->info.n_items = (int64_t)items.size();
     B->info.max_passes = maxp;
@@ -167,6 +163,31 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
   }
   return B;
 }
+
+static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
+                                    const qs_op* ops, const int64_t* state_off) {
+  QS_CHECK_ARG(nc >= 0, "n_circuits must be >= 0");
+  QS_CHECK_ARG(nc == 0 || (widths && op_off && state_off), "null batch descriptor");
+  for (int c = 0; c < nc; ++c) {
+    QS_CHECK_ARG(widths[c] >= 1 && widths[c] <= QS_MAX_QUBITS, "circuit width out of range");
+    QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
+  }
+  std::vector<qs_plan_s> plans;
+  plan_all(h, nc, widths, op_off, ops, plans);
+  std::vector<BatchUnit> units(nc);
+  for (int c = 0; c < nc; ++c) units[c] = BatchUnit{c, (uint64_t)state_off[c], nullptr, nullptr};
+  return qs_batch_build_units(h, plans, units, true);
+}
+
+void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states) {
+  B->stream = h->stream;
+  for (const auto& L : B->launches) {
+    const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
+    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef);
+  }
+}
+
+void qs_batch_release(qs_batch_plan_s* B) { free_bplan(B); }
 
 static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
   for (const auto& L : B->launches) {

@@ -94,6 +94,10 @@ enum DevKind : uint8_t {
                  // pairs (|t0=0 t1=1>, |t0=1 t1=0>) use c[1]; each pair as in
                  // DK_KRY (the dropped factors are already in the next diagonal)
   DK_CU2 = 16,   // DK_U2 with controls (rc on register bits, gc on the index)
+  DK_NOISE = 17, // state-dependent channel on tile position t0, alone in a
+                 // noise block (DevBlock.pos[6] == 1; tile == whole state):
+                 // d0 = QS_OP_AMP_DAMP or QS_OP_DEPHASE, gc = bits of the FP64
+                 // parameter, coef = index of its uniform / branch slot
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -195,14 +199,48 @@ struct __align__(16) PassItem {
   uint64_t ntiles;
   uint64_t tile_begin;   // prefix of ntiles over the item table
   uint32_t flags;
-  uint32_t pad[3];
+  uint32_t pad0;
+  const double* noise_u;   // uniforms of the pass's noise blocks (by DevOp.coef)
+  uint8_t* noise_branch;   // branch taken by each noise block (by DevOp.coef)
+  uint64_t pad1;
 };
+static_assert(sizeof(PassItem) == 64, "PassItem layout");
 // has2: the pass (or any item of the launch) holds a two-target op; ncoef:
 // the largest coefficient pool (float2) of the launch's passes.
 void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
                            uint32_t flags, int has2, int ncoef);
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
                           int maxT, int R, int has2, int ncoef);
+
+// Batch engine internals (qs_batch.cpp), shared with the noise-trajectory
+// runner: a batch is a set of host plans (each uploaded into one device
+// buffer) and units, each unit one state running one of the plans.
+struct BatchUnit {
+  int plan;                 // index into the plan list
+  uint64_t state_off;       // amplitude offset of the unit's state
+  const double* noise_u;    // device uniforms of the unit's noise blocks, or null
+  uint8_t* noise_branch;    // device branch record, or null
+};
+struct qs_batch_plan_s;
+qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
+                                      const std::vector<BatchUnit>& units, bool from_zero);
+void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states);
+void qs_batch_release(qs_batch_plan_s* B);
+
+// Deterministic uniforms in [0, 1) from a seed: splitmix64 (Steele, Lea and
+// Flood, 2014), top 53 bits.  Shared by the serving runtime's sampling and
+// the noise trajectories so that both draw the same stream for one seed.
+inline void qs_seed_uniforms(uint64_t seed, int64_t count, double* out) {
+  uint64_t x = seed;
+  for (int64_t i = 0; i < count; ++i) {
+    x += 0x9e3779b97f4a7c15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    out[i] = (double)(z >> 11) * 0x1.0p-53;
+  }
+}
 
 // Convenience used by several units.
 inline int qs_blocks_for(qs_context* h, uint64_t items, int threads, int per_sm = 8) {

@@ -450,6 +450,65 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
   }
 }
 
+// ------------------------------------------------------- noise blocks ------
+// A state-dependent channel (amplitude damping or dephasing) on tile position
+// q of a tile that holds the whole state: FP64 sums of |a|^2 over the q = 0
+// and q = 1 halves (fixed order: per thread, then warps in index order), the
+// jump branch when u < p1 = g * S1 / (S0 + S1), then the branch's Kraus
+// operator with exact renormalisation:
+//   no jump : a0 *= 1/sqrt(S0 + (1-g) S1),  a1 *= sqrt(1-g)/sqrt(S0 + (1-g) S1)
+//   damping : a0 = a1 / sqrt(S1),  a1 = 0          (E1 = [[0, sqrt g], [0, 0]])
+//   dephase : a0 = 0,  a1 *= 1 / sqrt(S1)          (E1 = [[0, 0], [0, sqrt l]])
+// All threads of the CTA take part; red holds 2 x 8 doubles.
+__device__ __noinline__ void noise_block(float2* tile, int T, const DevOp op, const double* nu, uint8_t* nb,
+                                        double* red) {
+  const int q = op.t0;
+  const uint32_t N = 1u << T;
+  double s0 = 0.0, s1 = 0.0;
+  for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+    const float2 a = tile[phys(i)];
+    const double p = (double)a.x * a.x + (double)a.y * a.y;
+    if ((i >> q) & 1u) s1 += p; else s0 += p;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((threadIdx.x & 31) == 0) { red[w] = s0; red[8 + w] = s1; }
+  __syncthreads();
+  double S0 = 0.0, S1 = 0.0;
+  for (int k = 0; k < nw; ++k) { S0 += red[k]; S1 += red[8 + k]; }
+  const double g = __longlong_as_double((long long)op.gc);
+  const double p1 = g * S1 / (S0 + S1);
+  const double u = nu ? nu[op.coef] : 1.0;
+  // the kept branch has norm^2 keep; a branch of zero weight is never taken
+  const double keep = S0 + (1.0 - g) * S1;
+  const bool jump = S1 > 0.0 && (u < p1 || !(keep > 0.0));
+  if (threadIdx.x == 0 && nb) nb[op.coef] = jump ? 1 : 0;
+  if (!jump) {
+    const double r = 1.0 / sqrt(keep);
+    const float f0 = (float)r, f1 = (float)(sqrt(1.0 - g) * r);
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+      const float f = ((i >> q) & 1u) ? f1 : f0;
+      float2& a = tile[phys(i)];
+      a = make_float2(a.x * f, a.y * f);
+    }
+  } else {
+    const float f = (float)(1.0 / sqrt(S1));
+    const bool damp = op.d0 == QS_OP_AMP_DAMP;
+    for (uint32_t c = threadIdx.x; c < (N >> 1); c += blockDim.x) {
+      const uint32_t i0 = (uint32_t)insert_zero(c, q), i1 = i0 | (1u << q);
+      float2& a0 = tile[phys(i0)];
+      float2& a1 = tile[phys(i1)];
+      const float2 v1 = make_float2(a1.x * f, a1.y * f);
+      if (damp) { a0 = v1; a1 = make_float2(0.f, 0.f); }
+      else { a0 = make_float2(0.f, 0.f); a1 = v1; }
+    }
+  }
+}
+
 // ---------------------------------------------------------- the kernel ----
 // R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs, 3 per
 // SM.  Narrower blocks use 256 threads.
@@ -467,6 +526,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
   uint64_t* dep_lo = reinterpret_cast<uint64_t*>(smem_raw + dep_off_bytes);
   uint64_t* dep_hi = dep_lo + 128;
   int* s_S = reinterpret_cast<int*>(dep_hi + 128);
+  __shared__ double s_red[16];  // noise-block reduction
 
   int cur = -1;
   const DevPass* P = nullptr;
@@ -540,6 +600,11 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
     const uint32_t ngroups = 1u << (T - R);
     for (int b = 0; b < nblocks; ++b) {
       const DevBlock blk = blocks[b];
+      if (blk.pos[6]) {  // noise block (only in programs whose tile is the whole state)
+        noise_block(tile, T, ops[blk.op_begin], I.noise_u, I.noise_branch, s_red);
+        __syncthreads();
+        continue;
+      }
       int pos[R];
       uint32_t pp[R];
 #pragma unroll

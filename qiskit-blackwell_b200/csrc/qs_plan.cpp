@@ -121,6 +121,8 @@ std::vector<IOp> normalise(int n, const qs_op* ops, int nops) {
         }
         break;
       }
+      case QS_OP_DEPOLARIZE: case QS_OP_AMP_DAMP: case QS_OP_DEPHASE:
+        throw qs_error(QS_ERR_INVALID, "noise channel op in a unitary program (use qs_noise_trajectories)");
       default:
         throw qs_error(QS_ERR_INVALID, "unknown op kind " + std::to_string(o.kind));
     }

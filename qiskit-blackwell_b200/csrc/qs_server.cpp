@@ -69,19 +69,6 @@ struct Request {
 
 using ReqP = std::shared_ptr<Request>;
 
-// Deterministic uniforms in [0, 1) from a seed (splitmix64, top 53 bits).
-void uniforms(uint64_t seed, int64_t count, double* out) {
-  uint64_t x = seed;
-  for (int64_t i = 0; i < count; ++i) {
-    x += 0x9e3779b97f4a7c15ull;
-    uint64_t z = x;
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    z ^= z >> 31;
-    out[i] = (double)(z >> 11) * 0x1.0p-53;
-  }
-}
-
 // Device buffer released when it leaves scope (stream-ordered).
 struct DevBuf {
   void* p = nullptr;
@@ -254,7 +241,7 @@ struct qs_server_s {
     std::vector<int64_t> host(total_shots);
     if (total_shots > 0) {
       std::vector<double> u(total_shots);
-      for (int c = 0; c < nc; ++c) uniforms(item[c]->seed, item[c]->shots, u.data() + shot_off[c]);
+      for (int c = 0; c < nc; ++c) qs_seed_uniforms(item[c]->seed, item[c]->shots, u.data() + shot_off[c]);
       DevBuf du((size_t)total_shots * 8, s), dout((size_t)total_shots * 8, s);
       QS_CUDA(cudaMemcpyAsync(du.p, u.data(), (size_t)total_shots * 8, cudaMemcpyHostToDevice, s));
       for (int c = 0; c < nc; ++c) {

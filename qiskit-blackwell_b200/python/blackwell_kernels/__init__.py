@@ -16,6 +16,7 @@ from .cuquantum import (  # noqa: F401
     rz_gate_diag, phase_gate_diag, t_gate_diag, s_gate_diag, z_gate_diag, cz_gate_diag,
     renormalize,
     spmv_csr, chebyshev_step, chebyshev_accum, chebyshev_step_accum,
+    apply_depolarizing, apply_amplitude_damping, apply_dephasing,
 )
 from .qv import (  # noqa: F401
     qv8_simulate, qv4_simulate_cuda, generate_qv8_circuits, heavy_output_probability,

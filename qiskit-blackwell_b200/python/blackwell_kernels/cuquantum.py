@@ -344,3 +344,33 @@ def z_gate_diag(device="cuda"):
 
 def cz_gate_diag(device="cuda"):
     return torch.tensor([1.0, 1.0, 1.0, -1.0], dtype=torch.complex64, device=device)
+
+
+# ------------------------------------------------------------------ noise
+# cuquantum.py:352-411 / noise_sm120.cu:238-373: one channel on one state,
+# random_val drawn with torch.rand when not given, branch code returned.
+def _noise(entry: str, state: torch.Tensor, target_qubit: int, prob: float, random_val) -> int:
+    n = check_state(state)
+    if random_val is None:
+        random_val = torch.rand(1).item()
+    out = C.c_int32(0)
+    _h(state.device.index).call(entry, _ptr(state), n, int(target_qubit), float(prob), float(random_val),
+                                C.byref(out))
+    return int(out.value)
+
+
+def apply_depolarizing(state: torch.Tensor, target_qubit: int, p: float, random_val: float = None) -> int:
+    """Identity w.p. 1-p, else Pauli X / Y / Z w.p. p/3 each; returns 0..3."""
+    return _noise("qs_apply_depolarizing", state, target_qubit, p, random_val)
+
+
+def apply_amplitude_damping(state: torch.Tensor, target_qubit: int, gamma: float, random_val: float = None) -> int:
+    """T1 decay: returns 1 when the decay branch E1 was taken, else 0.  The
+    jump branch is E1 = [[0, sqrt(gamma)], [0, 0]] exactly (the reference's
+    kernel keeps the |0> amplitudes there, noise_sm120.cu:200-204)."""
+    return _noise("qs_apply_amplitude_damping", state, target_qubit, gamma, random_val)
+
+
+def apply_dephasing(state: torch.Tensor, target_qubit: int, lam: float, random_val: float = None) -> int:
+    """T2 dephasing: returns 1 when the error branch E1 was taken, else 0."""
+    return _noise("qs_apply_dephasing", state, target_qubit, lam, random_val)

@@ -23,6 +23,7 @@ QS_ERR_BUDGET = 5
 
 # op kinds (include/qsim.h)
 OP_U1, OP_U2, OP_DIAG1, OP_DIAG2, OP_MCU1, OP_MCU2, OP_MCX, OP_MCSWAP, OP_MCPHASE, OP_Y, OP_RX, OP_RY, OP_RZ = range(1, 14)
+OP_DEPOLARIZE, OP_AMP_DAMP, OP_DEPHASE = 20, 21, 22
 
 
 class QsOp(C.Structure):
@@ -145,6 +146,10 @@ SIGNATURES = {
     "qs_cheb_step_accum": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _i64]),
     "qs_cheb_evolve": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _pd, _i, _d, _vp]),
     "qs_cheb_evolve_pauli": (_i, [_vp, _i, _vp, _vp, _pu64, _pu64, _pd, _i, _pd, _i, _d, _vp]),
+    "qs_apply_depolarizing": (_i, [_vp, _vp, _i, _i, _d, _d, _pi32]),
+    "qs_apply_amplitude_damping": (_i, [_vp, _vp, _i, _i, _d, _d, _pi32]),
+    "qs_apply_dephasing": (_i, [_vp, _vp, _i, _i, _d, _d, _pi32]),
+    "qs_noise_trajectories": (_i, [_vp, _i, _pop, _i, _i, _pu64, _vp, C.POINTER(C.c_uint8)]),
     "qs_batch_run": (_i, [_vp, _i, _pi32, _pi64, _pop, _vp, _pi64]),
     "qs_batch_plan_create": (_i, [_vp, _i, _pi32, _pi64, _pop, _pi64, C.POINTER(_vp)]),
     "qs_batch_plan_execute": (_i, [_vp, _vp, _vp]),

@@ -18,7 +18,11 @@ import numpy as np
 
 from . import gates as G
 from ._lib import (OP_DIAG1, OP_MCPHASE, OP_MCSWAP, OP_MCU1, OP_MCX, OP_RX, OP_RY, OP_RZ, OP_U1, OP_U2, OP_Y,
-                   OP_MCU2, OP_DIAG2)
+                   OP_MCU2, OP_DIAG2, OP_AMP_DAMP, OP_DEPHASE, OP_DEPOLARIZE)
+
+# Stochastic channels (one qubit, one probability parameter); only the
+# noise-trajectory runner accepts them.
+NOISE_OPS = {"depolarize": OP_DEPOLARIZE, "amplitude_damp": OP_AMP_DAMP, "dephase": OP_DEPHASE}
 
 OP_DTYPE = np.dtype([("kind", "<i4"), ("nq", "<i4"), ("q", "<i4", (8,)), ("param", "<i4"), ("flags", "<i4"),
                      ("m", "<f8", (32,))])
@@ -93,6 +97,11 @@ class Circuit:
             raise ValueError("unitary supports 1- and 2-qubit matrices")
         return self.append("unitary", qubits, matrix=m)
 
+    # -- noise channels (noise_sm120.cu semantics; run by qsim_b200.noise)
+    def depolarize(self, p, q): return self.append("depolarize", [q], [p])
+    def amplitude_damp(self, gamma, q): return self.append("amplitude_damp", [q], [gamma])
+    def dephase(self, lam, q): return self.append("dephase", [q], [lam])
+
     # -- non-unitary
     def measure(self, q, c): return self.append("measure", [q], clbits=[c])
     def reset(self, q): return self.append("reset", [q])
@@ -163,6 +172,9 @@ def lower(circuit: Circuit, strip_measure: bool = True) -> np.ndarray:
         elif name == "unitary":
             r["kind"] = OP_U1 if len(qs) == 1 else OP_U2
             _set_m(r, ins.matrix)
+        elif name in NOISE_OPS:
+            r["kind"] = NOISE_OPS[name]
+            r["m"][0] = float(ins.params[0])
         elif name == "y":
             r["kind"] = OP_Y
         elif name in G.DIAGONAL_1Q:
