@@ -640,8 +640,101 @@ def bench_qv_plain(args, dev):
             "clocks": clk.summary(), "gpu_launches": launches}, {"unit": "circuits/s"}
 
 
+def _per_channel_trajectories(qc, n_traj, dev):
+    """Trajectories/s through the reference's one-call-per-gate-or-channel
+    API (blackwell_kernels: apply_gate / apply_mcgate per gate, one
+    apply_depolarizing / apply_amplitude_damping / apply_dephasing call per
+    channel, each state-dependent one returning its branch to the host, as
+    the reference's do).  Gate matrices are built before timing."""
+    import time as _t
+    import numpy as np
+    import torch
+    import blackwell_kernels as bk
+    from qsim_b200 import gates as G
+    calls = []
+    xg = torch.tensor([[0, 1], [1, 0]], dtype=torch.complex64, device=f"cuda:{dev}")
+    for ins in qc.data:
+        if ins.name in ("ry", "rz"):
+            m = torch.tensor(G.mat1(ins.name, ins.params), dtype=torch.complex64, device=f"cuda:{dev}")
+            calls.append((bk.apply_gate, m, ins.qubits[0]))
+        elif ins.name == "cx":
+            calls.append((bk.apply_mcgate, xg, [ins.qubits[0]], ins.qubits[1]))
+        elif ins.name == "depolarize":
+            calls.append((bk.apply_depolarizing, ins.qubits[0], ins.params[0]))
+        elif ins.name == "amplitude_damp":
+            calls.append((bk.apply_amplitude_damping, ins.qubits[0], ins.params[0]))
+        elif ins.name == "dephase":
+            calls.append((bk.apply_dephasing, ins.qubits[0], ins.params[0]))
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    for _ in range(n_traj):
+        st = bk.state_init(qc.num_qubits)
+        for c in calls:
+            c[0](st, *c[1:])
+    torch.cuda.synchronize()
+    return n_traj / (_t.perf_counter() - t0)
+
+
+def bench_noisy(args, dev):
+    """Noise trajectories: a --qubits (default 12) qubit brickwork of 8 layers
+    (RY, RZ on every qubit, CX pairs) with depolarizing, amplitude-damping
+    and dephasing channels (1e-3 each) after every gate on each of its
+    qubits; --circuits trajectories (default 8192) per step, seeds advancing
+    every step.  value = trajectories/s of qs_noise_trajectories with the
+    seeds and circuit on the host and the states left on the device; e2e
+    also copies every channel's branch back to the host.  Compared with the
+    reference-style path: one API call per gate and per channel."""
+    import numpy as np
+    import torch
+    from qsim_b200 import engine as E
+    from qsim_b200 import workloads as W
+    from qsim_b200.noise import n_channels, run_trajectories
+    n = args.qubits if args.qubits != 32 else 12
+    T = args.circuits if args.circuits != 4096 else 8192
+    qc = W.noisy_brickwork(n, 8, seed=5)
+    nn = n_channels(qc)
+    out = torch.empty((T, 1 << n), dtype=torch.complex64, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    h = E._h(dev)
+    k = [0]
+
+    def step(branches=False):
+        k[0] += 1
+        return run_trajectories(qc, T, seed=k[0] * T, out=out, branches=branches)
+
+    for _ in range(args.warmup):
+        step()
+    l0 = h.launches()
+    with ClockSampler(dev) as clk:
+        t = _cuda_time(step, stream, args.steps)
+        launches = h.launches() - l0
+        t_e2e = _cuda_time(lambda: step(True), stream, args.steps)
+    t, t_e2e = reduce_max(t, f"cuda:{dev}"), reduce_max(t_e2e, f"cuda:{dev}")
+    per_step, per_e2e = t / args.steps, t_e2e / args.steps
+    ref_rate = _per_channel_trajectories(qc, 2, dev)
+    peak, src = measured_peaks()
+    algo = 8.0 * T * (1 << n)   # one level: each trajectory's state written once
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"metric": METRIC, "value": ws * T / per_step, "unit": "trajectories/s", "ms_per_step": per_step * 1e3,
+            "dtype": "c64 state, fp64 branch probabilities",
+            "config": {"workload": f"noisy: {n}-qubit brickwork x 8 layers, {nn} channels (depolarizing, amplitude "
+                                   f"damping, dephasing at 1e-3), {T} trajectories per step",
+                       "l2": f"{(T << n) * 8 >> 20} MiB of states per step"},
+            "per_channel_launches": {"value": ref_rate, "unit": "trajectories/s",
+                                     "note": "one blackwell_kernels call per gate and per channel"},
+            "roofline": {"bound": "hbm", "achieved": algo / per_step / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / per_step / 1e9 / peak, "traffic": None, "peak_source": src,
+                         "note": "the whole circuit runs in shared memory; HBM only sees each final state once, "
+                                 "so this fraction is low by design (the work is shared-memory sweeps)"},
+            "e2e": {"value": ws * T / per_e2e, "unit": "trajectories/s", "h2d_bytes_per_step": int(T * 64),
+                    "d2h_bytes_per_step": int(T * nn),
+                    "note": "item table (state offset, seed, branch slot per trajectory) in, every branch out; "
+                            "the shared program (a few hundred KB) is uploaded too"},
+            "clocks": clk.summary(), "gpu_launches": int(launches)}, {"unit": "trajectories/s"}
+
+
 WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
-             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain}
+             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy}
 
 
 # --------------------------------------------------------- CPU baseline
@@ -666,6 +759,18 @@ def cpu_baseline(workload: str, args) -> dict:
         return {"value": 1.0 / per_gate_32, "unit": "gates/s", "cores": cores, "kind": "port",
                 "sample": f"first {len(ops)} gates of the same generator at {n_s} qubits (FP64), "
                           f"time x 2^{args.qubits - n_s} (extrapolated to {args.qubits} qubits)"}
+    if workload == "noisy":
+        n = args.qubits if args.qubits != 32 else 12
+        qc = W.noisy_brickwork(n, 8, seed=5)
+        ops = np.ascontiguousarray(__import__("qsim_b200.circuit", fromlist=["lower"]).lower(qc))
+        t0 = time.perf_counter()
+        tot = 0
+        while time.perf_counter() - t0 < 10 or tot == 0:
+            O.noise_trajectory(n, ops, tot)
+            tot += 1
+        dt = time.perf_counter() - t0
+        return {"value": tot / dt, "unit": "trajectories/s", "cores": 1, "kind": "port",
+                "sample": f"{tot} trajectories of the same circuit (FP64 numpy restatement, one thread)"}
     # circuits/s workloads: QV circuits at widths drawn as in the batch
     rng = np.random.default_rng(7)
     ws_ = rng.integers(10, 21, size=24)

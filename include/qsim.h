@@ -410,14 +410,15 @@ int qs_apply_dephasing(qs_handle_t h, void* state, int n_qubits, int target, dou
 /* Batched noise trajectories (no reference counterpart; the reference
  * applies one channel per call with a host round trip each): n_traj
  * independent runs of one circuit whose ops may include QS_OP_DEPOLARIZE,
- * QS_OP_AMP_DAMP and QS_OP_DEPHASE.  Trajectory t draws one uniform per
- * noise op, in program order, from seeds[t] (splitmix64, top 53 bits, as
- * the serving runtime's sampling).  Depolarizing draws are resolved on the
- * host into exact Paulis that the planner fuses with the circuit; damping
- * and dephasing are decided on the device.  Up to 14 qubits each trajectory
- * runs start to finish in one CTA's shared memory (all trajectories in one
+ * QS_OP_AMP_DAMP and QS_OP_DEPHASE.  Trajectory t's uniform for noise op
+ * k (in program order) is value k of the splitmix64 stream of seeds[t] (top
+ * 53 bits, the serving runtime's sampling stream), so a trajectory gives the
+ * same result alone or in any batch.  Up to 14 qubits every channel is
+ * applied inside the tile-pass program and each trajectory runs start to
+ * finish in one CTA's shared memory (one program for all trajectories, one
  * launch per program level); wider states run the unitary segments as batch
- * launches and each state-dependent channel as two launches over all
+ * launches (depolarizing outcomes drawn on the host become Paulis fused by
+ * the planner) and each damping / dephasing channel as two launches over all
  * trajectories.  states: device [n_traj][2^n] complex64, written from
  * |0..0>.  branches_host (optional): [n_traj][n_noise] uint8, the branch of
  * every noise op (depolarizing 0..3, damping/dephasing 0/1).               */

@@ -121,7 +121,7 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
                                                    p.pass_offsets[L]);
         it.ntiles = 1ull << (p.n_qubits - T);
         it.flags = (L == 0 && from_zero) ? PI_FROM_ZERO : 0u;
-        it.noise_u = u.noise_u;
+        it.noise_seed = u.noise_seed;
         it.noise_branch = u.noise_branch;
         auto& g = groups[std::make_tuple(T, p.pass_R[L], p.pass_has2[L])];
         g.first.push_back(it);
@@ -175,7 +175,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
   std::vector<qs_plan_s> plans;
   plan_all(h, nc, widths, op_off, ops, plans);
   std::vector<BatchUnit> units(nc);
-  for (int c = 0; c < nc; ++c) units[c] = BatchUnit{c, (uint64_t)state_off[c], nullptr, nullptr};
+  for (int c = 0; c < nc; ++c) units[c] = BatchUnit{c, (uint64_t)state_off[c], 0, nullptr};
   return qs_batch_build_units(h, plans, units, true);
 }
 

@@ -94,10 +94,11 @@ enum DevKind : uint8_t {
                  // pairs (|t0=0 t1=1>, |t0=1 t1=0>) use c[1]; each pair as in
                  // DK_KRY (the dropped factors are already in the next diagonal)
   DK_CU2 = 16,   // DK_U2 with controls (rc on register bits, gc on the index)
-  DK_NOISE = 17, // state-dependent channel on tile position t0, alone in a
-                 // noise block (DevBlock.pos[6] == 1; tile == whole state):
-                 // d0 = QS_OP_AMP_DAMP or QS_OP_DEPHASE, gc = bits of the FP64
-                 // parameter, coef = index of its uniform / branch slot
+  DK_NOISE = 17, // stochastic channel on tile position t0, alone in a noise
+                 // block (DevBlock.pos[6] == 1; tile == whole state): d0 =
+                 // QS_OP_DEPOLARIZE, QS_OP_AMP_DAMP or QS_OP_DEPHASE, gc = bits
+                 // of the FP64 parameter, coef = the channel's index k (its
+                 // uniform is number k of the item's seed stream)
 };
 
 // Locator of a qubit inside a block: values < 8 are register positions; values
@@ -200,8 +201,8 @@ struct __align__(16) PassItem {
   uint64_t tile_begin;   // prefix of ntiles over the item table
   uint32_t flags;
   uint32_t pad0;
-  const double* noise_u;   // uniforms of the pass's noise blocks (by DevOp.coef)
-  uint8_t* noise_branch;   // branch taken by each noise block (by DevOp.coef)
+  uint64_t noise_seed;     // seed of the uniforms of the pass's noise blocks
+  uint8_t* noise_branch;   // branch taken by each noise block (by DevOp.coef), or null
   uint64_t pad1;
 };
 static_assert(sizeof(PassItem) == 64, "PassItem layout");
@@ -218,7 +219,7 @@ void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, in
 struct BatchUnit {
   int plan;                 // index into the plan list
   uint64_t state_off;       // amplitude offset of the unit's state
-  const double* noise_u;    // device uniforms of the unit's noise blocks, or null
+  uint64_t noise_seed;      // seed of the unit's noise-block uniforms
   uint8_t* noise_branch;    // device branch record, or null
 };
 struct qs_batch_plan_s;
@@ -228,18 +229,30 @@ void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states);
 void qs_batch_release(qs_batch_plan_s* B);
 
 // Deterministic uniforms in [0, 1) from a seed: splitmix64 (Steele, Lea and
-// Flood, 2014), top 53 bits.  Shared by the serving runtime's sampling and
-// the noise trajectories so that both draw the same stream for one seed.
+// Flood, 2014), top 53 bits.  The k-th value (from 0) mixes seed + (k+1)
+// times the golden-ratio increment, so any element can be computed on its
+// own, on the host or the device.  Shared by the serving runtime's sampling
+// and the noise trajectories so that both draw the same stream for a seed.
+__host__ __device__ inline double qs_seed_uniform_at(uint64_t seed, uint64_t k) {
+  uint64_t z = seed + (k + 1) * 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * 0x1.0p-53;
+}
 inline void qs_seed_uniforms(uint64_t seed, int64_t count, double* out) {
-  uint64_t x = seed;
-  for (int64_t i = 0; i < count; ++i) {
-    x += 0x9e3779b97f4a7c15ull;
-    uint64_t z = x;
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    z ^= z >> 31;
-    out[i] = (double)(z >> 11) * 0x1.0p-53;
-  }
+  for (int64_t i = 0; i < count; ++i) out[i] = qs_seed_uniform_at(seed, (uint64_t)i);
+}
+// Depolarizing branch for uniform u (the reference's ranges,
+// bwk/csrc/noise_sm120.cu:262-289): [0, 1-p) identity (0), then X (1), Y (2),
+// Z (3) on consecutive thirds of p.  Plain IEEE operations with no product
+// feeding a sum, so host and device agree bit for bit.
+__host__ __device__ inline int qs_depol_branch(double p, double u) {
+  if (u < 1.0 - p) return 0;
+  const double r = u - (1.0 - p), third = p / 3.0;
+  if (r < third) return 1;
+  if (r < 2.0 * third) return 2;
+  return 3;
 }
 
 // Convenience used by several units.

@@ -7,19 +7,22 @@
 //    amplitude damping and dephasing need P(q=1) of the current state, which
 //    is reduced in FP64 on the device and compared with the uniform there, so
 //    nothing waits for the host unless the caller asks for the branch;
-//  * batched trajectories of one noisy circuit.  Every trajectory draws its
-//    uniforms from its own seed.  Depolarizing outcomes do not depend on the
-//    state, so they are resolved on the host into Paulis that the FP64
-//    planner fuses with the gates (trajectories with the same outcomes share
-//    one program).  Damping and dephasing do depend on the state:
+//  * batched trajectories of one noisy circuit.  Trajectory t's uniform for
+//    channel k is number k of the splitmix64 stream of its seed, computed
+//    where it is used, so a trajectory's result does not depend on the
+//    batch it runs in:
 //      - up to 14 qubits a trajectory's state is one shared-memory tile, so
-//        the channel is a "noise block" inside the tile-pass program
-//        (qs_pass.cu: CTA-wide FP64 reduction, branch, Kraus operator) and a
-//        whole noisy circuit runs start to finish in one CTA per trajectory,
-//        all trajectories in one launch per program level;
-//      - wider states run the unitary segments between channels as batch
-//        launches and each channel as two launches over all trajectories
-//        (per-block FP64 partial sums, then branch + Kraus operator).
+//        every channel is a "noise block" inside the tile-pass program
+//        (qs_pass.cu: the depolarizing Pauli, or a CTA-wide FP64 reduction,
+//        the branch and the Kraus operator).  One program serves all
+//        trajectories; a whole noisy circuit runs start to finish in one CTA
+//        per trajectory, all trajectories in one launch per program level;
+//      - wider states run the unitary segments between state-dependent
+//        channels as batch launches and each such channel as two launches
+//        over all trajectories (per-block FP64 partial sums, then branch +
+//        Kraus operator).  There depolarizing outcomes are drawn on the host
+//        and become Paulis that the FP64 planner fuses with the gates
+//        (trajectories with the same outcomes share a program).
 #include "qs_api.h"
 #include "qs_common.cuh"
 #include <algorithm>
@@ -35,16 +38,6 @@ constexpr int kThreads = 256;
 
 bool is_noise(int kind) {
   return kind == QS_OP_DEPOLARIZE || kind == QS_OP_AMP_DAMP || kind == QS_OP_DEPHASE;
-}
-
-// Depolarizing branch for uniform u (noise_sm120.cu:262-289): [0, 1-p)
-// identity, then X, Y, Z on consecutive thirds of p.
-int depol_branch(double p, double u) {
-  if (u < 1.0 - p) return 0;
-  const double r = u - (1.0 - p), third = p / 3.0;
-  if (r < third) return 1;
-  if (r < 2.0 * third) return 2;
-  return 3;
 }
 
 // Exact Paulis on one state: 1 = X, 2 = Y, 3 = Z.
@@ -111,12 +104,14 @@ __global__ void __launch_bounds__(kThreads) k_noise_sums(const float2* __restric
 
 // Branch and Kraus operator of one channel on block b's share of the
 // amplitude pairs of state t (every block re-reduces the state's partials
-// in the same order, so all blocks take the same branch).  u: uniforms with
-// stride u_stride per state (index k), or null to use u_single.
+// in the same order, so all blocks take the same branch).  The uniform is
+// number k of seeds[t]'s stream, or u_single when seeds is null; the branch
+// goes to branch[t * branch_stride + k] when branch is not null.
 __global__ void __launch_bounds__(kThreads) k_noise_apply(float2* __restrict__ states, int n, int q, int kind,
                                                           double g, int bpt, const double2* __restrict__ partials,
-                                                          const double* __restrict__ u, double u_single,
-                                                          int u_stride, int k, uint8_t* __restrict__ branch, int t0) {
+                                                          const uint64_t* __restrict__ seeds, double u_single,
+                                                          int branch_stride, int k, uint8_t* __restrict__ branch,
+                                                          int t0) {
   const int t = t0 + blockIdx.y, b = blockIdx.x;
   __shared__ double sh[2];
   if (threadIdx.x < 32) {
@@ -136,8 +131,8 @@ __global__ void __launch_bounds__(kThreads) k_noise_apply(float2* __restrict__ s
   __syncthreads();
   const double S0 = sh[0], S1 = sh[1];
   const double p1 = g * S1 / (S0 + S1);
-  const size_t slot = (size_t)t * u_stride + k;
-  const double uu = u ? u[slot] : u_single;
+  const size_t slot = (size_t)t * branch_stride + k;
+  const double uu = seeds ? qs_seed_uniform_at(seeds[t], (uint64_t)k) : u_single;
   // the kept branch has norm^2 keep; a branch of zero weight is never taken
   const double keep = S0 + (1.0 - g) * S1;
   const bool jump = S1 > 0.0 && (uu < p1 || !(keep > 0.0));
@@ -173,15 +168,16 @@ __global__ void __launch_bounds__(kThreads) k_noise_apply(float2* __restrict__ s
 // One state-dependent channel over n_states states stored back to back;
 // partials: device scratch of n_states * blocks_per_state(n) double2.
 void launch_channel(qs_context* h, float2* states, int n, int n_states, int q, int kind, double g,
-                    double2* partials, const double* d_u, double u_single, int u_stride, int k, uint8_t* d_branch) {
+                    double2* partials, const uint64_t* d_seeds, double u_single, int branch_stride, int k,
+                    uint8_t* d_branch) {
   const int bpt = blocks_per_state(n);
   for (int t0 = 0; t0 < n_states; t0 += 65535) {
     const int nt = std::min(65535, n_states - t0);
     dim3 grid((unsigned)bpt, (unsigned)nt);
     k_noise_sums<<<grid, kThreads, 0, h->stream>>>(states, n, q, bpt, partials, t0);
     qs_after_launch(h, "k_noise_sums");
-    k_noise_apply<<<grid, kThreads, 0, h->stream>>>(states, n, q, kind, g, bpt, partials, d_u, u_single, u_stride,
-                                                    k, d_branch, t0);
+    k_noise_apply<<<grid, kThreads, 0, h->stream>>>(states, n, q, kind, g, bpt, partials, d_seeds, u_single,
+                                                    branch_stride, k, d_branch, t0);
     qs_after_launch(h, "k_noise_apply");
   }
 }
@@ -331,10 +327,11 @@ struct Merger {
   }
 };
 
-// A trajectory's op stream for one depolarizing outcome pattern `br`: each
-// depolarizing site becomes its Pauli (or nothing); every state-dependent
-// site ends a segment.  seg_site[s] is the site index that follows segment s.
-void segment_stream(const qs_op* ops, int nops, const std::vector<NoiseSite>& sites, const std::vector<uint8_t>& br,
+// The circuit's op stream cut into unitary segments; seg_site[s] is the
+// site that follows segment s.  With br (a depolarizing outcome pattern),
+// each depolarizing site becomes its Pauli (or nothing) and only the
+// state-dependent sites cut; without it every site cuts.
+void segment_stream(const qs_op* ops, int nops, const std::vector<NoiseSite>& sites, const std::vector<uint8_t>* br,
                     std::vector<std::vector<qs_op>>& seg_ops, std::vector<int>& seg_site) {
   seg_ops.assign(1, {});
   seg_site.clear();
@@ -342,8 +339,9 @@ void segment_stream(const qs_op* ops, int nops, const std::vector<NoiseSite>& si
   for (int i = 0; i < nops; ++i) {
     if (k < sites.size() && sites[k].op == i) {
       const NoiseSite& s = sites[k];
-      if (s.kind == QS_OP_DEPOLARIZE) {
-        if (br[k]) seg_ops.back().push_back(pauli_op(s.q, br[k]));
+      if (br && s.kind == QS_OP_DEPOLARIZE) {
+        const uint8_t b = (*br)[k];
+        if (b) seg_ops.back().push_back(pauli_op(s.q, b));
       } else {
         seg_site.push_back((int)k);
         seg_ops.emplace_back();
@@ -366,7 +364,7 @@ int qs_apply_depolarizing(qs_handle_t h, void* state, int n, int target, double 
   qs_check_qubit(target, n, "target");
   check_prob(p, "p");
   QS_CHECK_ARG(std::isfinite(u), "random value must be finite");
-  const int b = depol_branch(p, u);
+  const int b = qs_depol_branch(p, u);
   if (b) {
     const uint64_t npairs = 1ull << (n - 1);
     const int grid = qs_blocks_for(h, npairs, kThreads);
@@ -395,7 +393,7 @@ int qs_apply_dephasing(qs_handle_t h, void* state, int n, int target, double lam
 int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int n_traj, const uint64_t* seeds,
                           void* states, uint8_t* branches_host) {
   QS_REQUIRE_HANDLE(h);
-  double* d_u = nullptr;
+  uint64_t* d_seeds = nullptr;
   uint8_t* d_br = nullptr;
   qs_batch_plan_s* B = nullptr;
   try {
@@ -414,82 +412,83 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
     sites.push_back(NoiseSite{i, ops[i].kind, ops[i].q[0], ops[i].m[0]});
   }
   const int nn = (int)sites.size();
-  const size_t slots = (size_t)n_traj * (size_t)std::max(nn, 1);
-  std::vector<double> U(slots, 0.0);
-  std::vector<uint8_t> Br(slots, 0);
-  // depolarizing outcomes on the host; trajectories with the same outcomes
-  // share a program
-  std::map<std::vector<uint8_t>, int> pattern_id;
-  std::vector<std::vector<uint8_t>> patterns;
-  std::vector<int> traj_pattern(n_traj);
-  for (int t = 0; t < n_traj; ++t) {
-    if (nn) qs_seed_uniforms(seeds[t], nn, U.data() + (size_t)t * nn);
-    std::vector<uint8_t> key(nn, 0);
-    for (int k = 0; k < nn; ++k)
-      if (sites[k].kind == QS_OP_DEPOLARIZE)
-        key[k] = Br[(size_t)t * nn + k] = (uint8_t)depol_branch(sites[k].p, U[(size_t)t * nn + k]);
-    auto it = pattern_id.find(key);
-    if (it == pattern_id.end()) {
-      it = pattern_id.emplace(key, (int)patterns.size()).first;
-      patterns.push_back(key);
-    }
-    traj_pattern[t] = it->second;
-  }
-  QS_CUDA(cudaMallocAsync((void**)&d_u, slots * sizeof(double), h->stream));
-  QS_CUDA(cudaMallocAsync((void**)&d_br, slots, h->stream));
-  QS_CUDA(cudaMemcpyAsync(d_u, U.data(), slots * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  QS_CUDA(cudaMemcpyAsync(d_br, Br.data(), slots, cudaMemcpyHostToDevice, h->stream));
+  const bool want_br = branches_host && nn;
+  const size_t slots = (size_t)n_traj * (size_t)nn;
+  if (want_br) QS_CUDA(cudaMallocAsync((void**)&d_br, slots, h->stream));
   const uint64_t N = 1ull << n;
   int tb = 0, bb = 0;
   qs_plan_shape(h, n, false, tb, bb);
 
   if (n <= 14) {
-    // one merged whole-state program per pattern, one CTA per trajectory
-    std::vector<qs_plan_s> progs(patterns.size());
+    // one whole-state program with a noise block per channel, shared by all
+    // trajectories; one CTA per trajectory
+    std::vector<std::vector<qs_op>> seg;
+    std::vector<int> seg_site;
+    segment_stream(ops, nops, sites, nullptr, seg, seg_site);
     const size_t smem_left = 200 * 1024 - (8ull << n) - 2 * 128 * sizeof(uint64_t) - 16 * sizeof(int) - 16;
-    for (size_t pi = 0; pi < patterns.size(); ++pi) {
-      std::vector<std::vector<qs_op>> seg;
-      std::vector<int> seg_site;
-      segment_stream(ops, nops, sites, patterns[pi], seg, seg_site);
-      Merger m;
-      m.n = n;
-      m.R = std::min(bb, n);
-      m.coef_cap = std::min<size_t>(8192, smem_left / sizeof(float2));
-      m.out.n_qubits = n;
-      double flops = 0;
-      for (size_t s = 0; s < seg.size(); ++s) {
-        if (!seg[s].empty()) {
-          qs_plan_s p;
-          qs_build_plan(n, seg[s].data(), (int)seg[s].size(), tb, &p, bb);
-          m.add_plan(p);
-          flops += p.info.flops;
-        }
-        if (s < seg_site.size()) m.add_noise(sites[seg_site[s]], seg_site[s]);
+    Merger m;
+    m.n = n;
+    m.R = std::min(bb, n);
+    m.coef_cap = std::min<size_t>(8192, smem_left / sizeof(float2));
+    m.out.n_qubits = n;
+    double flops = 0;
+    for (size_t s = 0; s < seg.size(); ++s) {
+      if (!seg[s].empty()) {
+        qs_plan_s p;
+        qs_build_plan(n, seg[s].data(), (int)seg[s].size(), tb, &p, bb);
+        m.add_plan(p);
+        flops += p.info.flops;
       }
-      m.flush(true);
-      m.out.info.flops = flops;
-      progs[pi] = std::move(m.out);
+      if (s < seg_site.size()) m.add_noise(sites[seg_site[s]], seg_site[s]);
     }
+    m.flush(true);
+    m.out.info.flops = flops;
+    std::vector<qs_plan_s> progs(1);
+    progs[0] = std::move(m.out);
     std::vector<BatchUnit> units(n_traj);
     for (int t = 0; t < n_traj; ++t)
-      units[t] = BatchUnit{traj_pattern[t], (uint64_t)t * N, d_u + (size_t)t * nn, d_br + (size_t)t * nn};
+      units[t] = BatchUnit{0, (uint64_t)t * N, seeds[t], want_br ? d_br + (size_t)t * nn : nullptr};
     B = qs_batch_build_units(h, progs, units, true);
     qs_batch_launch(h, B, states);
     qs_batch_release(B);
     B = nullptr;
   } else {
-    // segments between state-dependent channels; each a batch over the
-    // trajectories, each channel two launches over all of them
+    // depolarizing outcomes on the host; trajectories with the same outcomes
+    // share their segment programs
+    std::vector<uint8_t> Br(want_br ? slots : 0, 0);
+    std::map<std::vector<uint8_t>, int> pattern_id;
+    std::vector<std::vector<uint8_t>> patterns;
+    std::vector<int> traj_pattern(n_traj);
+    for (int t = 0; t < n_traj; ++t) {
+      std::vector<uint8_t> key(nn, 0);
+      for (int k = 0; k < nn; ++k)
+        if (sites[k].kind == QS_OP_DEPOLARIZE) {
+          key[k] = (uint8_t)qs_depol_branch(sites[k].p, qs_seed_uniform_at(seeds[t], (uint64_t)k));
+          if (want_br) Br[(size_t)t * nn + k] = key[k];
+        }
+      auto it = pattern_id.find(key);
+      if (it == pattern_id.end()) {
+        it = pattern_id.emplace(key, (int)patterns.size()).first;
+        patterns.push_back(key);
+      }
+      traj_pattern[t] = it->second;
+    }
+    if (want_br) QS_CUDA(cudaMemcpyAsync(d_br, Br.data(), slots, cudaMemcpyHostToDevice, h->stream));
     std::vector<std::vector<std::vector<qs_op>>> seg_of(patterns.size());
     std::vector<int> seg_site;
-    for (size_t pi = 0; pi < patterns.size(); ++pi) segment_stream(ops, nops, sites, patterns[pi], seg_of[pi], seg_site);
+    for (size_t pi = 0; pi < patterns.size(); ++pi)
+      segment_stream(ops, nops, sites, &patterns[pi], seg_of[pi], seg_site);
     const size_t nseg = seg_site.size() + 1;
     bool need_init = false;
     for (int t = 0; t < n_traj; ++t) need_init |= seg_of[traj_pattern[t]][0].empty();
     if (need_init && qs_state_init_batched(h, states, n_traj, n) != QS_OK) throw qs_error(QS_ERR_CUDA, h->err);
     double2* partials = nullptr;
-    if (!seg_site.empty())
+    if (!seg_site.empty()) {
+      QS_CUDA(cudaMallocAsync((void**)&d_seeds, (size_t)n_traj * sizeof(uint64_t), h->stream));
+      QS_CUDA(cudaMemcpyAsync(d_seeds, seeds, (size_t)n_traj * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                              h->stream));
       partials = static_cast<double2*>(h->scratch_get((size_t)n_traj * blocks_per_state(n) * sizeof(double2)));
+    }
     for (size_t s = 0; s < nseg; ++s) {
       std::map<std::vector<uint8_t>, int> seg_plan;  // outcomes within the segment -> plan
       std::vector<qs_plan_s> plans;
@@ -512,7 +511,7 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
       }
       for (int t = 0; t < n_traj; ++t) {
         const int pl = plan_of_pattern[traj_pattern[t]];
-        if (pl >= 0) units.push_back(BatchUnit{pl, (uint64_t)t * N, nullptr, nullptr});
+        if (pl >= 0) units.push_back(BatchUnit{pl, (uint64_t)t * N, 0, nullptr});
       }
       if (!units.empty()) {
         B = qs_batch_build_units(h, plans, units, s == 0 && !need_init);
@@ -522,21 +521,25 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
       }
       if (s < seg_site.size()) {
         const NoiseSite& ns = sites[seg_site[s]];
-        launch_channel(h, (float2*)states, n, n_traj, ns.q, ns.kind, ns.p, partials, d_u, 0.0, nn, seg_site[s], d_br);
+        launch_channel(h, (float2*)states, n, n_traj, ns.q, ns.kind, ns.p, partials, d_seeds, 0.0, nn,
+                       seg_site[s], d_br);
       }
     }
   }
-  if (branches_host && nn)
-    QS_CUDA(cudaMemcpyAsync(branches_host, d_br, (size_t)n_traj * nn, cudaMemcpyDeviceToHost, h->stream));
-  QS_CUDA(cudaFreeAsync(d_u, h->stream));
-  d_u = nullptr;
-  QS_CUDA(cudaFreeAsync(d_br, h->stream));
-  d_br = nullptr;
-  if (branches_host && nn) QS_CUDA(cudaStreamSynchronize(h->stream));
+  if (want_br) {
+    QS_CUDA(cudaMemcpyAsync(branches_host, d_br, slots, cudaMemcpyDeviceToHost, h->stream));
+    QS_CUDA(cudaFreeAsync(d_br, h->stream));
+    d_br = nullptr;
+  }
+  if (d_seeds) {
+    QS_CUDA(cudaFreeAsync(d_seeds, h->stream));
+    d_seeds = nullptr;
+  }
+  if (want_br) QS_CUDA(cudaStreamSynchronize(h->stream));
   return QS_OK;
   } catch (const std::exception& e) {
     if (B) qs_batch_release(B);
-    if (d_u) cudaFreeAsync(d_u, h->stream);
+    if (d_seeds) cudaFreeAsync(d_seeds, h->stream);
     if (d_br) cudaFreeAsync(d_br, h->stream);
     const qs_error* qe = dynamic_cast<const qs_error*>(&e);
     h->err = e.what();

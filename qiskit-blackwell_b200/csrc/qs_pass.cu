@@ -451,19 +451,38 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 }
 
 // ------------------------------------------------------- noise blocks ------
-// A state-dependent channel (amplitude damping or dephasing) on tile position
-// q of a tile that holds the whole state: FP64 sums of |a|^2 over the q = 0
-// and q = 1 halves (fixed order: per thread, then warps in index order), the
-// jump branch when u < p1 = g * S1 / (S0 + S1), then the branch's Kraus
-// operator with exact renormalisation:
-//   no jump : a0 *= 1/sqrt(S0 + (1-g) S1),  a1 *= sqrt(1-g)/sqrt(S0 + (1-g) S1)
-//   damping : a0 = a1 / sqrt(S1),  a1 = 0          (E1 = [[0, sqrt g], [0, 0]])
-//   dephase : a0 = 0,  a1 *= 1 / sqrt(S1)          (E1 = [[0, 0], [0, sqrt l]])
+// A stochastic channel on tile position q of a tile that holds the whole
+// state.  Its uniform is number k (= op.coef) of the item's seed stream.
+//  * depolarizing: branch by the reference's ranges; X, Y or Z on the tile;
+//  * amplitude damping / dephasing: FP64 sums of |a|^2 over the q = 0 and
+//    q = 1 halves (fixed order: per thread, then warps in index order), the
+//    jump branch when u < p1 = g * S1 / (S0 + S1), then the branch's Kraus
+//    operator with exact renormalisation:
+//      no jump : a0 *= 1/sqrt(S0 + (1-g) S1),  a1 *= sqrt(1-g)/sqrt(S0 + (1-g) S1)
+//      damping : a0 = a1 / sqrt(S1),  a1 = 0          (E1 = [[0, sqrt g], [0, 0]])
+//      dephase : a0 = 0,  a1 *= 1 / sqrt(S1)          (E1 = [[0, 0], [0, sqrt l]])
 // All threads of the CTA take part; red holds 2 x 8 doubles.
-__device__ __noinline__ void noise_block(float2* tile, int T, const DevOp op, const double* nu, uint8_t* nb,
+__device__ __noinline__ void noise_block(float2* tile, int T, const DevOp op, uint64_t seed, uint8_t* nb,
                                         double* red) {
   const int q = op.t0;
   const uint32_t N = 1u << T;
+  const double g = __longlong_as_double((long long)op.gc);
+  const double u = qs_seed_uniform_at(seed, op.coef);
+  if (op.d0 == QS_OP_DEPOLARIZE) {
+    const int br = qs_depol_branch(g, u);
+    if (threadIdx.x == 0 && nb) nb[op.coef] = (uint8_t)br;
+    if (br == 0) return;
+    for (uint32_t c = threadIdx.x; c < (N >> 1); c += blockDim.x) {
+      const uint32_t i0 = (uint32_t)insert_zero(c, q), i1 = i0 | (1u << q);
+      float2& a0 = tile[phys(i0)];
+      float2& a1 = tile[phys(i1)];
+      const float2 v0 = a0, v1 = a1;
+      if (br == 1) { a0 = v1; a1 = v0; }
+      else if (br == 2) { a0 = make_float2(v1.y, -v1.x); a1 = make_float2(-v0.y, v0.x); }
+      else a1 = make_float2(-v1.x, -v1.y);
+    }
+    return;
+  }
   double s0 = 0.0, s1 = 0.0;
   for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
     const float2 a = tile[phys(i)];
@@ -480,9 +499,7 @@ __device__ __noinline__ void noise_block(float2* tile, int T, const DevOp op, co
   __syncthreads();
   double S0 = 0.0, S1 = 0.0;
   for (int k = 0; k < nw; ++k) { S0 += red[k]; S1 += red[8 + k]; }
-  const double g = __longlong_as_double((long long)op.gc);
   const double p1 = g * S1 / (S0 + S1);
-  const double u = nu ? nu[op.coef] : 1.0;
   // the kept branch has norm^2 keep; a branch of zero weight is never taken
   const double keep = S0 + (1.0 - g) * S1;
   const bool jump = S1 > 0.0 && (u < p1 || !(keep > 0.0));
@@ -601,7 +618,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
     for (int b = 0; b < nblocks; ++b) {
       const DevBlock blk = blocks[b];
       if (blk.pos[6]) {  // noise block (only in programs whose tile is the whole state)
-        noise_block(tile, T, ops[blk.op_begin], I.noise_u, I.noise_branch, s_red);
+        noise_block(tile, T, ops[blk.op_begin], I.noise_seed, I.noise_branch, s_red);
         __syncthreads();
         continue;
       }

@@ -12,6 +12,9 @@
 * ``efficient_su2`` / ``random_pauli_observable`` — Ry/Rz layers + CNOT chain
   ansatz with trainable parameters and a random Pauli-sum observable.
 * ``serving_hamiltonian`` / ``product_state`` — the Chebyshev requests.
+* ``noisy_brickwork`` — RY/RZ on every qubit and CX brickwork per layer, with
+  depolarizing, amplitude-damping and dephasing channels after every gate on
+  each of its qubits (the noise-trajectory workload).
 """
 from __future__ import annotations
 
@@ -163,3 +166,20 @@ def product_state(n: int, seed: int) -> np.ndarray:
         q = np.array([math.cos(a / 2) * np.exp(-0.5j * b), math.sin(a / 2) * np.exp(0.5j * b)])
         psi = np.kron(q, psi)  # new qubit is the most significant
     return psi
+
+
+def noisy_brickwork(n: int, layers: int, seed: int, depolarizing: float = 1e-3, amplitude_damping: float = 1e-3,
+                    dephasing: float = 1e-3) -> Circuit:
+    """Per layer: RY(a) RZ(b) on every qubit (angles uniform in [0, 2pi)),
+    then CX on (2i, 2i+1) for even layers and (2i+1, 2i+2) for odd ones; each
+    gate followed by the three channels on each qubit it touches."""
+    from .noise import add_noise
+    rng = np.random.default_rng(seed)
+    qc = Circuit(n, name=f"noisy_brickwork_{n}x{layers}")
+    for d in range(layers):
+        for q in range(n):
+            qc.ry(float(rng.uniform(0, 2 * math.pi)), q)
+            qc.rz(float(rng.uniform(0, 2 * math.pi)), q)
+        for q in range(d % 2, n - 1, 2):
+            qc.cx(q, q + 1)
+    return add_noise(qc, depolarizing=depolarizing, amplitude_damping=amplitude_damping, dephasing=dephasing)
