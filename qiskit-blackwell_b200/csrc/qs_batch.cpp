@@ -25,7 +25,7 @@ struct qs_batch_plan_s {
   int n_circuits = 0;
   void* d_blob = nullptr;          // all device programs
   void* d_items = nullptr;         // all PassItem tables
-  struct Launch { int T, R, has2, ncoef; size_t item_off; int n_items; uint64_t total_tiles; };
+  struct Launch { int T, R, has2, ncoef; size_t item_off; int n_items; uint64_t total_tiles; int threads; };
   std::vector<Launch> launches;
   qs_batch_info info{};
   // CUDA graph of the launch sequence, captured at the second execution on
@@ -79,7 +79,7 @@ void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t*
 // items by pass level, then by (T, R, has2), into launches.  Units that
 // share a plan share its device program.
 qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
-                                      const std::vector<BatchUnit>& units, bool from_zero) {
+                                      const std::vector<BatchUnit>& units, bool from_zero, int threads) {
   const int np = (int)plans.size();
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
@@ -140,6 +140,7 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
         uint64_t tb = 0;
         for (PassItem& it : g->second.first) { it.tile_begin = tb; tb += it.ntiles; items.push_back(it); }
         Lc.total_tiles = tb;
+        Lc.threads = threads;
         B->launches.push_back(Lc);
       }
     }
@@ -183,7 +184,7 @@ void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states) {
   B->stream = h->stream;
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
-    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef);
+    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
   }
 }
 
@@ -192,7 +193,7 @@ void qs_batch_release(qs_batch_plan_s* B) { free_bplan(B); }
 static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
-    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef);
+    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
   }
 }
 

@@ -210,8 +210,9 @@ static_assert(sizeof(PassItem) == 64, "PassItem layout");
 // the largest coefficient pool (float2) of the launch's passes.
 void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,
                            uint32_t flags, int has2, int ncoef);
+// threads: CTA size (a multiple of 32, at most the default); 0 = default.
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
-                          int maxT, int R, int has2, int ncoef);
+                          int maxT, int R, int has2, int ncoef, int threads = 0);
 
 // Batch engine internals (qs_batch.cpp), shared with the noise-trajectory
 // runner: a batch is a set of host plans (each uploaded into one device
@@ -223,8 +224,9 @@ struct BatchUnit {
   uint8_t* noise_branch;    // device branch record, or null
 };
 struct qs_batch_plan_s;
+// threads: CTA size of the batch's launches (0 = the tile-pass default).
 qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
-                                      const std::vector<BatchUnit>& units, bool from_zero);
+                                      const std::vector<BatchUnit>& units, bool from_zero, int threads = 0);
 void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states);
 void qs_batch_release(qs_batch_plan_s* B);
 

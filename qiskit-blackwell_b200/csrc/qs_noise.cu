@@ -27,6 +27,7 @@
 #include "qs_common.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 
@@ -35,6 +36,14 @@ using namespace qs;
 namespace {
 
 constexpr int kThreads = 256;
+
+// CTA size of the whole-state trajectory launches: 128 (measured on B200
+// against 64 and 256 on a 12-qubit, 840-channel circuit); QSIM_NOISE_THREADS
+// overrides (a multiple of 32; 0 = the tile-pass default).
+int noise_threads() {
+  const char* e = std::getenv("QSIM_NOISE_THREADS");
+  return e ? std::atoi(e) : 128;
+}
 
 bool is_noise(int kind) {
   return kind == QS_OP_DEPOLARIZE || kind == QS_OP_AMP_DAMP || kind == QS_OP_DEPHASE;
@@ -309,21 +318,32 @@ struct Merger {
     }
   }
 
-  void add_noise(const NoiseSite& s, int k) {
+  // One noise block for a run of consecutive channels (site index, site)
+  // on at most 4 distinct qubits.
+  void add_noise_group(const std::vector<std::pair<int, NoiseSite>>& group) {
     DevBlock b;
     std::memset(&b, 0, sizeof(b));
+    std::vector<int> qs;
+    for (const auto& e : group)
+      if (std::find(qs.begin(), qs.end(), e.second.q) == qs.end()) qs.push_back(e.second.q);
+    std::sort(qs.begin(), qs.end());  // the kernel inserts zeros at Q in ascending order
+    const int nq = (int)qs.size();
+    for (int j = 0; j < nq; ++j) b.pos[j] = (int8_t)qs[j];
+    b.pos[5] = (int8_t)nq;
     b.pos[6] = 1;
     b.op_begin = (int32_t)ops.size();
-    b.op_end = b.op_begin + 1;
-    DevOp d;
-    std::memset(&d, 0, sizeof(d));
-    d.kind = DK_NOISE;
-    d.t0 = (uint8_t)s.q;
-    d.d0 = (uint8_t)s.kind;
-    d.coef = (uint32_t)k;
-    std::memcpy(&d.gc, &s.p, sizeof(double));
+    for (const auto& e : group) {
+      DevOp d;
+      std::memset(&d, 0, sizeof(d));
+      d.kind = DK_NOISE;
+      d.t0 = (uint8_t)e.second.q;
+      d.d0 = (uint8_t)e.second.kind;
+      d.coef = (uint32_t)e.first;
+      std::memcpy(&d.gc, &e.second.p, sizeof(double));
+      ops.push_back(d);
+    }
+    b.op_end = (int32_t)ops.size();
     blocks.push_back(b);
-    ops.push_back(d);
   }
 };
 
@@ -425,6 +445,18 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
     std::vector<std::vector<qs_op>> seg;
     std::vector<int> seg_site;
     segment_stream(ops, nops, sites, nullptr, seg, seg_site);
+    // channels after (almost) every gate leave segments of one or two gates:
+    // 3-qubit register blocks then beat wider ones (smaller diagonal tables,
+    // so more CTAs per SM; measured 204 k vs 182 k trajectories/s on a
+    // 12-qubit, 840-channel circuit)
+    {
+      size_t nonempty = 0, gates = 0;
+      for (const auto& sg : seg) {
+        nonempty += !sg.empty();
+        gates += sg.size();
+      }
+      if (h->block_bits == 0 && nonempty && gates <= 4 * nonempty) bb = std::min(bb, 3);
+    }
     const size_t smem_left = 200 * 1024 - (8ull << n) - 2 * 128 * sizeof(uint64_t) - 16 * sizeof(int) - 16;
     Merger m;
     m.n = n;
@@ -432,15 +464,36 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
     m.coef_cap = std::min<size_t>(8192, smem_left / sizeof(float2));
     m.out.n_qubits = n;
     double flops = 0;
+    // consecutive channels (no gate between) share a block while they touch
+    // at most kGroupQubits qubits and number at most kGroupOps
+    constexpr int kGroupQubits = 4, kGroupOps = 32;
+    std::vector<std::pair<int, NoiseSite>> group;
+    auto group_qubits = [&](int extra) {
+      std::vector<int> qs;
+      for (const auto& e : group)
+        if (std::find(qs.begin(), qs.end(), e.second.q) == qs.end()) qs.push_back(e.second.q);
+      if (extra >= 0 && std::find(qs.begin(), qs.end(), extra) == qs.end()) qs.push_back(extra);
+      return (int)qs.size();
+    };
+    auto flush_group = [&]() {
+      if (!group.empty()) m.add_noise_group(group);
+      group.clear();
+    };
     for (size_t s = 0; s < seg.size(); ++s) {
       if (!seg[s].empty()) {
+        flush_group();
         qs_plan_s p;
         qs_build_plan(n, seg[s].data(), (int)seg[s].size(), tb, &p, bb);
         m.add_plan(p);
         flops += p.info.flops;
       }
-      if (s < seg_site.size()) m.add_noise(sites[seg_site[s]], seg_site[s]);
+      if (s < seg_site.size()) {
+        const NoiseSite& ns = sites[seg_site[s]];
+        if ((int)group.size() >= kGroupOps || group_qubits(ns.q) > kGroupQubits) flush_group();
+        group.emplace_back(seg_site[s], ns);
+      }
     }
+    flush_group();
     m.flush(true);
     m.out.info.flops = flops;
     std::vector<qs_plan_s> progs(1);
@@ -448,7 +501,7 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
     std::vector<BatchUnit> units(n_traj);
     for (int t = 0; t < n_traj; ++t)
       units[t] = BatchUnit{0, (uint64_t)t * N, seeds[t], want_br ? d_br + (size_t)t * nn : nullptr};
-    B = qs_batch_build_units(h, progs, units, true);
+    B = qs_batch_build_units(h, progs, units, true, noise_threads());
     qs_batch_launch(h, B, states);
     qs_batch_release(B);
     B = nullptr;

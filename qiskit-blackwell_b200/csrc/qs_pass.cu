@@ -451,78 +451,209 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 }
 
 // ------------------------------------------------------- noise blocks ------
-// A stochastic channel on tile position q of a tile that holds the whole
-// state.  Its uniform is number k (= op.coef) of the item's seed stream.
-//  * depolarizing: branch by the reference's ranges; X, Y or Z on the tile;
-//  * amplitude damping / dephasing: FP64 sums of |a|^2 over the q = 0 and
-//    q = 1 halves (fixed order: per thread, then warps in index order), the
-//    jump branch when u < p1 = g * S1 / (S0 + S1), then the branch's Kraus
-//    operator with exact renormalisation:
-//      no jump : a0 *= 1/sqrt(S0 + (1-g) S1),  a1 *= sqrt(1-g)/sqrt(S0 + (1-g) S1)
-//      damping : a0 = a1 / sqrt(S1),  a1 = 0          (E1 = [[0, sqrt g], [0, 0]])
-//      dephase : a0 = 0,  a1 *= 1 / sqrt(S1)          (E1 = [[0, 0], [0, sqrt l]])
-// All threads of the CTA take part; red holds 2 x 8 doubles.
-__device__ __noinline__ void noise_block(float2* tile, int T, const DevOp op, uint64_t seed, uint8_t* nb,
-                                        double* red) {
-  const int q = op.t0;
-  const uint32_t N = 1u << T;
-  const double g = __longlong_as_double((long long)op.gc);
-  const double u = qs_seed_uniform_at(seed, op.coef);
-  if (op.d0 == QS_OP_DEPOLARIZE) {
-    const int br = qs_depol_branch(g, u);
-    if (threadIdx.x == 0 && nb) nb[op.coef] = (uint8_t)br;
-    if (br == 0) return;
-    for (uint32_t c = threadIdx.x; c < (N >> 1); c += blockDim.x) {
-      const uint32_t i0 = (uint32_t)insert_zero(c, q), i1 = i0 | (1u << q);
-      float2& a0 = tile[phys(i0)];
-      float2& a1 = tile[phys(i1)];
-      const float2 v0 = a0, v1 = a1;
-      if (br == 1) { a0 = v1; a1 = v0; }
-      else if (br == 2) { a0 = make_float2(v1.y, -v1.x); a1 = make_float2(-v0.y, v0.x); }
-      else a1 = make_float2(-v1.x, -v1.y);
-    }
-    return;
+// A noise block holds a run of consecutive stochastic channels (no gate in
+// between) on at most 4 distinct qubits Q of a tile that is the whole state.
+// Channel k's uniform is value k (= op.coef) of the item's seed stream.
+// Every channel branch maps amplitudes as a'_i = c(bin(i)) * a_{i ^ m}, where
+// bin(i) is the index's bits on Q and m flips bits of Q:
+//   X: m = q, c = 1           Y: m = q, c = -i / +i (bit q clear / set)
+//   Z: c = +1 / -1            no jump: c = r / sqrt(1-g) r, r = 1/sqrt(S0 + (1-g) S1)
+//   damping jump: m = q, c = 1/sqrt(S1) / 0      dephasing jump: c = 0 / 1/sqrt(S1)
+// (E1 of damping is [[0, sqrt g], [0, 0]], of dephasing [[0, 0], [0, sqrt l]],
+// each renormalised exactly).  The form is closed under composition
+// (C'(b) = c(b) C(b ^ m), M' = M ^ m), and so is the bin histogram of |a|^2
+// (H'(b) = |c(b)|^2 H(b ^ m)).  So the block takes one histogram sweep (FP32
+// squares summed in FP64; only when a damping or dephasing channel needs
+// P(q=1)), decides every branch in order from the running histogram in FP64
+// (damping / dephasing: jump when u < p1 = g S1 / (S0 + S1); depolarizing:
+// the reference's ranges), and applies the composed map in one sweep
+// (factors rounded to FP32 once).  Q is ascending (bin bit j = qubit Q[j]).
+struct NoiseSmem {
+  double red[8 * 16];  // per-warp bin sums
+  float2 C[16];        // composed factor per bin
+  uint32_t M;          // composed flip mask over the bins (bit j = qubit Q[j])
+  uint32_t identity;   // 1: the composed map is the identity
+};
+
+// Swizzled offsets of the 2^NQ bins: a tile index is base | off(b), with the
+// Q bits of base clear, and phys is linear over GF(2), so
+// phys(base | off(b)) = phys(base) ^ phys(off(b)).
+template <int NQ>
+__device__ __forceinline__ void bin_offsets(const int (&Q)[4], uint32_t (&poff)[1 << NQ]) {
+#pragma unroll
+  for (int b = 0; b < (1 << NQ); ++b) {
+    uint32_t off = 0;
+#pragma unroll
+    for (int j = 0; j < NQ; ++j)
+      if ((b >> j) & 1) off |= 1u << Q[j];
+    poff[b] = phys(off);
   }
-  double s0 = 0.0, s1 = 0.0;
-  for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-    const float2 a = tile[phys(i)];
-    const double p = (double)a.x * a.x + (double)a.y * a.y;
-    if ((i >> q) & 1u) s1 += p; else s0 += p;
+}
+
+// Bin sums of |a|^2 (squares in FP32, sums in FP64; fixed order: per thread,
+// then a warp butterfly) into red[warp * 16 + bin].  Q ascending.
+template <int NQ>
+__device__ __forceinline__ void noise_hist(const float2* tile, uint32_t N, const int (&Q)[4], double* red) {
+  constexpr int NB = 1 << NQ;
+  uint32_t poff[NB];
+  bin_offsets<NQ>(Q, poff);
+  double acc[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) acc[b] = 0.0;
+  for (uint32_t r = threadIdx.x; r < (N >> NQ); r += blockDim.x) {
+    uint32_t base = r;
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) base = (uint32_t)insert_zero(base, Q[j]);
+    const uint32_t pb = phys(base);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const float2 a = tile[pb ^ poff[b]];
+      acc[b] += (double)fmaf(a.x, a.x, __fmul_rn(a.y, a.y));
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  for (int b = 0; b < NB; ++b) {
+    double v = acc[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[(threadIdx.x >> 5) * 16 + b] = v;
   }
-  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if ((threadIdx.x & 31) == 0) { red[w] = s0; red[8 + w] = s1; }
+}
+
+// a'(base | off(b)) = C[b] * a(base | off(b ^ M)) over every base.
+template <int NQ>
+__device__ __forceinline__ void noise_apply(float2* tile, uint32_t N, const int (&Q)[4], const NoiseSmem* sm) {
+  constexpr int NB = 1 << NQ;
+  uint32_t poff[NB];
+  bin_offsets<NQ>(Q, poff);
+  const uint32_t M = sm->M;
+  float2 Cv[NB], Cm[NB];  // C[b] and C[b ^ M]
+#pragma unroll
+  for (int b = 0; b < NB; ++b) { Cv[b] = sm->C[b]; Cm[b] = sm->C[b ^ M]; }
+  for (uint32_t r = threadIdx.x; r < (N >> NQ); r += blockDim.x) {
+    uint32_t base = r;
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) base = (uint32_t)insert_zero(base, Q[j]);
+    const uint32_t pb = phys(base);
+    if (M == 0) {
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        float2& a = tile[pb ^ poff[b]];
+        a = cmul(a, Cv[b]);
+      }
+    } else {
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int b2 = b ^ (int)M;
+        if (b2 < b) continue;
+        float2& ai = tile[pb ^ poff[b]];
+        float2& aj = tile[pb ^ poff[b2]];
+        const float2 vi = ai, vj = aj;
+        ai = cmul(vj, Cv[b]);
+        aj = cmul(vi, Cm[b]);
+      }
+    }
+  }
+}
+
+// Warp 0: the branch of every channel of the block, in order, and the
+// composed map.  Lane b < 2^nq holds bin b (its histogram entry and factor);
+// sums over bins are xor butterflies, so every lane gets the same bits.  A
+// branch's factor c(b) takes one of two values by bit q of the bin (lo for
+// bit clear, hi for bit set).
+__device__ __noinline__ void noise_decide(const DevOp* __restrict__ ops, int ob, int oe, const int (&Q)[4], int nq,
+                                         bool have_h, int nw, uint64_t seed, uint8_t* nb, NoiseSmem* sm) {
+  const int lane = threadIdx.x & 31;
+  const int NB = 1 << nq;
+  const bool mine = lane < NB;
+  double H = 0.0, Cr = 1.0, Ci = 0.0;
+  if (have_h && mine)
+    for (int w = 0; w < nw; ++w) H += sm->red[w * 16 + lane];
+  uint32_t mb = 0;
+  bool ident = true;
+  for (int o = ob; o < oe; ++o) {
+    const DevOp op = ops[o];
+    int j = 0;
+    while (j < nq - 1 && Q[j] != op.t0) ++j;
+    const int bit = 1 << j;
+    const bool set = (lane & bit) != 0;
+    const double g = __longlong_as_double((long long)op.gc);
+    const double u = qs_seed_uniform_at(seed, op.coef);
+    int m = 0;
+    double cr = 1.0, ci = 0.0;
+    if (op.d0 == QS_OP_DEPOLARIZE) {
+      const int br = qs_depol_branch(g, u);
+      if (lane == 0 && nb) nb[op.coef] = (uint8_t)br;
+      if (br == 0) continue;
+      if (br == 1) m = bit;
+      else if (br == 2) { m = bit; cr = 0.0; ci = set ? 1.0 : -1.0; }
+      else cr = set ? -1.0 : 1.0;
+    } else {
+      double s1 = set ? H : 0.0, s0 = set ? 0.0 : H;
+#pragma unroll
+      for (int x = 1; x < 16; x <<= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, x);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, x);
+      }
+      const double S0 = s0, S1 = s1;
+      const double p1 = g * S1 / (S0 + S1);
+      // the kept branch has norm^2 keep; a branch of zero weight is never taken
+      const double keep = S0 + (1.0 - g) * S1;
+      const bool jump = S1 > 0.0 && (u < p1 || !(keep > 0.0));
+      if (lane == 0 && nb) nb[op.coef] = jump ? 1 : 0;
+      if (!jump) {
+        const double r = 1.0 / sqrt(keep);
+        cr = set ? sqrt(1.0 - g) * r : r;
+      } else if (op.d0 == QS_OP_AMP_DAMP) {
+        m = bit;
+        cr = set ? 0.0 : 1.0 / sqrt(S1);
+      } else {
+        cr = set ? 1.0 / sqrt(S1) : 0.0;
+      }
+    }
+    ident = false;
+    // C'(b) = c(b) C(b ^ m), H'(b) = |c(b)|^2 H(b ^ m)
+    const double xr = __shfl_xor_sync(0xffffffffu, Cr, m), xi = __shfl_xor_sync(0xffffffffu, Ci, m);
+    const double xh = __shfl_xor_sync(0xffffffffu, H, m);
+    Cr = cr * xr - ci * xi;
+    Ci = cr * xi + ci * xr;
+    H = (cr * cr + ci * ci) * xh;
+    mb ^= (uint32_t)m;
+  }
+  if (mine) sm->C[lane] = make_float2((float)Cr, (float)Ci);
+  if (lane == 0) {
+    sm->M = mb;
+    sm->identity = ident ? 1u : 0u;
+  }
+}
+
+__device__ __noinline__ void noise_block(float2* tile, int T, const DevBlock blk, const DevOp* __restrict__ ops,
+                                        uint64_t seed, uint8_t* nb, NoiseSmem* sm) {
+  const uint32_t N = 1u << T;
+  const int nq = blk.pos[5];
+  int Q[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) Q[j] = blk.pos[j];
+  bool have_h = false;
+  for (int o = blk.op_begin; o < blk.op_end; ++o) have_h |= ops[o].d0 != QS_OP_DEPOLARIZE;
+  if (have_h) {
+    switch (nq) {
+      case 1: noise_hist<1>(tile, N, Q, sm->red); break;
+      case 2: noise_hist<2>(tile, N, Q, sm->red); break;
+      case 3: noise_hist<3>(tile, N, Q, sm->red); break;
+      default: noise_hist<4>(tile, N, Q, sm->red); break;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 32)
+    noise_decide(ops, blk.op_begin, blk.op_end, Q, nq, have_h, (int)(blockDim.x >> 5), seed, nb, sm);
   __syncthreads();
-  double S0 = 0.0, S1 = 0.0;
-  for (int k = 0; k < nw; ++k) { S0 += red[k]; S1 += red[8 + k]; }
-  const double p1 = g * S1 / (S0 + S1);
-  // the kept branch has norm^2 keep; a branch of zero weight is never taken
-  const double keep = S0 + (1.0 - g) * S1;
-  const bool jump = S1 > 0.0 && (u < p1 || !(keep > 0.0));
-  if (threadIdx.x == 0 && nb) nb[op.coef] = jump ? 1 : 0;
-  if (!jump) {
-    const double r = 1.0 / sqrt(keep);
-    const float f0 = (float)r, f1 = (float)(sqrt(1.0 - g) * r);
-    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-      const float f = ((i >> q) & 1u) ? f1 : f0;
-      float2& a = tile[phys(i)];
-      a = make_float2(a.x * f, a.y * f);
-    }
-  } else {
-    const float f = (float)(1.0 / sqrt(S1));
-    const bool damp = op.d0 == QS_OP_AMP_DAMP;
-    for (uint32_t c = threadIdx.x; c < (N >> 1); c += blockDim.x) {
-      const uint32_t i0 = (uint32_t)insert_zero(c, q), i1 = i0 | (1u << q);
-      float2& a0 = tile[phys(i0)];
-      float2& a1 = tile[phys(i1)];
-      const float2 v1 = make_float2(a1.x * f, a1.y * f);
-      if (damp) { a0 = v1; a1 = make_float2(0.f, 0.f); }
-      else { a0 = make_float2(0.f, 0.f); a1 = v1; }
-    }
+  if (sm->identity) return;
+  switch (nq) {
+    case 1: noise_apply<1>(tile, N, Q, sm); break;
+    case 2: noise_apply<2>(tile, N, Q, sm); break;
+    case 3: noise_apply<3>(tile, N, Q, sm); break;
+    default: noise_apply<4>(tile, N, Q, sm); break;
   }
 }
 
@@ -543,7 +674,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
   uint64_t* dep_lo = reinterpret_cast<uint64_t*>(smem_raw + dep_off_bytes);
   uint64_t* dep_hi = dep_lo + 128;
   int* s_S = reinterpret_cast<int*>(dep_hi + 128);
-  __shared__ double s_red[16];  // noise-block reduction
+  __shared__ NoiseSmem s_noise;  // noise blocks
 
   int cur = -1;
   const DevPass* P = nullptr;
@@ -618,7 +749,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
     for (int b = 0; b < nblocks; ++b) {
       const DevBlock blk = blocks[b];
       if (blk.pos[6]) {  // noise block (only in programs whose tile is the whole state)
-        noise_block(tile, T, ops[blk.op_begin], I.noise_seed, I.noise_branch, s_red);
+        noise_block(tile, T, blk, ops, I.noise_seed, I.noise_branch, &s_noise);
         __syncthreads();
         continue;
       }
@@ -723,8 +854,9 @@ int threads_for(int maxT, int R) {
 
 template <bool TWO>
 void dispatch_two(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
-                  uint64_t total, int maxT, int R, int ncoef) {
-  const int threads = threads_for(maxT, R);
+                  uint64_t total, int maxT, int R, int ncoef, int threads_req) {
+  int threads = threads_for(maxT, R);
+  if (threads_req > 0) threads = std::max(32, std::min(threads, threads_req));
   switch (R) {
     case 1: launch_R<1, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
     case 2: launch_R<2, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
@@ -736,10 +868,11 @@ void dispatch_two(qs_context* h, float2* base, const PassItem& single, const Pas
 }
 
 void dispatch(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
-              uint64_t total, int maxT, int R, int has2, int ncoef) {
+              uint64_t total, int maxT, int R, int has2, int ncoef, int threads_req = 0) {
   QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
-  if (has2) dispatch_two<true>(h, base, single, d_items, nitems, total, maxT, R, ncoef);
-  else dispatch_two<false>(h, base, single, d_items, nitems, total, maxT, R, ncoef);
+  QS_CHECK_ARG(threads_req == 0 || (threads_req % 32) == 0, "threads per CTA must be a multiple of 32");
+  if (has2) dispatch_two<true>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
+  else dispatch_two<false>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
 }
 
 }  // namespace
@@ -760,8 +893,8 @@ void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, in
 // Several (state, pass) items in one launch; d_items is a caller-owned device
 // table whose tile_begin fields hold the prefix sums of ntiles.
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
-                          int maxT, int R, int has2, int ncoef) {
+                          int maxT, int R, int has2, int ncoef, int threads) {
   if (n_items <= 0 || total_tiles == 0) return;
   PassItem dummy{};
-  dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R, has2, ncoef);
+  dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R, has2, ncoef, threads);
 }
