@@ -18,6 +18,7 @@
 #include "qs_api.h"
 #include "qs_common.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 
 using namespace qs;
@@ -469,7 +470,7 @@ __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __rest
 // the reference's ranges), and applies the composed map in one sweep
 // (factors rounded to FP32 once).  Q is ascending (bin bit j = qubit Q[j]).
 struct NoiseSmem {
-  double red[8 * 16];  // per-warp bin sums
+  double red[16 * 16];  // per-warp bin sums (at most 16 warps per CTA)
   float2 C[16];        // composed factor per bin
   uint32_t M;          // composed flip mask over the bins (bit j = qubit Q[j])
   uint32_t identity;   // 1: the composed map is the identity
@@ -662,10 +663,14 @@ __device__ __noinline__ void noise_block(float2* tile, int T, const DevBlock blk
 // SM.  Narrower blocks use 256 threads.
 constexpr int kMaxThreads(int R) { return R == 5 ? 128 : 256; }
 constexpr int kMinBlocks(int R) { return R == 5 ? 2 : 2; }
+// A 2^14-amplitude tile (128 KiB) leaves room for one CTA per SM; those
+// launches use a variant with twice the threads (same register cap per
+// thread) so that the SM still has 8-16 warps to switch between.
+constexpr int kBigThreads(int R) { return 2 * kMaxThreads(R); }
 
 // Dynamic shared memory: [tile 2^maxT float2][coefficient pool][dep tables].
-template <int R, bool TWO>
-__global__ void __launch_bounds__(kMaxThreads(R), kMinBlocks(R))
+template <int R, bool TWO, bool BIG>
+__global__ void __launch_bounds__(BIG ? kBigThreads(R) : kMaxThreads(R), BIG ? 1 : kMinBlocks(R))
 k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restrict__ items, int nitems,
        uint64_t total_tiles, uint32_t coef_off_bytes, uint32_t dep_off_bytes) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -806,7 +811,7 @@ struct LaunchCfg { int per_sm; };
 
 size_t coef_bytes_for(int ncoef) { return (((size_t)ncoef * sizeof(float2)) + 15) & ~size_t(15); }
 
-template <int R, bool TWO>
+template <int R, bool TWO, bool BIG>
 LaunchCfg configure(int smem, int threads) {
   static std::map<std::pair<int, int>, LaunchCfg> cache;
   auto key = std::make_pair(smem, threads);
@@ -817,18 +822,18 @@ LaunchCfg configure(int smem, int threads) {
   // any size stay valid.
   static bool attr_set = false;
   if (!attr_set) {
-    QS_CUDA(cudaFuncSetAttribute(k_pass<R, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
+    QS_CUDA(cudaFuncSetAttribute(k_pass<R, TWO, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
     attr_set = true;
   }
   int per_sm = 0;
-  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R, TWO>, threads, smem));
+  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R, TWO, BIG>, threads, smem));
   if (per_sm < 1) throw qs_error(QS_ERR_CUDA, "tile-pass kernel does not fit on an SM");
   LaunchCfg c{per_sm};
   cache[key] = c;
   return c;
 }
 
-template <int R, bool TWO>
+template <int R, bool TWO, bool BIG>
 void launch_R(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
               uint64_t total, int maxT, int threads, int ncoef) {
   const uint32_t tile_bytes = (uint32_t)(sizeof(float2) << maxT);
@@ -836,12 +841,21 @@ void launch_R(qs_context* h, float2* base, const PassItem& single, const PassIte
   const uint32_t dep_off = coef_off + (uint32_t)coef_bytes_for(ncoef);
   const int smem = (int)(dep_off + 2 * 128 * sizeof(uint64_t) + 16 * sizeof(int));
   QS_CHECK_ARG(smem <= kMaxPassSmem, "tile-pass program too large for shared memory (coefficient pool)");
-  LaunchCfg c = configure<R, TWO>(smem, threads);
+  LaunchCfg c = configure<R, TWO, BIG>(smem, threads);
   uint64_t grid = std::min<uint64_t>(total, (uint64_t)h->sm_count * c.per_sm);
   if (grid == 0) return;
-  k_pass<R, TWO><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total, coef_off,
-                                                               dep_off);
+  k_pass<R, TWO, BIG><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total,
+                                                                    coef_off, dep_off);
   qs_after_launch(h, "k_pass");
+}
+
+// QSIM_BIG_TILES=0 keeps 14-qubit tiles on the default CTA size.
+bool big_tiles_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_BIG_TILES");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 int threads_for(int maxT, int R) {
@@ -856,15 +870,25 @@ template <bool TWO>
 void dispatch_two(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
                   uint64_t total, int maxT, int R, int ncoef, int threads_req) {
   int threads = threads_for(maxT, R);
-  if (threads_req > 0) threads = std::max(32, std::min(threads, threads_req));
+  bool big = false;
+  if (threads_req > 0) {
+    threads = std::max(32, std::min(threads, threads_req));
+  } else if (maxT >= 14 && R >= 2 && (1 << (maxT - R)) >= 2 * threads && big_tiles_enabled()) {
+    threads *= 2;
+    big = true;
+  }
+#define QS_LAUNCH_R(RR)                                                                      \
+  (big ? launch_R<RR, TWO, true>(h, base, single, d_items, nitems, total, maxT, threads, ncoef) \
+       : launch_R<RR, TWO, false>(h, base, single, d_items, nitems, total, maxT, threads, ncoef))
   switch (R) {
-    case 1: launch_R<1, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
-    case 2: launch_R<2, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
-    case 3: launch_R<3, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
-    case 4: launch_R<4, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
-    case 5: launch_R<5, TWO>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 1: launch_R<1, TWO, false>(h, base, single, d_items, nitems, total, maxT, threads, ncoef); break;
+    case 2: QS_LAUNCH_R(2); break;
+    case 3: QS_LAUNCH_R(3); break;
+    case 4: QS_LAUNCH_R(4); break;
+    case 5: QS_LAUNCH_R(5); break;
     default: throw qs_error(QS_ERR_INVALID, "register block width must be 1..5");
   }
+#undef QS_LAUNCH_R
 }
 
 void dispatch(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
