@@ -236,6 +236,16 @@ int qs_measure(qs_handle_t h, void* state, int n_qubits, int target, double u, i
  * u_dev: device float64 [n_shots]; out_dev: device int64 [n_shots].         */
 int qs_sample(qs_handle_t h, const void* state, int n_qubits, const double* u_dev,
               int64_t n_shots, int64_t* out_dev);
+/* Shots from many states of any widths in three launches (no reference
+ * counterpart; the reference samples one state per call).  State t starts at
+ * amplitude state_offsets[t] of `states` and has widths[t] qubits; its
+ * shots[t] shots go to out_dev in state order.  Shot k of state t uses value
+ * k of seeds[t]'s splitmix64 uniform stream (the serving runtime's), drawn on
+ * the device; each state's CDF and search are exactly qs_sample's, so the
+ * shots equal qs_sample's with those uniforms.  widths, state_offsets, shots
+ * and seeds are host arrays.                                                */
+int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int32_t* widths,
+                      const int64_t* state_offsets, const int64_t* shots, const uint64_t* seeds, int64_t* out_dev);
 /* Reference: bwk/csrc/expectation_sm120.cu:45-80,179-202 (expectation_z)    */
 int qs_expect_z(qs_handle_t h, const void* state, int n_qubits, uint64_t z_mask, double* out_host);
 /* Reference: bwk/csrc/expectation_sm120.cu:100-163,204-239 (expectation_pauli),

@@ -7,6 +7,7 @@
 // a fixed strided subset sequentially, then the block reduces in a fixed tree
 // order.  Stage 2 is one block that reduces the per-block partials in order.
 #include "qs_api.h"
+#include <vector>
 #include "qs_common.cuh"
 #include <algorithm>
 #include <cmath>
@@ -181,10 +182,10 @@ __global__ void k_chunk_sums(const float2* __restrict__ s, uint64_t n, uint64_t 
 }
 
 // pass 2: exclusive scan of the chunk sums, one block, fixed order.
-// cbase[c] = sum_{c' < c} csum[c'];  cbase[nchunks] = total.
-__global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
-  __shared__ double ws[32];
-  __shared__ double carry;
+// cbase[c] = sum_{c' < c} csum[c'];  cbase[nchunks] = total.  The order
+// depends only on nchunks and the block size (1024 threads in every launch).
+__device__ __forceinline__ void chunk_scan_block(const double* __restrict__ csum, uint64_t nchunks,
+                                                 double* __restrict__ cbase, double* ws, double& carry) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   // each thread owns a contiguous run of `per` chunks
   const uint64_t per = (nchunks + blockDim.x - 1) / blockDim.x;
@@ -213,54 +214,122 @@ __global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, 
   if (tid == 0) cbase[nchunks] = carry;
 }
 
-// pass 3: one warp per shot.  Shot value u -> smallest i with cdf[i] >= u,
-// clamped to n-1 (reference semantics: sample_sm120.cu:61-68).
+__global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
+  __shared__ double ws[32];
+  __shared__ double carry;
+  chunk_scan_block(csum, nchunks, cbase, ws, carry);
+}
+
+// pass 3, one shot by one warp: u -> smallest i with cdf[i] >= u, clamped to
+// n-1 (reference semantics: sample_sm120.cu:61-68).  Every lane returns it.
+__device__ __forceinline__ int64_t sample_one(const float2* __restrict__ s, uint64_t n, uint64_t nchunks,
+                                              const double* __restrict__ cbase, double x) {
+  const int lane = threadIdx.x & 31;
+  // smallest chunk c with cbase[c+1] >= x
+  uint64_t lo = 0, hi = nchunks;  // search in [0, nchunks)
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (cbase[mid + 1] >= x) hi = mid; else lo = mid + 1;
+  }
+  if (lo >= nchunks) return (int64_t)(n - 1);
+  const uint64_t c = lo;
+  double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
+  double inc = warp_iscan(v);
+  const double base = cbase[c];
+  const bool hit = base + inc >= x;
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  if (m == 0) return (int64_t)min((c + 1) * (uint64_t)kChunk, n) - 1;
+  const int L = __ffs(m) - 1;
+  // lane L walks its segment
+  int64_t r = 0;
+  if (lane == L) {
+    double run = base + (inc - v);
+    const uint64_t st = c * kChunk + (uint64_t)L * kSeg;
+    uint64_t i = st;
+    r = -1;
+    for (int q = 0; q < kSeg; ++q, ++i) {
+      if (i >= n) break;
+      float2 a = s[i];
+      run += (double)a.x * a.x + (double)a.y * a.y;
+      if (run >= x) { r = (int64_t)i; break; }
+    }
+    if (r < 0) r = (int64_t)min(st + kSeg, n) - 1;
+  }
+  return __shfl_sync(0xffffffffu, r, L);
+}
+
 __global__ void k_sample(const float2* __restrict__ s, uint64_t n, uint64_t nchunks, const double* __restrict__ cbase,
                          const double* __restrict__ u, int64_t nshots, int64_t* __restrict__ out) {
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
   for (uint64_t k = warp; k < (uint64_t)nshots; k += nwarps) {
-    const double x = u[k];
-    // smallest chunk c with cbase[c+1] >= x
-    uint64_t lo = 0, hi = nchunks;  // search in [0, nchunks)
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (cbase[mid + 1] >= x) hi = mid; else lo = mid + 1;
-    }
-    int64_t result;
-    if (lo >= nchunks) {
-      result = (int64_t)(n - 1);
-    } else {
-      const uint64_t c = lo;
-      double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
-      double inc = warp_iscan(v);
-      const double base = cbase[c];
-      const bool hit = base + inc >= x;
-      const unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (m == 0) {
-        result = (int64_t)min((c + 1) * (uint64_t)kChunk, n) - 1;
-      } else {
-        const int L = __ffs(m) - 1;
-        // lane L walks its segment
-        int64_t r = 0;
-        if (lane == L) {
-          double run = base + (inc - v);
-          const uint64_t st = c * kChunk + (uint64_t)L * kSeg;
-          uint64_t i = st;
-          r = -1;
-          for (int q = 0; q < kSeg; ++q, ++i) {
-            if (i >= n) break;
-            float2 a = s[i];
-            run += (double)a.x * a.x + (double)a.y * a.y;
-            if (run >= x) { r = (int64_t)i; break; }
-          }
-          if (r < 0) r = (int64_t)min(st + kSeg, n) - 1;
-        }
-        result = __shfl_sync(0xffffffffu, r, L);
-      }
-    }
+    const int64_t result = sample_one(s, n, nchunks, cbase, u[k]);
     if (lane == 0) out[k] = result;
+  }
+}
+
+// ------------------------------------------------- batched sampling ------
+// Many states of any widths in three launches.  Each state's CDF is built and
+// searched exactly as qs_sample does it (same chunking, scan order and
+// search), and shot k of state t uses value k of seeds[t]'s uniform stream,
+// so the shots equal qs_sample's with those uniforms.
+struct SampleDesc {
+  uint64_t state_off;  // first amplitude of the state
+  uint64_t n;          // amplitudes (2^width)
+  uint64_t nchunks;
+  uint64_t chunk_off;  // prefix sum of nchunks
+  uint64_t shot_off;   // prefix sum of shots
+  uint64_t seed;
+};
+
+// last descriptor whose field `off` is <= g (descriptors sorted by it)
+template <uint64_t SampleDesc::*F>
+__device__ __forceinline__ int find_desc(const SampleDesc* __restrict__ d, int ns, uint64_t g) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (d[mid].*F <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_chunk_sums_b(const float2* __restrict__ base, const SampleDesc* __restrict__ d, int ns,
+                               uint64_t total_chunks, double* __restrict__ csum) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (uint64_t g = warp; g < total_chunks; g += nwarps) {
+    const int t = find_desc<&SampleDesc::chunk_off>(d, ns, g);
+    const SampleDesc D = d[t];
+    const uint64_t c = g - D.chunk_off;
+    double v = seg_sum(base + D.state_off, c * kChunk + (uint64_t)lane * kSeg, D.n);
+    v = warp_iscan(v);
+    if (lane == 31) csum[g] = v;
+  }
+}
+
+// one 1024-thread block per state; cbase of state t starts at chunk_off + t
+__global__ void k_chunk_scan_b(const double* __restrict__ csum, const SampleDesc* __restrict__ d,
+                               double* __restrict__ cbase) {
+  __shared__ double ws[32];
+  __shared__ double carry;
+  const SampleDesc D = d[blockIdx.x];
+  if (D.shot_off == d[blockIdx.x + 1].shot_off) return;  // no shots: nothing to scan (block-uniform)
+  chunk_scan_block(csum + D.chunk_off, D.nchunks, cbase + D.chunk_off + blockIdx.x, ws, carry);
+}
+
+__global__ void k_sample_b(const float2* __restrict__ base, const SampleDesc* __restrict__ d, int ns,
+                           uint64_t total_shots, const double* __restrict__ cbase, int64_t* __restrict__ out) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (uint64_t g = warp; g < total_shots; g += nwarps) {
+    const int t = find_desc<&SampleDesc::shot_off>(d, ns, g);
+    const SampleDesc D = d[t];
+    const double x = qs_seed_uniform_at(D.seed, g - D.shot_off);
+    const int64_t result = sample_one(base + D.state_off, D.n, D.nchunks, cbase + D.chunk_off + t, x);
+    if (lane == 0) out[g] = result;
   }
 }
 
@@ -477,6 +546,53 @@ int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n, const u
   k_pauli_apply<<<qs_blocks_for(h, N, kThreads), kThreads, sizeof(Term) * nterms, h->stream>>>(
       (const float2*)psi, (float2*)out, N, dT, nterms);
   qs_after_launch(h, "k_pauli_apply");
+  QS_API_END(h)
+}
+
+int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int32_t* widths,
+                      const int64_t* state_offsets, const int64_t* shots, const uint64_t* seeds, int64_t* out) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(n_states >= 0, "n_states must be >= 0");
+  if (n_states == 0) return QS_OK;
+  QS_CHECK_ARG(states && widths && state_offsets && shots && seeds, "null batch descriptor");
+  QS_CHECK_ARG(((uintptr_t)states & 15u) == 0, "states must be 16-byte aligned");
+  // descriptors, plus one sentinel holding the totals
+  std::vector<SampleDesc> desc(n_states + 1);
+  uint64_t chunks = 0, nshots = 0;
+  for (int t = 0; t < n_states; ++t) {
+    QS_CHECK_ARG(widths[t] >= 1 && widths[t] <= QS_MAX_QUBITS, "state width out of range");
+    QS_CHECK_ARG(state_offsets[t] >= 0 && shots[t] >= 0, "negative offset or shot count");
+    const uint64_t N = 1ull << widths[t];
+    SampleDesc& D = desc[t];
+    D.state_off = (uint64_t)state_offsets[t];
+    D.n = N;
+    D.nchunks = (N + kChunk - 1) / kChunk;
+    D.chunk_off = chunks;
+    D.shot_off = nshots;
+    D.seed = seeds[t];
+    chunks += D.nchunks;
+    nshots += (uint64_t)shots[t];
+  }
+  desc[n_states] = SampleDesc{0, 0, 0, chunks, nshots, 0};
+  if (nshots == 0) return QS_OK;
+  QS_CHECK_ARG(out != nullptr, "out pointer is null");
+  const size_t dbytes = ((desc.size() * sizeof(SampleDesc)) + 255) & ~size_t(255);
+  char* sc = static_cast<char*>(h->scratch_get(dbytes + sizeof(double) * (2 * chunks + n_states)));
+  auto* d_desc = reinterpret_cast<SampleDesc*>(sc);
+  double* csum = reinterpret_cast<double*>(sc + dbytes);
+  double* cbase = csum + chunks;
+  QS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(SampleDesc), cudaMemcpyHostToDevice, h->stream));
+  const int wpb = kThreads / 32;
+  k_chunk_sums_b<<<qs_blocks_for(h, chunks * 32, kThreads), kThreads, 0, h->stream>>>(
+      (const float2*)states, d_desc, n_states, chunks, csum);
+  qs_after_launch(h, "k_chunk_sums_b");
+  k_chunk_scan_b<<<(unsigned)n_states, 1024, 0, h->stream>>>(csum, d_desc, cbase);
+  qs_after_launch(h, "k_chunk_scan_b");
+  const uint64_t blocks = std::min<uint64_t>((nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
+  k_sample_b<<<(unsigned)blocks, kThreads, 0, h->stream>>>((const float2*)states, d_desc, n_states, nshots, cbase,
+                                                           out);
+  qs_after_launch(h, "k_sample_b");
   QS_API_END(h)
 }
 

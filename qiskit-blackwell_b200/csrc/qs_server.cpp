@@ -240,16 +240,17 @@ struct qs_server_s {
     const int64_t total_shots = shot_off[nc];
     std::vector<int64_t> host(total_shots);
     if (total_shots > 0) {
-      std::vector<double> u(total_shots);
-      for (int c = 0; c < nc; ++c) qs_seed_uniforms(item[c]->seed, item[c]->shots, u.data() + shot_off[c]);
-      DevBuf du((size_t)total_shots * 8, s), dout((size_t)total_shots * 8, s);
-      QS_CUDA(cudaMemcpyAsync(du.p, u.data(), (size_t)total_shots * 8, cudaMemcpyHostToDevice, s));
+      // every circuit's shots in one batched sampling call (uniforms drawn on
+      // the device from each request's seed)
+      std::vector<int64_t> shots(nc);
+      std::vector<uint64_t> seeds(nc);
       for (int c = 0; c < nc; ++c) {
-        if (item[c]->shots == 0) continue;
-        check(h, qs_sample(h, static_cast<float2*>(states.p) + st_off[c], widths[c],
-                           static_cast<double*>(du.p) + shot_off[c], item[c]->shots,
-                           static_cast<int64_t*>(dout.p) + shot_off[c]));
+        shots[c] = item[c]->shots;
+        seeds[c] = item[c]->seed;
       }
+      DevBuf dout((size_t)total_shots * 8, s);
+      check(h, qs_sample_batched(h, states.p, nc, widths.data(), st_off.data(), shots.data(), seeds.data(),
+                                 static_cast<int64_t*>(dout.p)));
       QS_CUDA(cudaMemcpyAsync(host.data(), dout.p, (size_t)total_shots * 8, cudaMemcpyDeviceToHost, s));
     }
     check(h, qs_sync(h));  // the plan and buffers outlive the queued work

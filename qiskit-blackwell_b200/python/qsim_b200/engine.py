@@ -259,6 +259,30 @@ def seed_uniforms(seed: int, count: int) -> np.ndarray:
     return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
 
 
+def sample_batched(states: torch.Tensor, widths, offsets, shots, seeds) -> torch.Tensor:
+    """Shots of many states (any widths) packed in one complex64 CUDA tensor,
+    in three launches: state t has widths[t] qubits from amplitude offsets[t]
+    and gets shots[t] shots drawn with seed_uniforms(seeds[t], shots[t]) (the
+    same shots as sample_seeded).  Returns one int64 device tensor, the
+    states' shots in order."""
+    if states.dtype != torch.complex64 or not states.is_cuda or not states.is_contiguous():
+        raise RuntimeError("states must be a contiguous complex64 CUDA tensor")
+    w = np.ascontiguousarray(widths, dtype=np.int32)
+    o = np.ascontiguousarray(offsets, dtype=np.int64)
+    k = np.ascontiguousarray(shots, dtype=np.int64)
+    sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64))
+    if not (w.shape == o.shape == k.shape == sd.shape) or w.ndim != 1:
+        raise ValueError("widths, offsets, shots and seeds need one entry per state")
+    if len(w) and int((o + (np.int64(1) << w.astype(np.int64))).max()) > states.numel():
+        raise ValueError("a state runs past the end of the states tensor")
+    out = torch.empty(int(k.sum()), dtype=torch.int64, device=states.device)
+    _h(states.device.index).call("qs_sample_batched", _ptr(states), int(len(w)),
+                                 w.ctypes.data_as(C.POINTER(C.c_int32)), o.ctypes.data_as(C.POINTER(C.c_int64)),
+                                 k.ctypes.data_as(C.POINTER(C.c_int64)), sd.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                 _ptr(out) if out.numel() else None)
+    return out
+
+
 def sample_seeded(state: torch.Tensor, shots: int, seed: int) -> torch.Tensor:
     """Shots drawn with seed_uniforms(seed, shots) (device tensor)."""
     u = torch.from_numpy(seed_uniforms(seed, shots)).to(state.device, non_blocking=False)

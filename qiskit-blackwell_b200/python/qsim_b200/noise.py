@@ -81,8 +81,15 @@ def run_trajectories(circuit, n_traj: int, seed: int = 0, seeds=None, device: in
 
 
 def sample_trajectories(states: torch.Tensor, shots_per_trajectory: int = 1, seed: int = 0) -> dict:
-    """Counts {hex(index): count} over every trajectory's shots; trajectory t
-    samples with the uniforms of seed + t."""
+    """Counts {hex(index): count} over every trajectory's shots (one batched
+    sampling call; histogrammed on the device); trajectory t samples with
+    the uniforms of seed + t."""
     from blackwell_backend.simulator import counts_from_samples
-    samples = [E.sample_seeded(states[t], int(shots_per_trajectory), int(seed) + t) for t in range(states.shape[0])]
-    return counts_from_samples(torch.cat(samples)) if samples else {}
+    T = int(states.shape[0])
+    if T == 0:
+        return {}
+    n = int(states.shape[1]).bit_length() - 1
+    seeds = np.uint64(int(seed) & (2 ** 64 - 1)) + np.arange(T, dtype=np.uint64)
+    samples = E.sample_batched(states.reshape(-1), np.full(T, n), np.arange(T, dtype=np.int64) << n,
+                               np.full(T, int(shots_per_trajectory)), seeds)
+    return counts_from_samples(samples)
