@@ -8,16 +8,25 @@
 // (2 Re<lam| dU/dtheta |psi_{l-1}> = 2 Re(-i/2 <lam|G U psi_{l-1}>) = Im<lam|G|psi_l>.)
 //
 // The forward pass uses the batch planner (all parameter vectors in one set
-// of tile-pass launches).  The reverse sweep runs one launch per gate over all
-// parameter vectors (grid.y = vector), updates psi and lam in the same pass
-// and accumulates the gradient term in FP64 with fixed-order per-vector
-// reductions (deterministic).  There is no reference counterpart
-// (ROADMAP.md:173-175 lists adjoint differentiation as future work).
+// of tile-pass launches).  The reverse sweep is cut into tile passes too:
+// consecutive (reversed) gates whose targets fit one tile of T qubits (the
+// low qubits plus those the gates touch; controls may lie anywhere) run in one
+// launch over all tiles of all parameter vectors.  A CTA stages the tile of
+// both psi and lam in shared memory, applies every gate's U^dag there and, for
+// each parameter gate, writes its FP64 partial of Im<lam|G|psi> (taken before
+// the gate is undone); a final kernel sums the partials in a fixed order
+// (deterministic).  So psi and lam cross HBM once per pass instead of once per
+// gate.  QSIM_ADJ_PASSES=0 selects the older one-launch-per-gate sweep (kept
+// for comparison; same arithmetic per gate, different summation order).
+// There is no reference counterpart (ROADMAP.md:173-175 lists adjoint
+// differentiation as future work).
 #include "qs_api.h"
 #include "qs_common.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <set>
 
 using namespace qs;
 
@@ -196,6 +205,164 @@ __global__ void k_adj_hpsi(float2* __restrict__ base, uint64_t vstride, uint64_t
   }
 }
 
+// ------------------------------------------------ reverse-sweep passes ----
+enum AdjKind : int32_t { AG_1Q = 1, AG_MCX = 2, AG_PHASE = 3, AG_U2 = 4 };
+
+struct AdjGate {
+  int32_t kind;
+  int32_t p0, p1;     // tile positions of the target(s); U2: p0 = matrix bit 0
+  int32_t gkind;      // 1Q parameter gate generator: 1 X, 2 Y, 3 Z; 0 none
+  int32_t slot;       // partial-sum slot of a parameter gate, else -1
+  int32_t mat;        // 1Q: op index into the per-(op, vector) U^dag table; U2: Mat4 index
+  int32_t neg;        // phase: negate instead of multiplying
+  int32_t pad;
+  uint64_t cmask;     // MCX controls / phase qubits, as a global index mask
+  float2 ph;          // phase factor (already conjugated)
+  float2 pad2;
+};
+
+struct PassArg {
+  int32_t S[16];      // tile positions (global qubits), ascending
+  int32_t T;
+  int32_t gb, ge;     // gate range of the pass
+  int32_t nslots;     // parameter-gate slots of the whole sweep
+};
+
+__device__ __forceinline__ double block_sum_fixed(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+  __syncthreads();
+  return t;  // valid on thread 0
+}
+
+// One reverse-sweep pass: CTA (tile, vector b).  Shared memory: psi tile,
+// lam tile (2^T float2 each), then the 2 x 128 dep tables.
+__global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base, uint64_t vstride, PassArg P,
+                                                      const AdjGate* __restrict__ gates,
+                                                      const Mat2* __restrict__ udag, int nb,
+                                                      const Mat4* __restrict__ u2, double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char adj_smem[];
+  const int T = P.T;
+  const uint32_t NT = 1u << T;
+  float2* sp = reinterpret_cast<float2*>(adj_smem);
+  float2* sl = sp + NT;
+  uint64_t* dep_lo = reinterpret_cast<uint64_t*>(sl + NT);
+  uint64_t* dep_hi = dep_lo + 128;
+  __shared__ double red[kThreads / 32];
+  const int b = blockIdx.y;
+  const uint64_t tile = blockIdx.x, ntiles = gridDim.x;
+  float2* psi = base + (uint64_t)b * vstride;
+  float2* lam = psi + (vstride / 3);
+  for (int e = threadIdx.x; e < 256; e += blockDim.x) {
+    const int part = e >> 7, x = e & 127;
+    uint64_t d = 0;
+    for (int k = 0; k < 7; ++k) {
+      const int kk = part * 7 + k;
+      if (kk < T && ((x >> k) & 1)) d |= 1ull << P.S[kk];
+    }
+    if (part == 0) dep_lo[x] = d; else dep_hi[x] = d;
+  }
+  uint64_t gbase = tile;
+  for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, P.S[k]);
+  __syncthreads();
+  auto gidx = [&](uint32_t i) { return gbase | dep_lo[i & 127] | dep_hi[i >> 7]; };
+  for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
+    const uint64_t g = gidx(i);
+    sp[i] = psi[g];
+    sl[i] = lam[g];
+  }
+  __syncthreads();
+  for (int gi = P.gb; gi < P.ge; ++gi) {
+    const AdjGate G = gates[gi];
+    if (G.kind == AG_1Q) {
+      const Mat2 U = udag[(uint64_t)G.mat * nb + b];
+      const int p = G.p0;
+      double acc = 0.0;
+      for (uint32_t c = threadIdx.x; c < (NT >> 1); c += blockDim.x) {
+        const uint32_t i0 = (uint32_t)insert_zero(c, p), i1 = i0 | (1u << p);
+        const float2 a0 = sp[i0], a1 = sp[i1], l0 = sl[i0], l1 = sl[i1];
+        if (G.gkind) {
+          float2 g0, g1;
+          if (G.gkind == 1) { g0 = a1; g1 = a0; }
+          else if (G.gkind == 2) { g0 = make_float2(a1.y, -a1.x); g1 = make_float2(-a0.y, a0.x); }
+          else { g0 = a0; g1 = make_float2(-a1.x, -a1.y); }
+          acc += (double)l0.x * g0.y - (double)l0.y * g0.x + (double)l1.x * g1.y - (double)l1.y * g1.x;
+        }
+        sp[i0] = cfma2(U.g[0], a0, U.g[1], a1);
+        sp[i1] = cfma2(U.g[2], a0, U.g[3], a1);
+        sl[i0] = cfma2(U.g[0], l0, U.g[1], l1);
+        sl[i1] = cfma2(U.g[2], l0, U.g[3], l1);
+      }
+      if (G.slot >= 0) {
+        const double t = block_sum_fixed(acc, red);
+        if (threadIdx.x == 0) partial[((uint64_t)b * P.nslots + G.slot) * ntiles + tile] = t;
+      }
+    } else if (G.kind == AG_MCX) {
+      const int p = G.p0;
+      for (uint32_t c = threadIdx.x; c < (NT >> 1); c += blockDim.x) {
+        const uint32_t i0 = (uint32_t)insert_zero(c, p), i1 = i0 | (1u << p);
+        if ((gidx(i0) & G.cmask) != G.cmask) continue;
+        const float2 a0 = sp[i0], l0 = sl[i0];
+        sp[i0] = sp[i1];
+        sp[i1] = a0;
+        sl[i0] = sl[i1];
+        sl[i1] = l0;
+      }
+    } else if (G.kind == AG_PHASE) {
+      for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
+        if ((gidx(i) & G.cmask) != G.cmask) continue;
+        const float2 a = sp[i], l = sl[i];
+        if (G.neg) { sp[i] = make_float2(-a.x, -a.y); sl[i] = make_float2(-l.x, -l.y); }
+        else { sp[i] = cmul_comp(a, G.ph); sl[i] = cmul_comp(l, G.ph); }
+      }
+    } else {  // AG_U2
+      const Mat4& U = u2[G.mat];
+      const int lo = min(G.p0, G.p1), hi = max(G.p0, G.p1);
+      const uint32_t s0 = 1u << G.p0, s1 = 1u << G.p1;
+      for (uint32_t c = threadIdx.x; c < (NT >> 2); c += blockDim.x) {
+        const uint32_t i = (uint32_t)insert_zero(insert_zero(c, lo), hi);
+        float2* vs[2] = {sp, sl};
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          float2* x = vs[v];
+          const float2 a0 = x[i], a1 = x[i | s0], a2 = x[i | s1], a3 = x[i | s0 | s1];
+          x[i] = cfma4(U.g + 0, a0, a1, a2, a3);
+          x[i | s0] = cfma4(U.g + 4, a0, a1, a2, a3);
+          x[i | s1] = cfma4(U.g + 8, a0, a1, a2, a3);
+          x[i | s0 | s1] = cfma4(U.g + 12, a0, a1, a2, a3);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
+    const uint64_t g = gidx(i);
+    psi[g] = sp[i];
+    lam[g] = sl[i];
+  }
+}
+
+// grads[b][param_of[s]] += sum over tiles of partial[b][s][tile], slots in
+// order, tiles in order (deterministic).
+__global__ void k_adj_slots(const double* __restrict__ partial, int nslots, uint64_t ntiles,
+                            const int32_t* __restrict__ param_of, double* __restrict__ grads, int nparams) {
+  __shared__ double red[kThreads / 32];
+  const int b = blockIdx.x;
+  for (int sidx = 0; sidx < nslots; ++sidx) {
+    double acc = 0.0;
+    const double* p = partial + ((uint64_t)b * nslots + sidx) * ntiles;
+    for (uint64_t t = threadIdx.x; t < ntiles; t += blockDim.x) acc += p[t];
+    const double t = block_sum_fixed(acc, red);
+    if (threadIdx.x == 0) grads[(uint64_t)b * nparams + param_of[sidx]] += t;
+  }
+}
+
 SortedQ sortedq(std::vector<int> q) {
   std::sort(q.begin(), q.end());
   SortedQ P;
@@ -221,6 +388,17 @@ void mat_1q(const qs_op& o, double theta, cd* m) {
   }
 }
 
+// Reverse-sweep tile width: two staged vectors of 2^12 complex64 = 64 KiB.
+constexpr int kAdjTileBits = 12;
+
+bool adj_passes_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_ADJ_PASSES");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 bool is_1q_kind(int k) {
   return k == QS_OP_RX || k == QS_OP_RY || k == QS_OP_RZ || k == QS_OP_U1 || k == QS_OP_DIAG1 || k == QS_OP_Y;
 }
@@ -233,6 +411,7 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   QS_REQUIRE_HANDLE(h);
   qs_batch_plan_t fwd = nullptr;
   void* dbuf = nullptr;
+  void* pbuf = nullptr;
   QS_API_BEGIN
   qs_check_state(work, n);
   QS_CHECK_ARG(nb >= 1 && nb <= 65535, "n_batch must be in [1, 65535]");
@@ -308,6 +487,130 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   }
 
   // ---- reverse sweep
+  for (int i = 0; i < nops; ++i) {
+    const qs_op& o = ops[i];
+    if (o.param < 0 || !is_1q_kind(o.kind)) continue;
+    QS_CHECK_ARG(o.kind == QS_OP_RX || o.kind == QS_OP_RY || o.kind == QS_OP_RZ,
+                 "only RX/RY/RZ ops may carry a parameter");
+  }
+  // the pass sweep keeps one FP64 partial per (vector, parameter gate, tile);
+  // past 1 GiB of partials the per-gate sweep (partials per block) is used
+  size_t n_param_gates = 0;
+  for (int i = 0; i < nops; ++i) n_param_gates += (ops[i].param >= 0 && is_1q_kind(ops[i].kind)) ? 1 : 0;
+  const bool use_passes = adj_passes_enabled() &&
+      (double)nb * (double)std::max<size_t>(n_param_gates, 1) *
+              std::ldexp(1.0, n - std::min(n, kAdjTileBits)) * sizeof(double) <= (double)(1ull << 30);
+  if (use_passes) {
+    const int T = std::min(n, kAdjTileBits);
+    const int L = std::min(n, 5);  // low qubits always in the tile (coalesced runs)
+    std::vector<AdjGate> gates;
+    std::vector<PassArg> passes;
+    std::vector<int32_t> param_of;
+    std::vector<Mat4> u2s;
+    std::set<int> S;
+    auto reset_S = [&]() { S.clear(); for (int q = 0; q < L; ++q) S.insert(q); };
+    std::vector<std::pair<int, std::vector<int>>> cur;  // (op index, targets)
+    auto close_pass = [&]() {
+      if (cur.empty()) return;
+      for (int q = 0; (int)S.size() < T && q < n; ++q) S.insert(q);  // fill the tile to T qubits
+      PassArg P;
+      std::memset(&P, 0, sizeof(P));
+      P.T = T;
+      int k = 0;
+      int pos[64];
+      for (int q : S) { P.S[k] = q; pos[q] = k; ++k; }
+      P.gb = (int)gates.size();
+      for (auto& e : cur) {
+        const qs_op& o = ops[e.first];
+        AdjGate G;
+        std::memset(&G, 0, sizeof(G));
+        G.slot = -1;
+        if (is_1q_kind(o.kind)) {
+          G.kind = AG_1Q;
+          G.p0 = pos[o.q[0]];
+          G.mat = e.first;
+          if (o.param >= 0) {
+            G.gkind = o.kind == QS_OP_RX ? 1 : o.kind == QS_OP_RY ? 2 : 3;
+            G.slot = (int)param_of.size();
+            param_of.push_back(o.param);
+          }
+        } else if (o.kind == QS_OP_MCX) {
+          G.kind = AG_MCX;
+          G.p0 = pos[o.q[o.nq - 1]];
+          for (int c = 0; c + 1 < o.nq; ++c) G.cmask |= 1ull << o.q[c];
+        } else if (o.kind == QS_OP_MCPHASE) {
+          G.kind = AG_PHASE;
+          for (int c = 0; c < o.nq; ++c) G.cmask |= 1ull << o.q[c];
+          G.neg = (o.m[0] == -1.0 && o.m[1] == 0.0) ? 1 : 0;
+          G.ph = make_float2((float)o.m[0], (float)-o.m[1]);
+        } else {
+          G.kind = AG_U2;
+          G.p0 = pos[o.q[0]];
+          G.p1 = pos[o.q[1]];
+          G.mat = (int)u2s.size();
+          Mat4 U;
+          for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+              U.g[4 * r + c] = make_float2((float)o.m[2 * (4 * c + r)], (float)-o.m[2 * (4 * c + r) + 1]);
+          u2s.push_back(U);
+        }
+        gates.push_back(G);
+      }
+      P.ge = (int)gates.size();
+      passes.push_back(P);
+      cur.clear();
+      reset_S();
+    };
+    reset_S();
+    for (int i = nops - 1; i >= 0; --i) {
+      const qs_op& o = ops[i];
+      std::vector<int> tq;
+      if (is_1q_kind(o.kind)) tq = {o.q[0]};
+      else if (o.kind == QS_OP_MCX) tq = {o.q[o.nq - 1]};
+      else if (o.kind == QS_OP_MCPHASE) tq = {};
+      else if (o.kind == QS_OP_U2) tq = {o.q[0], o.q[1]};
+      else throw qs_error(QS_ERR_INVALID, "op kind not supported by the adjoint sweep");
+      std::set<int> need = S;
+      need.insert(tq.begin(), tq.end());
+      if ((int)need.size() > T) {
+        close_pass();
+        need = S;
+        need.insert(tq.begin(), tq.end());
+      }
+      S = need;
+      cur.emplace_back(i, tq);
+    }
+    close_pass();
+    const int nslots = (int)param_of.size();
+    const uint64_t ntiles = 1ull << (n - T);
+    // device: gates | U2 matrices | slot -> parameter | partials
+    const size_t gbytes = gates.size() * sizeof(AdjGate), ubytes = u2s.size() * sizeof(Mat4);
+    const size_t pbytes = sizeof(int32_t) * std::max(nslots, 1);
+    const size_t parts = (size_t)nb * std::max(nslots, 1) * ntiles;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    QS_CUDA(cudaMalloc(&pbuf, al(gbytes) + al(ubytes) + al(pbytes) + sizeof(double) * parts));
+    char* pc = static_cast<char*>(pbuf);
+    auto* d_gates = reinterpret_cast<AdjGate*>(pc);
+    auto* d_u2 = reinterpret_cast<Mat4*>(pc + al(gbytes));
+    auto* d_param_of = reinterpret_cast<int32_t*>(pc + al(gbytes) + al(ubytes));
+    auto* d_parts = reinterpret_cast<double*>(pc + al(gbytes) + al(ubytes) + al(pbytes));
+    if (gbytes) QS_CUDA(cudaMemcpyAsync(d_gates, gates.data(), gbytes, cudaMemcpyHostToDevice, h->stream));
+    if (ubytes) QS_CUDA(cudaMemcpyAsync(d_u2, u2s.data(), ubytes, cudaMemcpyHostToDevice, h->stream));
+    if (nslots)
+      QS_CUDA(cudaMemcpyAsync(d_param_of, param_of.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
+    const size_t smem = sizeof(float2) * 2 * ((size_t)1 << T) + 2 * 128 * sizeof(uint64_t);
+    QS_CUDA(cudaFuncSetAttribute(k_adj_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (PassArg& P : passes) {
+      P.nslots = nslots;
+      k_adj_pass<<<dim3((unsigned)ntiles, nb), kThreads, smem, h->stream>>>((float2*)work, vstride, P, d_gates,
+                                                                           d_udag, nb, d_u2, d_parts);
+      qs_after_launch(h, "k_adj_pass");
+    }
+    if (nslots) {
+      k_adj_slots<<<nb, kThreads, 0, h->stream>>>(d_parts, nslots, ntiles, d_param_of, d_grads, nparams);
+      qs_after_launch(h, "k_adj_slots");
+    }
+  } else
   for (int i = nops - 1; i >= 0; --i) {
     const qs_op& o = ops[i];
     if (is_1q_kind(o.kind)) {
@@ -358,6 +661,8 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   QS_CUDA(cudaStreamSynchronize(h->stream));
   cudaFree(dbuf);
   dbuf = nullptr;
+  if (pbuf) cudaFree(pbuf);
+  pbuf = nullptr;
   qs_batch_plan_destroy(fwd);
   fwd = nullptr;
   return QS_OK;
@@ -366,6 +671,7 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
     h->err = e.what();
     cudaStreamSynchronize(h->stream);
     if (dbuf) cudaFree(dbuf);
+    if (pbuf) cudaFree(pbuf);
     if (fwd) qs_batch_plan_destroy(fwd);
     return e.code;
   }
@@ -373,6 +679,7 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
     h->err = e.what();
     cudaStreamSynchronize(h->stream);
     if (dbuf) cudaFree(dbuf);
+    if (pbuf) cudaFree(pbuf);
     if (fwd) qs_batch_plan_destroy(fwd);
     return QS_ERR_INVALID;
   }
