@@ -226,6 +226,8 @@ struct PassArg {
   int32_t T;
   int32_t gb, ge;     // gate range of the pass
   int32_t nslots;     // parameter-gate slots of the whole sweep
+  int32_t from_zero;  // forward: the tile starts as |0..0> instead of being loaded
+  int32_t pad[3];
 };
 
 __device__ __forceinline__ double block_sum_fixed(double v, double* red) {
@@ -241,8 +243,15 @@ __device__ __forceinline__ double block_sum_fixed(double v, double* red) {
   return t;  // valid on thread 0
 }
 
-// One reverse-sweep pass: CTA (tile, vector b).  Shared memory: psi tile,
-// lam tile (2^T float2 each), then the 2 x 128 dep tables.
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+// One pass: CTA (tile, vector b).  Reverse (FWD false): psi and lam tiles
+// staged, every gate's U^dag applied to both, parameter-gate partials
+// written.  Forward (FWD true): psi only, every gate's U applied (the
+// conjugate transpose of the stored U^dag), from |0..0> when P.from_zero.
+// Shared memory: psi tile, lam tile (reverse only; 2^T float2 each), then the
+// 2 x 128 dep tables.
+template <bool FWD>
 __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base, uint64_t vstride, PassArg P,
                                                       const AdjGate* __restrict__ gates,
                                                       const Mat2* __restrict__ udag, int nb,
@@ -251,8 +260,8 @@ __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base
   const int T = P.T;
   const uint32_t NT = 1u << T;
   float2* sp = reinterpret_cast<float2*>(adj_smem);
-  float2* sl = sp + NT;
-  uint64_t* dep_lo = reinterpret_cast<uint64_t*>(sl + NT);
+  float2* sl = FWD ? sp : sp + NT;
+  uint64_t* dep_lo = reinterpret_cast<uint64_t*>(sp + (FWD ? NT : 2 * NT));
   uint64_t* dep_hi = dep_lo + 128;
   __shared__ double red[kThreads / 32];
   const int b = blockIdx.y;
@@ -272,21 +281,39 @@ __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base
   for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, P.S[k]);
   __syncthreads();
   auto gidx = [&](uint32_t i) { return gbase | dep_lo[i & 127] | dep_hi[i >> 7]; };
-  for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
-    const uint64_t g = gidx(i);
-    sp[i] = psi[g];
-    sl[i] = lam[g];
+  if (FWD && P.from_zero) {
+    const bool first = gbase == 0;
+    for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) sp[i] = make_float2(first && i == 0 ? 1.f : 0.f, 0.f);
+  } else {
+    for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
+      const uint64_t g = gidx(i);
+      sp[i] = psi[g];
+      if (!FWD) sl[i] = lam[g];
+    }
   }
   __syncthreads();
   for (int gi = P.gb; gi < P.ge; ++gi) {
     const AdjGate G = gates[gi];
     if (G.kind == AG_1Q) {
-      const Mat2 U = udag[(uint64_t)G.mat * nb + b];
+      Mat2 U = udag[(uint64_t)G.mat * nb + b];
+      if (FWD) {
+        const float2 u1 = U.g[1];
+        U.g[0] = conjf2(U.g[0]);
+        U.g[1] = conjf2(U.g[2]);
+        U.g[2] = conjf2(u1);
+        U.g[3] = conjf2(U.g[3]);
+      }
       const int p = G.p0;
       double acc = 0.0;
       for (uint32_t c = threadIdx.x; c < (NT >> 1); c += blockDim.x) {
         const uint32_t i0 = (uint32_t)insert_zero(c, p), i1 = i0 | (1u << p);
-        const float2 a0 = sp[i0], a1 = sp[i1], l0 = sl[i0], l1 = sl[i1];
+        const float2 a0 = sp[i0], a1 = sp[i1];
+        if (FWD) {
+          sp[i0] = cfma2(U.g[0], a0, U.g[1], a1);
+          sp[i1] = cfma2(U.g[2], a0, U.g[3], a1);
+          continue;
+        }
+        const float2 l0 = sl[i0], l1 = sl[i1];
         if (G.gkind) {
           float2 g0, g1;
           if (G.gkind == 1) { g0 = a1; g1 = a0; }
@@ -299,7 +326,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base
         sl[i0] = cfma2(U.g[0], l0, U.g[1], l1);
         sl[i1] = cfma2(U.g[2], l0, U.g[3], l1);
       }
-      if (G.slot >= 0) {
+      if (!FWD && G.slot >= 0) {
         const double t = block_sum_fixed(acc, red);
         if (threadIdx.x == 0) partial[((uint64_t)b * P.nslots + G.slot) * ntiles + tile] = t;
       }
@@ -308,28 +335,42 @@ __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base
       for (uint32_t c = threadIdx.x; c < (NT >> 1); c += blockDim.x) {
         const uint32_t i0 = (uint32_t)insert_zero(c, p), i1 = i0 | (1u << p);
         if ((gidx(i0) & G.cmask) != G.cmask) continue;
-        const float2 a0 = sp[i0], l0 = sl[i0];
+        const float2 a0 = sp[i0];
         sp[i0] = sp[i1];
         sp[i1] = a0;
-        sl[i0] = sl[i1];
-        sl[i1] = l0;
+        if (!FWD) {
+          const float2 l0 = sl[i0];
+          sl[i0] = sl[i1];
+          sl[i1] = l0;
+        }
       }
     } else if (G.kind == AG_PHASE) {
+      const float2 ph = FWD ? conjf2(G.ph) : G.ph;
       for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
         if ((gidx(i) & G.cmask) != G.cmask) continue;
-        const float2 a = sp[i], l = sl[i];
-        if (G.neg) { sp[i] = make_float2(-a.x, -a.y); sl[i] = make_float2(-l.x, -l.y); }
-        else { sp[i] = cmul_comp(a, G.ph); sl[i] = cmul_comp(l, G.ph); }
+        const float2 a = sp[i];
+        sp[i] = G.neg ? make_float2(-a.x, -a.y) : cmul_comp(a, ph);
+        if (!FWD) {
+          const float2 l = sl[i];
+          sl[i] = G.neg ? make_float2(-l.x, -l.y) : cmul_comp(l, ph);
+        }
       }
     } else {  // AG_U2
-      const Mat4& U = u2[G.mat];
+      Mat4 U = u2[G.mat];
+      if (FWD) {
+        const Mat4 D = U;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) U.g[4 * r + c] = conjf2(D.g[4 * c + r]);
+      }
       const int lo = min(G.p0, G.p1), hi = max(G.p0, G.p1);
       const uint32_t s0 = 1u << G.p0, s1 = 1u << G.p1;
       for (uint32_t c = threadIdx.x; c < (NT >> 2); c += blockDim.x) {
         const uint32_t i = (uint32_t)insert_zero(insert_zero(c, lo), hi);
         float2* vs[2] = {sp, sl};
 #pragma unroll
-        for (int v = 0; v < 2; ++v) {
+        for (int v = 0; v < (FWD ? 1 : 2); ++v) {
           float2* x = vs[v];
           const float2 a0 = x[i], a1 = x[i | s0], a2 = x[i | s1], a3 = x[i | s0 | s1];
           x[i] = cfma4(U.g + 0, a0, a1, a2, a3);
@@ -344,7 +385,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_pass(float2* __restrict__ base
   for (uint32_t i = threadIdx.x; i < NT; i += blockDim.x) {
     const uint64_t g = gidx(i);
     psi[g] = sp[i];
-    lam[g] = sl[i];
+    if (!FWD) lam[g] = sl[i];
   }
 }
 
@@ -424,33 +465,31 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   for (int i = 0; i < nops; ++i)
     if (ops[i].param >= nparams) throw qs_error(QS_ERR_INVALID, "op param index out of range");
 
-  // ---- forward: one circuit per vector, params substituted
-  std::vector<qs_op> all((size_t)nops * nb);
-  std::vector<int64_t> ooff(nb + 1), soff(nb);
-  std::vector<int32_t> widths(nb, n);
-  for (int b = 0; b < nb; ++b) {
-    ooff[b] = (int64_t)b * nops;
-    soff[b] = (int64_t)(b * vstride);
-    for (int i = 0; i < nops; ++i) {
-      qs_op o = ops[i];
-      if (o.param >= 0) o.m[0] = params[(size_t)b * nparams + o.param];
-      all[(size_t)b * nops + i] = o;
-    }
+  for (int i = 0; i < nops; ++i) {
+    const qs_op& o = ops[i];
+    if (o.param >= 0 && is_1q_kind(o.kind))
+      QS_CHECK_ARG(o.kind == QS_OP_RX || o.kind == QS_OP_RY || o.kind == QS_OP_RZ,
+                   "only RX/RY/RZ ops may carry a parameter");
+    QS_CHECK_ARG(is_1q_kind(o.kind) || o.kind == QS_OP_MCX || o.kind == QS_OP_MCPHASE || o.kind == QS_OP_U2,
+                 "op kind not supported by the adjoint sweep");
   }
-  ooff[nb] = (int64_t)nops * nb;
-  int rc = qs_batch_plan_create(h, nb, widths.data(), ooff.data(), all.data(), soff.data(), &fwd);
-  if (rc != QS_OK) throw qs_error(rc, h->err);
-  rc = qs_batch_plan_execute(h, fwd, work);
-  if (rc != QS_OK) throw qs_error(rc, h->err);
+  // The pass sweeps keep one FP64 partial per (vector, parameter gate, tile);
+  // past 1 GiB of partials the per-gate sweep (partials per block) is used.
+  size_t n_param_gates = 0;
+  for (int i = 0; i < nops; ++i) n_param_gates += (ops[i].param >= 0 && is_1q_kind(ops[i].kind)) ? 1 : 0;
+  const int T = std::min(n, kAdjTileBits);
+  const uint64_t ntiles = 1ull << (n - T);
+  const bool use_passes = adj_passes_enabled() &&
+      (double)nb * (double)std::max<size_t>(n_param_gates, 1) * (double)ntiles * sizeof(double) <=
+          (double)(1ull << 30);
 
-  // ---- lam = H psi, E = Re<psi|lam>
   // device buffer: grads [nb][nparams] | energies [nb] | partial [nb][256] | U^dag tables
   const size_t ng = (size_t)nb * std::max(nparams, 1);
   const Slice sl = slice(N / 2);
   const Slice sd = slice(N);
   const int nbx = std::max(sl.nbx, sd.nbx);
   size_t bytes = sizeof(double) * (ng + nb + (size_t)nb * nbx) + sizeof(Mat2) * (size_t)nb * nops + 64;
-  QS_CUDA(cudaMalloc(&dbuf, bytes));
+  QS_CUDA(cudaMallocAsync(&dbuf, bytes, h->stream));
   double* d_grads = (double*)dbuf;
   double* d_energy = d_grads + ng;
   double* d_part = d_energy + nb;
@@ -475,6 +514,151 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   }
   QS_CUDA(cudaMemcpyAsync(d_udag, udag.data(), sizeof(Mat2) * udag.size(), cudaMemcpyHostToDevice, h->stream));
 
+  // ---- tile passes (forward order and reverse order)
+  std::vector<AdjGate> gates;
+  std::vector<PassArg> fpasses, rpasses;
+  std::vector<int32_t> param_of;
+  std::vector<Mat4> u2s;
+  AdjGate* d_gates = nullptr;
+  Mat4* d_u2 = nullptr;
+  int32_t* d_param_of = nullptr;
+  double* d_parts = nullptr;
+  size_t pass_smem[2] = {0, 0};
+  if (use_passes) {
+    const int L = std::min(n, 5);  // low qubits always in the tile (coalesced runs)
+    // Greedy cut of an op sequence into passes: a pass takes ops in order
+    // while their targets fit in T tile qubits.
+    auto build = [&](const std::vector<int>& order, bool reverse, std::vector<PassArg>& out) {
+      std::set<int> S;
+      std::vector<int> cur;
+      auto reset_S = [&]() { S.clear(); for (int q = 0; q < L; ++q) S.insert(q); };
+      auto close_pass = [&]() {
+        if (cur.empty()) return;
+        for (int q = 0; (int)S.size() < T && q < n; ++q) S.insert(q);  // fill the tile to T qubits
+        PassArg P;
+        std::memset(&P, 0, sizeof(P));
+        P.T = T;
+        int k = 0, pos[64];
+        for (int q : S) { P.S[k] = q; pos[q] = k; ++k; }
+        P.gb = (int)gates.size();
+        for (int i : cur) {
+          const qs_op& o = ops[i];
+          AdjGate G;
+          std::memset(&G, 0, sizeof(G));
+          G.slot = -1;
+          if (is_1q_kind(o.kind)) {
+            G.kind = AG_1Q;
+            G.p0 = pos[o.q[0]];
+            G.mat = i;
+            if (reverse && o.param >= 0) {
+              G.gkind = o.kind == QS_OP_RX ? 1 : o.kind == QS_OP_RY ? 2 : 3;
+              G.slot = (int)param_of.size();
+              param_of.push_back(o.param);
+            }
+          } else if (o.kind == QS_OP_MCX) {
+            G.kind = AG_MCX;
+            G.p0 = pos[o.q[o.nq - 1]];
+            for (int c = 0; c + 1 < o.nq; ++c) G.cmask |= 1ull << o.q[c];
+          } else if (o.kind == QS_OP_MCPHASE) {
+            G.kind = AG_PHASE;
+            for (int c = 0; c < o.nq; ++c) G.cmask |= 1ull << o.q[c];
+            G.neg = (o.m[0] == -1.0 && o.m[1] == 0.0) ? 1 : 0;
+            G.ph = make_float2((float)o.m[0], (float)-o.m[1]);
+          } else {
+            G.kind = AG_U2;
+            G.p0 = pos[o.q[0]];
+            G.p1 = pos[o.q[1]];
+            G.mat = (int)u2s.size();
+            Mat4 U;  // U^dag; the forward kernel transposes it back
+            for (int r = 0; r < 4; ++r)
+              for (int c = 0; c < 4; ++c)
+                U.g[4 * r + c] = make_float2((float)o.m[2 * (4 * c + r)], (float)-o.m[2 * (4 * c + r) + 1]);
+            u2s.push_back(U);
+          }
+          gates.push_back(G);
+        }
+        P.ge = (int)gates.size();
+        out.push_back(P);
+        cur.clear();
+        reset_S();
+      };
+      reset_S();
+      for (int i : order) {
+        const qs_op& o = ops[i];
+        std::vector<int> tq;
+        if (is_1q_kind(o.kind)) tq = {o.q[0]};
+        else if (o.kind == QS_OP_MCX) tq = {o.q[o.nq - 1]};
+        else if (o.kind == QS_OP_U2) tq = {o.q[0], o.q[1]};
+        std::set<int> need = S;
+        need.insert(tq.begin(), tq.end());
+        if ((int)need.size() > T) {
+          close_pass();
+          need = S;
+          need.insert(tq.begin(), tq.end());
+        }
+        S = need;
+        cur.push_back(i);
+      }
+      close_pass();
+    };
+    std::vector<int> order(nops);
+    for (int i = 0; i < nops; ++i) order[i] = i;
+    build(order, false, fpasses);
+    std::reverse(order.begin(), order.end());
+    build(order, true, rpasses);
+    if (!fpasses.empty()) fpasses[0].from_zero = 1;
+    const int nslots = (int)param_of.size();
+    for (auto& P : rpasses) P.nslots = nslots;
+    // device: gates | U2 matrices | slot -> parameter | partials
+    const size_t gbytes = gates.size() * sizeof(AdjGate), ubytes = u2s.size() * sizeof(Mat4);
+    const size_t pbytes = sizeof(int32_t) * std::max(nslots, 1);
+    const size_t parts = (size_t)nb * std::max(nslots, 1) * ntiles;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    QS_CUDA(cudaMallocAsync(&pbuf, al(gbytes) + al(ubytes) + al(pbytes) + sizeof(double) * parts, h->stream));
+    char* pc = static_cast<char*>(pbuf);
+    d_gates = reinterpret_cast<AdjGate*>(pc);
+    d_u2 = reinterpret_cast<Mat4*>(pc + al(gbytes));
+    d_param_of = reinterpret_cast<int32_t*>(pc + al(gbytes) + al(ubytes));
+    d_parts = reinterpret_cast<double*>(pc + al(gbytes) + al(ubytes) + al(pbytes));
+    if (gbytes) QS_CUDA(cudaMemcpyAsync(d_gates, gates.data(), gbytes, cudaMemcpyHostToDevice, h->stream));
+    if (ubytes) QS_CUDA(cudaMemcpyAsync(d_u2, u2s.data(), ubytes, cudaMemcpyHostToDevice, h->stream));
+    if (nslots)
+      QS_CUDA(cudaMemcpyAsync(d_param_of, param_of.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
+    pass_smem[0] = sizeof(float2) * ((size_t)1 << T) + 2 * 128 * sizeof(uint64_t);  // forward
+    pass_smem[1] = sizeof(float2) * 2 * ((size_t)1 << T) + 2 * 128 * sizeof(uint64_t);
+    QS_CUDA(cudaFuncSetAttribute(k_adj_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem[0]));
+    QS_CUDA(cudaFuncSetAttribute(k_adj_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem[1]));
+  }
+
+  // ---- forward
+  if (use_passes) {
+    for (const PassArg& P : fpasses) {
+      k_adj_pass<true><<<dim3((unsigned)ntiles, nb), kThreads, pass_smem[0], h->stream>>>(
+          (float2*)work, vstride, P, d_gates, d_udag, nb, d_u2, nullptr);
+      qs_after_launch(h, "k_adj_pass");
+    }
+  } else {
+    // one circuit per vector, params substituted, through the batch planner
+    std::vector<qs_op> all((size_t)nops * nb);
+    std::vector<int64_t> ooff(nb + 1), soff(nb);
+    std::vector<int32_t> widths(nb, n);
+    for (int b = 0; b < nb; ++b) {
+      ooff[b] = (int64_t)b * nops;
+      soff[b] = (int64_t)(b * vstride);
+      for (int i = 0; i < nops; ++i) {
+        qs_op o = ops[i];
+        if (o.param >= 0) o.m[0] = params[(size_t)b * nparams + o.param];
+        all[(size_t)b * nops + i] = o;
+      }
+    }
+    ooff[nb] = (int64_t)nops * nb;
+    int rc = qs_batch_plan_create(h, nb, widths.data(), ooff.data(), all.data(), soff.data(), &fwd);
+    if (rc != QS_OK) throw qs_error(rc, h->err);
+    rc = qs_batch_plan_execute(h, fwd, work);
+    if (rc != QS_OK) throw qs_error(rc, h->err);
+  }
+
+  // ---- lam = H psi, E = Re<psi|lam>
   TermL* dT = (TermL*)qs_upload_terms(h, 0, n, xm, zm, coefs, nterms);
   {
     dim3 grid((unsigned)std::min<uint64_t>((N + kThreads - 1) / kThreads, 64), nb);
@@ -487,127 +671,15 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   }
 
   // ---- reverse sweep
-  for (int i = 0; i < nops; ++i) {
-    const qs_op& o = ops[i];
-    if (o.param < 0 || !is_1q_kind(o.kind)) continue;
-    QS_CHECK_ARG(o.kind == QS_OP_RX || o.kind == QS_OP_RY || o.kind == QS_OP_RZ,
-                 "only RX/RY/RZ ops may carry a parameter");
-  }
-  // the pass sweep keeps one FP64 partial per (vector, parameter gate, tile);
-  // past 1 GiB of partials the per-gate sweep (partials per block) is used
-  size_t n_param_gates = 0;
-  for (int i = 0; i < nops; ++i) n_param_gates += (ops[i].param >= 0 && is_1q_kind(ops[i].kind)) ? 1 : 0;
-  const bool use_passes = adj_passes_enabled() &&
-      (double)nb * (double)std::max<size_t>(n_param_gates, 1) *
-              std::ldexp(1.0, n - std::min(n, kAdjTileBits)) * sizeof(double) <= (double)(1ull << 30);
   if (use_passes) {
-    const int T = std::min(n, kAdjTileBits);
-    const int L = std::min(n, 5);  // low qubits always in the tile (coalesced runs)
-    std::vector<AdjGate> gates;
-    std::vector<PassArg> passes;
-    std::vector<int32_t> param_of;
-    std::vector<Mat4> u2s;
-    std::set<int> S;
-    auto reset_S = [&]() { S.clear(); for (int q = 0; q < L; ++q) S.insert(q); };
-    std::vector<std::pair<int, std::vector<int>>> cur;  // (op index, targets)
-    auto close_pass = [&]() {
-      if (cur.empty()) return;
-      for (int q = 0; (int)S.size() < T && q < n; ++q) S.insert(q);  // fill the tile to T qubits
-      PassArg P;
-      std::memset(&P, 0, sizeof(P));
-      P.T = T;
-      int k = 0;
-      int pos[64];
-      for (int q : S) { P.S[k] = q; pos[q] = k; ++k; }
-      P.gb = (int)gates.size();
-      for (auto& e : cur) {
-        const qs_op& o = ops[e.first];
-        AdjGate G;
-        std::memset(&G, 0, sizeof(G));
-        G.slot = -1;
-        if (is_1q_kind(o.kind)) {
-          G.kind = AG_1Q;
-          G.p0 = pos[o.q[0]];
-          G.mat = e.first;
-          if (o.param >= 0) {
-            G.gkind = o.kind == QS_OP_RX ? 1 : o.kind == QS_OP_RY ? 2 : 3;
-            G.slot = (int)param_of.size();
-            param_of.push_back(o.param);
-          }
-        } else if (o.kind == QS_OP_MCX) {
-          G.kind = AG_MCX;
-          G.p0 = pos[o.q[o.nq - 1]];
-          for (int c = 0; c + 1 < o.nq; ++c) G.cmask |= 1ull << o.q[c];
-        } else if (o.kind == QS_OP_MCPHASE) {
-          G.kind = AG_PHASE;
-          for (int c = 0; c < o.nq; ++c) G.cmask |= 1ull << o.q[c];
-          G.neg = (o.m[0] == -1.0 && o.m[1] == 0.0) ? 1 : 0;
-          G.ph = make_float2((float)o.m[0], (float)-o.m[1]);
-        } else {
-          G.kind = AG_U2;
-          G.p0 = pos[o.q[0]];
-          G.p1 = pos[o.q[1]];
-          G.mat = (int)u2s.size();
-          Mat4 U;
-          for (int r = 0; r < 4; ++r)
-            for (int c = 0; c < 4; ++c)
-              U.g[4 * r + c] = make_float2((float)o.m[2 * (4 * c + r)], (float)-o.m[2 * (4 * c + r) + 1]);
-          u2s.push_back(U);
-        }
-        gates.push_back(G);
-      }
-      P.ge = (int)gates.size();
-      passes.push_back(P);
-      cur.clear();
-      reset_S();
-    };
-    reset_S();
-    for (int i = nops - 1; i >= 0; --i) {
-      const qs_op& o = ops[i];
-      std::vector<int> tq;
-      if (is_1q_kind(o.kind)) tq = {o.q[0]};
-      else if (o.kind == QS_OP_MCX) tq = {o.q[o.nq - 1]};
-      else if (o.kind == QS_OP_MCPHASE) tq = {};
-      else if (o.kind == QS_OP_U2) tq = {o.q[0], o.q[1]};
-      else throw qs_error(QS_ERR_INVALID, "op kind not supported by the adjoint sweep");
-      std::set<int> need = S;
-      need.insert(tq.begin(), tq.end());
-      if ((int)need.size() > T) {
-        close_pass();
-        need = S;
-        need.insert(tq.begin(), tq.end());
-      }
-      S = need;
-      cur.emplace_back(i, tq);
-    }
-    close_pass();
-    const int nslots = (int)param_of.size();
-    const uint64_t ntiles = 1ull << (n - T);
-    // device: gates | U2 matrices | slot -> parameter | partials
-    const size_t gbytes = gates.size() * sizeof(AdjGate), ubytes = u2s.size() * sizeof(Mat4);
-    const size_t pbytes = sizeof(int32_t) * std::max(nslots, 1);
-    const size_t parts = (size_t)nb * std::max(nslots, 1) * ntiles;
-    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    QS_CUDA(cudaMalloc(&pbuf, al(gbytes) + al(ubytes) + al(pbytes) + sizeof(double) * parts));
-    char* pc = static_cast<char*>(pbuf);
-    auto* d_gates = reinterpret_cast<AdjGate*>(pc);
-    auto* d_u2 = reinterpret_cast<Mat4*>(pc + al(gbytes));
-    auto* d_param_of = reinterpret_cast<int32_t*>(pc + al(gbytes) + al(ubytes));
-    auto* d_parts = reinterpret_cast<double*>(pc + al(gbytes) + al(ubytes) + al(pbytes));
-    if (gbytes) QS_CUDA(cudaMemcpyAsync(d_gates, gates.data(), gbytes, cudaMemcpyHostToDevice, h->stream));
-    if (ubytes) QS_CUDA(cudaMemcpyAsync(d_u2, u2s.data(), ubytes, cudaMemcpyHostToDevice, h->stream));
-    if (nslots)
-      QS_CUDA(cudaMemcpyAsync(d_param_of, param_of.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
-    const size_t smem = sizeof(float2) * 2 * ((size_t)1 << T) + 2 * 128 * sizeof(uint64_t);
-    QS_CUDA(cudaFuncSetAttribute(k_adj_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    for (PassArg& P : passes) {
-      P.nslots = nslots;
-      k_adj_pass<<<dim3((unsigned)ntiles, nb), kThreads, smem, h->stream>>>((float2*)work, vstride, P, d_gates,
-                                                                           d_udag, nb, d_u2, d_parts);
+    for (const PassArg& P : rpasses) {
+      k_adj_pass<false><<<dim3((unsigned)ntiles, nb), kThreads, pass_smem[1], h->stream>>>(
+          (float2*)work, vstride, P, d_gates, d_udag, nb, d_u2, d_parts);
       qs_after_launch(h, "k_adj_pass");
     }
-    if (nslots) {
-      k_adj_slots<<<nb, kThreads, 0, h->stream>>>(d_parts, nslots, ntiles, d_param_of, d_grads, nparams);
+    if (!param_of.empty()) {
+      k_adj_slots<<<nb, kThreads, 0, h->stream>>>(d_parts, (int)param_of.size(), ntiles, d_param_of, d_grads,
+                                                  nparams);
       qs_after_launch(h, "k_adj_slots");
     }
   } else
@@ -658,11 +730,11 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   }
   QS_CUDA(cudaMemcpyAsync(grads, d_grads, sizeof(double) * (size_t)nb * nparams, cudaMemcpyDeviceToHost, h->stream));
   QS_CUDA(cudaMemcpyAsync(energies, d_energy, sizeof(double) * nb, cudaMemcpyDeviceToHost, h->stream));
-  QS_CUDA(cudaStreamSynchronize(h->stream));
-  cudaFree(dbuf);
+  QS_CUDA(cudaFreeAsync(dbuf, h->stream));
   dbuf = nullptr;
-  if (pbuf) cudaFree(pbuf);
+  if (pbuf) QS_CUDA(cudaFreeAsync(pbuf, h->stream));
   pbuf = nullptr;
+  QS_CUDA(cudaStreamSynchronize(h->stream));
   qs_batch_plan_destroy(fwd);
   fwd = nullptr;
   return QS_OK;
@@ -670,16 +742,16 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
   catch (const qs_error& e) {
     h->err = e.what();
     cudaStreamSynchronize(h->stream);
-    if (dbuf) cudaFree(dbuf);
-    if (pbuf) cudaFree(pbuf);
+    if (dbuf) cudaFreeAsync(dbuf, h->stream);
+    if (pbuf) cudaFreeAsync(pbuf, h->stream);
     if (fwd) qs_batch_plan_destroy(fwd);
     return e.code;
   }
   catch (const std::exception& e) {
     h->err = e.what();
     cudaStreamSynchronize(h->stream);
-    if (dbuf) cudaFree(dbuf);
-    if (pbuf) cudaFree(pbuf);
+    if (dbuf) cudaFreeAsync(dbuf, h->stream);
+    if (pbuf) cudaFreeAsync(pbuf, h->stream);
     if (fwd) qs_batch_plan_destroy(fwd);
     return QS_ERR_INVALID;
   }
