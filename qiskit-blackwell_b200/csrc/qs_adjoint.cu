@@ -531,9 +531,12 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
     auto build = [&](const std::vector<int>& order, bool reverse, std::vector<PassArg>& out) {
       std::set<int> S;
       std::vector<int> cur;
-      auto reset_S = [&]() { S.clear(); for (int q = 0; q < L; ++q) S.insert(q); };
+      auto reset_S = [&]() {
+        S.clear();
+        for (int q = 0; q < (T == n ? n : L); ++q) S.insert(q);
+      };
       auto close_pass = [&]() {
-        if (cur.empty()) return;
+        if (cur.empty()) { reset_S(); return; }
         for (int q = 0; (int)S.size() < T && q < n; ++q) S.insert(q);  // fill the tile to T qubits
         PassArg P;
         std::memset(&P, 0, sizeof(P));
@@ -582,22 +585,62 @@ extern "C" int qs_adjoint_gradient(qs_handle_t h, int n, const qs_op* ops, int n
         cur.clear();
         reset_S();
       };
+      // List scheduling: an op is ready when it is the next op of the order
+      // on every qubit it touches (ops on disjoint qubits commute, and so do
+      // their contributions to the gradient); a pass keeps taking ready ops
+      // whose targets are in its tile, and adds the targets of the earliest
+      // ready op to the tile while room is left.
+      const int m = (int)order.size();
+      std::vector<std::vector<int>> touch(m), targ(m);
+      std::vector<std::vector<int>> per_q(n);  // positions in `order` touching each qubit
+      for (int k = 0; k < m; ++k) {
+        const qs_op& o = ops[order[k]];
+        if (is_1q_kind(o.kind)) targ[k] = {o.q[0]};
+        else if (o.kind == QS_OP_MCX) targ[k] = {o.q[o.nq - 1]};
+        else if (o.kind == QS_OP_U2) targ[k] = {o.q[0], o.q[1]};
+        touch[k].assign(o.q, o.q + o.nq);
+        for (int q : touch[k]) per_q[q].push_back(k);
+      }
+      std::vector<size_t> head(n, 0);  // next unscheduled position per qubit
+      std::vector<char> done(m, 0);
+      auto ready = [&](int k) {
+        for (int q : touch[k])
+          if (per_q[q][head[q]] != k) return false;
+        return true;
+      };
+      auto fits = [&](int k) {
+        for (int q : targ[k])
+          if (!S.count(q)) return false;
+        return true;
+      };
+      int remaining = m, first = 0;
       reset_S();
-      for (int i : order) {
-        const qs_op& o = ops[i];
-        std::vector<int> tq;
-        if (is_1q_kind(o.kind)) tq = {o.q[0]};
-        else if (o.kind == QS_OP_MCX) tq = {o.q[o.nq - 1]};
-        else if (o.kind == QS_OP_U2) tq = {o.q[0], o.q[1]};
-        std::set<int> need = S;
-        need.insert(tq.begin(), tq.end());
-        if ((int)need.size() > T) {
-          close_pass();
-          need = S;
-          need.insert(tq.begin(), tq.end());
+      while (remaining > 0) {
+        bool progress = true;
+        while (progress) {
+          progress = false;
+          for (int k = first; k < m; ++k) {
+            if (done[k] || !ready(k) || !fits(k)) continue;
+            done[k] = 1;
+            --remaining;
+            for (int q : touch[k]) ++head[q];
+            cur.push_back(order[k]);
+            progress = true;
+          }
+          while (first < m && done[first]) ++first;
         }
-        S = need;
-        cur.push_back(i);
+        if (remaining == 0) break;
+        // widen the tile with the earliest ready op's targets, or close the pass
+        int pick = -1;
+        for (int k = first; k < m && pick < 0; ++k)
+          if (!done[k] && ready(k)) pick = k;
+        std::set<int> need = S;
+        need.insert(targ[pick].begin(), targ[pick].end());
+        if ((int)need.size() <= T) {
+          S = need;
+        } else {
+          close_pass();
+        }
       }
       close_pass();
     };
