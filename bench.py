@@ -733,8 +733,103 @@ def bench_noisy(args, dev):
             "clocks": clk.summary(), "gpu_launches": int(launches)}, {"unit": "trajectories/s"}
 
 
+# The reference's published single-kernel times at 20 qubits and its QV-20
+# end-to-end time (RTX 5090; README.md:152,160-167 of the reference).
+REF_MICRO_US = {"apply_gate": 4.2, "apply_gate_2q": 6.2, "apply_diagonal": 4.1, "apply_diagonal_phase": 2.1,
+                "apply_mcgate": 5.0, "measure_qubit": 24.7, "sample_1000": 20.5, "apply_gates_fused_10": 10.3}
+REF_QV20_E2E_MS = 126.0
+
+
+def bench_micro(args, dev):
+    """The operations the reference publishes times for, at 20 qubits (an
+    8 MiB state, L2-resident as in the reference's table), through the
+    blackwell_kernels API with the gates as CUDA tensors: device time per
+    call (CUDA events over --circuits calls, default 200, after warm-up).
+    value = QV-20 (depth 20, seed 20) end to end with 8192 shots through
+    BlackwellSimulator.run (plan cached after the first call), circuits/s."""
+    import numpy as np
+    import torch
+    import blackwell_kernels as bk
+    from blackwell_backend import BlackwellSimulator
+    from qsim_b200 import workloads as W
+    from qsim_b200.circuit import Circuit
+    n = 20
+    reps = args.circuits if args.circuits != 4096 else 200
+    state = bk.state_init(n)
+    bk.apply_gate(state, bk.hadamard_gate(), 0)
+    stream = torch.cuda.current_stream(dev)
+    H, U2, D = bk.hadamard_gate(), bk.random_unitary_4x4(), bk.rz_gate_diag(0.3)
+    X = bk.pauli_x_gate()
+    gates10 = torch.stack([bk.random_unitary() for _ in range(10)])
+    targets10 = torch.arange(10, dtype=torch.int32, device=f"cuda:{dev}") * 2
+    ops = {
+        "apply_gate": lambda k: bk.apply_gate(state, H, 7 + (k & 1)),
+        "apply_gate_2q": lambda k: bk.apply_gate_2q(state, U2, 3, 11),
+        "apply_diagonal": lambda k: bk.apply_diagonal(state, D, 9),
+        "apply_diagonal_phase": lambda k: bk.apply_diagonal_phase(state, complex(0.6, 0.8), 9),
+        "apply_mcgate": lambda k: bk.apply_mcgate(state, X, [2, 5], 14),
+        "measure_qubit": lambda k: bk.measure_qubit(bk.apply_gate(state, H, 4), 4, 0.5),
+        "sample_1000": lambda k: bk.sample(state, 1000),
+        "apply_gates_fused_10": lambda k: bk.apply_gates_fused(state, gates10, targets10),
+    }
+    out = {}
+    for name, fn in ops.items():
+        for k in range(5):
+            fn(k)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(reps):
+            fn(k)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        us = ev0.elapsed_time(ev1) * 1e3 / reps
+        if name == "measure_qubit":
+            us -= out["apply_gate"]["b200_us"]  # each call re-mixes qubit 4 with one H first
+        out[name] = {"b200_us": us, "reference_rtx5090_us": REF_MICRO_US[name]}
+    # QV-20 end to end
+    qv = W.qv_ops(n, n, 20)
+    qc = Circuit(n, n, name="qv20")
+    for r in qv:
+        m = (np.asarray(r["m"][:32]).reshape(16, 2) @ np.array([1, 1j])).reshape(4, 4)
+        qc.unitary(m, [int(r["q"][0]), int(r["q"][1])])
+    for q in range(n):
+        qc.measure(q, q)
+    sim = BlackwellSimulator(device=f"cuda:{dev}")
+    for _ in range(max(1, args.warmup)):
+        sim.run(qc, shots=8192, seed=1)
+    times = []
+    l0 = E_launches(dev)
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = sim.run(qc, shots=8192, seed=k)
+            _ = res.get_counts()
+            times.append(time.perf_counter() - t0)
+    launches = E_launches(dev) - l0
+    t = reduce_max(float(np.median(times)), f"cuda:{dev}")
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"metric": METRIC, "value": ws / t, "unit": "circuits/s", "ms_per_step": t * 1e3,
+            "dtype": "c64 (fp32; compensated 1Q/2Q kernels), fp64 reductions",
+            "config": {"workload": "micro: 20-qubit kernels through blackwell_kernels (CUDA-tensor gates), and "
+                                   "QV-20 (depth 20, seed 20) with 8192 shots through BlackwellSimulator.run",
+                       "l2": "8 MiB state, L2-resident (as the reference's table)"},
+            "kernels": out,
+            "qv20_e2e": {"b200_ms": t * 1e3, "reference_rtx5090_ms": REF_QV20_E2E_MS},
+            "e2e": {"value": ws / t, "unit": "circuits/s", "h2d_bytes_per_step": int(qv.nbytes),
+                    "d2h_bytes_per_step": 8192 * 8,
+                    "note": "host circuit in, counts out (histogram on the device)"},
+            "clocks": clk.summary(), "gpu_launches": int(launches)}, {"unit": "circuits/s"}
+
+
+def E_launches(dev):
+    from qsim_b200 import engine as E
+    return int(E._h(dev).L.qs_launch_count(None))
+
+
 WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
-             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy}
+             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy, "micro": bench_micro}
 
 
 # --------------------------------------------------------- CPU baseline
@@ -759,6 +854,16 @@ def cpu_baseline(workload: str, args) -> dict:
         return {"value": 1.0 / per_gate_32, "unit": "gates/s", "cores": cores, "kind": "port",
                 "sample": f"first {len(ops)} gates of the same generator at {n_s} qubits (FP64), "
                           f"time x 2^{args.qubits - n_s} (extrapolated to {args.qubits} qubits)"}
+    if workload == "micro":
+        t0 = time.perf_counter()
+        tot = 0
+        while time.perf_counter() - t0 < 10 or tot == 0:
+            psi = O.simulate(20, W.qv_ops(20, 20, 20))
+            O.sample_indices(psi, np.random.default_rng(tot).random(8192))
+            tot += 1
+        dt = time.perf_counter() - t0
+        return {"value": tot / dt, "unit": "circuits/s", "cores": cores, "kind": "port",
+                "sample": f"{tot} runs of QV-20 + 8192 shots (FP64 C restatement, OpenMP)"}
     if workload == "noisy":
         n = args.qubits if args.qubits != 32 else 12
         qc = W.noisy_brickwork(n, 8, seed=5)

@@ -155,6 +155,18 @@ int qs_apply_1q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64,
 int qs_apply_2q(qs_handle_t h, void* state, int n_qubits, const float* gate_c64, int q0, int q1);
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:43-59,118-146 (apply_diagonal) */
 int qs_apply_diag1(qs_handle_t h, void* state, int n_qubits, const float* diag_c64, int target);
+/* The same four gates with the matrix in DEVICE memory (complex64,
+ * row-major; the diagonal as 2 complex64): the kernel reads it, so no host
+ * copy and no stream synchronisation per call.  This is how the reference's
+ * bindings take their gate tensors (bwk/csrc/apply_gate_sm120.cu:274-277,
+ * apply_gate2q_sm120.cu:239-242, apply_diagonal_sm120.cu:124-127,
+ * apply_mcgate_sm120.cu:109: the gate must be a CUDA tensor).  The pointer is
+ * checked to be device or managed memory.                                   */
+int qs_apply_1q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_dev, int target);
+int qs_apply_2q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_dev, int q0, int q1);
+int qs_apply_diag1_dev(qs_handle_t h, void* state, int n_qubits, const void* diag_dev, int target);
+int qs_apply_mc1q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_dev, const int* controls,
+                      int n_controls, int target);
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:64-83,150-175 (apply_diagonal_phase) */
 int qs_apply_phase(qs_handle_t h, void* state, int n_qubits, float phase_re, float phase_im, int target);
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:88-105,177-208 (apply_diagonal_2q);

@@ -2,6 +2,9 @@
 #include "qs_api.h"
 #include <atomic>
 #include <cstring>
+#include <cstdlib>
+#include <set>
+#include <mutex>
 
 static thread_local std::string g_tls_err;
 void qs_set_tls_error(const std::string& m) { g_tls_err = m; }
@@ -54,6 +57,25 @@ extern "C" {
 
 const char* qs_version(void) { return "qsim-b200 0.1.0 (sm_100a)"; }
 
+// The library's stream-ordered allocations (plan programs, batch tables,
+// adjoint and noise buffers) come from the device's default memory pool.
+// With the pool's default release threshold of 0, everything freed is handed
+// back to the driver at each synchronisation and mapped again by the next
+// allocation, which costs milliseconds per call; keeping up to 4 GiB cached
+// in this process avoids that (a runtime attribute of this process's pool,
+// gone when the process exits).  QSIM_POOL_KEEP_BYTES overrides the amount.
+static void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::set<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done.insert(device).second) return;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess || !pool) return;
+  const char* e = std::getenv("QSIM_POOL_KEEP_BYTES");
+  uint64_t keep = e ? std::strtoull(e, nullptr, 10) : (4ull << 30);
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
+
 int qs_create(int device, qs_handle_t* out) {
   qs_context* h = nullptr;
   QS_API_BEGIN
@@ -63,6 +85,7 @@ int qs_create(int device, qs_handle_t* out) {
   QS_CUDA(cudaGetDeviceCount(&count));
   QS_CHECK_ARG(device >= 0 && device < count, "device index out of range");
   QS_CUDA(cudaSetDevice(device));
+  keep_pool_memory(device);
   h = new qs_context();
   h->device = device;
   h->jit_mode = qs_jit_env_mode();

@@ -47,8 +47,20 @@ __device__ __forceinline__ void apply2(const G2& G, float2& a0, float2& a1) {
   a0 = n0; a1 = n1;
 }
 
+// A gate given by value, or read by every thread from device memory when gd
+// is not null (callers whose matrix lives in a device tensor, so that no
+// host copy and no stream synchronisation is needed).
+__device__ __forceinline__ G2 gate2(const G2& G, const float2* __restrict__ gd) {
+  if (!gd) return G;
+  G2 R;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) R.g[i] = gd[i];
+  return R;
+}
+
 // target 0: the pair is one float4.
-__global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G) {
+__global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G0, const float2* __restrict__ gd) {
+  const G2 G = gate2(G0, gd);
   for (uint64_t p = gtid(); p < npairs; p += gstride()) {
     float4 v = ld4(s + 2 * p);
     float2 a0 = lo2(v), a1 = hi2(v);
@@ -58,7 +70,8 @@ __global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G) {
 }
 
 // target t >= 1: two neighbouring pairs per thread, two float4 accesses.
-__global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G) {
+__global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G0, const float2* __restrict__ gd) {
+  const G2 G = gate2(G0, gd);
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i0 = insert_zero(2 * it, t);
@@ -83,8 +96,24 @@ __device__ __forceinline__ void apply4(const G4& G, float2& a0, float2& a1, floa
   a0 = o[0]; a1 = o[1]; a2 = o[2]; a3 = o[3];
 }
 
+// As gate2 for 4x4; swap: exchange the roles of matrix index bits 0 and 1.
+__device__ __forceinline__ G4 gate4(const G4& G, const float2* __restrict__ gd, int swap) {
+  if (!gd) return G;
+  G4 R;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int pr = swap ? ((r & 1) << 1 | r >> 1) : r, pc = swap ? ((c & 1) << 1 | c >> 1) : c;
+      R.g[4 * r + c] = gd[4 * pr + pc];
+    }
+  return R;
+}
+
 // lo == 0: a00,a01 adjacent and a10,a11 adjacent.
-__global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G) {
+__global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G0, const float2* __restrict__ gd,
+                         int swap) {
+  const G4 G = gate4(G0, gd, swap);
   const uint64_t sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nquads; it += gstride()) {
     uint64_t i00 = insert_zero(insert_zero(it, 0), hi);
@@ -97,7 +126,9 @@ __global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G) 
 }
 
 // lo >= 1: two neighbouring quads per thread.
-__global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi, G4 G) {
+__global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi, G4 G0,
+                         const float2* __restrict__ gd, int swap) {
+  const G4 G = gate4(G0, gd, swap);
   const uint64_t sl = 1ull << lo, sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i00 = insert_zero(insert_zero(2 * it, lo), hi);
@@ -114,7 +145,9 @@ __global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi
 }
 
 // ----------------------------------------------------------- diagonal -----
-__global__ void k_diag1(float2* __restrict__ s, uint64_t nvec, int t, float2 d0, float2 d1) {
+__global__ void k_diag1(float2* __restrict__ s, uint64_t nvec, int t, float2 d0v, float2 d1v,
+                        const float2* __restrict__ gd) {
+  const float2 d0 = gd ? gd[0] : d0v, d1 = gd ? gd[1] : d1v;
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     uint64_t idx = 2 * i;
     float4 v = ld4(s + idx);
@@ -152,7 +185,9 @@ __global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G
 }
 
 // ------------------------------------------------- multi-controlled -------
-__global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t, G2 G) {
+__global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t, G2 G0,
+                       const float2* __restrict__ gd) {
+  const G2 G = gate2(G0, gd);
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i0 = insert_zeros(it, P.pos, P.k) | cmask;
@@ -270,11 +305,12 @@ void check_controls(const int* controls, int nc, int n) {
 }  // namespace
 
 // Exposed to other units (apply_gates_fused fallback and tests).
-void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs_total, int t, const G2& G);
+void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs_total, int t, const G2& G,
+                  const float2* gd = nullptr);
 
-void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs, int t, const G2& G) {
-  if (t == 0) LAUNCH(h, k_1q_t0, npairs, s, npairs, G);
-  else LAUNCH(h, k_1q_tn, npairs / 2, s, npairs / 2, t, G);
+void qs_launch_1q(qs_context* h, float2* s, uint64_t npairs, int t, const G2& G, const float2* gd) {
+  if (t == 0) LAUNCH(h, k_1q_t0, npairs, s, npairs, G, gd);
+  else LAUNCH(h, k_1q_tn, npairs / 2, s, npairs / 2, t, G, gd);
 }
 
 extern "C" {
@@ -369,6 +405,80 @@ int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n, const 
   QS_API_END(h)
 }
 
+// Gates whose matrix is a device array (complex64, row-major): the kernel
+// reads it, so the call neither copies it to the host nor waits for the
+// stream.  The pointer must be device (or managed) memory.
+static void check_dev_ptr(const void* p, const char* what) {
+  QS_CHECK_ARG(p != nullptr && ((uintptr_t)p & 7u) == 0, std::string(what) + " must be 8-byte aligned");
+  cudaPointerAttributes a;
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  QS_CHECK_ARG(e == cudaSuccess && (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged),
+               std::string(what) + " is not device memory");
+}
+
+int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  check_dev_ptr(gate_dev, "gate");
+  qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G2{}, static_cast<const float2*>(gate_dev));
+  QS_API_END(h)
+}
+
+int qs_apply_2q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int q0, int q1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(n >= 2, "a 2-qubit gate needs n >= 2");
+  qs_check_qubit(q0, n, "qubit0");
+  qs_check_qubit(q1, n, "qubit1");
+  QS_CHECK_ARG(q0 != q1, "qubit0 and qubit1 must differ");
+  check_dev_ptr(gate_dev, "gate");
+  const int lo = std::min(q0, q1), hi = std::max(q0, q1), swap = q0 > q1 ? 1 : 0;
+  const float2* gd = static_cast<const float2*>(gate_dev);
+  uint64_t nquads = 1ull << (n - 2);
+  if (lo == 0) LAUNCH(h, k_2q_lo0, nquads, (float2*)state, nquads, hi, G4{}, gd, swap);
+  else LAUNCH(h, k_2q_gen, nquads / 2, (float2*)state, nquads / 2, lo, hi, G4{}, gd, swap);
+  QS_API_END(h)
+}
+
+int qs_apply_diag1_dev(qs_handle_t h, void* state, int n, const void* diag_dev, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  check_dev_ptr(diag_dev, "diag");
+  uint64_t nvec = (1ull << n) / 2;
+  LAUNCH(h, k_diag1, nvec, (float2*)state, nvec, t, make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+         static_cast<const float2*>(diag_dev));
+  QS_API_END(h)
+}
+
+int qs_apply_mc1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, const int* controls, int nc, int t) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t, n, "target");
+  check_controls(controls, nc, n);
+  check_dev_ptr(gate_dev, "gate");
+  const float2* gd = static_cast<const float2*>(gate_dev);
+  if (nc == 0) { qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G2{}, gd); return QS_OK; }
+  int all[QS_MAX_CONTROLS + 1];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t, "target_qubit must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = t;
+  Sorted P = make_sorted(all, nc + 1);
+  QS_CHECK_ARG(nc + 1 <= n, "more gate qubits than state qubits");
+  uint64_t items = 1ull << (n - nc - 1);
+  LAUNCH(h, k_mc1q, items, (float2*)state, items, P, cmask, t, G2{}, gd);
+  QS_API_END(h)
+}
+
 int qs_apply_2q(qs_handle_t h, void* state, int n, const float* gate, int q0, int q1) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
@@ -381,8 +491,8 @@ int qs_apply_2q(qs_handle_t h, void* state, int n, const float* gate, int q0, in
   int lo = q0, hi = q1;
   if (q0 > q1) { G = swap_bits(G); lo = q1; hi = q0; }
   uint64_t nquads = 1ull << (n - 2);
-  if (lo == 0) LAUNCH(h, k_2q_lo0, nquads, (float2*)state, nquads, hi, G);
-  else LAUNCH(h, k_2q_gen, nquads / 2, (float2*)state, nquads / 2, lo, hi, G);
+  if (lo == 0) LAUNCH(h, k_2q_lo0, nquads, (float2*)state, nquads, hi, G, nullptr, 0);
+  else LAUNCH(h, k_2q_gen, nquads / 2, (float2*)state, nquads / 2, lo, hi, G, nullptr, 0);
   QS_API_END(h)
 }
 
@@ -393,7 +503,7 @@ int qs_apply_diag1(qs_handle_t h, void* state, int n, const float* diag, int t) 
   qs_check_qubit(t, n, "target");
   QS_CHECK_ARG(diag != nullptr, "diag pointer is null");
   uint64_t nvec = (1ull << n) / 2;
-  LAUNCH(h, k_diag1, nvec, (float2*)state, nvec, t, f2(diag), f2(diag + 2));
+  LAUNCH(h, k_diag1, nvec, (float2*)state, nvec, t, f2(diag), f2(diag + 2), nullptr);
   QS_API_END(h)
 }
 
@@ -444,7 +554,7 @@ int qs_apply_mc1q(qs_handle_t h, void* state, int n, const float* gate, const in
   Sorted P = make_sorted(all, nc + 1);
   QS_CHECK_ARG(nc + 1 <= n, "more gate qubits than state qubits");
   uint64_t items = 1ull << (n - nc - 1);
-  LAUNCH(h, k_mc1q, items, (float2*)state, items, P, cmask, t, G);
+  LAUNCH(h, k_mc1q, items, (float2*)state, items, P, cmask, t, G, nullptr);
   QS_API_END(h)
 }
 

@@ -1393,11 +1393,8 @@ int qs_run_circuit(qs_handle_t h, void* state, int n, const qs_op* ops, int nops
   int rc = qs_plan_create(h, n, ops, nops, &p);
   if (rc != QS_OK) return rc;
   rc = qs_plan_execute(h, p, state);
-  // The device program must outlive the queued passes.
-  if (rc == QS_OK) {
-    cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) { h->err = cudaGetErrorString(e); rc = QS_ERR_CUDA; }
-  }
+  // No wait: qs_plan_destroy frees the device program stream-ordered after
+  // the queued passes.
   qs_plan_destroy(p);
   return rc;
 }

@@ -33,6 +33,19 @@ def _gate_host(gate, shape) -> np.ndarray:
     return np.ascontiguousarray(g.view(np.float32).reshape(-1))
 
 
+def _gate_dev(gate, shape, state: torch.Tensor):
+    """A gate that is already a complex64 CUDA tensor of the right shape on
+    the state's device, made contiguous (a device copy if needed), else None.
+    The caller passes its data_ptr() while holding the tensor, so the memory
+    stays allocated until the gate kernel is queued; after that torch reuses
+    it only for work queued later on the stream.  The kernel reads the gate
+    itself: no host copy, no stream synchronisation."""
+    if (isinstance(gate, torch.Tensor) and gate.is_cuda and gate.dtype == torch.complex64
+            and tuple(gate.shape) == shape and gate.device == state.device):
+        return gate if gate.is_contiguous() else gate.contiguous()
+    return None
+
+
 def _fp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -51,6 +64,10 @@ def _ints(x) -> np.ndarray:
 def apply_gate(state: torch.Tensor, gate: torch.Tensor, target_qubit: int) -> torch.Tensor:
     """Single-qubit gate in place (cuquantum.py:40-51)."""
     n = check_state(state)
+    gd = _gate_dev(gate, (2, 2), state)
+    if gd is not None:
+        _h(state.get_device()).call("qs_apply_1q_dev", state.data_ptr(), n, gd.data_ptr(), int(target_qubit))
+        return state
     g = _gate_host(gate, (2, 2))
     _h(state.device.index).call("qs_apply_1q", _ptr(state), n, _fp(g), int(target_qubit))
     return state
@@ -62,8 +79,12 @@ def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: 
     n = check_state(state)
     if qubit0 == qubit1:
         raise RuntimeError("qubit0 and qubit1 must differ")
-    g = _gate_host(gate, (4, 4))
     lo, hi = min(qubit0, qubit1), max(qubit0, qubit1)
+    gd = _gate_dev(gate, (4, 4), state)
+    if gd is not None:
+        _h(state.get_device()).call("qs_apply_2q_dev", state.data_ptr(), n, gd.data_ptr(), int(lo), int(hi))
+        return state
+    g = _gate_host(gate, (4, 4))
     _h(state.device.index).call("qs_apply_2q", _ptr(state), n, _fp(g), int(lo), int(hi))
     return state
 
@@ -93,6 +114,10 @@ def apply_gates_reg_tiled(state: torch.Tensor, gates: torch.Tensor, targets: tor
 
 def apply_diagonal(state: torch.Tensor, diag: torch.Tensor, target_qubit: int) -> torch.Tensor:
     n = check_state(state)
+    dd = _gate_dev(diag, (2,), state)
+    if dd is not None:
+        _h(state.get_device()).call("qs_apply_diag1_dev", state.data_ptr(), n, dd.data_ptr(), int(target_qubit))
+        return state
     d = _gate_host(diag, (2,))
     _h(state.device.index).call("qs_apply_diag1", _ptr(state), n, _fp(d), int(target_qubit))
     return state
@@ -129,11 +154,17 @@ def _is_swap(g: np.ndarray) -> bool:
 def apply_mcgate(state: torch.Tensor, gate: torch.Tensor, controls, target_qubit: int) -> torch.Tensor:
     """Multi-controlled 2x2 (cuquantum.py:297-317); an exact X moves values."""
     n = check_state(state)
-    g = _gate_host(gate, (2, 2))
     c = _ints(controls)
     if c.size > 7:
         raise RuntimeError("controls must have 0-7 elements")
     h = _h(state.device.index)
+    gd = _gate_dev(gate, (2, 2), state)
+    if gd is not None:
+        # the matrix stays on the device; an X there is still exact (the
+        # compensated 2x2 product of 0s and 1s rounds nothing)
+        h.call("qs_apply_mc1q_dev", state.data_ptr(), n, gd.data_ptr(), _ip(c), int(c.size), int(target_qubit))
+        return state
+    g = _gate_host(gate, (2, 2))
     if _is_x(g):
         h.call("qs_apply_mcx", _ptr(state), n, _ip(c), int(c.size), int(target_qubit))
     else:
@@ -310,7 +341,7 @@ def _haar(dim, device):
     z = torch.randn(dim, dim, dtype=torch.complex64)
     q, r = torch.linalg.qr(z)
     d = torch.diagonal(r)
-    return (q * (d / d.abs()).unsqueeze(0)).to(device)
+    return (q * (d / d.abs()).unsqueeze(0)).contiguous().to(device)
 
 
 def random_unitary(device="cuda"):

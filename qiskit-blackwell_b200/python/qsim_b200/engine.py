@@ -32,9 +32,16 @@ def _wait_uses(plan) -> None:
         ev.synchronize()
 
 
+try:  # torch's current stream as a raw pointer, without building a Stream object per call
+    _raw_stream = torch._C._cuda_getCurrentRawStream
+except AttributeError:  # pragma: no cover - older torch
+    _raw_stream = None
+
+
 def _h(device: int | None = None) -> _lib.Handle:
     dev = torch.cuda.current_device() if device is None else int(device)
-    return _lib.handle(dev, torch.cuda.current_stream(dev).cuda_stream)
+    sp = _raw_stream(dev) if _raw_stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    return _lib.handle(dev, sp)
 
 
 def autotune_batch(widths, op_offsets, ops, device: int | None = None) -> dict:
