@@ -408,12 +408,17 @@ int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n, const 
 // Gates whose matrix is a device array (complex64, row-major): the kernel
 // reads it, so the call neither copies it to the host nor waits for the
 // stream.  The pointer must be device (or managed) memory.
-static void check_dev_ptr(const void* p, const char* what) {
+// The last pointer that passed is remembered per handle (a gate tensor is
+// usually reused call after call): under unified addressing a device
+// address never becomes a pageable host address.
+static void check_dev_ptr(qs_context* h, const void* p, const char* what) {
   QS_CHECK_ARG(p != nullptr && ((uintptr_t)p & 7u) == 0, std::string(what) + " must be 8-byte aligned");
+  if (p == h->dev_ptr_ok) return;
   cudaPointerAttributes a;
   const cudaError_t e = cudaPointerGetAttributes(&a, p);
   QS_CHECK_ARG(e == cudaSuccess && (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged),
                std::string(what) + " is not device memory");
+  h->dev_ptr_ok = p;
 }
 
 int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int t) {
@@ -421,7 +426,7 @@ int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int
   QS_API_BEGIN
   qs_check_state(state, n);
   qs_check_qubit(t, n, "target");
-  check_dev_ptr(gate_dev, "gate");
+  check_dev_ptr(h, gate_dev, "gate");
   qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G2{}, static_cast<const float2*>(gate_dev));
   QS_API_END(h)
 }
@@ -434,7 +439,7 @@ int qs_apply_2q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int
   qs_check_qubit(q0, n, "qubit0");
   qs_check_qubit(q1, n, "qubit1");
   QS_CHECK_ARG(q0 != q1, "qubit0 and qubit1 must differ");
-  check_dev_ptr(gate_dev, "gate");
+  check_dev_ptr(h, gate_dev, "gate");
   const int lo = std::min(q0, q1), hi = std::max(q0, q1), swap = q0 > q1 ? 1 : 0;
   const float2* gd = static_cast<const float2*>(gate_dev);
   uint64_t nquads = 1ull << (n - 2);
@@ -448,7 +453,7 @@ int qs_apply_diag1_dev(qs_handle_t h, void* state, int n, const void* diag_dev, 
   QS_API_BEGIN
   qs_check_state(state, n);
   qs_check_qubit(t, n, "target");
-  check_dev_ptr(diag_dev, "diag");
+  check_dev_ptr(h, diag_dev, "diag");
   uint64_t nvec = (1ull << n) / 2;
   LAUNCH(h, k_diag1, nvec, (float2*)state, nvec, t, make_float2(0.f, 0.f), make_float2(0.f, 0.f),
          static_cast<const float2*>(diag_dev));
@@ -461,7 +466,7 @@ int qs_apply_mc1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, c
   qs_check_state(state, n);
   qs_check_qubit(t, n, "target");
   check_controls(controls, nc, n);
-  check_dev_ptr(gate_dev, "gate");
+  check_dev_ptr(h, gate_dev, "gate");
   const float2* gd = static_cast<const float2*>(gate_dev);
   if (nc == 0) { qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G2{}, gd); return QS_OK; }
   int all[QS_MAX_CONTROLS + 1];

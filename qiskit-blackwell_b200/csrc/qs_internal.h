@@ -45,6 +45,7 @@ struct qs_context {
   int jit_mode = 1;
   int jit_min_qubits = 24;
   int64_t launches = 0;
+  const void* dev_ptr_ok = nullptr;  // last pointer found to be device memory (qs_apply_*_dev)
 
   // grow-only device scratch (reductions, sampling partials, ...)
   void* scratch = nullptr;
