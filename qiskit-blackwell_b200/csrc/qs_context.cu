@@ -72,8 +72,9 @@ static void keep_pool_memory(int device) {
   cudaMemPool_t pool = nullptr;
   if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess || !pool) return;
   const char* e = std::getenv("QSIM_POOL_KEEP_BYTES");
-  uint64_t keep = e ? std::strtoull(e, nullptr, 10) : (4ull << 30);
-  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  uint64_t keep = e ? std::strtoull(e, nullptr, 10) : (4ull << 30), cur = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur >= keep) return;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);  // only ever raised here
 }
 
 int qs_create(int device, qs_handle_t* out) {
