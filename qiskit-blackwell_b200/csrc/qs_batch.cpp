@@ -50,7 +50,7 @@ void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t*
               std::vector<qs_plan_s>& plans) {
   plans.resize(nc);
   std::vector<std::string> errs(nc);
-  unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
   if (nc < 64) nt = 1;
   std::vector<std::thread> pool;
   for (unsigned t = 0; t < nt; ++t) {
