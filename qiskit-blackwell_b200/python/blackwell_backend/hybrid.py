@@ -54,6 +54,10 @@ _REFERENCE_NATIVE = {
     "measure", "barrier", "reset",
 }
 
+# Stochastic channels (qsim_b200.circuit.NOISE_OPS): only the plain route
+# runs them (as one trajectory per shot).
+_NOISE_NAMES = {"depolarize", "amplitude_damp", "dephase"}
+
 # Largest amplitude count of one batch plan on the batched route (2^26
 # complex64 = 512 MiB of states, the serving runtime's batch cap).
 BATCH_AMPS = 1 << 26
@@ -139,6 +143,8 @@ class RoutingPolicy:
             return "batched"
         if analysis is None:
             analysis = analyze_circuit(circuit)
+        if analysis["gate_names"] & _NOISE_NAMES:
+            return "blackwell"          # noise channels run as trajectories on the plain path
         if batch_size > 1 and analysis["num_qubits"] <= self.batch_max_qubits:
             if batch_size >= self.batch_min_circuits or analysis["non_native_ratio"] > self.non_native_threshold:
                 return "batched"
@@ -356,6 +362,8 @@ class HybridSimulator:
 
     # ---------------------------------------------------------- routes ----
     def _run_blackwell(self, circ: Circuit, shots, seed):
+        if analyze_circuit(circ)["gate_names"] & _NOISE_NAMES:
+            return self._blackwell.run(circ, shots=shots, seed=seed)   # one trajectory per shot
         clean = self._blackwell._strip_measurements(circ)
         state, _, elapsed = self._blackwell._execute_circuit(clean)
         samples = E.sample_seeded(state, shots, seed)

@@ -187,12 +187,36 @@ class BlackwellSimulator:
         out.data = [i for i in circ.data if i.name not in ("measure", "reset")]
         return out
 
+    def _run_noisy(self, clean: Circuit, shots: int, seed):
+        """Counts of a circuit with noise channels: one trajectory per shot
+        (qs_noise_trajectories), trajectories run in chunks of at most 2^26
+        amplitudes; trajectory k of the run uses seed + k."""
+        from qsim_b200.noise import run_trajectories, sample_trajectories
+        base = int(seed) if seed is not None else int(np.random.default_rng().integers(0, 2 ** 62))
+        per_chunk = max(1, (1 << 26) >> clean.num_qubits)
+        counts = {}
+        t0 = time.perf_counter()
+        for k0 in range(0, shots, per_chunk):
+            k = min(per_chunk, shots - k0)
+            states, _ = run_trajectories(clean, k, seed=base + k0, device=self._dev_index, branches=False)
+            for key, c in sample_trajectories(states, 1, seed=base + k0).items():
+                counts[key] = counts.get(key, 0) + c
+        torch.cuda.synchronize()
+        return counts, time.perf_counter() - t0
+
     def run(self, circuit, shots=1024, seed=None):
-        """Counts from the pre-measurement statevector (simulator.py:555-604)."""
+        """Counts from the pre-measurement statevector (simulator.py:555-604).
+        A circuit carrying noise channels (depolarize / amplitude_damp /
+        dephase) is sampled as one stochastic trajectory per shot."""
         if seed is not None:
             torch.manual_seed(seed)
             np.random.seed(seed)
         clean = self._strip_measurements(circuit)
+        from qsim_b200.circuit import NOISE_OPS
+        if any(ins.name in NOISE_OPS for ins in clean.data):
+            counts, elapsed = self._run_noisy(clean, int(shots), seed)
+            return _make_result(counts, shots, {"name": clean.name, "n_qubits": clean.num_qubits}, elapsed,
+                                {"method": "noise trajectories (one per shot)"})
         state, _, elapsed = self._execute_circuit(clean)
         samples = E.sample(state, shots)            # stays on the device
         n = clean.num_qubits

@@ -140,3 +140,25 @@ def test_unitary_plan_rejects_channels():
     qc.dephase(0.1, 0)
     with pytest.raises(RuntimeError, match="noise channel"):
         E.Plan(3, lower(qc))
+
+
+def test_simulator_run_samples_noisy_circuit_as_trajectories():
+    """BlackwellSimulator.run on a circuit with channels: one trajectory per
+    shot, in chunks (14 qubits: 4096 trajectories per chunk, so 5000 shots
+    take two)."""
+    from blackwell_backend import BlackwellSimulator, HybridSimulator
+    qc = Circuit(14, name="decay")
+    qc.x(13)
+    qc.amplitude_damp(0.3, 13)
+    res = BlackwellSimulator().run(qc, shots=5000, seed=4)
+    counts = res.get_counts()
+    assert sum(counts.values()) == 5000
+    assert set(counts) <= {hex(0), hex(1 << 13)}
+    n0 = counts.get(hex(0), 0)
+    assert 1500 - 4 * 33 < n0 < 1500 + 4 * 33          # P(decay) = 0.3, 4 sigma
+    again = BlackwellSimulator().run(qc, shots=5000, seed=4).get_counts()
+    assert again == counts                               # seeded trajectories
+    hy = HybridSimulator(workers=1, budget_bytes=1 << 30)
+    r = hy.run(qc, shots=200, seed=1)
+    assert r.metadata["backend_used"] == "blackwell" and sum(r.get_counts().values()) == 200
+    hy.close()

@@ -91,3 +91,11 @@ def test_seed_uniforms_match_splitmix_loop():
         assert np.array_equal(u, loop(s, 257))
         assert u.min() >= 0.0 and u.max() < 1.0
     assert seed_uniforms(3, 0).shape == (0,)
+
+
+def test_policy_keeps_noisy_circuits_on_plain_path():
+    qc = Circuit(4, name="noisy")
+    qc.h(0)
+    qc.amplitude_damp(0.1, 0)
+    p = RoutingPolicy()
+    assert p.choose(qc, batch_size=8) == "blackwell"
