@@ -45,6 +45,9 @@ class Sampler:
         for k, qc in enumerate(circuits):
             if isinstance(qc, tuple):
                 qc = qc[0]
+            if _is_noisy(qc):   # one trajectory per shot
+                out.append(self.sim.run(qc, shots=shots, seed=None if seed is None else int(seed) + k).get_counts())
+                continue
             g = None
             if seed is not None:
                 g = torch.Generator(device=f"cuda:{self.sim._dev_index}")
@@ -54,14 +57,45 @@ class Sampler:
         return out
 
 
+def _is_noisy(qc) -> bool:
+    from qsim_b200.circuit import NOISE_OPS, from_qiskit
+    return any(ins.name in NOISE_OPS for ins in from_qiskit(qc).data)
+
+
 class Estimator:
-    def __init__(self, simulator: BlackwellSimulator | None = None):
+    """trajectories / seed: a circuit with noise channels is estimated as the
+    mean of <psi_t|H|psi_t> over that many seeded trajectories (an unbiased
+    estimate of Tr(rho H)); noiseless circuits are exact."""
+
+    def __init__(self, simulator: BlackwellSimulator | None = None, trajectories: int = 1024, seed: int = 0):
         self.sim = simulator or BlackwellSimulator()
+        self.trajectories = int(trajectories)
+        self.seed = int(seed)
+
+    def _noisy_value(self, qc, obs) -> float:
+        from qsim_b200.circuit import from_qiskit
+        from qsim_b200.noise import run_trajectories
+        circ = self.sim._strip_measurements(from_qiskit(qc))
+        n = circ.num_qubits
+        ps = _as_pauli_sum(obs, n)
+        if ps.num_qubits != n:
+            raise ValueError(f"observable acts on {ps.num_qubits} qubits, circuit has {n}")
+        per_chunk = max(1, (1 << 26) >> n)
+        total, done = 0.0, 0
+        while done < self.trajectories:
+            k = min(per_chunk, self.trajectories - done)
+            states, _ = run_trajectories(circ, k, seed=self.seed + done, device=self.sim._dev_index, branches=False)
+            total += sum(E.expect_pauli_sum(states[t], ps) for t in range(k))
+            done += k
+        return total / self.trajectories
 
     def run(self, pubs) -> np.ndarray:
         """pubs: iterable of (circuit, observable) pairs."""
         vals = []
         for qc, obs in pubs:
+            if _is_noisy(qc):
+                vals.append(self._noisy_value(qc, obs))
+                continue
             state = self.sim.run_statevector_tensor(qc)
             n = state.numel().bit_length() - 1
             ps = _as_pauli_sum(obs, n)

@@ -42,3 +42,30 @@ def test_estimator_matches_oracle():
     v2 = Estimator().run([(qc2, ps)])[0]
     psi = O.simulate(6, lower(qc2))
     assert abs(v2 - O.pauli_expectation(psi, ps.x, ps.z, ps.real_coefs())) < 1e-6
+
+
+def test_primitives_on_noisy_circuits():
+    """Sampler: one trajectory per shot; Estimator: the trajectory mean of
+    <H>, against Tr(rho H) from the oracle's Kraus-sum density matrix."""
+    from blackwell_backend.primitives import Estimator, Sampler
+    from qsim_b200.circuit import lower
+    from qsim_b200.noise import add_noise
+    qc = Circuit(3, name="noisy3")
+    qc.h(0)
+    qc.cx(0, 1)
+    qc.ry(0.7, 2)
+    qc = add_noise(qc, depolarizing=0.05, amplitude_damping=0.2, dephasing=0.1)
+    counts = Sampler().run([qc], shots=3000, seed=2)[0]
+    assert sum(counts.values()) == 3000
+    rho = O.kraus_density(3, lower(qc))
+    obs = [("ZII", 1.0), ("IZZ", 0.5), ("XXI", -0.25)]
+    zi = np.diag([1, 1, 1, 1, -1, -1, -1, -1]).astype(complex)          # Z on qubit 2 (leftmost label)
+    z = np.diag([1, -1]).astype(complex)
+    x = np.array([[0, 1], [1, 0]], dtype=complex)
+    i2 = np.eye(2)
+    H = 1.0 * np.kron(np.kron(z, i2), i2) + 0.5 * np.kron(np.kron(i2, z), z) - 0.25 * np.kron(np.kron(x, x), i2)
+    exact = float(np.real(np.trace(rho @ H)))
+    T = 20000
+    val = Estimator(trajectories=T, seed=5).run([(qc, obs)])[0]
+    assert abs(val - exact) < 5 * 1.75 / np.sqrt(T)                      # |H| <= 1.75, 5 sigma
+    assert np.allclose(zi, np.kron(np.kron(z, i2), i2))
