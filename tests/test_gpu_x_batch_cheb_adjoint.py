@@ -272,3 +272,31 @@ def test_autotune_widths_then_alone_equals_batch():
             assert np.array_equal(alone.cpu().numpy(), got), (c, n)
     finally:
         E.autotune_clear()
+
+
+def test_adjoint_per_gate_fallback_agrees(tmp_path):
+    """The one-launch-per-gate sweep (used past 1 GiB of pass partials, or
+    with QSIM_ADJ_PASSES=0) gives the same gradients as the tile passes."""
+    import os
+    import subprocess
+    import sys
+    code = r"""
+import sys, numpy as np
+sys.path[:0] = %r
+from qsim_b200 import engine as E, workloads as W
+from qsim_b200.circuit import lower
+qc, npar = W.efficient_su2(14, reps=2)
+qc.cz(0, 13)
+ops = lower(qc)
+ps = W.random_pauli_observable(14, 12, seed=3)
+P = np.random.default_rng(2).uniform(0, 6.28, (2, npar))
+e, g = E.adjoint_gradient(14, ops, npar, P, ps)
+np.save(sys.argv[1], np.concatenate([e, g.ravel()]))
+""" % (sys.path[:6],)
+    out = {}
+    for flag in ("1", "0"):
+        path = str(tmp_path / f"adj_{flag}.npy")
+        env = dict(os.environ, QSIM_ADJ_PASSES=flag)
+        subprocess.run([sys.executable, "-c", code, path], env=env, check=True, timeout=300)
+        out[flag] = np.load(path)
+    np.testing.assert_allclose(out["1"], out["0"], atol=1e-6)
