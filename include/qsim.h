@@ -446,6 +446,13 @@ int qs_apply_dephasing(qs_handle_t h, void* state, int n_qubits, int target, dou
  * every noise op (depolarizing 0..3, damping/dephasing 0/1).               */
 int qs_noise_trajectories(qs_handle_t h, int n_qubits, const qs_op* ops, int n_ops, int n_traj,
                           const uint64_t* seeds, void* states, uint8_t* branches_host);
+/* Host-only inspection (no GPU needed; no reference counterpart): the
+ * whole-state device program qs_noise_trajectories runs for a noisy circuit
+ * of 1..14 qubits (passes back to back, as qs_plan_program; channel groups
+ * are blocks with pos[6] = 1).  block_bits 0 = automatic.  Writes it to out
+ * when cap suffices; *needed = its size in bytes.                           */
+int qs_noise_program(int n_qubits, const qs_op* ops, int n_ops, int block_bits, void* out, size_t cap,
+                     size_t* needed);
 
 #ifdef __cplusplus
 }

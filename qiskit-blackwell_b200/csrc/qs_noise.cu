@@ -373,6 +373,81 @@ void segment_stream(const qs_op* ops, int nops, const std::vector<NoiseSite>& si
   }
 }
 
+// The noise channels of a circuit, in program order (checked).
+std::vector<NoiseSite> noise_sites(int n, const qs_op* ops, int nops) {
+  std::vector<NoiseSite> sites;
+  for (int i = 0; i < nops; ++i) {
+    if (!is_noise(ops[i].kind)) continue;
+    QS_CHECK_ARG(ops[i].nq == 1, "a noise channel acts on one qubit");
+    qs_check_qubit(ops[i].q[0], n, "noise");
+    check_prob(ops[i].m[0], "noise channel parameter");
+    sites.push_back(NoiseSite{i, ops[i].kind, ops[i].q[0], ops[i].m[0]});
+  }
+  return sites;
+}
+
+// The program of a noisy circuit on up to 14 qubits: its unitary segments
+// planned as whole-state passes, consecutive channels grouped into noise
+// blocks between them.  auto_bb: the block width was not fixed by the caller.
+qs_plan_s whole_state_program(int n, const qs_op* ops, int nops, const std::vector<NoiseSite>& sites, int tb, int bb,
+                              bool auto_bb) {
+  std::vector<std::vector<qs_op>> seg;
+  std::vector<int> seg_site;
+  segment_stream(ops, nops, sites, nullptr, seg, seg_site);
+  // channels after (almost) every gate leave segments of one or two gates:
+  // 3-qubit register blocks then beat wider ones (smaller diagonal tables,
+  // so more CTAs per SM; measured 204 k vs 182 k trajectories/s on a
+  // 12-qubit, 840-channel circuit)
+  {
+    size_t nonempty = 0, gates = 0;
+    for (const auto& sg : seg) {
+      nonempty += !sg.empty();
+      gates += sg.size();
+    }
+    if (auto_bb && nonempty && gates <= 4 * nonempty) bb = std::min(bb, 3);
+  }
+  const size_t smem_left = 200 * 1024 - (8ull << n) - 2 * 128 * sizeof(uint64_t) - 16 * sizeof(int) - 16;
+  Merger m;
+  m.n = n;
+  m.R = std::min(bb, n);
+  m.coef_cap = std::min<size_t>(8192, smem_left / sizeof(float2));
+  m.out.n_qubits = n;
+  double flops = 0;
+  // consecutive channels (no gate between) share a block while they touch
+  // at most kGroupQubits qubits and number at most kGroupOps
+  constexpr int kGroupQubits = 4, kGroupOps = 32;
+  std::vector<std::pair<int, NoiseSite>> group;
+  auto group_qubits = [&](int extra) {
+    std::vector<int> qs;
+    for (const auto& e : group)
+      if (std::find(qs.begin(), qs.end(), e.second.q) == qs.end()) qs.push_back(e.second.q);
+    if (extra >= 0 && std::find(qs.begin(), qs.end(), extra) == qs.end()) qs.push_back(extra);
+    return (int)qs.size();
+  };
+  auto flush_group = [&]() {
+    if (!group.empty()) m.add_noise_group(group);
+    group.clear();
+  };
+  for (size_t s = 0; s < seg.size(); ++s) {
+    if (!seg[s].empty()) {
+      flush_group();
+      qs_plan_s p;
+      qs_build_plan(n, seg[s].data(), (int)seg[s].size(), tb, &p, bb);
+      m.add_plan(p);
+      flops += p.info.flops;
+    }
+    if (s < seg_site.size()) {
+      const NoiseSite& ns = sites[seg_site[s]];
+      if ((int)group.size() >= kGroupOps || group_qubits(ns.q) > kGroupQubits) flush_group();
+      group.emplace_back(seg_site[s], ns);
+    }
+  }
+  flush_group();
+  m.flush(true);
+  m.out.info.flops = flops;
+  return std::move(m.out);
+}
+
 }  // namespace
 
 extern "C" {
@@ -410,6 +485,20 @@ int qs_apply_dephasing(qs_handle_t h, void* state, int n, int target, double lam
   QS_API_END(h)
 }
 
+int qs_noise_program(int n, const qs_op* ops, int nops, int block_bits, void* out, size_t cap, size_t* needed) {
+  qs_context* h = nullptr;
+  QS_API_BEGIN
+  QS_CHECK_ARG(needed != nullptr, "needed is null");
+  QS_CHECK_ARG(n >= 1 && n <= 14, "whole-state noise programs hold 1 to 14 qubits");
+  QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops), "ops pointer is null");
+  QS_CHECK_ARG(block_bits == 0 || (block_bits >= 2 && block_bits <= 5), "block_bits must be 0 (auto) or in [2, 5]");
+  const std::vector<NoiseSite> sites = noise_sites(n, ops, nops);
+  const qs_plan_s p = whole_state_program(n, ops, nops, sites, 13, block_bits ? block_bits : 4, block_bits == 0);
+  *needed = p.blob.size();
+  if (out && cap >= p.blob.size() && !p.blob.empty()) std::memcpy(out, p.blob.data(), p.blob.size());
+  QS_API_END(h)
+}
+
 int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int n_traj, const uint64_t* seeds,
                           void* states, uint8_t* branches_host) {
   QS_REQUIRE_HANDLE(h);
@@ -422,15 +511,7 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
   QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops), "ops pointer is null");
   QS_CHECK_ARG(n_traj == 0 || seeds, "seeds pointer is null");
   if (n_traj == 0) return QS_OK;
-  // noise sites, in program order
-  std::vector<NoiseSite> sites;
-  for (int i = 0; i < nops; ++i) {
-    if (!is_noise(ops[i].kind)) continue;
-    QS_CHECK_ARG(ops[i].nq == 1, "a noise channel acts on one qubit");
-    qs_check_qubit(ops[i].q[0], n, "noise");
-    check_prob(ops[i].m[0], "noise channel parameter");
-    sites.push_back(NoiseSite{i, ops[i].kind, ops[i].q[0], ops[i].m[0]});
-  }
+  const std::vector<NoiseSite> sites = noise_sites(n, ops, nops);
   const int nn = (int)sites.size();
   const bool want_br = branches_host && nn;
   const size_t slots = (size_t)n_traj * (size_t)nn;
@@ -440,64 +521,10 @@ int qs_noise_trajectories(qs_handle_t h, int n, const qs_op* ops, int nops, int 
   qs_plan_shape(h, n, false, tb, bb);
 
   if (n <= 14) {
-    // one whole-state program with a noise block per channel, shared by all
-    // trajectories; one CTA per trajectory
-    std::vector<std::vector<qs_op>> seg;
-    std::vector<int> seg_site;
-    segment_stream(ops, nops, sites, nullptr, seg, seg_site);
-    // channels after (almost) every gate leave segments of one or two gates:
-    // 3-qubit register blocks then beat wider ones (smaller diagonal tables,
-    // so more CTAs per SM; measured 204 k vs 182 k trajectories/s on a
-    // 12-qubit, 840-channel circuit)
-    {
-      size_t nonempty = 0, gates = 0;
-      for (const auto& sg : seg) {
-        nonempty += !sg.empty();
-        gates += sg.size();
-      }
-      if (h->block_bits == 0 && nonempty && gates <= 4 * nonempty) bb = std::min(bb, 3);
-    }
-    const size_t smem_left = 200 * 1024 - (8ull << n) - 2 * 128 * sizeof(uint64_t) - 16 * sizeof(int) - 16;
-    Merger m;
-    m.n = n;
-    m.R = std::min(bb, n);
-    m.coef_cap = std::min<size_t>(8192, smem_left / sizeof(float2));
-    m.out.n_qubits = n;
-    double flops = 0;
-    // consecutive channels (no gate between) share a block while they touch
-    // at most kGroupQubits qubits and number at most kGroupOps
-    constexpr int kGroupQubits = 4, kGroupOps = 32;
-    std::vector<std::pair<int, NoiseSite>> group;
-    auto group_qubits = [&](int extra) {
-      std::vector<int> qs;
-      for (const auto& e : group)
-        if (std::find(qs.begin(), qs.end(), e.second.q) == qs.end()) qs.push_back(e.second.q);
-      if (extra >= 0 && std::find(qs.begin(), qs.end(), extra) == qs.end()) qs.push_back(extra);
-      return (int)qs.size();
-    };
-    auto flush_group = [&]() {
-      if (!group.empty()) m.add_noise_group(group);
-      group.clear();
-    };
-    for (size_t s = 0; s < seg.size(); ++s) {
-      if (!seg[s].empty()) {
-        flush_group();
-        qs_plan_s p;
-        qs_build_plan(n, seg[s].data(), (int)seg[s].size(), tb, &p, bb);
-        m.add_plan(p);
-        flops += p.info.flops;
-      }
-      if (s < seg_site.size()) {
-        const NoiseSite& ns = sites[seg_site[s]];
-        if ((int)group.size() >= kGroupOps || group_qubits(ns.q) > kGroupQubits) flush_group();
-        group.emplace_back(seg_site[s], ns);
-      }
-    }
-    flush_group();
-    m.flush(true);
-    m.out.info.flops = flops;
+    // one whole-state program with a noise block per channel group, shared
+    // by all trajectories; one CTA per trajectory
     std::vector<qs_plan_s> progs(1);
-    progs[0] = std::move(m.out);
+    progs[0] = whole_state_program(n, ops, nops, sites, tb, bb, h->block_bits == 0);
     std::vector<BatchUnit> units(n_traj);
     for (int t = 0; t < n_traj; ++t)
       units[t] = BatchUnit{0, (uint64_t)t * N, seeds[t], want_br ? d_br + (size_t)t * nn : nullptr};

@@ -154,6 +154,7 @@ SIGNATURES = {
     "qs_apply_amplitude_damping": (_i, [_vp, _vp, _i, _i, _d, _d, _pi32]),
     "qs_apply_dephasing": (_i, [_vp, _vp, _i, _i, _d, _d, _pi32]),
     "qs_sample_batched": (_i, [_vp, _vp, _i, _pi32, _pi64, _pi64, _pu64, _vp]),
+    "qs_noise_program": (_i, [_i, _pop, _i, _i, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "qs_noise_trajectories": (_i, [_vp, _i, _pop, _i, _i, _pu64, _vp, C.POINTER(C.c_uint8)]),
     "qs_batch_run": (_i, [_vp, _i, _pi32, _pi64, _pop, _vp, _pi64]),
     "qs_batch_plan_create": (_i, [_vp, _i, _pi32, _pi64, _pop, _pi64, C.POINTER(_vp)]),

@@ -30,7 +30,7 @@ OP_DT = np.dtype({"names": ["kind", "t0", "t1", "rc", "d0", "d1", "ncoef", "pad0
 assert PASS_DT.itemsize == 112 and BLOCK_DT.itemsize == 16
 
 DK_U1, DK_U2, DK_X, DK_SWAP, DK_Y = 1, 2, 3, 4, 5
-DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE, DK_XRY, DK_CU2 = 10, 11, 12, 13, 14, 15, 16
+DK_RY, DK_DTAB, DK_KRY, DK_KU1, DK_SCALE, DK_XRY, DK_CU2, DK_NOISE = 10, 11, 12, 13, 14, 15, 16, 17
 
 
 def program(n, ops, tile_bits=0, block_bits=0, specialised=False) -> bytes:
@@ -66,7 +66,22 @@ def _bits(raw, k):
     return int(w[0]), int(w[1])
 
 
-def run(n, blob: bytes, psi: np.ndarray) -> np.ndarray:
+def noise_program(n, ops, block_bits=0) -> bytes:
+    """The whole-state program `qs_noise_trajectories` runs (n <= 14)."""
+    L = _lib.load()
+    ops = np.ascontiguousarray(ops)
+    p = ops.ctypes.data_as(C.POINTER(_lib.QsOp))
+    need = C.c_size_t(0)
+    _lib.check(L.qs_noise_program(n, p, len(ops), block_bits, None, 0, C.byref(need)))
+    buf = (C.c_char * max(1, need.value))()
+    _lib.check(L.qs_noise_program(n, p, len(ops), block_bits, buf, need.value, C.byref(need)))
+    return bytes(buf)[: need.value]
+
+
+def run(n, blob: bytes, psi: np.ndarray, seed=None, branches=None) -> np.ndarray:
+    """Apply the program to psi.  Noise blocks draw channel k's uniform as
+    value k of `seed`'s splitmix64 stream and append (k, branch) to
+    `branches` when it is a list."""
     psi = np.array(psi, dtype=np.complex128)
     idx = np.arange(1 << n, dtype=np.uint64)
     for hdr, blocks, dops, raw in decode(blob):
@@ -74,6 +89,10 @@ def run(n, blob: bytes, psi: np.ndarray) -> np.ndarray:
         R = int(hdr["R"])
         cf = raw[0::2].astype(np.float64) + 1j * raw[1::2].astype(np.float64)
         for b in blocks:
+            if int(b["pos"][6]):
+                assert seed is not None, "a noise program needs a seed"
+                psi = _noise_block(psi, idx, S, b, dops, int(seed), branches)
+                continue
             regq = [S[int(p)] for p in b["pos"][:R]]
             rmask = 0
             for q in regq:
@@ -89,6 +108,90 @@ def run(n, blob: bytes, psi: np.ndarray) -> np.ndarray:
             for o in dops[int(b["op_begin"]): int(b["op_end"])]:
                 psi = _apply(psi, o, cf, raw, regq, R, idx, gidx, jreg)
     return psi
+
+
+def _uniform_at(seed, k):
+    """Value k of splitmix64 from seed (Steele, Lea and Flood, 2014), top 53
+    bits scaled to [0, 1)."""
+    m = (1 << 64) - 1
+    z = (seed + (k + 1) * 0x9E3779B97F4A7C15) & m
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    z ^= z >> 31
+    return (z >> 11) * 2.0 ** -53
+
+
+def _depol_branch(p, u):
+    if u < 1.0 - p:
+        return 0
+    r, third = u - (1.0 - p), p / 3.0
+    return 1 if r < third else (2 if r < 2.0 * third else 3)
+
+
+def _noise_block(psi, idx, S, b, dops, seed, branches):
+    """A noise block as the kernel runs it: the bin histogram of |a|^2 over
+    the block's qubits Q, every channel's branch decided in order from the
+    running histogram, and the composed map a'(i) = C[bin(i)] a(i ^ M)
+    applied once with C rounded to FP32."""
+    nq = int(b["pos"][5])
+    pos = [int(x) for x in b["pos"][:nq]]
+    Q = [S[p] for p in pos]
+    NB = 1 << nq
+    binv = np.zeros(idx.shape, dtype=np.int64)
+    for j, q in enumerate(Q):
+        binv |= ((idx >> np.uint64(q)) & np.uint64(1)).astype(np.int64) << j
+    ops = dops[int(b["op_begin"]): int(b["op_end"])]
+    H = np.bincount(binv, weights=np.abs(psi) ** 2, minlength=NB)
+    C = np.ones(NB, dtype=np.complex128)
+    bins = np.arange(NB)
+    Mb, ident = 0, True
+    for o in ops:
+        assert int(o["kind"]) == DK_NOISE
+        j = pos.index(int(o["t0"]))
+        bit = 1 << j
+        st = (bins & bit) != 0
+        g = float(np.array([int(o["gc"])], dtype=np.uint64).view(np.float64)[0])
+        k = int(o["coef"])
+        u = _uniform_at(seed, k)
+        m, c = 0, np.ones(NB, dtype=np.complex128)
+        if int(o["d0"]) == 20:
+            br = _depol_branch(g, u)
+            if branches is not None:
+                branches.append((k, br))
+            if br == 0:
+                continue
+            if br == 1:
+                m = bit
+            elif br == 2:
+                m, c = bit, np.where(st, 1j, -1j)
+            else:
+                c = np.where(st, -1.0, 1.0).astype(np.complex128)
+        else:
+            S0, S1 = float(H[~st].sum()), float(H[st].sum())
+            p1 = g * S1 / (S0 + S1)
+            keep = S0 + (1.0 - g) * S1
+            jump = S1 > 0.0 and (u < p1 or not keep > 0.0)
+            if branches is not None:
+                branches.append((k, int(jump)))
+            if not jump:
+                r = 1.0 / np.sqrt(keep)
+                c = np.where(st, np.sqrt(1.0 - g) * r, r).astype(np.complex128)
+            elif int(o["d0"]) == 21:
+                m, c = bit, np.where(st, 0.0, 1.0 / np.sqrt(S1)).astype(np.complex128)
+            else:
+                c = np.where(st, 1.0 / np.sqrt(S1), 0.0).astype(np.complex128)
+        ident = False
+        C = c * C[bins ^ m]
+        H = np.abs(c) ** 2 * H[bins ^ m]
+        Mb ^= m
+    if ident:
+        return psi
+    C = C.astype(np.complex64).astype(np.complex128)
+    flip = 0
+    for j, q in enumerate(Q):
+        if (Mb >> j) & 1:
+            flip |= 1 << q
+    return C[binv] * psi[(idx ^ np.uint64(flip)).astype(np.int64)]
 
 
 def _pairs(idx, q):
