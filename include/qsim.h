@@ -225,7 +225,10 @@ int qs_plan_jit_check(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, 
  * form).  For inspection and tests of the planner; no reference counterpart. */
 int qs_plan_program(int n_qubits, const qs_op* ops, int n_ops, int tile_bits, int block_bits, int specialised,
                     void* out, size_t cap, size_t* needed);
-/* plan + execute in one call (the plan is freed afterwards).               */
+/* plan + execute in one call.  The handle keeps the plans of its 16 most
+ * recent circuits (of at most 4096 ops): running the same op records again
+ * on the same stream reuses the plan without planning or upload.  Also what
+ * qs_apply_gates_fused runs through.                                        */
 int qs_run_circuit(qs_handle_t h, void* state, int n_qubits, const qs_op* ops, int n_ops);
 
 /* ------------------------------------------------------- reductions ------ */

@@ -113,6 +113,7 @@ int qs_destroy(qs_handle_t h) {
   cudaSetDevice(h->device);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+  qs_run_cache_clear(h);
   if (h->scratch) cudaFree(h->scratch);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

@@ -32,6 +32,8 @@ struct qs_error : std::runtime_error {
   } while (0)
 
 // ------------------------------------------------------------- context ----
+struct qs_plan_s;
+
 struct qs_context {
   int device = 0;
   int sm_count = 148;
@@ -53,6 +55,14 @@ struct qs_context {
   // pinned host staging for scalar results
   double* pinned = nullptr;
   size_t pinned_bytes = 0;
+  // qs_run_circuit's recently run plans (qs_plan.cpp), least recent first
+  struct RunEntry {
+    uint64_t hash;
+    int n, tile_bits, block_bits, specialised;
+    std::vector<qs_op> ops;
+    qs_plan_s* plan;
+  };
+  std::vector<RunEntry> run_cache;
 
   void* scratch_get(size_t bytes);
   double* pinned_get(size_t bytes);
@@ -188,6 +198,8 @@ void qs_plan_upload(qs_context* h, qs_plan_s* p);
 // Stream-ordered free after the work queued on `stream` (the stream the
 // program last ran on; no device-wide synchronisation).
 void qs_plan_free_device(void* d, cudaStream_t stream);
+// Frees the plans qs_run_circuit keeps (stream-ordered after their last run).
+void qs_run_cache_clear(qs_context* h);
 // Runs every pass on n_states equal-width states stored back to back.
 void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint64_t n_states);
 

@@ -1285,6 +1285,34 @@ void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint6
   }
 }
 
+// qs_run_circuit's plan cache: entries per handle, and the largest circuit kept.
+constexpr size_t kRunCacheEntries = 16;
+constexpr int kRunCacheMaxOps = 4096;
+
+static uint64_t fnv1a(const void* data, size_t bytes, uint64_t seed) {
+  const unsigned char* b = static_cast<const unsigned char*>(data);
+  uint64_t x = 0xcbf29ce484222325ull ^ seed;
+  for (size_t i = 0; i < bytes; ++i) x = (x ^ b[i]) * 0x100000001b3ull;
+  return x;
+}
+
+// A cached plan last ran on plan->stream.  While that is the handle's stream
+// the program is freed stream-ordered behind the runs.  Otherwise that stream
+// may since have been destroyed: wait for the device, then free it on the
+// handle's stream.
+static void run_cache_free(qs_context* h, qs_plan_s* p) {
+  if (p->stream != h->stream) {
+    cudaDeviceSynchronize();
+    p->stream = h->stream;
+  }
+  qs_plan_destroy(p);
+}
+
+void qs_run_cache_clear(qs_context* h) {
+  for (auto& e : h->run_cache) run_cache_free(h, e.plan);
+  h->run_cache.clear();
+}
+
 extern "C" {
 
 int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* out) {
@@ -1389,14 +1417,52 @@ int qs_plan_destroy(qs_plan_t plan) {
 }
 
 int qs_run_circuit(qs_handle_t h, void* state, int n, const qs_op* ops, int nops) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(nops >= 0 && (nops == 0 || ops), "ops pointer is null");
+  // A circuit run again (the same op records, width and plan shape) on the
+  // same stream reuses its plan: no planning and no program upload.  Entries
+  // are keyed on the full records, so a hit runs exactly the plan a fresh
+  // call would build, and every run of an entry is on one stream.
+  int tb = 0, bb = 0;
+  const int spec = h->jit_mode == 2 ? 1 : 0;
+  qs_plan_shape(h, n, spec != 0, tb, bb);
+  const bool cacheable = nops <= kRunCacheMaxOps;
+  const uint64_t key = cacheable ? fnv1a(ops, sizeof(qs_op) * (size_t)nops, (uint64_t)n * 0x100000001b3ull) : 0;
+  auto& cache = h->run_cache;
+  for (size_t i = 0; cacheable && i < cache.size(); ++i) {
+    qs_context::RunEntry& e = cache[i];
+    if (e.hash != key || e.n != n || e.tile_bits != tb || e.block_bits != bb || e.specialised != spec ||
+        e.plan->stream != h->stream || (int)e.ops.size() != nops ||
+        (nops && std::memcmp(e.ops.data(), ops, sizeof(qs_op) * (size_t)nops)))
+      continue;
+    qs_context::RunEntry hit = std::move(e);
+    cache.erase(cache.begin() + (long)i);
+    const int rc = qs_plan_execute(h, hit.plan, state);
+    if (rc != QS_OK) {
+      qs_plan_destroy(hit.plan);
+      return rc;
+    }
+    cache.push_back(std::move(hit));
+    return QS_OK;
+  }
   qs_plan_t p = nullptr;
   int rc = qs_plan_create(h, n, ops, nops, &p);
   if (rc != QS_OK) return rc;
   rc = qs_plan_execute(h, p, state);
-  // No wait: qs_plan_destroy frees the device program stream-ordered after
-  // the queued passes.
-  qs_plan_destroy(p);
-  return rc;
+  if (rc != QS_OK || !cacheable) {
+    // No wait: qs_plan_destroy frees the device program stream-ordered after
+    // the queued passes.
+    qs_plan_destroy(p);
+    return rc;
+  }
+  if (cache.size() >= kRunCacheEntries) {
+    run_cache_free(h, cache.front().plan);
+    cache.erase(cache.begin());
+  }
+  cache.push_back(qs_context::RunEntry{key, n, tb, bb, spec, std::vector<qs_op>(ops, ops + nops), p});
+  return QS_OK;
+  QS_API_END(h)
 }
 
 int qs_apply_gates_fused(qs_handle_t h, void* state, int n, const float* gates, const int* targets, int ngates) {

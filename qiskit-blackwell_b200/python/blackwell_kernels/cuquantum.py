@@ -92,6 +92,12 @@ def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: 
 def apply_gates_fused(state: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
     """K 1Q gates in one fused program (cuquantum.py:69-80)."""
     n = check_state(state)
+    if (isinstance(gates, torch.Tensor) and isinstance(targets, torch.Tensor)
+            and gates.device == state.device and targets.device == state.device):
+        # both to pinned host memory on the current stream, one wait for the pair
+        gates = gates.detach().to("cpu", torch.complex64, non_blocking=True)
+        targets = targets.detach().to("cpu", non_blocking=True)
+        torch.cuda.current_stream(state.device).synchronize()
     if isinstance(gates, torch.Tensor):
         g = gates.detach().to("cpu", torch.complex64).contiguous().numpy()
     else:

@@ -74,3 +74,76 @@ def test_host_pointer_rejected():
     host = np.eye(2, dtype=np.complex64)
     with pytest.raises(_lib.QsimError, match="device memory"):
         E._h(a.device.index).call("qs_apply_1q_dev", E._ptr(a), 4, C.c_void_p(host.ctypes.data), 0)
+
+
+def _fused_ref(psi, gates, targets):
+    """FP64: the 1Q gates applied one after another."""
+    import sv_oracle as O
+    from qsim_b200.circuit import Circuit, lower
+    n = int(psi.size).bit_length() - 1
+    qc = Circuit(n)
+    for g, t in zip(gates, targets):
+        qc.unitary(np.asarray(g, dtype=np.complex128), [int(t)])
+    return O.simulate(n, lower(qc), psi.astype(np.complex128))
+
+
+def test_fused_gates_device_and_host_inputs_and_repeats():
+    """apply_gates_fused with CUDA or host gate/target tensors gives the same
+    bits; calling it again with the same gates reuses the plan (the result
+    equals two fresh applications), and new gate values on the same targets
+    are not served a stale plan."""
+    n = 12
+    gates = torch.stack([bk.random_unitary() for _ in range(10)]).contiguous()
+    targets = torch.arange(10, dtype=torch.int32, device="cuda")
+    a, b = _state(n, 5), _state(n, 5)
+    psi0 = a.cpu().numpy()
+    bk.apply_gates_fused(a, gates, targets)
+    bk.apply_gates_fused(b, gates.cpu(), targets.cpu().tolist())
+    assert np.array_equal(_bits(a), _bits(b))
+    g_h = gates.cpu().numpy()
+    ref = _fused_ref(psi0, g_h, range(10))
+    assert np.abs(a.cpu().numpy() - ref).max() < 1e-5
+    for _ in range(3):                                  # cache hits
+        bk.apply_gates_fused(a, gates, targets)
+    ref2 = ref
+    for _ in range(3):
+        ref2 = _fused_ref(ref2.astype(np.complex64), g_h, range(10))
+    assert np.abs(a.cpu().numpy() - ref2).max() < 1e-4
+    gates2 = torch.stack([bk.random_unitary() for _ in range(10)]).contiguous()
+    c = _state(n, 5)
+    bk.apply_gates_fused(c, gates2, targets)
+    ref3 = _fused_ref(psi0, gates2.cpu().numpy(), range(10))
+    assert np.abs(c.cpu().numpy() - ref3).max() < 1e-5
+    # another stream: built afresh there, same bits
+    d = _state(n, 5)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        bk.apply_gates_fused(d, gates2, targets)
+    s.synchronize()
+    assert np.array_equal(_bits(c), _bits(d))
+
+
+def test_run_circuit_cache_many_circuits():
+    """More distinct circuits than the handle keeps: every call still runs
+    its own circuit (evictions free programs without disturbing later runs)."""
+    import sv_oracle as O
+    from qsim_b200 import workloads as W
+    h = E._h(0)
+    n = 10
+    outs = []
+    for rep in range(2):
+        # the second sweep, in reverse, hits the 16 kept plans, then evicts
+        for seed in (range(20) if rep == 0 else reversed(range(20))):
+            ops = W.qv_ops(n, 4, seed=seed)
+            st = torch.zeros(1 << n, dtype=torch.complex64, device="cuda")
+            st[0] = 1
+            h.call("qs_run_circuit", E._ptr(st), n, ops.ctypes.data_as(C.POINTER(_lib.QsOp)), len(ops))
+            outs.append((seed, st))
+    torch.cuda.synchronize()
+    first = {}
+    for seed, st in outs:
+        ref = O.simulate(n, W.qv_ops(n, 4, seed=seed))
+        assert abs(1 - O.fidelity(st.cpu().numpy(), ref)) <= 1e-6
+        if seed in first:
+            assert np.array_equal(_bits(st), _bits(first[seed]))
+        first[seed] = st
