@@ -280,6 +280,7 @@ def test_adjoint_per_gate_fallback_agrees(tmp_path):
     import os
     import subprocess
     import sys
+    ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     code = r"""
 import sys, numpy as np
 sys.path[:0] = %r
@@ -292,7 +293,7 @@ ps = W.random_pauli_observable(14, 12, seed=3)
 P = np.random.default_rng(2).uniform(0, 6.28, (2, npar))
 e, g = E.adjoint_gradient(14, ops, npar, P, ps)
 np.save(sys.argv[1], np.concatenate([e, g.ravel()]))
-""" % (sys.path[:6],)
+""" % ([os.path.join(ROOT, "qiskit-blackwell_b200", "python"), os.path.join(ROOT, "oracle")],)
     out = {}
     for flag in ("1", "0"):
         path = str(tmp_path / f"adj_{flag}.npy")
