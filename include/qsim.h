@@ -317,7 +317,10 @@ int qs_cheb_evolve_pauli(qs_handle_t h, int n_qubits, const void* psi, void* out
 /* Many independent circuits of uneven width, states packed back to back.
  * ops for circuit c are ops[op_offsets[c] .. op_offsets[c+1]); its state
  * starts at amplitude state_offsets[c] of `states`.  States are initialised
- * to |0..0> by the call.  Reference precedent: bwk/csrc/qv8_sim_sm120.cu:58-151,
+ * to |0..0> by the call.  Large batches are planned in up to 8 slices, each
+ * launched as soon as it is planned (host planning overlaps the GPU); if a
+ * later slice fails to plan, earlier ones have run and the error is returned
+ * after they finish.  Reference precedent: bwk/csrc/qv8_sim_sm120.cu:58-151,
  * bwk/csrc/batch_sm120.cu:53-279 (fixed widths only).                       */
 int qs_batch_run(qs_handle_t h, int n_circuits, const int32_t* widths, const int64_t* op_offsets,
                  const qs_op* ops, void* states, const int64_t* state_offsets);

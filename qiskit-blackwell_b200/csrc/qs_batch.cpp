@@ -85,7 +85,13 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
   B->device = h->device;
   B->n_circuits = (int)units.size();
   B->stream = h->stream;
+  // The copies go on the upload stream, and the host waits for that stream
+  // alone: work already queued on h->stream keeps running meanwhile.  Once
+  // the host has seen the copies (and the stream-ordered allocations) done,
+  // any stream may use the buffers; they are freed on h->stream.
+  cudaStream_t us = nullptr;
   try {
+    us = qs_upload_stream(h);
     // concatenate device programs
     std::vector<size_t> boff(np);
     size_t total = 0;
@@ -97,8 +103,8 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
     for (int c = 0; c < np; ++c)
       if (!plans[c].blob.empty()) std::memcpy(blob.data() + boff[c], plans[c].blob.data(), plans[c].blob.size());
     if (total) {
-      QS_CUDA(cudaMallocAsync(&B->d_blob, total, h->stream));
-      QS_CUDA(cudaMemcpyAsync(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice, h->stream));
+      QS_CUDA(cudaMallocAsync(&B->d_blob, total, us));
+      QS_CUDA(cudaMemcpyAsync(B->d_blob, blob.data(), total, cudaMemcpyHostToDevice, us));
     }
     for (const BatchUnit& u : units) {
       QS_CHECK_ARG(u.plan >= 0 && u.plan < np, "internal: unit plan index out of range");
@@ -146,12 +152,12 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
     }
     for (const BatchUnit& u : units) flops += plans[u.plan].info.flops;
     if (!items.empty()) {
-      QS_CUDA(cudaMallocAsync(&B->d_items, items.size() * sizeof(PassItem), h->stream));
+      QS_CUDA(cudaMallocAsync(&B->d_items, items.size() * sizeof(PassItem), us));
       QS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice,
-                              h->stream));
+                              us));
     }
     // blob/items are host temporaries: wait for the copies before they go
-    QS_CUDA(cudaStreamSynchronize(h->stream));
+    QS_CUDA(cudaStreamSynchronize(us));
     B->info.n_circuits = (int32_t)units.size();
     B->info.n_launches = (int32_t)B->launches.size();
     B->info.n_items = (int64_t)items.size();
@@ -159,11 +165,17 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
     B->info.bytes_moved = bytes;
     B->info.flops = flops;
   } catch (...) {
+    if (us) cudaStreamSynchronize(us);  // no copy may still target the buffers
     free_bplan(B);
     throw;
   }
   return B;
 }
+
+// qs_batch_run slices: at most this many, each of at least half this many
+// circuits (smaller batches run as one slice).
+constexpr int kMaxSlices = 8;
+constexpr int kSliceMinCircuits = 256;
 
 static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
                                     const qs_op* ops, const int64_t* state_off) {
@@ -285,26 +297,56 @@ int qs_batch_plan_destroy(qs_batch_plan_t B) {
   return QS_OK;
 }
 
+// A one-shot batch is planned in slices of about equal op counts, and each
+// slice is launched as soon as it is planned: the host plans slice k+1 (and
+// copies its programs on the upload stream) while the GPU runs slice k.
+static int run_slices(int nc) {
+  if (nc < kSliceMinCircuits) return 1;
+  return std::min(kMaxSlices, nc / (kSliceMinCircuits / 2));
+}
+
 int qs_batch_run(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops,
                  void* states, const int64_t* state_off) {
   QS_REQUIRE_HANDLE(h);
-  qs_batch_plan_s* B = nullptr;
+  std::vector<qs_batch_plan_s*> Bs;
+  auto release = [&]() {
+    if (!Bs.empty()) cudaStreamSynchronize(h->stream);  // programs must outlive the launches
+    for (auto* B : Bs) free_bplan(B);
+    Bs.clear();
+  };
   QS_API_BEGIN
-  B = build_batch(h, nc, widths, op_off, ops, state_off);
-  run_batch(h, B, states);
-  QS_CUDA(cudaStreamSynchronize(h->stream));  // programs must outlive the launches
-  free_bplan(B);
-  B = nullptr;
+  QS_CHECK_ARG(nc >= 0, "n_circuits must be >= 0");
+  QS_CHECK_ARG(nc == 0 || (widths && op_off && state_off), "null batch descriptor");
+  for (int c = 0; c < nc; ++c) {
+    QS_CHECK_ARG(widths[c] >= 1 && widths[c] <= QS_MAX_QUBITS, "circuit width out of range");
+    QS_CHECK_ARG(state_off[c] >= 0 && (state_off[c] & 1) == 0, "state offsets must be even and >= 0");
+    QS_CHECK_ARG(op_off[c] >= 0 && op_off[c + 1] >= op_off[c], "op_offsets must be non-decreasing");
+  }
+  const int ns = run_slices(nc);
+  const int64_t ops_total = nc ? op_off[nc] - op_off[0] : 0;
+  int c0 = 0;
+  for (int s = 0; s < ns && c0 < nc; ++s) {
+    int c1 = nc;
+    if (s + 1 < ns) {  // first circuit past s+1 equal shares of the ops
+      const int64_t goal = op_off[0] + ops_total * (s + 1) / ns;
+      c1 = c0 + 1;
+      while (c1 < nc && op_off[c1] < goal) ++c1;
+    }
+    Bs.push_back(build_batch(h, c1 - c0, widths + c0, op_off + c0, ops, state_off + c0));
+    run_batch(h, Bs.back(), states);
+    c0 = c1;
+  }
+  release();
   return QS_OK;
   }
   catch (const qs_error& e) {
     h->err = e.what();
-    if (B) { cudaStreamSynchronize(h->stream); free_bplan(B); }
+    release();
     return e.code;
   }
   catch (const std::exception& e) {
     h->err = e.what();
-    if (B) { cudaStreamSynchronize(h->stream); free_bplan(B); }
+    release();
     return QS_ERR_INVALID;
   }
 }

@@ -53,6 +53,11 @@ void qs_after_launch(qs_context* h, const char* what) {
     throw qs_error(QS_ERR_CUDA, std::string(what) + ": launch failed: " + cudaGetErrorString(e));
 }
 
+cudaStream_t qs_upload_stream(qs_context* h) {
+  if (!h->upload_stream) QS_CUDA(cudaStreamCreateWithFlags(&h->upload_stream, cudaStreamNonBlocking));
+  return h->upload_stream;
+}
+
 extern "C" {
 
 const char* qs_version(void) { return "qsim-b200 0.1.0 (sm_100a)"; }
@@ -114,6 +119,10 @@ int qs_destroy(qs_handle_t h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
   qs_run_cache_clear(h);
+  if (h->upload_stream) {
+    cudaStreamSynchronize(h->upload_stream);
+    cudaStreamDestroy(h->upload_stream);
+  }
   if (h->scratch) cudaFree(h->scratch);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

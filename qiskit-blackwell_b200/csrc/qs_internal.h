@@ -39,6 +39,9 @@ struct qs_context {
   int sm_count = 148;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // Host-to-device copies of batch programs, so that building a batch does
+  // not wait for the work queued on `stream` (created on first use).
+  cudaStream_t upload_stream = nullptr;
   std::string err;
   int tile_bits = 0;    // 0: 13, or the autotuned value for the width
   int block_bits = 0;   // 0: 5 for specialised plans, 4 for the generic kernel
@@ -67,6 +70,9 @@ struct qs_context {
   void* scratch_get(size_t bytes);
   double* pinned_get(size_t bytes);
 };
+
+// The handle's upload stream (non-blocking; created on first use).
+cudaStream_t qs_upload_stream(qs_context* h);
 
 // Records a launch and checks the launch status.
 void qs_after_launch(qs_context* h, const char* what);

@@ -192,6 +192,26 @@ class BatchPlan:
         return states
 
 
+def batch_run(widths, op_offsets, ops, state_offsets, states: torch.Tensor) -> torch.Tensor:
+    """One-shot batch (qs_batch_run): every circuit from |0..0> into its
+    slice of `states`, planned, run and freed in one call that returns when
+    the states are final.  Large batches are planned in slices that overlap
+    the GPU running the previous slice."""
+    widths = np.ascontiguousarray(widths, dtype=np.int32)
+    op_offsets = np.ascontiguousarray(op_offsets, dtype=np.int64)
+    state_offsets = np.ascontiguousarray(state_offsets, dtype=np.int64)
+    if len(op_offsets) != len(widths) + 1 or len(state_offsets) != len(widths):
+        raise ValueError("op_offsets needs n_circuits + 1 entries, state_offsets n_circuits")
+    need = int((state_offsets + (1 << widths.astype(np.int64))).max()) if len(widths) else 0
+    if states.numel() < need or states.dtype != torch.complex64 or not states.is_cuda:
+        raise RuntimeError("states buffer too small or not complex64 CUDA")
+    ops, p = _ops_ptr(ops)
+    _h(states.device.index).call("qs_batch_run", int(len(widths)), widths.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 op_offsets.ctypes.data_as(C.POINTER(C.c_int64)), p, _ptr(states),
+                                 state_offsets.ctypes.data_as(C.POINTER(C.c_int64)))
+    return states
+
+
 def run_ops(state: torch.Tensor, ops: np.ndarray) -> torch.Tensor:
     n = check_state(state)
     ops, p = _ops_ptr(ops)

@@ -33,6 +33,34 @@ def test_batch_uneven_widths_vs_oracle_and_alone():
         assert np.array_equal(alone.cpu().numpy(), got), (c, n)
 
 
+def test_one_shot_batch_slices_equal_batch_plan():
+    """qs_batch_run plans a large batch in slices launched as they are ready;
+    every state is bit-identical to the reusable plan's, and a bad circuit
+    is reported without leaving work queued."""
+    widths, oo, ops, so = W.qv_batch(600, 6, 15, seed=12)
+    bp = E.BatchPlan(widths, oo, ops, so)
+    a = bp.alloc_states()
+    bp.execute(a)
+    b = torch.full_like(a, 7.0)
+    E.batch_run(widths, oo, ops, so, b)
+    torch.cuda.synchronize()
+    av, bv = a.cpu().numpy(), b.cpu().numpy()
+    for c in range(len(widths)):
+        n = int(widths[c])
+        assert np.array_equal(av[so[c]: so[c] + (1 << n)], bv[so[c]: so[c] + (1 << n)]), c
+    for c in (0, 299, 599):
+        n = int(widths[c])
+        ref = O.simulate(n, ops[oo[c]: oo[c + 1]])
+        assert abs(1 - O.fidelity(bv[so[c]: so[c] + (1 << n)], ref)) <= 1e-6
+    bad = ops.copy()
+    bad["q"][oo[550]][0] = 40                     # qubit out of range in a late slice
+    with pytest.raises(Exception):
+        E.batch_run(widths, oo, bad, so, b)
+    torch.cuda.synchronize()
+    E.batch_run(widths, oo, ops, so, b)           # the handle still works
+    assert np.array_equal(b.cpu().numpy()[: len(av)], av)
+
+
 def test_qv8_and_qv4_match_reference_golden():
     import blackwell_kernels as bk
     d = np.load(os.path.join(GOLD, "qv8_ref.npz"))
