@@ -23,8 +23,30 @@ void qs_set_tls_error(const std::string& m);
   }                                                                          \
   return QS_OK;
 
+// Makes `dev` the calling thread's current device for the rest of the scope
+// and restores the previous one at its end, so a handle's work always goes to
+// its own device whatever device the caller had current.
+struct qs_device_guard {
+  int prev = -1;
+  explicit qs_device_guard(int dev) {
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~qs_device_guard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  qs_device_guard(const qs_device_guard&) = delete;
+  qs_device_guard& operator=(const qs_device_guard&) = delete;
+};
+
+// First statement of every entry point that takes a handle: rejects a null
+// handle and selects the handle's device until the call returns.
 #define QS_REQUIRE_HANDLE(h)                                                 \
-  do { if (!(h)) { qs_set_tls_error("null handle"); return QS_ERR_INVALID; } } while (0)
+  if (!(h)) {                                                                \
+    qs_set_tls_error("null handle");                                         \
+    return QS_ERR_INVALID;                                                   \
+  }                                                                          \
+  const qs_device_guard qs_device_guard_((h)->device)
 
 inline void qs_check_state(const void* state, int n_qubits) {
   QS_CHECK_ARG(state != nullptr, "state pointer is null");

@@ -90,7 +90,10 @@ int qs_create(int device, qs_handle_t* out) {
   int count = 0;
   QS_CUDA(cudaGetDeviceCount(&count));
   QS_CHECK_ARG(device >= 0 && device < count, "device index out of range");
-  QS_CUDA(cudaSetDevice(device));
+  const qs_device_guard on_device(device);  // the caller's device again on return
+  int cur = -1;
+  QS_CUDA(cudaGetDevice(&cur));
+  if (cur != device) QS_CUDA(cudaSetDevice(device));  // reports why the guard could not select it
   keep_pool_memory(device);
   h = new qs_context();
   h->device = device;
@@ -115,7 +118,7 @@ int qs_create(int device, qs_handle_t* out) {
 
 int qs_destroy(qs_handle_t h) {
   if (!h) return QS_OK;
-  cudaSetDevice(h->device);
+  const qs_device_guard on_device(h->device);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
   qs_run_cache_clear(h);

@@ -20,6 +20,9 @@
 #include <algorithm>
 #include <cstdlib>
 #include <map>
+#include <mutex>
+#include <set>
+#include <tuple>
 
 using namespace qs;
 
@@ -811,19 +814,23 @@ struct LaunchCfg { int per_sm; };
 
 size_t coef_bytes_for(int ncoef) { return (((size_t)ncoef * sizeof(float2)) + 15) & ~size_t(15); }
 
+// Launch shapes per (device, dynamic shared memory, threads).  Handles on
+// several host threads launch concurrently, so the table is locked.
 template <int R, bool TWO, bool BIG>
-LaunchCfg configure(int smem, int threads) {
-  static std::map<std::pair<int, int>, LaunchCfg> cache;
-  auto key = std::make_pair(smem, threads);
+LaunchCfg configure(int device, int smem, int threads) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, LaunchCfg> cache;
+  static std::set<int> attr_set;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_tuple(device, smem, threads);
   auto f = cache.find(key);
   if (f != cache.end()) return f->second;
-  // The attribute is a per-function maximum: set it once to the largest tile
-  // (2^14 amplitudes) plus the largest coefficient pool, so that launches of
-  // any size stay valid.
-  static bool attr_set = false;
-  if (!attr_set) {
+  // The attribute is a per-function maximum on each device: set it once to
+  // the largest tile (2^14 amplitudes) plus the largest coefficient pool, so
+  // that launches of any size stay valid.
+  if (!attr_set.count(device)) {
     QS_CUDA(cudaFuncSetAttribute(k_pass<R, TWO, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
-    attr_set = true;
+    attr_set.insert(device);
   }
   int per_sm = 0;
   QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass<R, TWO, BIG>, threads, smem));
@@ -841,7 +848,7 @@ void launch_R(qs_context* h, float2* base, const PassItem& single, const PassIte
   const uint32_t dep_off = coef_off + (uint32_t)coef_bytes_for(ncoef);
   const int smem = (int)(dep_off + 2 * 128 * sizeof(uint64_t) + 16 * sizeof(int));
   QS_CHECK_ARG(smem <= kMaxPassSmem, "tile-pass program too large for shared memory (coefficient pool)");
-  LaunchCfg c = configure<R, TWO, BIG>(smem, threads);
+  LaunchCfg c = configure<R, TWO, BIG>(h->device, smem, threads);
   uint64_t grid = std::min<uint64_t>(total, (uint64_t)h->sm_count * c.per_sm);
   if (grid == 0) return;
   k_pass<R, TWO, BIG><<<(unsigned)grid, threads, smem, h->stream>>>(base, single, d_items, nitems, total,

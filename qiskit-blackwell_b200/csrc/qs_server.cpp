@@ -181,7 +181,9 @@ struct qs_server_s {
 
   void worker_loop() {
     qs_handle_t h = nullptr;
-    const int rc = qs_create(device, &h);
+    // This thread's own CUDA calls (buffers, copies) go to the server's device.
+    int rc = cudaSetDevice(device) == cudaSuccess ? QS_OK : QS_ERR_CUDA;
+    if (rc == QS_OK) rc = qs_create(device, &h);
     for (;;) {
       std::vector<ReqP> item;
       {
