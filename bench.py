@@ -733,6 +733,97 @@ def bench_noisy(args, dev):
             "clocks": clk.summary(), "gpu_launches": int(launches)}, {"unit": "trajectories/s"}
 
 
+def bench_chebyshev(args, dev):
+    """Chebyshev evolution exp(-iHt)|psi> at the largest size of the serving
+    mix's evolution requests: --qubits (default 22) qubits, H = ring J ZZ +
+    h X field + 20 random K (XX + YY) pairs (seed n), t = 10, precision 1e-6,
+    seeded product state.  value = evolutions/s of the matrix-free path
+    (chebyshev_evolve_pauli) on a resident state; e2e = host state in, host
+    state out.  The CSR path with the reference's algorithm (chebyshev_evolve
+    over a CSR of the same H) is timed beside it.  Roofline per degree:
+    matrix-free 40 N bytes (read x_k, x_(k-1) and the accumulator, write
+    x_(k+1) and the accumulator); CSR 12 nnz + 4 (N+1) + 40 N."""
+    import numpy as np
+    import torch
+    from blackwell_backend.chebyshev import chebyshev_evolve, chebyshev_evolve_pauli
+    from blackwell_backend.hamiltonian import HamiltonianCSR
+    from qsim_b200 import workloads as W
+    from qsim_b200.paulis import csr_from_paulis
+    n = args.qubits if args.qubits != 32 else 22
+    N = 1 << n
+    t_evo, prec = 10.0, 1e-6
+    H = W.serving_hamiltonian(n, seed=n)
+    psi_h = np.ascontiguousarray(W.product_state(n, seed=n).astype(np.complex64))
+    psi = torch.from_numpy(psi_h).to(f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    res_pf = {}
+
+    def step_pf():
+        res_pf["out"], res_pf["info"] = chebyshev_evolve_pauli(psi, H, t_evo, precision=prec)
+
+    for _ in range(args.warmup):
+        step_pf()
+    from qsim_b200 import engine as E
+    h = E._h(dev)
+    l0 = h.launches()
+    with ClockSampler(dev) as clk:
+        t_pf = _cuda_time(step_pf, stream, args.steps)
+        launches = h.launches() - l0
+
+        def step_e2e():
+            d = torch.from_numpy(psi_h).to(f"cuda:{dev}", non_blocking=False)
+            o, _ = chebyshev_evolve_pauli(d, H, t_evo, precision=prec)
+            return o.cpu()
+
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_e2e()
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+    K = int(res_pf["info"]["chebyshev_degree"])
+    # the CSR path (reference algorithm) on the same H
+    row_ptr, col, val = csr_from_paulis(H)
+    nnz = int(row_ptr[-1])
+    csr = HamiltonianCSR(torch.from_numpy(row_ptr).to(f"cuda:{dev}"), torch.from_numpy(col).to(f"cuda:{dev}"),
+                         torch.from_numpy(val).to(f"cuda:{dev}"), n, H.spectral_bound(), paulis=H)
+    res_csr = {}
+
+    def step_csr():
+        res_csr["out"], res_csr["info"] = chebyshev_evolve(psi, csr, t_evo, precision=prec)
+
+    step_csr()
+    t_csr = _cuda_time(step_csr, stream, max(1, args.steps))
+    a = res_pf["out"].cpu().numpy().astype(np.complex128)
+    b = res_csr["out"].cpu().numpy().astype(np.complex128)
+    fid = float(abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real))
+    t_pf, t_csr, t_e2e = (reduce_max(x, f"cuda:{dev}") for x in (t_pf, t_csr, t_e2e))
+    per, per_csr, per_e2e = t_pf / args.steps, t_csr / max(1, args.steps), t_e2e / args.steps
+    peak, src = measured_peaks()
+    algo_pf = 40.0 * N                                   # bytes per degree
+    algo_csr = 12.0 * nnz + 4.0 * (N + 1) + 40.0 * N
+    ach_pf = algo_pf * K / per / 1e9
+    ach_csr = algo_csr * K / per_csr / 1e9
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"metric": METRIC, "value": ws / per, "unit": "evolutions/s", "ms_per_step": per * 1e3,
+            "dtype": "c64 vectors (fp32 FMA), fp64 Bessel coefficients",
+            "config": {"workload": f"chebyshev: {n} qubits, ring ZZ + X field + 20 XX+YY pairs ({len(H.x)} Pauli "
+                                   f"terms), t = {t_evo}, precision {prec}, degree K = {K}",
+                       "l2": f"3 vectors of {(8 * N) >> 20} MiB (the recurrence re-reads them every degree)"},
+            "roofline": {"bound": "hbm", "achieved": ach_pf, "peak": peak, "unit": "GB/s", "frac": ach_pf / peak,
+                         "traffic": None, "peak_source": src, "kernel": "k_chebp_fused (matrix-free, one per degree)",
+                         "algorithmic_bytes_per_launch": algo_pf,
+                         "note": "each amplitude also gathers x_k[i ^ x_t] for every Pauli term (from L2 when the "
+                                 "vector fits there), so the kernel is bound by those gathers, not by its 40 N bytes"},
+            "csr_path": {"value": 1.0 / per_csr, "unit": "evolutions/s", "nnz": nnz,
+                         "roofline": {"achieved": ach_csr, "frac": ach_csr / peak, "unit": "GB/s",
+                                      "kernel": "k_cheb_fused (CSR SpMV + step + accumulate)",
+                                      "algorithmic_bytes_per_launch": algo_csr},
+                         "fidelity_vs_matrix_free": fid},
+            "e2e": {"value": ws / per_e2e, "unit": "evolutions/s", "h2d_bytes_per_step": 8 * N,
+                    "d2h_bytes_per_step": 8 * N, "note": "host product state in, evolved state out"},
+            "clocks": clk.summary(), "gpu_launches": int(launches)}, {"unit": "evolutions/s"}
+
+
 # The reference's published single-kernel times at 20 qubits and its QV-20
 # end-to-end time (RTX 5090; README.md:152,160-167 of the reference).
 REF_MICRO_US = {"apply_gate": 4.2, "apply_gate_2q": 6.2, "apply_diagonal": 4.1, "apply_diagonal_phase": 2.1,
@@ -829,7 +920,8 @@ def E_launches(dev):
 
 
 WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
-             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy, "micro": bench_micro}
+             "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy, "micro": bench_micro,
+             "chebyshev": bench_chebyshev}
 
 
 # --------------------------------------------------------- CPU baseline
@@ -876,6 +968,29 @@ def cpu_baseline(workload: str, args) -> dict:
         dt = time.perf_counter() - t0
         return {"value": tot / dt, "unit": "trajectories/s", "cores": 1, "kind": "port",
                 "sample": f"{tot} trajectories of the same circuit (FP64 numpy restatement, one thread)"}
+    if workload == "chebyshev":
+        # scipy's expm_multiply (the reference's FP64 Chebyshev oracle family)
+        # on the same generator at 16 qubits, scaled by 2^(n-16) and by the
+        # ratio of the Chebyshev degrees (work per step ~ N x degree)
+        import scipy.sparse as sp
+        from scipy.sparse.linalg import expm_multiply
+        from blackwell_backend.chebyshev import chebyshev_coefficients
+        from qsim_b200.paulis import csr_from_paulis
+        n = args.qubits if args.qubits != 32 else 22
+        n_s = min(n, 16)
+        Hs = W.serving_hamiltonian(n_s, seed=n_s)
+        rp, ci, va = csr_from_paulis(Hs)
+        A = sp.csr_matrix((va.astype(np.complex128), ci, rp), shape=(1 << n_s, 1 << n_s))
+        psi = W.product_state(n_s, seed=n_s)
+        t0 = time.perf_counter()
+        expm_multiply(-1j * 10.0 * A, psi)
+        dt = time.perf_counter() - t0
+        k_s = chebyshev_coefficients(10.0, Hs.spectral_bound(), 1e-6)[1]
+        k_n = chebyshev_coefficients(10.0, W.serving_hamiltonian(n, seed=n).spectral_bound(), 1e-6)[1]
+        per = dt * 2 ** (n - n_s) * k_n / k_s
+        return {"value": 1.0 / per, "unit": "evolutions/s", "cores": cores, "kind": "port",
+                "sample": f"scipy expm_multiply (FP64) at {n_s} qubits, t = 10, x 2^{n - n_s} x degree ratio "
+                          f"{k_n}/{k_s} (extrapolated to {n} qubits)"}
     # circuits/s workloads: QV circuits at widths drawn as in the batch
     rng = np.random.default_rng(7)
     ws_ = rng.integers(10, 21, size=24)
