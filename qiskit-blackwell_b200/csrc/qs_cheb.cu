@@ -224,6 +224,93 @@ __global__ void k_chebp_fused(const PTerm* __restrict__ terms, int nterms, uint6
   }
 }
 
+// Up to 32 qubits the matrix-free recurrence uses 32-bit indices and splits
+// H into its diagonal and off-diagonal parts:
+//   * terms with x_t = 0 sum to a real diagonal D_i = sum_t c_t (-1)^{popc(i & z_t)},
+//     tabulated once per evolution (FP64 sums rounded to FP32, 4 B per
+//     amplitude), so the degree loop reads D_i instead of evaluating them;
+//   * the other terms are sorted by X mask and paired: both terms of a pair
+//     share one gather x[i ^ x] (e.g. X_a X_b and Y_a Y_b), and a lone term
+//     has a zero partner.  The sign (-1)^{popc(j & z)} is applied by flipping
+//     the sign bit of the weight.
+struct __align__(16) PPair { uint32_t x, z0, z1, pad; float w0r, w0i, w1r, w1i; };
+struct __align__(16) PDiag { uint64_t z; double c; };
+
+__global__ void k_chebp_diag(const PDiag* __restrict__ terms, int nterms, uint64_t n, float* __restrict__ D) {
+  extern __shared__ PDiag sd[];
+  for (int k = threadIdx.x; k < nterms; k += blockDim.x) sd[k] = terms[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    double d = 0.0;
+    for (int k = 0; k < nterms; ++k) d += (__popcll(i & sd[k].z) & 1) ? -sd[k].c : sd[k].c;
+    D[i] = (float)d;
+  }
+}
+
+__device__ __forceinline__ float flip_if(float w, uint32_t sbit) { return __int_as_float(__float_as_int(w) ^ sbit); }
+
+__device__ __forceinline__ float2 hx_row_pairs(const PPair* __restrict__ st, int npairs, const float2* __restrict__ x,
+                                               const float* __restrict__ D, uint32_t i) {
+  float re = 0.f, im = 0.f;
+  if (D) {
+    const float d = D[i];
+    const float2 v = x[i];
+    re = d * v.x;
+    im = d * v.y;
+  }
+  for (int k = 0; k < npairs; ++k) {
+    const PPair P = st[k];
+    const uint32_t j = i ^ P.x;
+    const float2 v = x[j];
+    const uint32_t s0 = (uint32_t)(__popc(j & P.z0) & 1) << 31, s1 = (uint32_t)(__popc(j & P.z1) & 1) << 31;
+    const float wr = flip_if(P.w0r, s0) + flip_if(P.w1r, s1);
+    const float wi = flip_if(P.w0i, s0) + flip_if(P.w1i, s1);
+    re = fmaf(wr, v.x, fmaf(-wi, v.y, re));
+    im = fmaf(wr, v.y, fmaf(wi, v.x, im));
+  }
+  return make_float2(re, im);
+}
+
+__global__ void k_chebp_first_pairs(const PPair* __restrict__ pairs, int npairs, uint64_t n,
+                                    const float* __restrict__ D, const float2* __restrict__ x0,
+                                    float2* __restrict__ x1, float2* __restrict__ out, float scale, float2 c0,
+                                    float2 c1) {
+  extern __shared__ PPair sp[];
+  for (int k = threadIdx.x; k < npairs; k += blockDim.x) sp[k] = pairs[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const float2 d = hx_row_pairs(sp, npairs, x0, D, (uint32_t)i);
+    const float2 t = make_float2(scale * d.x, scale * d.y);
+    x1[i] = t;
+    const float2 a0 = x0[i];
+    float2 a;
+    a.x = c0.x * a0.x - c0.y * a0.y;
+    a.y = c0.x * a0.y + c0.y * a0.x;
+    a.x = fmaf(c1.x, t.x, fmaf(-c1.y, t.y, a.x));
+    a.y = fmaf(c1.x, t.y, fmaf(c1.y, t.x, a.y));
+    out[i] = a;
+  }
+}
+
+__global__ void k_chebp_fused_pairs(const PPair* __restrict__ pairs, int npairs, uint64_t n,
+                                    const float* __restrict__ D, const float2* __restrict__ xk,
+                                    float2* __restrict__ xprev, float2* __restrict__ out, float two_scale,
+                                    float2 c) {
+  extern __shared__ PPair sp[];
+  for (int k = threadIdx.x; k < npairs; k += blockDim.x) sp[k] = pairs[k];
+  __syncthreads();
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const float2 d = hx_row_pairs(sp, npairs, xk, D, (uint32_t)i);
+    const float2 p = xprev[i];
+    const float2 t = make_float2(fmaf(two_scale, d.x, -p.x), fmaf(two_scale, d.y, -p.y));
+    xprev[i] = t;
+    float2 a = out[i];
+    a.x = fmaf(c.x, t.x, fmaf(-c.y, t.y, a.x));
+    a.y = fmaf(c.x, t.y, fmaf(c.y, t.x, a.y));
+    out[i] = a;
+  }
+}
+
 int pick_V(int64_t nrows, const int32_t* rp_dev, qs_context* h) {
   // mean row length from the first and last row pointers
   int32_t ends[2] = {0, 0};
@@ -357,18 +444,74 @@ int qs_cheb_evolve_pauli(qs_handle_t h, int n, const void* psi, void* out, const
     const int ny = __builtin_popcountll(xm[k] & zm[k]) & 3;
     T[k] = PTerm{xm[k], zm[k], (float)(coefs[k] * pr[ny]), (float)(coefs[k] * pim[ny]), 0.f, 0.f};
   }
-  PTerm* dT = (PTerm*)h->scratch_get(sizeof(PTerm) * nterms);
-  QS_CUDA(cudaMemcpyAsync(dT, T.data(), sizeof(PTerm) * nterms, cudaMemcpyHostToDevice, h->stream));
   const uint64_t N = 1ull << n;
   float2* x0 = (float2*)work;
   float2* x1 = x0 + N;
+  auto C = [&](int k) { return make_float2((float)coeffs[2 * k], (float)coeffs[2 * k + 1]); };
+  const float two_scale = (float)(2.0 * scale);
+  if (n <= 32) {
+    // diagonal terms and X-mask pairs (see PPair)
+    std::vector<PDiag> dg;
+    std::vector<int> off;
+    for (int k = 0; k < nterms; ++k) {
+      if (xm[k] == 0) dg.push_back(PDiag{zm[k], coefs[k]});
+      else off.push_back(k);
+    }
+    std::stable_sort(off.begin(), off.end(), [&](int a, int b) { return xm[a] < xm[b]; });
+    std::vector<PPair> pr;
+    for (size_t u = 0; u < off.size();) {
+      const PTerm& A = T[off[u]];
+      PPair P{(uint32_t)A.x, (uint32_t)A.z, 0u, 0u, A.wr, A.wi, 0.f, 0.f};
+      if (u + 1 < off.size() && xm[off[u + 1]] == xm[off[u]]) {
+        const PTerm& B = T[off[u + 1]];
+        P.z1 = (uint32_t)B.z;
+        P.w1r = B.wr;
+        P.w1i = B.wi;
+        u += 2;
+      } else {
+        u += 1;
+      }
+      pr.push_back(P);
+    }
+    const size_t pbytes = sizeof(PPair) * pr.size(), dbytes = sizeof(PDiag) * dg.size();
+    char* dmem = (char*)h->scratch_get(std::max<size_t>(16, pbytes + dbytes));
+    const PPair* dP = (const PPair*)dmem;
+    const PDiag* dD = (const PDiag*)(dmem + pbytes);
+    if (pbytes) QS_CUDA(cudaMemcpyAsync(dmem, pr.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
+    if (dbytes) QS_CUDA(cudaMemcpyAsync(dmem + pbytes, dg.data(), dbytes, cudaMemcpyHostToDevice, h->stream));
+    float* D = nullptr;
+    if (!dg.empty()) {
+      QS_CUDA(cudaMallocAsync((void**)&D, sizeof(float) * N, h->stream));
+      k_chebp_diag<<<qs_blocks_for(h, N, kThreads), kThreads, dbytes, h->stream>>>(dD, (int)dg.size(), N, D);
+      qs_after_launch(h, "k_chebp_diag");
+    }
+    try {
+      QS_CUDA(cudaMemcpyAsync(x0, psi, sizeof(float2) * N, cudaMemcpyDeviceToDevice, h->stream));
+      const unsigned grid = (unsigned)qs_blocks_for(h, N, kThreads, 8);
+      const int np = (int)pr.size();
+      k_chebp_first_pairs<<<grid, kThreads, pbytes, h->stream>>>(dP, np, N, D, x0, x1, (float2*)out,
+                                                                 (float)scale, C(0), C(1));
+      qs_after_launch(h, "k_chebp_first_pairs");
+      for (int k = 2; k <= K; ++k) {
+        k_chebp_fused_pairs<<<grid, kThreads, pbytes, h->stream>>>(dP, np, N, D, x1, x0, (float2*)out,
+                                                                   two_scale, C(k));
+        qs_after_launch(h, "k_chebp_fused_pairs");
+        std::swap(x0, x1);
+      }
+    } catch (...) {
+      if (D) cudaFreeAsync(D, h->stream);
+      throw;
+    }
+    if (D) QS_CUDA(cudaFreeAsync(D, h->stream));
+    return QS_OK;
+  }
+  PTerm* dT = (PTerm*)h->scratch_get(sizeof(PTerm) * nterms);
+  QS_CUDA(cudaMemcpyAsync(dT, T.data(), sizeof(PTerm) * nterms, cudaMemcpyHostToDevice, h->stream));
   QS_CUDA(cudaMemcpyAsync(x0, psi, sizeof(float2) * N, cudaMemcpyDeviceToDevice, h->stream));
   const unsigned grid = (unsigned)qs_blocks_for(h, N, kThreads, 8);
   const size_t smem = sizeof(PTerm) * nterms;
-  auto C = [&](int k) { return make_float2((float)coeffs[2 * k], (float)coeffs[2 * k + 1]); };
   k_chebp_first<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x0, x1, (float2*)out, (float)scale, C(0), C(1));
   qs_after_launch(h, "k_chebp_first");
-  const float two_scale = (float)(2.0 * scale);
   for (int k = 2; k <= K; ++k) {
     k_chebp_fused<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x1, x0, (float2*)out, two_scale, C(k));
     qs_after_launch(h, "k_chebp_fused");
