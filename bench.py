@@ -1047,8 +1047,9 @@ def main():
                 "config": {"workload": args.workload}, "data": "synthetic",
                 "cpu_baseline": {**info, "value": v},
                 "e2e": {"value": v, "unit": info["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                "note": "reference CPU path = FP64 statevector restatement (oracle/sv64.c); qiskit_aer is not "
-                        "installed and the reference's CUDA extension needs torch headers (not buildable here)"}
+                "note": "the reference has no CPU implementation of this path (its FP64 oracle is qiskit_aer, "
+                        "not installed, and its CUDA extension is not a CPU path): the FP64 CPU restatement "
+                        "named in cpu_baseline.sample stands in"}
         print(json.dumps(line))
         return 0
 
