@@ -17,11 +17,20 @@ Workloads (--workload):
             gradients, Chebyshev evolutions) at rates 50..2000 req/s through
             the continuous-batching server; value = served requests/s at the
             highest rate, p50/p99 per rate, serial plain execution beside it.
+  chebyshev exp(-iHt)|psi> at 22 qubits (84 Pauli terms, t = 10); value =
+            evolutions/s of the matrix-free path, the CSR path beside it.
+  noisy     12-qubit noisy brickwork, 8192 seeded trajectories per step;
+            value = trajectories/s.
+  micro     the reference's published single-operation times at 20 qubits
+            and QV-20 end to end with 8192 shots; value = circuits/s.
+  qv_plain  one QV circuit (--qubits) on the plain path.
 
---impl reference times the CPU implementation of the same workload: the FP64
-statevector restatement (oracle/sv64.c, OpenMP on all host cores) on a
-bounded sample, scaled to the metric's unit.  It is the only other place this
-file runs oracle/ code besides the cpu_baseline leg.
+--impl reference times the CPU implementation of the same workload on a
+bounded sample, scaled to the metric's unit, with every host core busy: the
+FP64 statevector restatement (oracle/sv64.c, OpenMP) for circuits, and for
+trajectories and evolutions one worker process per core (numpy trajectories,
+scipy expm_multiply).  It is the only other place this file runs oracle/ code
+besides the cpu_baseline leg.
 
 Multi-GPU (torchrun, one process per GPU): the workloads do not shard, so
 each rank runs an independent replica; value = total units / max-over-ranks
@@ -925,6 +934,49 @@ WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": ben
 
 
 # --------------------------------------------------------- CPU baseline
+def _cpu_worker(kind: str, n: int, seconds: float, seed0: int):
+    """One process of a parallel CPU sample (started with the spawn method):
+    runs work items of `kind` for about `seconds` on one thread; returns
+    (items done, elapsed seconds)."""
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+    sys.path[:0] = [os.path.join(ROOT, "qiskit-blackwell_b200", "python"), os.path.join(ROOT, "oracle")]
+    import numpy as np
+    import sv_oracle as O
+    from qsim_b200 import workloads as W
+    if kind == "noisy":
+        from qsim_b200.circuit import lower
+        ops = np.ascontiguousarray(lower(W.noisy_brickwork(n, 8, seed=5)))
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < seconds or k == 0:
+            O.noise_trajectory(n, ops, seed0 + k)
+            k += 1
+        return k, time.perf_counter() - t0
+    if kind == "chebyshev":
+        import scipy.sparse as sp
+        from scipy.sparse.linalg import expm_multiply
+        from qsim_b200.paulis import csr_from_paulis
+        H = W.serving_hamiltonian(n, seed=n)
+        rp, ci, va = csr_from_paulis(H)
+        A = sp.csr_matrix((va.astype(np.complex128), ci, rp), shape=(1 << n, 1 << n))
+        psi = W.product_state(n, seed=n)
+        t0 = time.perf_counter()
+        expm_multiply(-1j * 10.0 * A, psi)
+        return 1, time.perf_counter() - t0
+    raise ValueError(kind)
+
+
+def _parallel_rate(kind: str, n: int, seconds: float, procs: int):
+    """Items per second of `procs` concurrent _cpu_worker processes:
+    (total items, slowest worker's elapsed seconds)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")   # safe after CUDA initialisation
+    with ctx.Pool(procs) as pool:
+        res = pool.starmap(_cpu_worker, [(kind, n, seconds, 1_000_003 * w) for w in range(procs)])
+    return sum(r[0] for r in res), max(r[1] for r in res)
+
+
 def cpu_baseline(workload: str, args) -> dict:
     """FP64 CPU restatement (oracle/sv64.c, OpenMP, all host cores) on a
     bounded sample, scaled to the workload's unit."""
@@ -958,39 +1010,24 @@ def cpu_baseline(workload: str, args) -> dict:
                 "sample": f"{tot} runs of QV-20 + 8192 shots (FP64 C restatement, OpenMP)"}
     if workload == "noisy":
         n = args.qubits if args.qubits != 32 else 12
-        qc = W.noisy_brickwork(n, 8, seed=5)
-        ops = np.ascontiguousarray(__import__("qsim_b200.circuit", fromlist=["lower"]).lower(qc))
-        t0 = time.perf_counter()
-        tot = 0
-        while time.perf_counter() - t0 < 10 or tot == 0:
-            O.noise_trajectory(n, ops, tot)
-            tot += 1
-        dt = time.perf_counter() - t0
-        return {"value": tot / dt, "unit": "trajectories/s", "cores": 1, "kind": "port",
-                "sample": f"{tot} trajectories of the same circuit (FP64 numpy restatement, one thread)"}
+        tot, dt = _parallel_rate("noisy", n, 10.0, cores)
+        return {"value": tot / dt, "unit": "trajectories/s", "cores": cores, "kind": "port",
+                "sample": f"{tot} trajectories of the same circuit (FP64 numpy restatement), one process per "
+                          f"core for ~10 s"}
     if workload == "chebyshev":
         # scipy's expm_multiply (the reference's FP64 Chebyshev oracle family)
         # on the same generator at 16 qubits, scaled by 2^(n-16) and by the
         # ratio of the Chebyshev degrees (work per step ~ N x degree)
-        import scipy.sparse as sp
-        from scipy.sparse.linalg import expm_multiply
         from blackwell_backend.chebyshev import chebyshev_coefficients
-        from qsim_b200.paulis import csr_from_paulis
         n = args.qubits if args.qubits != 32 else 22
         n_s = min(n, 16)
-        Hs = W.serving_hamiltonian(n_s, seed=n_s)
-        rp, ci, va = csr_from_paulis(Hs)
-        A = sp.csr_matrix((va.astype(np.complex128), ci, rp), shape=(1 << n_s, 1 << n_s))
-        psi = W.product_state(n_s, seed=n_s)
-        t0 = time.perf_counter()
-        expm_multiply(-1j * 10.0 * A, psi)
-        dt = time.perf_counter() - t0
-        k_s = chebyshev_coefficients(10.0, Hs.spectral_bound(), 1e-6)[1]
+        tot, dt = _parallel_rate("chebyshev", n_s, 0.0, cores)
+        k_s = chebyshev_coefficients(10.0, W.serving_hamiltonian(n_s, seed=n_s).spectral_bound(), 1e-6)[1]
         k_n = chebyshev_coefficients(10.0, W.serving_hamiltonian(n, seed=n).spectral_bound(), 1e-6)[1]
-        per = dt * 2 ** (n - n_s) * k_n / k_s
+        per = dt / tot * 2 ** (n - n_s) * k_n / k_s
         return {"value": 1.0 / per, "unit": "evolutions/s", "cores": cores, "kind": "port",
-                "sample": f"scipy expm_multiply (FP64) at {n_s} qubits, t = 10, x 2^{n - n_s} x degree ratio "
-                          f"{k_n}/{k_s} (extrapolated to {n} qubits)"}
+                "sample": f"scipy expm_multiply (FP64), {tot} concurrent evolutions at {n_s} qubits (one process "
+                          f"per core), t = 10, x 2^{n - n_s} x degree ratio {k_n}/{k_s} (extrapolated to {n} qubits)"}
     # circuits/s workloads: QV circuits at widths drawn as in the batch
     rng = np.random.default_rng(7)
     ws_ = rng.integers(10, 21, size=24)
