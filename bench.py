@@ -1014,6 +1014,68 @@ def cpu_baseline(workload: str, args) -> dict:
         return {"value": tot / dt, "unit": "trajectories/s", "cores": cores, "kind": "port",
                 "sample": f"{tot} trajectories of the same circuit (FP64 numpy restatement), one process per "
                           f"core for ~10 s"}
+    if workload == "serving":
+        # The same request sequence executed one by one on the CPU, as a
+        # model: each kind is timed at a small width and scaled per request
+        # by 2^(w - w_s) and by its gate count or Chebyshev degree.
+        import scipy.sparse as sp
+        from scipy.sparse.linalg import expm_multiply
+        from blackwell_backend.chebyshev import chebyshev_coefficients
+        from qsim_b200.circuit import lower
+        from qsim_b200.paulis import csr_from_paulis
+        ws_ = 14
+        t0 = time.perf_counter()
+        psi = O.simulate(ws_, W.qv_ops(ws_, ws_, 1))
+        O.sample_indices(psi, np.random.default_rng(0).random(1024))
+        t_qv = time.perf_counter() - t0
+        qc, npar_s = W.efficient_su2(ws_, reps=4)
+        obs = W.random_pauli_observable(ws_, 256, seed=ws_)
+        th = np.random.default_rng(1).uniform(0, 2 * math.pi, npar_s)
+        t0 = time.perf_counter()
+        O.energy(ws_, lower(qc), th, obs.x, obs.z, obs.real_coefs())
+        t_en = time.perf_counter() - t0
+        Hs = W.serving_hamiltonian(ws_, seed=ws_)
+        rp, ci, va = csr_from_paulis(Hs)
+        A = sp.csr_matrix((va.astype(np.complex128), ci, rp), shape=(1 << ws_, 1 << ws_))
+        t0 = time.perf_counter()
+        expm_multiply(-1j * 10.0 * A, W.product_state(ws_, seed=ws_))
+        t_ev = time.perf_counter() - t0
+        k_s = chebyshev_coefficients(10.0, Hs.spectral_bound(), 1e-6)[1]
+        mix = ServingMix(args.requests, seed=4)
+        total = 0.0
+        for spc in mix.specs:
+            w = spc[1]
+            if spc[0] == "qv":
+                total += t_qv * 2.0 ** (w - ws_) * (w / ws_) ** 2
+            elif spc[0] == "grad":
+                total += 2 * (10 * w) * t_en * 2.0 ** (w - ws_) * (w / ws_)
+            else:
+                k_w = chebyshev_coefficients(spc[3], W.serving_hamiltonian(w, seed=w).spectral_bound(), 1e-6)[1]
+                total += t_ev * 2.0 ** (w - ws_) * k_w / k_s
+        return {"value": len(mix.specs) / total, "unit": "requests/s", "cores": cores, "kind": "port",
+                "sample": f"model of the {len(mix.specs)}-request mix run serially on the FP64 CPU restatements: "
+                          f"QV + 1024 shots, one energy and one expm_multiply (t = 10) timed at {ws_} qubits, "
+                          f"scaled per request by 2^(w-{ws_}) and gate count (gradients: parameter shift, 2 x "
+                          f"n_params energies) or Chebyshev degree"}
+    if workload == "adjoint":
+        # Parameter shift on the FP64 restatement: 2 x n_params energies per
+        # gradient (the reference has no gradient path; a statevector
+        # simulator without adjoint support differentiates this way).
+        from qsim_b200.circuit import lower
+        n = args.qubits if args.qubits != 32 else 20
+        qc, npar = W.efficient_su2(n, reps=4)
+        ops = lower(qc)
+        obs = W.random_pauli_observable(n, 256, seed=3)
+        theta = np.random.default_rng(8).uniform(0, 2 * math.pi, npar)
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < 10 or k == 0:
+            O.energy(n, ops, theta, obs.x, obs.z, obs.real_coefs())
+            k += 1
+        per_energy = (time.perf_counter() - t0) / k
+        return {"value": 1.0 / (2 * npar * per_energy), "unit": "gradients/s", "cores": cores, "kind": "port",
+                "sample": f"{k} FP64 energy evaluations at {n} qubits (C restatement, OpenMP, with the numpy "
+                          f"Pauli expectation), x {2 * npar} per parameter-shift gradient"}
     if workload == "chebyshev":
         # scipy's expm_multiply (the reference's FP64 Chebyshev oracle family)
         # on the same generator at 16 qubits, scaled by 2^(n-16) and by the
