@@ -59,3 +59,17 @@ def test_reference_arm_only_rank0_prints():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reference_arm_units_match_each_workload():
+    """The reference arm reports each workload in its metric's unit (the
+    driver divides the two arms' values), here on quick variants."""
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    for wl, extra, unit in (("serving", ["--requests", "20"], "requests/s"),
+                            ("adjoint", ["--qubits", "10"], "gradients/s")):
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", wl,
+                            "--steps", "1", "--warmup", "0", *extra], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr
+        line = json.loads(r.stdout.strip().splitlines()[-1])
+        assert line["unit"] == unit and line["cpu_baseline"]["unit"] == unit and line["value"] > 0, line
