@@ -1,8 +1,8 @@
 """Generate golden fixtures from the reference's own Python code.
 
 Run in a checkout that has the reference tree (read-only) at REF (default
-/root/reference, override with QSIM_REFERENCE).  Writes tests/golden/*.npz;
-the GPU box never needs the reference.
+/root/reference, override with QSIM_REFERENCE).  Writes tests/golden/*.npz,
+so the tests themselves never need the reference tree.
 
 Pieces of the reference that run on a CPU without qiskit and without its
 compiled extension:
