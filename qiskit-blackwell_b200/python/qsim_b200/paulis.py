@@ -98,32 +98,40 @@ class PauliSum:
         return H
 
 
-def csr_from_paulis(ps: PauliSum):
+def csr_from_paulis(ps: PauliSum, rows_per_chunk: int = 1 << 17):
     """CSR (row_ptr int32, col int32, val complex64) of the Pauli sum, FP64
-    accumulation, exact zeros dropped, columns sorted within each row."""
+    accumulation, exact zeros dropped, columns sorted within each row.
+
+    Row r holds one entry per distinct X mask, at column r ^ X.  Rows are
+    built in chunks: the entries of a chunk as a [rows, masks] array, each
+    row's entries sorted by column, zeros dropped."""
     n = ps.num_qubits
     N = 1 << n
-    rows = np.arange(N, dtype=np.uint64)
     xs = np.unique(ps.x)
-    vals = np.zeros((xs.size, N), dtype=np.complex128)
-    for k, X in enumerate(xs):
-        sel = ps.x == X
-        for z, c in zip(ps.z[sel], ps.coefs[sel]):
-            ny = bin(int(X & z)).count("1")
-            col_bits = rows ^ X  # column j = r ^ X ; sign from j & z
-            sgn = 1.0 - 2.0 * (np.bitwise_count(col_bits & z) & 1)
-            vals[k] += (c * (1j ** ny)) * sgn
-    cols = (rows[None, :] ^ xs[:, None]).astype(np.int64)  # [nx, N]
-    # per row: entries sorted by column
-    order = np.argsort(cols, axis=0, kind="stable")
-    cols_s = np.take_along_axis(cols, order, axis=0).T  # [N, nx]
-    vals_s = np.take_along_axis(vals, order, axis=0).T
-    keep = vals_s != 0
-    counts = keep.sum(axis=1)
+    slot = np.searchsorted(xs, ps.x)
+    # FP64 weight of each term: c * i^(number of Y factors)
+    w = [c * (1j ** bin(int(x & z)).count("1")) for x, z, c in zip(ps.x, ps.z, ps.coefs)]
+    counts = np.zeros(N, dtype=np.int64)
+    col_parts, val_parts = [], []
+    for r0 in range(0, N, rows_per_chunk):
+        rows = np.arange(r0, min(N, r0 + rows_per_chunk), dtype=np.uint64)
+        cols_t = xs[:, None] ^ rows[None, :]                             # [nx, R], contiguous per mask
+        vals_t = np.zeros(cols_t.shape, dtype=np.complex128)
+        for t in range(len(w)):
+            k = slot[t]
+            sgn = 1.0 - 2.0 * (np.bitwise_count(cols_t[k] & ps.z[t]) & 1)  # sign from column bits & z
+            vals_t[k] += w[t] * sgn
+        cols, vals = cols_t.T, vals_t.T                                  # [R, nx]
+        order = np.argsort(cols, axis=1, kind="stable")
+        cols_s = np.take_along_axis(cols, order, axis=1)
+        vals_s = np.take_along_axis(vals, order, axis=1)
+        keep = vals_s != 0
+        counts[r0: r0 + len(rows)] = keep.sum(axis=1)
+        col_parts.append(cols_s[keep].astype(np.int32))
+        val_parts.append(vals_s[keep].astype(np.complex64))
     row_ptr = np.zeros(N + 1, dtype=np.int64)
     np.cumsum(counts, out=row_ptr[1:])
     if row_ptr[-1] >= 2 ** 31:
         raise ValueError("CSR too large for int32 indices")
-    col_idx = cols_s[keep].astype(np.int32)
-    values = vals_s[keep].astype(np.complex64)
-    return row_ptr.astype(np.int32), col_idx, values
+    return (row_ptr.astype(np.int32), np.concatenate(col_parts) if col_parts else np.zeros(0, np.int32),
+            np.concatenate(val_parts) if val_parts else np.zeros(0, np.complex64))
