@@ -308,7 +308,9 @@ int qs_cheb_evolve(qs_handle_t h, const int32_t* row_ptr, const int32_t* col_idx
 /* Matrix-free form of qs_cheb_evolve: H = sum_t coefs[t] P_t given by Pauli
  * masks (as qs_expect_pauli_sum), applied on the fly, so no CSR bytes are
  * read (the reference always builds a CSR, blackwell_backend/hamiltonian.py:45-69).
- * work: 2 * 2^n complex64. */
+ * work: 2 * 2^n complex64.  Up to 32 qubits the terms without X or Y factors
+ * are tabulated once as a real diagonal (4 B per amplitude, a stream-ordered
+ * allocation freed by the call) and the others are paired by X mask. */
 int qs_cheb_evolve_pauli(qs_handle_t h, int n_qubits, const void* psi, void* out, const uint64_t* x_masks,
                          const uint64_t* z_masks, const double* coefs, int n_terms, const double* coeffs, int K,
                          double scale, void* work);
