@@ -66,7 +66,9 @@ def test_reference_arm_units_match_each_workload():
     driver divides the two arms' values), here on quick variants."""
     env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
     for wl, extra, unit in (("serving", ["--requests", "20"], "requests/s"),
-                            ("adjoint", ["--qubits", "10"], "gradients/s")):
+                            ("adjoint", ["--qubits", "10"], "gradients/s"),
+                            ("chebyshev", ["--qubits", "12"], "evolutions/s"),
+                            ("noisy", ["--qubits", "6"], "trajectories/s")):
         r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", wl,
                             "--steps", "1", "--warmup", "0", *extra], env=env, capture_output=True, text=True,
                            timeout=300)
