@@ -280,7 +280,11 @@ int qs_expect_pauli_sum(qs_handle_t h, const void* state, int n_qubits,
  * fail with QS_ERR_INVALID.  All calls share that array: calls that overlap on
  * the GPU race and must be serialised by the caller.  The first call on a
  * device looks up the array's address (cudaGetSymbolAddress); make it before
- * any stream capture begins. */
+ * any stream capture begins.  With lazy module loading (the CUDA default)
+ * that first call is also when the driver places the array in device
+ * memory, so a caller that accounts for every byte makes a warm-up call at
+ * start-up.  The address is kept until exit: do not use the library on a
+ * device after cudaDeviceReset. */
 #define QS_NOALLOC_MAX_TERMS 1024
 int qs_expect_pauli_sum_noalloc(qs_handle_t h, const void* state, int n_qubits,
                                 const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,

@@ -182,3 +182,26 @@ double sv64_max_abs_err_c64(const float* a, const cplx* b, int n) {
   }
   return m;
 }
+
+/* sum_t c_t <psi|P_t|psi> with P = i^{|x&z|} X^x Z^z, in FP64: the same
+ * definition as the numpy restatement sv_oracle.pauli_expectation (and the
+ * reference's expectation_pauli, bwk/csrc/expectation_sm120.cu:100-163,
+ * generalised to any X/Y/Z string). */
+double sv64_expect_pauli(const cplx* psi, int n, const uint64_t* x, const uint64_t* z, const double* c,
+                         int nterms) {
+  const uint64_t N = 1ull << n;
+  double tot = 0.0;
+  for (int t = 0; t < nterms; ++t) {
+    const int ny = __builtin_popcountll(x[t] & z[t]) & 3;
+    const cplx ph = ny == 0 ? 1.0 : ny == 1 ? I : ny == 2 ? -1.0 : -I;
+    double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+    for (int64_t i = 0; i < (int64_t)N; ++i) {
+      const uint64_t j = (uint64_t)i ^ x[t];
+      const double sg = (__builtin_popcountll(j & z[t]) & 1) ? -1.0 : 1.0;
+      acc += creal(conj(psi[i]) * ph * sg * psi[j]);
+    }
+    tot += c[t] * acc;
+  }
+  return tot;
+}

@@ -54,6 +54,8 @@ def lib():
         L.sv64_fidelity_c64.restype = C.c_double
         L.sv64_max_abs_err_c64.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.sv64_max_abs_err_c64.restype = C.c_double
+        L.sv64_expect_pauli.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.sv64_expect_pauli.restype = C.c_double
         _lib = L
     return _lib
 
@@ -181,6 +183,18 @@ def sample_indices(psi: np.ndarray, u: np.ndarray) -> np.ndarray:
     return np.minimum(out, psi.size - 1)
 
 
+def pauli_expectation_c(psi: np.ndarray, x, z, c) -> float:
+    """pauli_expectation by the C oracle (FP64, OpenMP): for 20+ qubits and
+    hundreds of terms, where the numpy loop takes seconds per call."""
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = int(psi.size).bit_length() - 1
+    x = np.ascontiguousarray(x, dtype=np.uint64)
+    z = np.ascontiguousarray(z, dtype=np.uint64)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    return float(lib().sv64_expect_pauli(psi.ctypes.data, n, x.ctypes.data, z.ctypes.data, c.ctypes.data,
+                                         int(c.size)))
+
+
 def pauli_expectation(psi: np.ndarray, x, z, c) -> float:
     """sum_t c_t <psi|P_t|psi>, P = i^{|x&z|} X^x Z^z."""
     idx = np.arange(psi.size, dtype=np.uint64)
@@ -211,7 +225,10 @@ def energy(n: int, ops, params_row, x, z, c) -> float:
     ops = np.array(_ops(ops), copy=True)
     sel = ops["param"] >= 0
     ops["m"][sel, 0] = np.asarray(params_row, dtype=np.float64)[ops["param"][sel]]
-    return pauli_expectation(simulate(n, ops), x, z, c)
+    psi = simulate(n, ops)
+    if n >= 14:
+        return pauli_expectation_c(psi, x, z, c)
+    return pauli_expectation(psi, x, z, c)
 
 
 def grad_central_fd(n, ops, params_row, x, z, c, which, h=1e-3):

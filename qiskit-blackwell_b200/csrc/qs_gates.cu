@@ -407,18 +407,27 @@ int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n, const 
 
 // Gates whose matrix is a device array (complex64, row-major): the kernel
 // reads it, so the call neither copies it to the host nor waits for the
-// stream.  The pointer must be device (or managed) memory.
-// The last pointer that passed is remembered per handle (a gate tensor is
-// usually reused call after call): under unified addressing a device
-// address never becomes a pageable host address.
+// stream.  The pointer must be device memory of the handle's own GPU (or
+// managed memory): a gate on another GPU would be read across the link, or
+// fault when peer access is off.
+// The last pointer that passed is remembered per handle together with the
+// device it was checked for (a gate tensor is usually reused call after
+// call).  An address that was freed and handed out again by another
+// allocation of the same GPU is still device memory of that GPU, so the
+// remembered answer stays true for it.
 static void check_dev_ptr(qs_context* h, const void* p, const char* what) {
   QS_CHECK_ARG(p != nullptr && ((uintptr_t)p & 7u) == 0, std::string(what) + " must be 8-byte aligned");
-  if (p == h->dev_ptr_ok) return;
+  if (p == h->dev_ptr_ok && h->dev_ptr_ok_device == h->device) return;
   cudaPointerAttributes a;
   const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) (void)cudaGetLastError();  // clear the sticky-free error state of the query
   QS_CHECK_ARG(e == cudaSuccess && (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged),
                std::string(what) + " is not device memory");
+  QS_CHECK_ARG(a.type == cudaMemoryTypeManaged || a.device == h->device,
+               std::string(what) + " is device memory of GPU " + std::to_string(a.device) +
+                   ", not of the handle's GPU " + std::to_string(h->device));
   h->dev_ptr_ok = p;
+  h->dev_ptr_ok_device = h->device;
 }
 
 int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int t) {

@@ -51,6 +51,7 @@ struct qs_context {
   int jit_min_qubits = 24;
   int64_t launches = 0;
   const void* dev_ptr_ok = nullptr;  // last pointer found to be device memory (qs_apply_*_dev)
+  int dev_ptr_ok_device = -1;        // the device dev_ptr_ok was checked against
 
   // grow-only device scratch (reductions, sampling partials, ...)
   void* scratch = nullptr;

@@ -14,8 +14,12 @@
 // Limits and sharing rules:
 //   * at most QS_NOALLOC_MAX_TERMS (1024) Pauli terms per call; the block
 //     partials never exceed 1024 (the same slicing as qs_expect_pauli_sum);
-//   * every GPU that loads libqsim holds the array (about 40 KiB) until the
-//     process exits;
+//   * every GPU that uses it holds the array (about 40 KiB) until the process
+//     exits.  With lazy module loading (CUDA_MODULE_LOADING=LAZY, the
+//     default) the driver loads this file's module, and so places the array
+//     in device memory, at the first call on each device: that first call is
+//     the one that takes device memory, so a caller that accounts for every
+//     byte makes a warm-up call at start-up;
 //   * all calls share it and it keeps the previous call's contents: nothing in
 //     it has to start at zero (each call writes the term table, every block's
 //     partial and the result before reading them), but calls that overlap on
@@ -23,7 +27,9 @@
 //     serialised by the caller;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins.
+//     before any stream capture begins.  The address is kept for the life of
+//     the process: after cudaDeviceReset (which also ends every handle's
+//     streams) libqsim must not be used on that device again.
 #include "qs_api.h"
 #include "qs_common.cuh"
 #include <mutex>

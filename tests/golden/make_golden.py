@@ -1,8 +1,10 @@
 """Generate golden fixtures from the reference's own Python code.
 
-Run in a checkout that has the reference tree (read-only) at REF (default
-/root/reference, override with QSIM_REFERENCE).  Writes tests/golden/*.npz,
-so the tests themselves never need the reference tree.
+Run with QSIM_REFERENCE set to the root of a checkout of the reference
+project (read-only is enough), e.g.
+``QSIM_REFERENCE=<path to the reference> python tests/golden/make_golden.py``.
+Writes tests/golden/*.npz, so the tests themselves never need the reference
+tree.
 
 Pieces of the reference that run on a CPU without qiskit and without its
 compiled extension:
@@ -21,7 +23,7 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("QSIM_REFERENCE", "/root/reference")
+REF = os.environ.get("QSIM_REFERENCE", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -65,6 +67,8 @@ def cheb():
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set QSIM_REFERENCE to the root of a checkout of the reference project")
     qv8()
     qv4()
     cheb()

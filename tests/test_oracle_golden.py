@@ -216,3 +216,16 @@ def test_oracle_sampling_and_expectation_semantics():
     y = O.pauli_expectation(psi, [1], [1], [1.0])
     Y = np.kron(np.eye(8), np.array([[0, -1j], [1j, 0]]))
     assert abs(y - np.real(np.vdot(psi, Y @ psi))) < 1e-12
+
+
+@pytest.mark.parametrize("n", [3, 9, 14])
+def test_c_pauli_expectation_equals_numpy(n):
+    """The C oracle's Pauli-sum expectation (used for 20+ qubits) against the
+    numpy restatement, X/Y/Z strings of weight 1-4 with Y phases."""
+    rng = np.random.default_rng(n)
+    psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    psi /= np.linalg.norm(psi)
+    ps = W.random_pauli_observable(n, 48, seed=n + 1, wmax=min(4, n))
+    a = O.pauli_expectation(psi, ps.x, ps.z, ps.real_coefs())
+    b = O.pauli_expectation_c(psi, ps.x, ps.z, ps.real_coefs())
+    assert abs(a - b) <= 1e-12 * max(1.0, abs(a))

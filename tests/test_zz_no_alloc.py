@@ -22,7 +22,7 @@ def _observable(n, n_terms, seed):
     x = np.zeros(n_terms, dtype=np.uint64)
     z = np.zeros(n_terms, dtype=np.uint64)
     for k in range(n_terms):
-        for q in rng.choice(n, int(rng.integers(1, 5)), replace=False):
+        for q in rng.choice(n, min(n, int(rng.integers(1, 5))), replace=False):
             p = int(rng.integers(1, 4))          # 1 = X, 2 = Y, 3 = Z
             if p in (1, 2):
                 x[k] |= np.uint64(1 << int(q))
@@ -47,7 +47,10 @@ def test_noalloc_expectation_matches_allocating_entry_point():
     try:
         u64 = C.POINTER(C.c_uint64)
         f64 = C.POINTER(C.c_double)
-        for call, (n, nt) in enumerate([(14, 200), (18, 64)]):   # two calls in a row
+        # two calls in a row, then the two ends of the fixed scratch: the
+        # full 1024-term table with all 1024 block partials (n = 22), and a
+        # one-qubit state (one block)
+        for call, (n, nt) in enumerate([(14, 200), (18, 64), (22, 1024), (1, 3)]):
             s = _state(n, 10 + call)
             x, z, c = _observable(n, nt, 20 + call)
             torch.cuda.synchronize()
