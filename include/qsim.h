@@ -126,6 +126,21 @@ int  qs_set_jit(qs_handle_t h, int mode, int min_qubits);
 /* Number of kernels this handle has launched since creation; h = NULL gives
  * the count over every handle of the process.                               */
 int64_t qs_launch_count(qs_handle_t h);
+/* Status word of the handle's device-side waits.  The specialised tile
+ * passes of 10..13-qubit tiles run as pipelined kernels (TMA copies through
+ * a ring of shared-memory stages, producer and consumer warps synchronised
+ * by mbarriers); every one of their waits is bounded, and a wait that runs
+ * out ORs a cause into this word (1: the copy warp, 2: the compute warps)
+ * and its CTA returns, leaving that part of the state unfinished.  Waits on
+ * the handle's stream, stores the word in *code (0 = no wait ran out) and
+ * clears it.  No reference counterpart (the reference has no device-side
+ * waits).                                                                   */
+int qs_device_status(qs_handle_t h, int* code);
+/* Test hook for the above: with on = 1, the next pipelined tile pass this
+ * handle launches withholds its first tile's copy and gives its waits 50 ms,
+ * so its bounded waits run out and qs_device_status reports them; the hook
+ * then switches itself off.  No reference counterpart.                     */
+int qs_set_wait_test(qs_handle_t h, int on);
 
 /* ------------------------------------------------------------ states ----- */
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:109-113,210-224 (state_init) */

@@ -101,6 +101,8 @@ int qs_create(int device, qs_handle_t* out) {
   QS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
   QS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
+  QS_CUDA(cudaMalloc(&h->dev_status, 256));
+  QS_CUDA(cudaMemset(h->dev_status, 0, 256));
   *out = h;
   return QS_OK;
   }
@@ -127,6 +129,7 @@ int qs_destroy(qs_handle_t h) {
     cudaStreamDestroy(h->upload_stream);
   }
   if (h->scratch) cudaFree(h->scratch);
+  if (h->dev_status) cudaFree(h->dev_status);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -182,5 +185,24 @@ int qs_set_jit(qs_handle_t h, int mode, int min_qubits) {
 }
 
 int64_t qs_launch_count(qs_handle_t h) { return h ? h->launches : g_launches.load(); }
+
+int qs_device_status(qs_handle_t h, int* code) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(code != nullptr, "code is null");
+  uint32_t w = 0;
+  QS_CUDA(cudaMemcpyAsync(&w, h->dev_status, sizeof(w), cudaMemcpyDeviceToHost, h->stream));
+  QS_CUDA(cudaStreamSynchronize(h->stream));
+  *code = (int)w;
+  if (w) QS_CUDA(cudaMemsetAsync(h->dev_status, 0, sizeof(w), h->stream));
+  QS_API_END(h)
+}
+
+int qs_set_wait_test(qs_handle_t h, int on) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  h->wait_test = on ? 1 : 0;
+  QS_API_END(h)
+}
 
 }  // extern "C"

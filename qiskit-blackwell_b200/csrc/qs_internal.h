@@ -50,6 +50,13 @@ struct qs_context {
   int jit_mode = 1;
   int jit_min_qubits = 24;
   int64_t launches = 0;
+  // Device status word of the pipelined tile passes: a kernel whose bounded
+  // wait gave up ORs a cause into it (1 producer, 2 consumers); read and
+  // cleared by qs_device_status.  Allocated at the first pipelined launch.
+  uint32_t* dev_status = nullptr;
+  // Test hook (qs_set_wait_test): the next pipelined pass withholds its first
+  // tile so that the consumers' bounded wait runs out.
+  int wait_test = 0;
   const void* dev_ptr_ok = nullptr;  // last pointer found to be device memory (qs_apply_*_dev)
   int dev_ptr_ok_device = -1;        // the device dev_ptr_ok was checked against
 
@@ -163,6 +170,14 @@ struct JitJob;
 struct JitPass {
   void* fn = nullptr;  // CUfunction
   int threads = 0, smem = 0, per_sm = 0;
+  // Pipelined passes (qs_jit.cpp): tiles move by TMA through a ring of
+  // shared-memory stages; the kernel takes a tensor map of the state whose
+  // dimensions start at the bits st[0..rank-1] (st[0] = 0, 8-byte elements)
+  // and whose box spans 2^boxb[d] elements in dimension d.
+  int pipe = 0;
+  int rank = 0;
+  int st[5] = {0, 0, 0, 0, 0};
+  int boxb[5] = {0, 0, 0, 0, 0};
 };
 
 struct qs_plan_s {

@@ -51,6 +51,7 @@ struct Api {
   decltype(&cuFuncSetAttribute) FuncSetAttribute = nullptr;
   decltype(&cuLaunchKernel) LaunchKernel = nullptr;
   decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) Occupancy = nullptr;
+  decltype(&cuTensorMapEncodeTiled) EncodeTiled = nullptr;  // optional: pipelined passes
 };
 
 Api& g_api = *new Api;  // never destroyed (background compiles may outlive main)
@@ -91,6 +92,7 @@ void load_api() {
              sym(cu, "cuLaunchKernel", g_api.LaunchKernel) &&
              sym(cu, "cuOccupancyMaxActiveBlocksPerMultiprocessor", g_api.Occupancy)) {
     g_api.driver_ok = true;
+    sym(cu, "cuTensorMapEncodeTiled", g_api.EncodeTiled);
   } else {
     g_api.why_driver = "a CUDA driver entry point is missing";
   }
@@ -548,6 +550,406 @@ std::string gen_pass(const DevPass& P, const DevBlock* blocks, const DevOp* ops,
   return s.str();
 }
 
+// ------------------------------------------------ pipelined tile passes
+// A persistent kernel per pass: one CTA per SM (two for 12-qubit tiles)
+// walks its tiles through a ring of NS shared-memory stages.  One producer
+// warp moves tiles with TMA tensor copies (cp.async.bulk.tensor): loads
+// complete on the stage's "full" mbarrier, and a stage whose tile the
+// consumers have finished (its "done" mbarrier) is written back by a TMA
+// store and, once the store has read it, refilled with the tile NS ahead.
+// The consumer warps run the pass's register blocks on the stage, so the
+// next tile's load, this tile's arithmetic and the previous tile's store
+// overlap.  Every wait is bounded: a wait that runs out ORs a cause into the
+// handle's status word and the CTA returns after its copies in flight end.
+//
+// The tensor map views the state as up to 5 dimensions of 8-byte elements:
+// dimension 0 covers bits [0, st1) with a box of 16 amplitudes (128 bytes,
+// the 128-byte swizzle span), dimension d covers [st_d, st_{d+1}) with a box
+// over the tile run that starts at st_d.  A tile's high positions form runs
+// of consecutive qubits; the (at most 4) longest runs become box dimensions
+// and the other positions are walked by issuing one box per combination.
+// In shared memory a box is row-major over its dimensions, boxes follow one
+// another, and the hardware swizzle XORs address bits [4:6] with [7:9]; so
+// amplitude i of the tile (bit k = qubit S[k]) sits at a linear (XOR) image
+// of i that the generator folds into every register block's addresses.
+struct PipeShape {
+  int rank = 0;
+  int st[5] = {0, 0, 0, 0, 0};
+  int boxb[5] = {0, 0, 0, 0, 0};
+  int box_bits = 0;          // log2 amplitudes per box
+  std::vector<int> U;        // high tile positions (global qubits) walked box by box
+  std::vector<uint32_t> A;   // A[k]: shared-memory amplitude index of tile bit k (swizzled)
+};
+
+constexpr int kPipeStages = 3;
+
+bool pipe_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_TMA_PASS");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+
+// The pipelined kernel handles 10..13-qubit tiles that hold qubits 0..3
+// (every tile the planner builds does) on states of at most 32 qubits (the
+// dimension-0 coordinate is a signed 32-bit value).
+bool pipe_shape(const DevPass& P, PipeShape& sh) {
+  const int T = P.T;
+  if (!pipe_enabled() || T < 10 || T > 13 || P.n_qubits > 32) return false;
+  for (int k = 0; k < 4; ++k)
+    if (P.S[k] != k) return false;
+  std::vector<std::pair<int, int>> runs;  // (first qubit, length)
+  for (int k = 4; k < T; ++k) {
+    if (!runs.empty() && runs.back().first + runs.back().second == P.S[k]) ++runs.back().second;
+    else runs.push_back({P.S[k], 1});
+  }
+  std::vector<std::pair<int, int>> pieces;  // a box dimension spans at most 256 elements
+  for (auto r : runs) {
+    while (r.second > 8) {
+      pieces.push_back({r.first, 8});
+      r.first += 8;
+      r.second -= 8;
+    }
+    pieces.push_back(r);
+  }
+  std::vector<int> idx(pieces.size());
+  for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return pieces[a].second > pieces[b].second; });
+  idx.resize(std::min<size_t>(4, idx.size()));
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return pieces[a].first < pieces[b].first; });
+  sh.rank = 1 + (int)idx.size();
+  sh.st[0] = 0;
+  sh.boxb[0] = 4;
+  sh.box_bits = 4;
+  std::vector<int> smem_bit(64, -1);  // qubit -> shared-memory index bit
+  for (int q = 0; q < 4; ++q) smem_bit[q] = q;
+  for (size_t d = 0; d < idx.size(); ++d) {
+    const auto& pc = pieces[idx[d]];
+    sh.st[d + 1] = pc.first;
+    sh.boxb[d + 1] = pc.second;
+    for (int o = 0; o < pc.second; ++o) smem_bit[pc.first + o] = sh.box_bits + o;
+    sh.box_bits += pc.second;
+  }
+  if (sh.rank < 2 || sh.st[1] > 31 || sh.box_bits < 7) return false;  // swizzle atoms of 1024 bytes
+  int next = sh.box_bits;
+  for (int k = 4; k < T; ++k)
+    if (smem_bit[P.S[k]] < 0) {
+      sh.U.push_back(P.S[k]);
+      smem_bit[P.S[k]] = next++;
+    }
+  sh.A.resize(T);
+  for (int k = 0; k < T; ++k) {
+    const uint32_t m = 1u << smem_bit[P.S[k]];
+    sh.A[k] = m ^ (((m >> 4) & 7u) << 1);  // 128-byte swizzle, in amplitude units
+  }
+  return true;
+}
+
+// Lane bits of a register block: the 5 non-register tile bits that put a
+// warp's 32 groups on the most shared-memory banks (8-byte accesses: address
+// bits 0..3; 16-byte pair accesses: bits 1..3), then the rest in order.
+std::vector<int> lane_order(const std::vector<int>& nr, const std::vector<uint32_t>& A, bool pair) {
+  std::vector<int> order;
+  std::vector<uint32_t> basis;
+  auto reduce = [&](uint32_t v) {
+    for (uint32_t b : basis) v = std::min(v, v ^ b);
+    return v;
+  };
+  for (int k : nr) {
+    if (order.size() >= 5) break;
+    const uint32_t v = reduce(pair ? (A[k] >> 1) & 7u : A[k] & 15u);
+    if (v) {
+      basis.push_back(v);
+      std::sort(basis.rbegin(), basis.rend());
+      order.push_back(k);
+    }
+  }
+  for (int k : nr)
+    if (std::find(order.begin(), order.end(), k) == order.end()) order.push_back(k);
+  return order;
+}
+
+std::string gen_block_fn_pipe(int b, const DevBlock& B, int T, int R, int nc, const DevOp* ops, const float2* coef,
+                              bool inline_fn, const std::vector<uint32_t>& A) {
+  const int J = 1 << R;
+  const uint32_t ngroups = 1u << (T - R);
+  std::vector<int> nr;
+  for (int k = 0; k < T; ++k) {
+    bool reg = false;
+    for (int r = 0; r < R; ++r) reg |= (B.pos[r] == k);
+    if (!reg) nr.push_back(k);
+  }
+  const bool pair = B.pos[0] == 0;  // register bit 0 is tile bit 0: (j, j|1) are adjacent
+  const std::vector<int> ord = lane_order(nr, A, pair);
+  std::vector<uint32_t> off(J);
+  for (int j = 0; j < J; ++j) {
+    uint32_t x = 0;
+    for (int k = 0; k < R; ++k)
+      if ((j >> k) & 1) x ^= A[B.pos[k]];
+    off[j] = x;
+  }
+  Block G;
+  G.v.resize(J);
+  for (int j = 0; j < J; ++j) G.v[j] = "v" + std::to_string(j);
+  gen_block(G, R, ops, B.op_begin, B.op_end, coef);
+  std::ostringstream o;
+  o << "__device__ " << (inline_fn ? "__forceinline__" : "__noinline__") << " void blk" << b
+    << "(u32 soff, u64 gbase, const u64* __restrict__ dep_lo, u32 tid) {\n";
+  o << "  float2* tile = reinterpret_cast<float2*>(smem_raw + soff);\n";
+  o << "  #pragma unroll 1\n";
+  o << "  for (u32 g = tid; g < " << ngroups << "u; g += " << nc << "u) {\n";
+  o << "      u32 pb = 0u;\n";
+  if (G.uses_g) o << "      u32 base = 0u;\n";
+  for (size_t j = 0; j < ord.size(); ++j) {
+    o << "      { const u32 m_ = 0u - ((g >> " << j << ") & 1u); pb ^= m_ & " << A[ord[j]] << "u;";
+    if (G.uses_g) o << " base |= m_ & " << (1u << ord[j]) << "u;";
+    o << " }\n";
+  }
+  if (G.uses_g) {
+    if (B.pos[7] != 0) o << "      const u64 gidx = gbase | dep_lo[base & 127u] | dep_lo[128u + (base >> 7)];\n";
+    else o << "      const u64 gidx = 0ull;\n";
+  }
+  // address of amplitude j: pb ^ off[j] = (pb ^ lo) + hi (pb and hi share
+  // no bit at or above bit 4, and the swizzle only rewrites bits 1..3)
+  std::map<uint32_t, std::string> lo_addr;
+  auto addr = [&](int j) {
+    const uint32_t lo = off[j] & 15u, hi = off[j] & ~15u;
+    auto it = lo_addr.find(lo);
+    if (it == lo_addr.end()) {
+      const std::string n = "pa" + std::to_string(lo);
+      o << "      const u32 " << n << " = pb ^ " << lo << "u;\n";
+      it = lo_addr.emplace(lo, n).first;
+    }
+    return it->second + " + " + std::to_string(hi) + "u";
+  };
+  for (int j = 0; j < J; ++j) {
+    if (pair && (j & 1)) continue;
+    const std::string a = addr(j);
+    if (pair) {
+      o << "      const float4 w" << j << " = *reinterpret_cast<const float4*>(tile + (" << a << "));\n";
+      o << "      const float2 v" << j << " = make_float2(w" << j << ".x, w" << j << ".y);\n";
+      o << "      const float2 v" << (j + 1) << " = make_float2(w" << j << ".z, w" << j << ".w);\n";
+    } else {
+      o << "      const float2 v" << j << " = tile[" << a << "];\n";
+    }
+  }
+  o << G.o.str();
+  for (int j = 0; j < J; ++j) {
+    if (pair && (j & 1)) continue;
+    if (pair)
+      o << "      *reinterpret_cast<float4*>(tile + (" << addr(j) << ")) = make_float4(" << G.v[j] << ".x, " << G.v[j]
+        << ".y, " << G.v[j + 1] << ".x, " << G.v[j + 1] << ".y);\n";
+    else
+      o << "      tile[" << addr(j) << "] = " << G.v[j] << ";\n";
+  }
+  o << "  }\n}\n";
+  return o.str();
+}
+
+const char* kPipePrelude = R"(
+struct __align__(64) TMap { unsigned long long v[16]; };
+__device__ __forceinline__ u32 su32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ u64 gtimer() { u64 t; asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t)); return t; }
+__device__ __forceinline__ void mb_init(u32 b, u32 n) { asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(b), "r"(n) : "memory"); }
+__device__ __forceinline__ void mb_arrive(u32 b) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" :: "r"(b) : "memory");
+}
+__device__ __forceinline__ void mb_expect(u32 b, u32 bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" :: "r"(b), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mb_try(u32 b, u32 par) {
+  u32 ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(b), "r"(par) : "memory");
+  return ok != 0u;
+}
+// Bounded wait for the phase of parity `par`: false once `limit` ns passed.
+__device__ __forceinline__ bool mb_wait(u32 b, u32 par, u64 limit) {
+  if (mb_try(b, par)) return true;
+  const u64 t0 = gtimer();
+  for (;;) {
+    if (mb_try(b, par)) return true;
+    if (gtimer() - t0 > limit) return false;
+  }
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" :: "n"(QS_NC) : "memory"); }
+)";
+
+std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp* ops, const float2* coef,
+                          const PipeShape& sh, int min_blocks) {
+  const int T = P.T, R = P.R;
+  const int nc = std::min(256, 1 << (T - R));  // consumer threads (a multiple of 32: T - R >= 5)
+  const uint32_t tile_bytes = 8u << T;
+  const int nbox = 1 << sh.U.size();
+  const uint32_t box_bytes = 8u << sh.box_bits;
+  std::ostringstream s;
+  s << kPrelude;
+  s << "#define QS_NC " << nc << "\n";
+  s << kPipePrelude;
+  s << "extern __shared__ __align__(1024) unsigned char smem_raw[];\n";
+  s << "__device__ const u64 kDep[256] = {";
+  for (int e = 0; e < 256; ++e) {
+    const int part = e >> 7, x = e & 127;
+    uint64_t d = 0;
+    for (int k = 0; k < 7; ++k) {
+      const int kk = part * 7 + k;
+      if (kk < T && ((x >> k) & 1)) d |= 1ull << P.S[kk];
+    }
+    s << (e ? "," : "") << d << "ull";
+  }
+  s << "};\n";
+  const bool inline_blocks = P.nblocks <= 4;
+  for (int b = 0; b < P.nblocks; ++b) s << gen_block_fn_pipe(b, blocks[b], T, R, nc, ops, coef, inline_blocks, sh.A);
+  // global index of the first amplitude of tile t
+  s << "__device__ __forceinline__ u64 tile_base(u64 t) {\n  u64 g = t;\n";
+  for (int k = 0; k < T; ++k) s << "  g = ins0(g, " << P.S[k] << ");\n";
+  s << "  return g;\n}\n";
+  // one TMA box: global start g -> coordinates
+  const int rk = sh.rank;
+  auto coords = [&](std::ostringstream& o) {
+    o << "      const int c0 = (int)(g & " << ((1ull << sh.st[1]) - 1ull) << "ull);\n";
+    for (int d = 1; d < rk; ++d) {
+      if (d + 1 < rk)
+        o << "      const int c" << d << " = (int)((g >> " << sh.st[d] << ") & " << ((1ull << (sh.st[d + 1] - sh.st[d])) - 1ull)
+          << "ull);\n";
+      else
+        o << "      const int c" << d << " = (int)(g >> " << sh.st[d] << ");\n";
+    }
+  };
+  auto clist = [&]() {
+    std::string c;
+    for (int d = 0; d < rk; ++d) c += (d ? ", %" : "%") + std::to_string(d + 2);
+    return c;
+  };
+  auto cargs = [&]() {
+    std::string c;
+    for (int d = 0; d < rk; ++d) c += ", \"r\"(c" + std::to_string(d) + ")";
+    return c;
+  };
+  auto box_start = [&](std::ostringstream& o) {
+    o << "      u64 g = gb;\n";
+    for (size_t k = 0; k < sh.U.size(); ++k) o << "      if ((u >> " << k << ") & 1u) g |= " << (1ull << sh.U[k]) << "ull;\n";
+  };
+  s << "__device__ __forceinline__ void load_tile(const TMap* tm, u64 gb, u32 stage, u32 bar, u32 lane) {\n";
+  s << "  for (u32 u = lane; u < " << nbox << "u; u += 32u) {\n";
+  box_start(s);
+  coords(s);
+  s << "      asm volatile(\"cp.async.bulk.tensor." << rk
+    << "d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {" << clist() << "}], [%" << (rk + 2)
+    << "];\" :: \"r\"(stage + u * " << box_bytes << "u), \"l\"(reinterpret_cast<u64>(tm))" << cargs()
+    << ", \"r\"(bar) : \"memory\");\n";
+  s << "  }\n}\n";
+  s << "__device__ __forceinline__ void store_tile(const TMap* tm, u64 gb, u32 stage, u32 lane) {\n";
+  s << "  for (u32 u = lane; u < " << nbox << "u; u += 32u) {\n";
+  box_start(s);
+  coords(s);
+  s << "      asm volatile(\"cp.async.bulk.tensor." << rk << "d.global.shared::cta.tile.bulk_group [%0, {"
+    << [&]() {
+         std::string c;
+         for (int d = 0; d < rk; ++d) c += (d ? ", %" : "%") + std::to_string(d + 1);
+         return c;
+       }()
+    << "}], [%" << (rk + 1) << "];\" :: \"l\"(reinterpret_cast<u64>(tm))" << cargs() << ", \"r\"(stage + u * "
+    << box_bytes << "u) : \"memory\");\n";
+  s << "  }\n  bulk_commit();\n}\n";
+
+  const uint32_t smem_stages = kPipeStages * tile_bytes;
+  s << "extern \"C\" __global__ void __launch_bounds__(" << (nc + 32) << ", " << min_blocks
+    << ") qs_tile_pass(const __grid_constant__ TMap tmap, u64 ntiles, u32 flags, u64 nmask, u32* status, u64 limit) {\n";
+  s << "  const u32 raw = su32(smem_raw);\n";
+  s << "  const u32 pad = (1024u - (raw & 1023u)) & 1023u;\n";
+  s << "  unsigned char* smem = smem_raw + pad;\n";
+  s << "  const u32 stage0 = su32(smem);\n";
+  s << "  u64* dep_lo = reinterpret_cast<u64*>(smem + " << smem_stages << ");\n";
+  s << "  const u32 bar_full = su32(dep_lo + 256), bar_done = bar_full + " << 8 * kPipeStages << "u;\n";
+  s << "  volatile u32* abort_flag = reinterpret_cast<volatile u32*>(dep_lo + 256 + " << 2 * kPipeStages << ");\n";
+  s << "  const u32 tid = threadIdx.x;\n";
+  s << "  for (u32 e = tid; e < 256u; e += blockDim.x) dep_lo[e] = kDep[e];\n";
+  s << "  if (tid == 0) {\n";
+  s << "    for (u32 k = 0; k < " << kPipeStages << "u; ++k) { mb_init(bar_full + 8u * k, 1u); mb_init(bar_done + 8u * k, "
+    << nc << "u); }\n";
+  s << "    *abort_flag = 0u;\n";
+  s << "    asm volatile(\"fence.mbarrier_init.release.cluster;\\nfence.proxy.async.shared::cta;\" ::: \"memory\");\n";
+  s << "  }\n  __syncthreads();\n";
+  s << "  const u64 mine = blockIdx.x < ntiles ? (ntiles - 1ull - blockIdx.x) / gridDim.x + 1ull : 0ull;\n";
+  s << "  const bool from_zero = (flags & 1u) != 0u;\n";
+  // ---- producer warp
+  s << "  if (tid >= " << nc << "u) {\n";
+  s << "    const u32 lane = tid & 31u;\n";
+  s << "    const TMap* tm = &tmap;\n";
+  s << "    bool fail = false;\n";
+  s << "    long long armed[" << kPipeStages << "];\n";
+  s << "    for (int k = 0; k < " << kPipeStages << "; ++k) armed[k] = -1;\n";
+  s << "    u64 i = 0;\n";
+  s << "    for (; i < mine; ++i) {\n";
+  s << "      const u32 st = (u32)(i % " << kPipeStages << "u);\n";
+  s << "      if (i >= " << kPipeStages << "u) {\n";
+  s << "        const u64 j = i - " << kPipeStages << "u;\n";
+  s << "        if (!mb_wait(bar_done + 8u * st, (u32)((j / " << kPipeStages << "u) & 1u), limit)) { fail = true; break; }\n";
+  s << "        store_tile(tm, tile_base(blockIdx.x + j * gridDim.x), stage0 + st * " << tile_bytes << "u, lane);\n";
+  s << "        bulk_wait_read0();\n";
+  s << "        __syncwarp();\n";
+  s << "      }\n";
+  s << "      if (from_zero) { if (lane == 0u) mb_arrive(bar_full + 8u * st); }\n";
+  s << "      else if (!((flags & 4u) && i == 0ull)) {\n";
+  s << "        if (lane == 0u) mb_expect(bar_full + 8u * st, " << tile_bytes << "u);\n";
+  s << "        __syncwarp();\n";
+  s << "        load_tile(tm, tile_base(blockIdx.x + i * gridDim.x), stage0 + st * " << tile_bytes
+    << "u, bar_full + 8u * st, lane);\n";
+  s << "        armed[st] = (long long)i;\n";
+  s << "      }\n";
+  s << "    }\n";
+  s << "    if (!fail) {\n";
+  s << "      for (u64 j = mine > " << kPipeStages << "u ? mine - " << kPipeStages << "u : 0ull; j < mine; ++j) {\n";
+  s << "        const u32 st = (u32)(j % " << kPipeStages << "u);\n";
+  s << "        if (!mb_wait(bar_done + 8u * st, (u32)((j / " << kPipeStages << "u) & 1u), limit)) { fail = true; break; }\n";
+  s << "        store_tile(tm, tile_base(blockIdx.x + j * gridDim.x), stage0 + st * " << tile_bytes << "u, lane);\n";
+  s << "      }\n";
+  s << "    }\n";
+  s << "    bulk_wait0();\n";
+  s << "    if (fail) {\n";
+  s << "      if (lane == 0u) atomicOr(status, 1u);\n";
+  s << "      // loads still in flight land in this CTA's shared memory: wait (bounded) for them\n";
+  s << "      for (int k = 0; k < " << kPipeStages << "; ++k)\n";
+  s << "        if (armed[k] >= 0) (void)mb_wait(bar_full + 8u * k, (u32)(((u64)armed[k] / " << kPipeStages
+    << "u) & 1u), limit);\n";
+  s << "    }\n";
+  s << "    return;\n";
+  s << "  }\n";
+  // ---- consumer warps
+  s << "  for (u64 i = 0; i < mine; ++i) {\n";
+  s << "    const u32 st = (u32)(i % " << kPipeStages << "u);\n";
+  s << "    if (!mb_wait(bar_full + 8u * st, (u32)((i / " << kPipeStages << "u) & 1u), limit)) *abort_flag = 1u;\n";
+  s << "    consumers_sync();\n";
+  s << "    if (*abort_flag) { if (tid == 0u) atomicOr(status, 2u); return; }\n";
+  s << "    const u32 soff = pad + st * " << tile_bytes << "u;\n";
+  s << "    float2* tile = reinterpret_cast<float2*>(smem_raw + soff);\n";
+  s << "    const u64 gbase = tile_base(blockIdx.x + i * gridDim.x);\n";
+  s << "    if (from_zero) {\n";
+  s << "      float4* t4 = reinterpret_cast<float4*>(tile);\n";
+  s << "      for (u32 c = tid; c < " << (tile_bytes / 16) << "u; c += " << nc << "u) t4[c] = make_float4(0.f, 0.f, 0.f, 0.f);\n";
+  s << "      consumers_sync();\n";
+  s << "      if (tid == 0u && (gbase & nmask) == 0ull) tile[0] = make_float2(1.f, 0.f);\n";
+  s << "      consumers_sync();\n";
+  s << "    }\n";
+  for (int b = 0; b < P.nblocks; ++b) {
+    s << "    blk" << b << "(soff, gbase, dep_lo, tid);\n";
+    if (b + 1 < P.nblocks) s << "    consumers_sync();\n";
+  }
+  s << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n";
+  s << "    mb_arrive(bar_done + 8u * st);\n";
+  s << "  }\n";
+  s << "}\n";
+  return s.str();
+}
+
+int pipe_smem(int T) { return kPipeStages * (8 << T) + 1024 + 256 * 8 + 2 * kPipeStages * 8 + 16; }
+int pipe_threads(int T, int R) { return std::min(256, 1 << (T - R)) + 32; }
+
 uint64_t fnv1a(const std::string& s) {
   uint64_t h = 1469598103934665603ull;
   for (unsigned char ch : s) {
@@ -644,9 +1046,33 @@ bool qs_jit_compile_only(const qs_plan_s* p, std::string& err) {
 // Source of one pass from its device-program bytes (header first).
 static std::string pass_source(const char* base) {
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
-  return gen_pass(P, reinterpret_cast<const DevBlock*>(base + P.block_off),
-                  reinterpret_cast<const DevOp*>(base + P.op_off), reinterpret_cast<const float2*>(base + P.coef_off),
-                  min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R), P.R));
+  const DevBlock* blocks = reinterpret_cast<const DevBlock*>(base + P.block_off);
+  const DevOp* ops = reinterpret_cast<const DevOp*>(base + P.op_off);
+  const float2* coef = reinterpret_cast<const float2*>(base + P.coef_off);
+  PipeShape sh;
+  if (P.R <= 5 && pipe_shape(P, sh))
+    return gen_pass_pipe(P, blocks, ops, coef, sh, min_blocks_for(pipe_smem(P.T), pipe_threads(P.T, P.R), P.R));
+  return gen_pass(P, blocks, ops, coef, min_blocks_for(pass_smem(P.T), pass_threads(P.T, P.R), P.R));
+}
+
+// Launch shape of a pass's kernel (pipelined or single-buffered).
+static void pass_launch_shape(const char* base, JitPass& K) {
+  const DevPass& P = *reinterpret_cast<const DevPass*>(base);
+  PipeShape sh;
+  if (P.R <= 5 && pipe_shape(P, sh)) {
+    K.pipe = 1;
+    K.threads = pipe_threads(P.T, P.R);
+    K.smem = pipe_smem(P.T);
+    K.rank = sh.rank;
+    for (int d = 0; d < 5; ++d) {
+      K.st[d] = sh.st[d];
+      K.boxb[d] = sh.boxb[d];
+    }
+  } else {
+    K.pipe = 0;
+    K.threads = pass_threads(P.T, P.R);
+    K.smem = pass_smem(P.T);
+  }
 }
 
 std::string qs_jit_source(const qs_plan_s* p, size_t i) { return pass_source(p->blob.data() + p->pass_offsets[i]); }
@@ -675,7 +1101,8 @@ std::string pass_key(const qs_plan_s* p, size_t i) {
   const char* base = p->blob.data() + p->pass_offsets[i];
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
   std::string k(base, base + P.bytes);
-  k += "|t" + std::to_string(pass_threads(P.T, P.R)) + "|s" + std::to_string(scalar_every());
+  k += "|t" + std::to_string(pass_threads(P.T, P.R)) + "|s" + std::to_string(scalar_every()) + "|p" +
+       std::to_string(pipe_enabled() ? 1 : 0);
   return k;
 }
 
@@ -749,8 +1176,12 @@ void run_job(JitJob& J, unsigned max_threads) {
     }
     JitPass K;
     K.fn = fn;
-    K.threads = pass_threads(J.T[i], J.R[i]);
-    K.smem = pass_smem(J.T[i]);
+    pass_launch_shape(J.progs[i].data(), K);
+    if (K.pipe && !g_api.EncodeTiled) {
+      J.err = "cuTensorMapEncodeTiled is missing from the driver";
+      J.state = 2;
+      return;
+    }
     if (g_api.FuncSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, K.smem) != CUDA_SUCCESS ||
         g_api.Occupancy(&K.per_sm, fn, K.threads, (size_t)K.smem) != CUDA_SUCCESS || K.per_sm < 1) {
       J.err = "a specialised tile pass does not fit on an SM";
@@ -863,17 +1294,59 @@ void qs_jit_tiered(qs_context* h, qs_plan_s* p) {
   if (st != 0) p->jit_job.reset();
 }
 
+// Tensor map of `state` (n_states states of n qubits back to back) for a
+// pipelined pass: dimension d starts at qubit st[d] and ends where the next
+// starts (the last one spans the rest of the buffer); 8-byte elements, a box
+// of 16 elements x 2^boxb[d], 128-byte swizzle.
+static void encode_state_map(const JitPass& K, void* state, uint64_t total_amps, CUtensorMap* m) {
+  cuuint64_t dim[5], stride[4];
+  cuuint32_t box[5], estr[5];
+  const int rk = K.rank;
+  for (int d = 0; d < rk; ++d) {
+    const int lo = K.st[d];
+    dim[d] = d + 1 < rk ? (1ull << (K.st[d + 1] - lo)) : (total_amps >> lo);
+    box[d] = 1u << K.boxb[d];
+    estr[d] = 1;
+    if (d > 0) stride[d - 1] = (1ull << lo) * 8ull;
+  }
+  const CUresult rc = g_api.EncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rk, state, dim, stride, box, estr,
+                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS)
+    throw qs_error(QS_ERR_CUDA, "cuTensorMapEncodeTiled failed for a pipelined tile pass (CUresult " +
+                                    std::to_string((int)rc) + ")");
+}
+
 void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t i, void* state, uint64_t ntiles, uint32_t flags) {
   const JitPass& K = p->jit[i];
   float2* st = static_cast<float2*>(state);
   uint64_t nt = ntiles;
   uint32_t fl = flags;
   uint64_t nmask = (1ull << p->n_qubits) - 1ull;
-  void* args[] = {&st, &nt, &fl, &nmask};
   const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)h->sm_count * (uint64_t)K.per_sm);
   if (grid == 0) return;
-  const CUresult rc = g_api.LaunchKernel((CUfunction)K.fn, (unsigned)grid, 1, 1, (unsigned)K.threads, 1, 1,
-                                         (unsigned)K.smem, (CUstream)h->stream, args, nullptr);
+  CUresult rc;
+  if (K.pipe) {
+    alignas(64) CUtensorMap tm;
+    const int T = p->pass_T[i];
+    encode_state_map(K, state, ntiles << T, &tm);
+    // bounded waits: 4 s (a tile's copy takes microseconds; the margin covers
+    // time slicing with other processes); the wait test uses 50 ms
+    uint64_t limit = 4000000000ull;
+    if (h->wait_test) {
+      fl |= 4u;
+      limit = 50000000ull;
+      h->wait_test = 0;
+    }
+    uint32_t* status = h->dev_status;
+    void* args[] = {&tm, &nt, &fl, &nmask, &status, &limit};
+    rc = g_api.LaunchKernel((CUfunction)K.fn, (unsigned)grid, 1, 1, (unsigned)K.threads, 1, 1, (unsigned)K.smem,
+                            (CUstream)h->stream, args, nullptr);
+  } else {
+    void* args[] = {&st, &nt, &fl, &nmask};
+    rc = g_api.LaunchKernel((CUfunction)K.fn, (unsigned)grid, 1, 1, (unsigned)K.threads, 1, 1, (unsigned)K.smem,
+                            (CUstream)h->stream, args, nullptr);
+  }
   if (rc != CUDA_SUCCESS)
     throw qs_error(QS_ERR_CUDA, "launch of a specialised tile pass failed (CUresult " + std::to_string((int)rc) + ")");
   qs_after_launch(h, "qs_tile_pass");

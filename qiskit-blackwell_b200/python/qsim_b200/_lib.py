@@ -85,6 +85,8 @@ SIGNATURES = {
     "qs_set_block_bits": (_i, [_vp, _i]),
     "qs_set_jit": (_i, [_vp, _i, _i]),
     "qs_launch_count": (_i64, [_vp]),
+    "qs_device_status": (_i, [_vp, _pi]),
+    "qs_set_wait_test": (_i, [_vp, _i]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
     "qs_state_alloc": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
     "qs_state_free": (_i, [_vp, _vp]),

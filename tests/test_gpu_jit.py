@@ -115,3 +115,56 @@ def test_tiered_mode_switches_over_and_matches():
         assert _same_bits(ref2, s.cpu().numpy())
     finally:
         E.set_jit(1, 24)
+
+
+@pytest.mark.parametrize("tile_bits", [12, 13])
+def test_pipelined_passes_24_qubits_bit_identical(tile_bits):
+    """24 qubits of the layered generator: tiles whose high qubits form up
+    to ten runs (box dimensions plus boxes walked one by one), from |0..0>
+    and from a given state, on the pipelined kernels (TMA stage ring) and
+    the generic interpreter."""
+    ops = W.layers_ops(24, 8, seed=5)
+    ref, _ = _run(24, ops, 0, None, tile_bits, 5)
+    got, info = _run(24, ops, 2, None, tile_bits, 5)
+    assert info["n_jit_passes"] == info["n_passes"] > 3
+    assert _same_bits(ref, got)
+    rng = np.random.default_rng(8)
+    psi0 = (rng.standard_normal(1 << 24) + 1j * rng.standard_normal(1 << 24)).astype(np.complex64)
+    psi0 /= np.float32(np.linalg.norm(psi0))
+    ref, _ = _run(24, ops, 0, psi0, tile_bits, 5)
+    got, _ = _run(24, ops, 2, psi0, tile_bits, 5)
+    assert _same_bits(ref, got)
+
+
+def test_pipelined_pass_bounded_wait_reports_status():
+    """The pipelined pass's waits are bounded: with its first tile's copy
+    withheld (the test hook), the consumer and producer waits run out after
+    50 ms, the status word reports both, and the handle keeps working."""
+    import ctypes as C
+    n = 20
+    ops = W.layers_ops(n, 4, seed=9)
+    h = E._h()
+    E.set_jit(2)
+    try:
+        plan = E.Plan(n, ops)
+        s = E.empty_state(n)
+        plan.execute_from_zero(s)
+        torch.cuda.synchronize()
+        assert plan.refresh_info()["n_jit_passes"] == plan.info["n_passes"]
+        code = C.c_int(-1)
+        h.call("qs_device_status", C.byref(code))
+        assert code.value == 0
+        h.call("qs_set_wait_test", 1)
+        plan.execute(s)                # the first pass loads: its first tile never arrives
+        torch.cuda.synchronize()
+        h.call("qs_device_status", C.byref(code))
+        assert code.value == 3, code.value
+        h.call("qs_device_status", C.byref(code))
+        assert code.value == 0         # read and cleared
+        plan.execute_from_zero(s)      # the context is usable and the result right
+        torch.cuda.synchronize()
+        assert abs(1 - O.fidelity(s.cpu().numpy(), O.simulate(n, ops))) <= 1e-6
+        h.call("qs_device_status", C.byref(code))
+        assert code.value == 0
+    finally:
+        E.set_jit(1, 24)
