@@ -153,6 +153,48 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def describe(workload: str, args) -> str:
+    """The workload named by what it is, with its sizes: the `config`
+    string both arms print (no GPU needed)."""
+    if workload == "layers32":
+        from qsim_b200 import workloads as W
+        n = args.qubits
+        ngates = len(W.layers_ops(n, 20, seed=0))
+        return (f"layers32: {n} qubits (2^{n} complex64 = {(8 << n) >> 30} GiB), 20 layers "
+                f"U(2)+CZ brickwork+Toffoli/5, {ngates} gates, seed 0")
+    if workload == "qv_batch":
+        return f"qv_batch: {args.circuits} QV circuits, widths U[10,20], depth=width, seeds 1e6*1+i"
+    if workload == "qv12":
+        return "qv12: 12 qubits, depth 12, seed 0 (72 U(4))"
+    if workload == "serving":
+        return (f"serving: {args.requests} seeded requests (50% QV 10-28q 1024 shots, 25% EfficientSU2 "
+                f"energy+gradient 12-22q, 25% Chebyshev evolution 12-22q), Poisson arrivals at "
+                f"{args.rates} req/s, the sequence replayed at each rate; 150 GB budget, {args.workers} worker "
+                f"streams, {args.server} server")
+    if workload == "adjoint":
+        n = args.qubits if args.qubits != 32 else 20
+        return f"adjoint: EfficientSU2 {n} qubits, 4 reps, {2 * n * 5} params, 256-term observable, batch 64"
+    if workload == "qv_plain":
+        n = args.qubits if args.qubits != 32 else 24
+        return f"qv_plain: {n} qubits, depth {n}, seed 1000"
+    if workload == "noisy":
+        from qsim_b200 import workloads as W
+        from qsim_b200.circuit import NOISE_OPS, from_qiskit
+        n = args.qubits if args.qubits != 32 else 12
+        T = args.circuits if args.circuits != 4096 else 8192
+        nn = sum(1 for ins in from_qiskit(W.noisy_brickwork(n, 8, seed=5)).data if ins.name in NOISE_OPS)
+        return (f"noisy: {n}-qubit brickwork x 8 layers, {nn} channels (depolarizing, amplitude damping, "
+                f"dephasing at 1e-3), {T} trajectories per step")
+    if workload == "chebyshev":
+        n = args.qubits if args.qubits != 32 else 22
+        return (f"chebyshev: {n} qubits, ring ZZ + X field + 20 XX+YY pairs ({2 * n + 40} Pauli terms), t = 10.0, "
+                f"precision 1e-06")
+    if workload == "micro":
+        return ("micro: 20-qubit kernels through blackwell_kernels (CUDA-tensor gates), and QV-20 (depth 20, "
+                "seed 20) with 8192 shots through BlackwellSimulator.run")
+    raise ValueError(workload)
+
+
 # ------------------------------------------------------------ workloads
 def _cuda_time(fn, stream, steps):
     import torch
@@ -223,8 +265,7 @@ def bench_layers32(args, dev):
     res = {
         "metric": METRIC, "value": ws * ngates / per_step, "unit": "gates/s",
         "ms_per_step": per_step * 1e3, "dtype": "c64 (fp32 FMA; fp64 host fusion)",
-        "config": {"workload": f"layers32: {n} qubits (2^{n} complex64 = {(8 << n) >> 30} GiB), {layers} layers "
-                               f"U(2)+CZ brickwork+Toffoli/5, {ngates} gates, seed 0",
+        "config": {"workload": describe("layers32", args),
                    "passes": P, "tile_bits": info["tile_bits"], "blocks": info["n_blocks"],
                    "fused_ops": info["n_ops_fused"], "specialised_passes": info["n_jit_passes"],
                    "l2": "state 32 GiB >> 126 MB L2 (no flush needed)"},
@@ -328,7 +369,7 @@ def bench_qv_batch(args, dev):
     res = {
         "metric": METRIC, "value": ws * C / per_step, "unit": "circuits/s", "ms_per_step": per_step * 1e3,
         "dtype": "c64 (fp32 FMA; fp64 host fusion)",
-        "config": {"workload": f"qv_batch: {C} QV circuits, widths U[10,20], depth=width, seeds 1e6*1+i",
+        "config": {"workload": describe("qv_batch", args),
                    "launches_per_step": bp.info["n_launches"], "items": bp.info["n_items"],
                    "autotuned_tile_block_bits": {str(k): list(v) for k, v in tuned.items()},
                    "autotune_seconds": t_tune, "cuda_graph": "captured at the 2nd execution, replayed",
@@ -370,7 +411,7 @@ def bench_qv12(args, dev):
     per_step = t / args.steps
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return {"metric": METRIC, "value": ws / per_step, "unit": "circuits/s", "ms_per_step": per_step * 1e3,
-            "dtype": "c64", "config": {"workload": "qv12: 12 qubits, depth 12, seed 0 (72 U(4))"},
+            "dtype": "c64", "config": {"workload": describe("qv12", args)},
             "clocks": clk.summary(), "gpu_launches": args.steps}, {"unit": "circuits/s"}
 
 
@@ -531,10 +572,7 @@ def bench_serving(args, dev):
     res = {
         "metric": METRIC, "value": ws * n_req / top_mk, "unit": "requests/s",
         "ms_per_step": top_mk * 1e3, "dtype": "c64 state (fp32 FMA), fp64 reductions",
-        "config": {"workload": f"serving: {n_req} seeded requests (50% QV 10-28q 1024 shots, 25% EfficientSU2 "
-                               f"energy+gradient 12-22q, 25% Chebyshev evolution 12-22q), Poisson arrivals "
-                               f"replayed at each rate; 150 GB budget, {args.workers} worker streams, "
-                               f"{args.server} server",
+        "config": {"workload": describe("serving", args),
                    "rates_rps": rates, "step": "one replay of the request sequence at the highest rate",
                    "l2": "states up to 2 GiB each; no flush"},
         "sweep": sweep,
@@ -604,8 +642,7 @@ def bench_adjoint(args, dev):
     amp = B << n
     return {"metric": METRIC, "value": ws * B / t_g, "unit": "gradients/s", "ms_per_step": t_g * 1e3,
             "dtype": "c64 state, fp64 gradient accumulation",
-            "config": {"workload": f"adjoint: EfficientSU2 {n} qubits, 4 reps, {npar} params, 256-term observable, "
-                                   f"batch {B}", "l2": f"{amp * 8 >> 20} MiB of states per batch > L2"},
+            "config": {"workload": describe("adjoint", args), "l2": f"{amp * 8 >> 20} MiB of states per batch > L2"},
             "forward_ms": t_f * 1e3, "gradient_over_forward": t_g / t_f,
             "energy_agreement": float(np.max(np.abs(e_f - e_g))),
             "e2e": {"value": ws * B / t_g, "unit": "gradients/s", "h2d_bytes_per_step": int(params.nbytes + ops.nbytes),
@@ -642,7 +679,7 @@ def bench_qv_plain(args, dev):
     algo = (8.0 + 16.0 * (info["n_passes"] - 1)) * (1 << n)
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return {"metric": METRIC, "value": ws / per_step, "unit": "circuits/s", "ms_per_step": per_step * 1e3,
-            "dtype": "c64", "config": {"workload": f"qv_plain: {n} qubits, depth {n}, seed 1000",
+            "dtype": "c64", "config": {"workload": describe("qv_plain", args),
                                        "passes": info["n_passes"], "specialised_passes": info["n_jit_passes"]},
             "roofline": {"bound": "hbm", "achieved": algo / per_step / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / per_step / 1e9 / peak, "traffic": None, "peak_source": src},
@@ -726,8 +763,7 @@ def bench_noisy(args, dev):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return {"metric": METRIC, "value": ws * T / per_step, "unit": "trajectories/s", "ms_per_step": per_step * 1e3,
             "dtype": "c64 state, fp64 branch probabilities",
-            "config": {"workload": f"noisy: {n}-qubit brickwork x 8 layers, {nn} channels (depolarizing, amplitude "
-                                   f"damping, dephasing at 1e-3), {T} trajectories per step",
+            "config": {"workload": describe("noisy", args),
                        "l2": f"{(T << n) * 8 >> 20} MiB of states per step"},
             "per_channel_launches": {"value": ref_rate, "unit": "trajectories/s",
                                      "note": "one blackwell_kernels call per gate and per channel"},
@@ -815,8 +851,7 @@ def bench_chebyshev(args, dev):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return {"metric": METRIC, "value": ws / per, "unit": "evolutions/s", "ms_per_step": per * 1e3,
             "dtype": "c64 vectors (fp32 FMA), fp64 Bessel coefficients",
-            "config": {"workload": f"chebyshev: {n} qubits, ring ZZ + X field + 20 XX+YY pairs ({len(H.x)} Pauli "
-                                   f"terms), t = {t_evo}, precision {prec}, degree K = {K}",
+            "config": {"workload": describe("chebyshev", args), "degree": K,
                        "l2": f"3 vectors of {(8 * N) >> 20} MiB (the recurrence re-reads them every degree)"},
             "roofline": {"bound": "hbm", "achieved": ach_pf, "peak": peak, "unit": "GB/s", "frac": ach_pf / peak,
                          "traffic": None, "peak_source": src, "kernel": "k_chebp_fused (matrix-free, one per degree)",
@@ -912,8 +947,7 @@ def bench_micro(args, dev):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return {"metric": METRIC, "value": ws / t, "unit": "circuits/s", "ms_per_step": t * 1e3,
             "dtype": "c64 (fp32; compensated 1Q/2Q kernels), fp64 reductions",
-            "config": {"workload": "micro: 20-qubit kernels through blackwell_kernels (CUDA-tensor gates), and "
-                                   "QV-20 (depth 20, seed 20) with 8192 shots through BlackwellSimulator.run",
+            "config": {"workload": describe("micro", args),
                        "l2": "8 MiB state, L2-resident (as the reference's table)"},
             "kernels": out,
             "qv20_e2e": {"b200_ms": t * 1e3, "reference_rtx5090_ms": REF_QV20_E2E_MS},
@@ -931,6 +965,43 @@ def E_launches(dev):
 WORKLOADS = {"layers32": bench_layers32, "qv_batch": bench_qv_batch, "qv12": bench_qv12, "serving": bench_serving,
              "adjoint": bench_adjoint, "qv_plain": bench_qv_plain, "noisy": bench_noisy, "micro": bench_micro,
              "chebyshev": bench_chebyshev}
+
+
+def headline_sub_records(args, dev) -> dict:
+    """The metric's served/batched halves beside the default 32-qubit line,
+    each with its own timed region and clock record: `batched` = the
+    qv_batch workload (4096 QV circuits of widths 10-20 against one plan and
+    one launch sequence per circuit), `serving` = the serving workload on a
+    trimmed request count at three rates (p50/p99 per rate, against serial
+    plain execution of the same requests)."""
+    import copy
+    from qsim_b200 import engine as E
+    E.set_jit(1, 24, dev)   # the library default: the 32-qubit line compiled every pass first
+    a = copy.copy(args)
+    a.circuits, a.steps, a.warmup = 4096, max(3, min(args.steps, 5)), 3
+    qb, _ = bench_qv_batch(a, dev)
+    batched = {
+        "workload": describe("qv_batch", a), "value": qb["value"], "unit": qb["unit"], "steps": a.steps,
+        "ms_per_step": qb["ms_per_step"],
+        "per_circuit_launches": qb["per_circuit_launches"], "per_gate_launches": qb["per_gate_launches"],
+        "over_per_circuit_launches": qb["value"] / qb["per_circuit_launches"]["value"],
+        "over_per_gate_launches": qb["value"] / qb["per_gate_launches"]["value"],
+        "e2e": qb["e2e"], "roofline": qb["roofline"], "gpu_launches": qb["gpu_launches"], "clocks": qb["clocks"],
+        "launches_per_step": qb["config"].get("launches_per_step"),
+    }
+    a = copy.copy(args)
+    a.requests, a.rates, a.workers, a.server, a.warmup = 120, "100,500,2000", 4, "native", 1
+    sv, _ = bench_serving(a, dev)
+    serving = {
+        "workload": describe("serving", a), "value": sv["value"], "unit": sv["unit"],
+        "served_circuits_per_s": sv["served_circuits_per_s"],
+        "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+        "sweep": [{k: r[k] for k in ("rate_rps", "served_rps", "qv_circuits_per_s", "p50_ms", "p99_ms", "makespan_s")}
+                  for r in sv["sweep"]],
+        "serial_plain": sv["serial_plain"], "e2e": sv["e2e"], "gpu_launches": sv["gpu_launches"],
+        "clocks": sv["clocks"],
+    }
+    return {"batched": batched, "serving": serving}
 
 
 # --------------------------------------------------------- CPU baseline
@@ -1128,6 +1199,8 @@ def main():
     ap.add_argument("--server", default="native", choices=["native", "python"],
                     help="serving: the C++ runtime (qs_server_*) or the Python one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="layers32: skip the batched and serving sub-records of the headline metric")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
     ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")
     ap.add_argument("--jit", type=int, default=-1,
@@ -1149,7 +1222,7 @@ def main():
         v = float(sorted(vals)[len(vals) // 2])
         line = {"metric": METRIC, "value": v, "unit": info["unit"], "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
-                "config": {"workload": args.workload}, "data": "synthetic",
+                "config": {"workload": describe(args.workload, args)}, "data": "synthetic",
                 "cpu_baseline": {**info, "value": v},
                 "e2e": {"value": v, "unit": info["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference has no CPU implementation of this path (its FP64 oracle is qiskit_aer, "
@@ -1172,6 +1245,14 @@ def main():
         E._h(dev).call("qs_set_tile_bits", int(args.tile_bits))
         E._h(dev).call("qs_set_block_bits", int(args.block_bits))
     res, meta = WORKLOADS[args.workload](args, dev)
+    # one config dict for both arms: the workload string; our arm's plan
+    # details beside it
+    cfg = res.pop("config", {})
+    res["config"] = {"workload": cfg.get("workload", describe(args.workload, args))}
+    if len(cfg) > 1:
+        res["workload_details"] = {k: v for k, v in cfg.items() if k != "workload"}
+    if args.workload == "layers32" and ws == 1 and not args.no_sub:
+        res.update(headline_sub_records(args, dev))
     if rank == 0:
         res.update({"n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded numpy PCG64)"})

@@ -75,3 +75,21 @@ def test_reference_arm_units_match_each_workload():
         assert r.returncode == 0, r.stderr
         line = json.loads(r.stdout.strip().splitlines()[-1])
         assert line["unit"] == unit and line["cpu_baseline"]["unit"] == unit and line["value"] > 0, line
+
+
+def test_reference_arm_config_is_the_shared_workload_string():
+    """Both arms print config = {"workload": describe(...)}, so the two lines
+    name the same workload."""
+    import argparse
+    sys.path.insert(0, ROOT)
+    import bench
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "qv12",
+                        "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    ns = argparse.Namespace(qubits=32, circuits=4096, requests=200, rates="50,100,200,500,1000,2000", workers=4,
+                            server="native")
+    assert line["config"] == {"workload": bench.describe("qv12", ns)}
+    assert bench.describe("layers32", ns).startswith("layers32: 32 qubits") and "954 gates" in \
+        bench.describe("layers32", ns)
