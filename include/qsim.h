@@ -276,6 +276,15 @@ int qs_sample(qs_handle_t h, const void* state, int n_qubits, const double* u_de
  * and seeds are host arrays.                                                */
 int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int32_t* widths,
                       const int64_t* state_offsets, const int64_t* shots, const uint64_t* seeds, int64_t* out_dev);
+/* Reference: blackwell_backend/simulator.py:579-586 (the counts loop over the
+ * shots).  Histogram of n_shots outcomes held on the device (e.g. qs_sample's
+ * output): a hash table in the handle's scratch counts them on the GPU and
+ * only the distinct outcomes come back, as n_distinct (outcome, count) int64
+ * pairs in pairs_host (room for `capacity` pairs; QS_ERR_INVALID if there
+ * are more, with *n_distinct set so the caller can retry).  The pairs come
+ * in no particular order.  Waits for the handle's stream.                  */
+int qs_counts(qs_handle_t h, const int64_t* shots_dev, int64_t n_shots, int64_t* pairs_host, int64_t capacity,
+              int64_t* n_distinct);
 /* Reference: bwk/csrc/expectation_sm120.cu:45-80,179-202 (expectation_z)    */
 int qs_expect_z(qs_handle_t h, const void* state, int n_qubits, uint64_t z_mask, double* out_host);
 /* Reference: bwk/csrc/expectation_sm120.cu:100-163,204-239 (expectation_pauli),

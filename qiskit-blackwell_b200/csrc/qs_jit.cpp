@@ -583,6 +583,20 @@ struct PipeShape {
 
 constexpr int kPipeStages = 3;
 
+// Consumer groups: the compute warps split into groups that take alternate
+// tiles of the ring (group g: tiles g, g + groups, ...), each synchronising
+// on a named barrier of its own, so one group's shared-memory loads overlap
+// the other group's arithmetic instead of every warp waiting in the same
+// phase.  QSIM_PIPE_GROUPS = 1 or 2 (default 2 when the CTA has >= 8 warps).
+int pipe_groups(int nc) {
+  static const int env = [] {
+    const char* e = std::getenv("QSIM_PIPE_GROUPS");
+    return e ? std::atoi(e) : 0;
+  }();
+  const int g = env == 1 || env == 2 ? env : 2;
+  return (nc / g) % 32 == 0 && nc / g >= 64 ? g : 1;
+}
+
 bool pipe_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("QSIM_TMA_PASS");
@@ -776,19 +790,20 @@ __device__ __forceinline__ bool mb_wait(u32 b, u32 par, u64 limit) {
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" :: "n"(QS_NC) : "memory"); }
+__device__ __forceinline__ void consumers_sync(u32 grp) { asm volatile("bar.sync %0, %1;" :: "r"(grp + 1u), "n"(QS_NCG) : "memory"); }
 )";
 
 std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp* ops, const float2* coef,
                           const PipeShape& sh, int min_blocks) {
   const int T = P.T, R = P.R;
   const int nc = std::min(256, 1 << (T - R));  // consumer threads (a multiple of 32: T - R >= 5)
+  const int ngrp = pipe_groups(nc), ncg = nc / ngrp;
   const uint32_t tile_bytes = 8u << T;
   const int nbox = 1 << sh.U.size();
   const uint32_t box_bytes = 8u << sh.box_bits;
   std::ostringstream s;
   s << kPrelude;
-  s << "#define QS_NC " << nc << "\n";
+  s << "#define QS_NC " << nc << "\n#define QS_NCG " << ncg << "\n";
   s << kPipePrelude;
   s << "extern __shared__ __align__(1024) unsigned char smem_raw[];\n";
   s << "__device__ const u64 kDep[256] = {";
@@ -803,7 +818,7 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
   }
   s << "};\n";
   const bool inline_blocks = P.nblocks <= 4;
-  for (int b = 0; b < P.nblocks; ++b) s << gen_block_fn_pipe(b, blocks[b], T, R, nc, ops, coef, inline_blocks, sh.A);
+  for (int b = 0; b < P.nblocks; ++b) s << gen_block_fn_pipe(b, blocks[b], T, R, ncg, ops, coef, inline_blocks, sh.A);
   // global index of the first amplitude of tile t
   s << "__device__ __forceinline__ u64 tile_base(u64 t) {\n  u64 g = t;\n";
   for (int k = 0; k < T; ++k) s << "  g = ins0(g, " << P.S[k] << ");\n";
@@ -871,7 +886,7 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
   s << "  for (u32 e = tid; e < 256u; e += blockDim.x) dep_lo[e] = kDep[e];\n";
   s << "  if (tid == 0) {\n";
   s << "    for (u32 k = 0; k < " << kPipeStages << "u; ++k) { mb_init(bar_full + 8u * k, 1u); mb_init(bar_done + 8u * k, "
-    << nc << "u); }\n";
+    << ncg << "u); }\n";
   s << "    *abort_flag = 0u;\n";
   s << "    asm volatile(\"fence.mbarrier_init.release.cluster;\\nfence.proxy.async.shared::cta;\" ::: \"memory\");\n";
   s << "  }\n  __syncthreads();\n";
@@ -920,25 +935,26 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
   s << "    }\n";
   s << "    return;\n";
   s << "  }\n";
-  // ---- consumer warps
-  s << "  for (u64 i = 0; i < mine; ++i) {\n";
+  // ---- consumer warps: group grp takes tiles grp, grp + ngrp, ...
+  s << "  const u32 grp = tid / " << ncg << "u, lt = tid % " << ncg << "u;\n";
+  s << "  for (u64 i = grp; i < mine; i += " << ngrp << "u) {\n";
   s << "    const u32 st = (u32)(i % " << kPipeStages << "u);\n";
   s << "    if (!mb_wait(bar_full + 8u * st, (u32)((i / " << kPipeStages << "u) & 1u), limit)) *abort_flag = 1u;\n";
-  s << "    consumers_sync();\n";
-  s << "    if (*abort_flag) { if (tid == 0u) atomicOr(status, 2u); return; }\n";
+  s << "    consumers_sync(grp);\n";
+  s << "    if (*abort_flag) { if (lt == 0u) atomicOr(status, 2u); return; }\n";
   s << "    const u32 soff = pad + st * " << tile_bytes << "u;\n";
   s << "    float2* tile = reinterpret_cast<float2*>(smem_raw + soff);\n";
   s << "    const u64 gbase = tile_base(blockIdx.x + i * gridDim.x);\n";
   s << "    if (from_zero) {\n";
   s << "      float4* t4 = reinterpret_cast<float4*>(tile);\n";
-  s << "      for (u32 c = tid; c < " << (tile_bytes / 16) << "u; c += " << nc << "u) t4[c] = make_float4(0.f, 0.f, 0.f, 0.f);\n";
-  s << "      consumers_sync();\n";
-  s << "      if (tid == 0u && (gbase & nmask) == 0ull) tile[0] = make_float2(1.f, 0.f);\n";
-  s << "      consumers_sync();\n";
+  s << "      for (u32 c = lt; c < " << (tile_bytes / 16) << "u; c += " << ncg
+    << "u) t4[c] = make_float4(0.f, 0.f, 0.f, 0.f);\n";
+  s << "      if (lt == 0u && (gbase & nmask) == 0ull) tile[0] = make_float2(1.f, 0.f);  // lt 0 zeroed t4[0]\n";
+  s << "      consumers_sync(grp);\n";
   s << "    }\n";
   for (int b = 0; b < P.nblocks; ++b) {
-    s << "    blk" << b << "(soff, gbase, dep_lo, tid);\n";
-    if (b + 1 < P.nblocks) s << "    consumers_sync();\n";
+    s << "    blk" << b << "(soff, gbase, dep_lo, lt);\n";
+    if (b + 1 < P.nblocks) s << "    consumers_sync(grp);\n";
   }
   s << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n";
   s << "    mb_arrive(bar_done + 8u * st);\n";
@@ -1102,7 +1118,7 @@ std::string pass_key(const qs_plan_s* p, size_t i) {
   const DevPass& P = *reinterpret_cast<const DevPass*>(base);
   std::string k(base, base + P.bytes);
   k += "|t" + std::to_string(pass_threads(P.T, P.R)) + "|s" + std::to_string(scalar_every()) + "|p" +
-       std::to_string(pipe_enabled() ? 1 : 0);
+       std::to_string(pipe_enabled() ? 1 : 0) + "|g" + std::to_string(pipe_groups(256));
   return k;
 }
 

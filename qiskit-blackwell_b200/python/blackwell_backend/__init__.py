@@ -9,6 +9,7 @@ from .simulator import BlackwellSimulator, Result, counts_from_samples  # noqa: 
 from .hamiltonian import HamiltonianCSR  # noqa: F401
 from .chebyshev import chebyshev_coefficients, chebyshev_evolve, chebyshev_evolve_pauli  # noqa: F401
 from .hybrid import HybridSimulator, RoutingPolicy, analyze_circuit  # noqa: F401
+from .backend import BlackwellBackend  # noqa: F401
 
 __all__ = ["BlackwellSimulator", "HamiltonianCSR", "chebyshev_coefficients", "chebyshev_evolve", "Result",
-           "HybridSimulator", "RoutingPolicy", "analyze_circuit"]
+           "HybridSimulator", "RoutingPolicy", "analyze_circuit", "BlackwellBackend"]

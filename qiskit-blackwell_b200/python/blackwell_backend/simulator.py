@@ -74,14 +74,12 @@ def _make_result(counts, shots, header, elapsed, metadata=None):
 
 def counts_from_samples(samples) -> dict:
     """{hex(index): count} as the reference builds it (simulator.py:579-586).
-    A device tensor is histogrammed on the device and only the distinct
-    outcomes and their counts are copied back (the reference loops over every
-    shot in Python)."""
+    A device tensor is histogrammed on the device by libqsim (qs_counts) and
+    only the distinct outcomes and their counts are copied back (the
+    reference copies every shot and loops over them in Python)."""
     if isinstance(samples, torch.Tensor) and samples.is_cuda:
-        vals, cnt = torch.unique(samples, return_counts=True)
-        vals, cnt = vals.cpu().numpy(), cnt.cpu().numpy()
-    else:
-        vals, cnt = np.unique(np.asarray(samples, dtype=np.int64), return_counts=True)
+        return {hex(k): c for k, c in E.counts(samples.to(torch.int64)).items()}
+    vals, cnt = np.unique(np.asarray(samples, dtype=np.int64), return_counts=True)
     return {hex(int(v)): int(c) for v, c in zip(vals, cnt)}
 
 

@@ -85,6 +85,7 @@ SIGNATURES = {
     "qs_set_block_bits": (_i, [_vp, _i]),
     "qs_set_jit": (_i, [_vp, _i, _i]),
     "qs_launch_count": (_i64, [_vp]),
+    "qs_counts": (_i, [_vp, _vp, _i64, _pi64, _i64, _pi64]),
     "qs_device_status": (_i, [_vp, _pi]),
     "qs_set_wait_test": (_i, [_vp, _i]),
     "qs_state_init": (_i, [_vp, _vp, _i]),

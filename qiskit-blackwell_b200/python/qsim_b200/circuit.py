@@ -90,6 +90,35 @@ class Circuit:
     toffoli = ccx
     def mcx(self, controls, t): return self.append("mcx", list(controls) + [t])
     def cswap(self, c, a, b): return self.append("cswap", [c, a, b])
+    # Qiskit's other standard gates (lowered to the same op kinds)
+    def cy(self, c, t): return self.append("cy", [c, t])
+    def ch(self, c, t): return self.append("ch", [c, t])
+    def csx(self, c, t): return self.append("csx", [c, t])
+    def crx(self, th, c, t): return self.append("crx", [c, t], [th])
+    def cry(self, th, c, t): return self.append("cry", [c, t], [th])
+    def cu1(self, lam, c, t): return self.append("cu1", [c, t], [lam])
+    def cu3(self, th, phi, lam, c, t): return self.append("cu3", [c, t], [th, phi, lam])
+    def cs(self, c, t): return self.append("cs", [c, t])
+    def csdg(self, c, t): return self.append("csdg", [c, t])
+    def ccz(self, a, b, c): return self.append("ccz", [a, b, c])
+    def mcp(self, lam, controls, t): return self.append("mcp", list(controls) + [t], [lam])
+    def rxx(self, th, a, b): return self.append("rxx", [a, b], [th])
+    def ryy(self, th, a, b): return self.append("ryy", [a, b], [th])
+    def rzz(self, th, a, b): return self.append("rzz", [a, b], [th])
+    def rzx(self, th, a, b): return self.append("rzx", [a, b], [th])
+    def iswap(self, a, b): return self.append("iswap", [a, b])
+    def dcx(self, a, b): return self.append("dcx", [a, b])
+    def r(self, th, phi, q): return self.append("r", [q], [th, phi])
+
+    def mcu(self, matrix, controls, targets):
+        """A 2x2 or 4x4 matrix on `targets` (bit 0 = first target), applied
+        where every control qubit is |1>."""
+        m = np.asarray(matrix, dtype=np.complex128)
+        targets = list(targets)
+        if len(targets) not in (1, 2) or m.shape != (2 ** len(targets),) * 2:
+            raise ValueError("mcu takes a 2x2 matrix on one target or a 4x4 on two")
+        return self.append("mcu", list(controls) + targets, [len(targets)], matrix=m)
+
     def unitary(self, matrix, qubits):
         m = np.asarray(matrix, dtype=np.complex128)
         qubits = list(qubits)
@@ -114,30 +143,89 @@ class Circuit:
         return sum(1 for i in self.data if i.name not in ("barrier",))
 
 
+# Instruction names lower() handles directly.
+LOWERABLE = (G.NATIVE_1Q | G.NATIVE_2Q | G.NATIVE_MC | set(G.CONTROLLED_1Q) | set(G.CONTROLLED_PHASE)
+             | set(G.PAULI_ROT_2Q) | set(NOISE_OPS)
+             | {"iswap", "dcx", "r", "unitary", "mcu", "measure", "reset", "barrier"})
+
+
+def _float_params(op, name):
+    out = []
+    for p in getattr(op, "params", ()):
+        try:
+            out.append(float(p))
+        except (TypeError, ValueError):
+            raise ValueError(f"unbound parameter in {name}") from None
+    return out
+
+
+def _convert(out: Circuit, op, qs, cs, depth: int) -> None:
+    """Appends one Qiskit operation acting on qubits `qs` (indices of `out`).
+
+    The reference transpiles every circuit to its native basis before
+    compiling it (blackwell_backend/simulator.py:489-498).  Here:
+      * gates lower() knows keep their name (and parameters);
+      * a controlled gate (num_ctrl_qubits, base_gate, ctrl_state) whose base
+        acts on 1 or 2 qubits becomes one multi-controlled op with the base
+        gate's matrix; controls that must be |0> are wrapped in exact X gates;
+      * any other 1- or 2-qubit gate becomes a `unitary` from to_matrix();
+      * anything else is expanded through its `definition` circuit.
+    A definition's global phase is dropped, as the reference does (it never
+    reads global_phase), so statevectors agree up to a global phase."""
+    name = op.name.lower()
+    if name == "delay":
+        return
+    if name == "unitary":
+        out.unitary(np.asarray(op.to_matrix()), qs)
+        return
+    if name in LOWERABLE:
+        out.append(name, qs, _float_params(op, name), cs)
+        return
+    nc = int(getattr(op, "num_ctrl_qubits", 0) or 0)
+    base = getattr(op, "base_gate", None)
+    if nc > 0 and base is not None and len(qs) - nc in (1, 2) and hasattr(base, "to_matrix"):
+        state = getattr(op, "ctrl_state", None)
+        state = (1 << nc) - 1 if state is None else (int(state, 2) if isinstance(state, str) else int(state))
+        flips = [qs[i] for i in range(nc) if not (state >> i) & 1]
+        for q in flips:
+            out.x(q)
+        if getattr(base, "name", "") == "x" and len(qs) - nc == 1:
+            out.mcx(qs[:nc], qs[nc])                  # exact, as the native mcx
+        else:
+            out.mcu(np.asarray(base.to_matrix()), qs[:nc], qs[nc:])
+        for q in flips:
+            out.x(q)
+        return
+    if len(qs) in (1, 2) and hasattr(op, "to_matrix"):
+        try:
+            m = np.asarray(op.to_matrix(), dtype=np.complex128)
+        except Exception:
+            m = None
+        if m is not None and m.shape == (2 ** len(qs),) * 2:
+            out.unitary(m, qs)
+            return
+    d = getattr(op, "definition", None)
+    if d is not None and depth < 32:
+        qmap = {q: qs[i] for i, q in enumerate(d.qubits)}
+        cmap = {c: cs[i] for i, c in enumerate(getattr(d, "clbits", ())) if i < len(cs)}
+        for inst in d.data:
+            _convert(out, inst.operation, [qmap[q] for q in inst.qubits], [cmap[c] for c in inst.clbits if c in cmap],
+                     depth + 1)
+        return
+    raise ValueError(f"Unsupported instruction: {name}")
+
+
 def from_qiskit(qc) -> Circuit:
-    """Convert a qiskit.QuantumCircuit (duck-typed) into a Circuit."""
+    """Convert a qiskit.QuantumCircuit (duck-typed: num_qubits, num_clbits,
+    qubits, clbits, data of instructions with .operation/.qubits/.clbits)
+    into a Circuit; gates outside the lowered set go through _convert."""
     if isinstance(qc, Circuit):
         return qc
     qidx = {q: i for i, q in enumerate(qc.qubits)}
     cidx = {c: i for i, c in enumerate(qc.clbits)}
     out = Circuit(qc.num_qubits, qc.num_clbits, getattr(qc, "name", "circuit"))
     for inst in qc.data:
-        op = inst.operation
-        name = op.name.lower()
-        qs = [qidx[q] for q in inst.qubits]
-        cs = [cidx[c] for c in inst.clbits]
-        params = []
-        for p in op.params:
-            try:
-                params.append(float(p))
-            except (TypeError, ValueError):
-                if name == "unitary":
-                    continue
-                raise ValueError(f"unbound parameter in {name}")
-        if name == "unitary":
-            out.unitary(np.asarray(op.to_matrix()), qs)
-        else:
-            out.append(name, qs, params, cs)
+        _convert(out, inst.operation, [qidx[q] for q in inst.qubits], [cidx[c] for c in inst.clbits], 0)
     return out
 
 
@@ -151,7 +239,7 @@ def _set_m(rec, mat):
 def lower(circuit: Circuit, strip_measure: bool = True) -> np.ndarray:
     """Circuit -> qs_op structured array (measure/reset/barrier dropped when
     strip_measure, else rejected; they are handled by the backend)."""
-    recs = np.zeros(len(circuit.data), dtype=OP_DTYPE)
+    recs = np.zeros(2 * len(circuit.data), dtype=OP_DTYPE)
     k = 0
     for ins in circuit.data:
         name, qs = ins.name, ins.qubits
@@ -202,6 +290,34 @@ def lower(circuit: Circuit, strip_measure: bool = True) -> np.ndarray:
         elif name == "cu":
             r["kind"] = OP_MCU1
             _set_m(r, G.cu_target(ins.params))
+        elif name in G.CONTROLLED_1Q:
+            r["kind"] = OP_MCU1
+            _set_m(r, G.mat1(G.CONTROLLED_1Q[name], ins.params))
+        elif name in G.CONTROLLED_PHASE:
+            r["kind"] = OP_MCPHASE
+            _set_m(r, [complex(G.CONTROLLED_PHASE[name](ins.params))])
+        elif name == "rzz":
+            r["kind"] = OP_DIAG2
+            _set_m(r, np.diagonal(G.pauli_rot2("z", "z", float(ins.params[0]))))
+        elif name in G.PAULI_ROT_2Q:
+            r["kind"] = OP_U2
+            _set_m(r, G.pauli_rot2(*G.PAULI_ROT_2Q[name], float(ins.params[0])))
+        elif name == "iswap":
+            r["kind"] = OP_U2
+            _set_m(r, G.ISWAP)
+        elif name == "r":
+            r["kind"] = OP_U1
+            _set_m(r, G.r_gate(float(ins.params[0]), float(ins.params[1])))
+        elif name == "mcu":
+            r["kind"] = OP_MCU1 if int(ins.params[0]) == 1 else OP_MCU2
+            _set_m(r, ins.matrix)
+        elif name == "dcx":
+            # CX(q0 -> q1) then CX(q1 -> q0): two exact permutations
+            r["kind"] = OP_MCX
+            k += 1
+            r2 = recs[k]
+            r2["param"], r2["nq"], r2["kind"] = -1, 2, OP_MCX
+            r2["q"][:2] = (qs[1], qs[0])
         else:
             raise ValueError(f"Unsupported instruction: {name}")
         k += 1

@@ -273,6 +273,33 @@ def sample(state: torch.Tensor, shots: int, generator: torch.Generator | None = 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 
 
+def counts(shots: torch.Tensor) -> dict:
+    """{outcome: count} of int64 shots held on the device (qs_counts: hash
+    histogram on the GPU, only the distinct outcomes copied back), in
+    ascending outcome order."""
+    if not shots.is_cuda or shots.dtype != torch.int64:
+        raise RuntimeError("shots must be an int64 CUDA tensor")
+    shots = shots.contiguous()
+    n = int(shots.numel())
+    if n == 0:
+        return {}
+    h = _h(shots.device.index)
+    cap = min(n, 1 << 16)
+    nd = C.c_int64(0)
+    while True:
+        pairs = np.empty((cap, 2), dtype=np.int64)
+        rc = h.L.qs_counts(h.h, _ptr(shots), n, pairs.ctypes.data_as(C.POINTER(C.c_int64)), cap, C.byref(nd))
+        if rc == 0:
+            break
+        if nd.value > cap:          # more distinct outcomes than room: retry with enough
+            cap = int(nd.value)
+            continue
+        _lib.check(rc, h.h)
+    pairs = pairs[: nd.value]
+    order = np.argsort(pairs[:, 0], kind="stable")
+    return {int(k): int(c) for k, c in pairs[order]}
+
+
 def seed_uniforms(seed: int, count: int) -> np.ndarray:
     """The native server's per-request uniforms: splitmix64 (Steele, Lea and
     Flood, 2014) from `seed`, top 53 bits scaled to [0, 1).  Sampling with

@@ -71,6 +71,39 @@ NATIVE_1Q = {"h", "x", "y", "z", "s", "sdg", "t", "tdg", "rx", "ry", "rz", "p", 
 NATIVE_2Q = {"cx", "cz", "swap", "cp", "crz", "cu"}
 NATIVE_MC = {"ccx", "mcx", "c3x", "c4x", "cswap", "toffoli", "cnot"}
 
+# Qiskit's standard controlled single-qubit gates: name -> the target gate
+# (controls first, target last; every control must be |1>).
+CONTROLLED_1Q = {"cy": "y", "ch": "h", "csx": "sx", "crx": "rx", "cry": "ry", "cu3": "u3"}
+# Controlled phases: name -> function of the params giving the phase applied
+# where every listed qubit is |1> (exact as one MCPHASE op).
+CONTROLLED_PHASE = {
+    "cp": lambda p: cmath.exp(1j * float(p[0])), "cphase": lambda p: cmath.exp(1j * float(p[0])),
+    "cu1": lambda p: cmath.exp(1j * float(p[0])), "mcp": lambda p: cmath.exp(1j * float(p[0])),
+    "mcphase": lambda p: cmath.exp(1j * float(p[0])), "mcu1": lambda p: cmath.exp(1j * float(p[0])),
+    "cs": lambda p: 1j, "csdg": lambda p: -1j, "ccz": lambda p: -1.0,
+}
+# Two-qubit Pauli rotations exp(-i theta/2 P1 (x) P0), P0 on the first listed
+# qubit (Qiskit's RXX/RYY/RZZ/RZX: RZX has Z on the first qubit, X on the second).
+PAULI_ROT_2Q = {"rxx": ("x", "x"), "ryy": ("y", "y"), "rzz": ("z", "z"), "rzx": ("z", "x")}
+_PAULI = {"x": np.array([[0, 1], [1, 0]], dtype=np.complex128),
+          "y": np.array([[0, -1j], [1j, 0]], dtype=np.complex128),
+          "z": np.array([[1, 0], [0, -1]], dtype=np.complex128)}
+
+
+def pauli_rot2(p0: str, p1: str, theta: float) -> np.ndarray:
+    """exp(-i theta/2 P1 (x) P0) as a 4x4 with index bit 0 = the qubit of P0."""
+    P = np.kron(_PAULI[p1], _PAULI[p0])
+    return math.cos(theta / 2) * np.eye(4, dtype=np.complex128) - 1j * math.sin(theta / 2) * P
+
+
+def r_gate(theta: float, phi: float) -> np.ndarray:
+    """Qiskit's RGate: exp(-i theta/2 (cos(phi) X + sin(phi) Y))."""
+    c, s = math.cos(theta / 2), math.sin(theta / 2)
+    return np.array([[c, -1j * cmath.exp(-1j * phi) * s], [-1j * cmath.exp(1j * phi) * s, c]], dtype=np.complex128)
+
+
+ISWAP = np.array([[1, 0, 0, 0], [0, 0, 1j, 0], [0, 1j, 0, 0], [0, 0, 0, 1]], dtype=np.complex128)
+
 
 def cu_target(params) -> np.ndarray:
     """Target block of cu(theta, phi, lam, gamma) (simulator.py:199-208)."""
