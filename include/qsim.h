@@ -129,18 +129,22 @@ int64_t qs_launch_count(qs_handle_t h);
 /* Status word of the handle's device-side waits.  The specialised tile
  * passes of 10..13-qubit tiles run as pipelined kernels (TMA copies through
  * a ring of shared-memory stages, producer and consumer warps synchronised
- * by mbarriers); every one of their waits is bounded, and a wait that runs
- * out ORs a cause into this word (1: the copy warp, 2: the compute warps)
- * and its CTA returns, leaving that part of the state unfinished.  Waits on
- * the handle's stream, stores the word in *code (0 = no wait ran out) and
+ * by mbarriers), and a batch plan runs as one persistent launch whose CTAs
+ * wait for a state's previous pass before its next; every one of these waits
+ * is bounded, and a wait that runs out ORs a cause into this word (1: a
+ * pass's copy warp, 2: a pass's compute warps, 4: a batch dependency) and
+ * its CTA returns, leaving that part of the state unfinished.  Waits on the
+ * handle's stream, stores the word in *code (0 = no wait ran out) and
  * clears it.  No reference counterpart (the reference has no device-side
  * waits).                                                                   */
 int qs_device_status(qs_handle_t h, int* code);
-/* Test hook for the above: with on = 1, the next pipelined tile pass this
- * handle launches withholds its first tile's copy and gives its waits 50 ms,
- * so its bounded waits run out and qs_device_status reports them; the hook
- * then switches itself off.  No reference counterpart.                     */
-int qs_set_wait_test(qs_handle_t h, int on);
+/* Test hook for the above: mode 1 = the next pipelined tile pass this handle
+ * launches withholds its first tile's copy; mode 2 = the next persistent
+ * batch launch leaves one pass of one state uncounted, so the state's next
+ * pass never sees it finished.  Either way the waits get 50 ms, run out,
+ * and qs_device_status reports them; the hook then switches itself off.
+ * No reference counterpart.                                                */
+int qs_set_wait_test(qs_handle_t h, int mode);
 
 /* ------------------------------------------------------------ states ----- */
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:109-113,210-224 (state_init) */

@@ -34,6 +34,12 @@ struct qs_batch_plan_s {
   cudaStream_t stream = nullptr;   // stream of the last upload/execution
   cudaGraphExec_t graph = nullptr;
   void* graph_states = nullptr;
+  // one persistent launch (k_pass_queue) instead of `launches`
+  bool queue = false;
+  uint32_t* d_counters = nullptr;  // 2 + q_items words
+  int q_items = 0, q_maxT = 0, q_has2 = 0, q_ncoef = 0;
+  uint64_t q_tiles = 0;
+  uint32_t q_withhold = 0xffffffffu;  // an item with a dependent (the wait-test hook withholds it)
 };
 
 namespace {
@@ -43,6 +49,7 @@ void free_bplan(qs_batch_plan_s* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   qs_plan_free_device(b->d_blob, b->stream);
   qs_plan_free_device(b->d_items, b->stream);
+  qs_plan_free_device(b->d_counters, b->stream);
   delete b;
 }
 
@@ -79,7 +86,8 @@ void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t*
 // items by pass level, then by (T, R, has2), into launches.  Units that
 // share a plan share its device program.
 qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
-                                      const std::vector<BatchUnit>& units, bool from_zero, int threads) {
+                                      const std::vector<BatchUnit>& units, bool from_zero, int threads,
+                                      bool queue) {
   const int np = (int)plans.size();
   auto* B = new qs_batch_plan_s();
   B->device = h->device;
@@ -114,7 +122,45 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
     for (auto& p : plans) maxp = std::max(maxp, (int)p.pass_offsets.size());
     std::vector<PassItem> items;
     double bytes = 0, flops = 0;
-    for (int L = 0; L < maxp; ++L) {
+    if (queue) {
+      // one persistent launch: items level by level (larger tiles first
+      // within a level), each linked to its state's previous-level item
+      B->queue = true;
+      std::vector<uint32_t> last(units.size(), 0xffffffffu);
+      uint64_t tb = 0;
+      for (int L = 0; L < maxp; ++L) {
+        std::vector<std::pair<int, size_t>> lvl;  // (T, unit)
+        for (size_t u = 0; u < units.size(); ++u)
+          if (L < (int)plans[units[u].plan].pass_offsets.size()) lvl.push_back({plans[units[u].plan].pass_T[L], u});
+        std::stable_sort(lvl.begin(), lvl.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        for (auto& e : lvl) {
+          const BatchUnit& un = units[e.second];
+          const qs_plan_s& p = plans[un.plan];
+          PassItem it{};
+          it.state_off = un.state_off;
+          it.pass = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[un.plan] +
+                                                     p.pass_offsets[L]);
+          it.ntiles = 1ull << (p.n_qubits - p.pass_T[L]);
+          it.tile_begin = tb;
+          tb += it.ntiles;
+          it.flags = (L == 0 && from_zero) ? PI_FROM_ZERO : 0u;
+          it.pred = last[e.second];
+          if (it.pred != 0xffffffffu && B->q_withhold == 0xffffffffu) B->q_withhold = it.pred;
+          it.noise_seed = un.noise_seed;
+          it.noise_branch = un.noise_branch;
+          last[e.second] = (uint32_t)items.size();
+          items.push_back(it);
+          B->q_maxT = std::max(B->q_maxT, p.pass_T[L]);
+          B->q_has2 |= p.pass_has2[L];
+          B->q_ncoef = std::max(B->q_ncoef, p.pass_ncoef[L]);
+          bytes += ((L == 0 && from_zero) ? 8.0 : 16.0) * std::ldexp(1.0, p.n_qubits);
+        }
+      }
+      B->q_items = (int)items.size();
+      B->q_tiles = tb;
+      if (!items.empty()) QS_CUDA(cudaMallocAsync(&B->d_counters, sizeof(uint32_t) * (2 + items.size()), us));
+    }
+    for (int L = 0; L < (queue ? 0 : maxp); ++L) {
       // key: (T, R, has2); value: items and the largest coefficient pool
       std::map<std::tuple<int, int, int>, std::pair<std::vector<PassItem>, int>> groups;
       for (const BatchUnit& u : units) {
@@ -159,7 +205,7 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
     // blob/items are host temporaries: wait for the copies before they go
     QS_CUDA(cudaStreamSynchronize(us));
     B->info.n_circuits = (int32_t)units.size();
-    B->info.n_launches = (int32_t)B->launches.size();
+    B->info.n_launches = B->queue ? (B->q_items ? 1 : 0) : (int32_t)B->launches.size();
     B->info.n_items = (int64_t)items.size();
     B->info.max_passes = maxp;
     B->info.bytes_moved = bytes;
@@ -177,6 +223,16 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
 constexpr int kMaxSlices = 8;
 constexpr int kSliceMinCircuits = 256;
 
+// QSIM_BATCH_QUEUE=0 runs batches as one launch per (level, tile shape)
+// instead of one persistent launch.
+static bool batch_queue_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_BATCH_QUEUE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
                                     const qs_op* ops, const int64_t* state_off) {
   QS_CHECK_ARG(nc >= 0, "n_circuits must be >= 0");
@@ -189,11 +245,30 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
   plan_all(h, nc, widths, op_off, ops, plans);
   std::vector<BatchUnit> units(nc);
   for (int c = 0; c < nc; ++c) units[c] = BatchUnit{c, (uint64_t)state_off[c], 0, nullptr};
-  return qs_batch_build_units(h, plans, units, true);
+  return qs_batch_build_units(h, plans, units, true, 0, batch_queue_enabled());
+}
+
+// Bounded dependency waits: 4 s (a tile takes microseconds; the margin
+// covers time slicing with other processes); the wait test uses 50 ms and
+// withholds one item that has a dependent.
+static void launch_queue_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
+  uint32_t withhold = 0xffffffffu;
+  uint64_t limit = 4000000000ull;
+  if (h->wait_test == 2) {
+    withhold = B->q_withhold;
+    limit = 50000000ull;
+    h->wait_test = 0;
+  }
+  qs_launch_pass_queue(h, states, static_cast<const PassItem*>(B->d_items), B->q_items, B->q_tiles, B->q_maxT,
+                       B->q_has2, B->q_ncoef, B->d_counters, withhold, limit);
 }
 
 void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states) {
   B->stream = h->stream;
+  if (B->queue) {
+    launch_queue_batch(h, B, states);
+    return;
+  }
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
     qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
@@ -203,6 +278,10 @@ void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states) {
 void qs_batch_release(qs_batch_plan_s* B) { free_bplan(B); }
 
 static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
+  if (B->queue) {
+    launch_queue_batch(h, B, states);
+    return;
+  }
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
     qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
@@ -223,7 +302,7 @@ static bool graphs_enabled() {
 static void run_batch_graphed(qs_context* h, qs_batch_plan_s* B, void* states) {
   ++B->executions;
   B->stream = h->stream;
-  if (!graphs_enabled() || B->executions < 2 || B->launches.empty() || !h->own_stream) {
+  if (!graphs_enabled() || B->executions < 2 || B->info.n_launches == 0 || !h->own_stream || h->wait_test) {
     run_batch(h, B, states);
     return;
   }
@@ -258,10 +337,10 @@ static void run_batch_graphed(qs_context* h, qs_batch_plan_s* B, void* states) {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) throw qs_error(QS_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
     B->graph_states = states;
-    qs_count_launches(h, -(int64_t)B->launches.size());  // captured, not launched
+    qs_count_launches(h, -(int64_t)B->info.n_launches);  // captured, not launched
   }
   QS_CUDA(cudaGraphLaunch(B->graph, h->stream));
-  qs_count_launches(h, (int64_t)B->launches.size());
+  qs_count_launches(h, (int64_t)B->info.n_launches);
 }
 
 extern "C" {

@@ -201,7 +201,8 @@ int qs_device_status(qs_handle_t h, int* code) {
 int qs_set_wait_test(qs_handle_t h, int on) {
   QS_REQUIRE_HANDLE(h);
   QS_API_BEGIN
-  h->wait_test = on ? 1 : 0;
+  QS_CHECK_ARG(on >= 0 && on <= 2, "wait test: 0 off, 1 next pipelined pass, 2 next persistent batch launch");
+  h->wait_test = on;
   QS_API_END(h)
 }
 

@@ -235,7 +235,7 @@ struct __align__(16) PassItem {
   uint64_t ntiles;
   uint64_t tile_begin;   // prefix of ntiles over the item table
   uint32_t flags;
-  uint32_t pad0;
+  uint32_t pred;           // persistent batch launch: index of the same state's previous-pass item (~0u: none)
   uint64_t noise_seed;     // seed of the uniforms of the pass's noise blocks
   uint8_t* noise_branch;   // branch taken by each noise block (by DevOp.coef), or null
   uint64_t pad1;
@@ -249,6 +249,10 @@ void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, in
 void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
                           int maxT, int R, int has2, int ncoef, int threads = 0);
 
+// The whole batch in one persistent launch (qs_pass.cu, k_pass_queue).
+void qs_launch_pass_queue(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
+                          int maxT, int has2, int ncoef, uint32_t* counters, uint32_t withhold, uint64_t limit_ns);
+
 // Batch engine internals (qs_batch.cpp), shared with the noise-trajectory
 // runner: a batch is a set of host plans (each uploaded into one device
 // buffer) and units, each unit one state running one of the plans.
@@ -260,8 +264,10 @@ struct BatchUnit {
 };
 struct qs_batch_plan_s;
 // threads: CTA size of the batch's launches (0 = the tile-pass default).
+// queue: run the whole batch as one persistent launch (unitary programs only).
 qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s>& plans,
-                                      const std::vector<BatchUnit>& units, bool from_zero, int threads = 0);
+                                      const std::vector<BatchUnit>& units, bool from_zero, int threads = 0,
+                                      bool queue = false);
 void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states);
 void qs_batch_release(qs_batch_plan_s* B);
 

@@ -537,7 +537,10 @@ std::string gen_pass(const DevPass& P, const DevBlock* blocks, const DevOp* ops,
        "      asm volatile(\"cp.async.commit_group;\\ncp.async.wait_group 0;\\n\" ::: \"memory\");\n"
        "    }\n"
        "    __syncthreads();\n";
+  // a from-|0> pass leaves every tile but the first of each state at +0
+  s << "    if (!(flags & 1u) || (gbase & nmask) == 0ull) {\n";
   for (int b = 0; b < P.nblocks; ++b) s << "    blk" << b << "(gbase);\n    __syncthreads();\n";
+  s << "    }\n";
   s << "    for (u32 c = threadIdx.x; c < " << npairs << "u; c += " << threads
     << "u) {\n"
        "      const u32 i = c << 1;\n"
@@ -952,10 +955,14 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
   s << "      if (lt == 0u && (gbase & nmask) == 0ull) tile[0] = make_float2(1.f, 0.f);  // lt 0 zeroed t4[0]\n";
   s << "      consumers_sync(grp);\n";
   s << "    }\n";
+  // a from-|0> pass leaves every tile but the first of each state at +0
+  // (the interpreter skips them too, so both give the same bits)
+  s << "    if (!from_zero || (gbase & nmask) == 0ull) {\n";
   for (int b = 0; b < P.nblocks; ++b) {
     s << "    blk" << b << "(soff, gbase, dep_lo, lt);\n";
     if (b + 1 < P.nblocks) s << "    consumers_sync(grp);\n";
   }
+  s << "    }\n";
   s << "    asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n";
   s << "    mb_arrive(bar_done + 8u * st);\n";
   s << "  }\n";
@@ -1349,7 +1356,7 @@ void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t i, void* state, uin
     // bounded waits: 4 s (a tile's copy takes microseconds; the margin covers
     // time slicing with other processes); the wait test uses 50 ms
     uint64_t limit = 4000000000ull;
-    if (h->wait_test) {
+    if (h->wait_test == 1) {
       fl |= 4u;
       limit = 50000000ull;
       h->wait_test = 0;

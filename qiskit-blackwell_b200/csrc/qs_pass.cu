@@ -661,6 +661,51 @@ __device__ __noinline__ void noise_block(float2* tile, int T, const DevBlock blk
   }
 }
 
+// One register block over the tile: every thread gathers the 2^R amplitudes
+// of each of its groups (Gray-code walk over the swizzled addresses), runs
+// the block's ops in registers and scatters them back.
+template <int R, bool TWO>
+__device__ __forceinline__ void register_block(float2* tile, const DevBlock& blk, const DevOp* __restrict__ ops,
+                                               const float2* __restrict__ s_coef, uint32_t ngroups, uint64_t gbase,
+                                               const uint64_t* dep_lo, const uint64_t* dep_hi) {
+  int pos[R];
+  uint32_t pp[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) { pos[k] = blk.pos[k]; pp[k] = phys(1u << pos[k]); }
+  const bool need_g = blk.pos[7] != 0;
+  for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+    uint32_t base = g;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const uint32_t lo = base & ((1u << pos[k]) - 1u);
+      base = ((base ^ lo) << 1) | lo;
+    }
+    const uint32_t pb = phys(base);
+    const uint64_t gidx = need_g ? (gbase | dep_lo[base & 127] | dep_hi[base >> 7]) : 0ull;
+    float2 v[1 << R];
+    // Gray-code walk: consecutive indices differ in one register bit
+    {
+      uint32_t a = pb;
+#pragma unroll
+      for (int q = 0; q < (1 << R); ++q) {
+        const int j = q ^ (q >> 1);
+        if (q) a ^= pp[__ffs(q) - 1];
+        v[j] = tile[a];
+      }
+    }
+    run_ops<R, TWO>(v, ops, blk.op_begin, blk.op_end, s_coef, gidx);
+    {
+      uint32_t a = pb;
+#pragma unroll
+      for (int q = 0; q < (1 << R); ++q) {
+        const int j = q ^ (q >> 1);
+        if (q) a ^= pp[__ffs(q) - 1];
+        tile[a] = v[j];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------- the kernel ----
 // R = 5 keeps 32 amplitudes (64 registers) per thread: 128-thread CTAs, 3 per
 // SM.  Narrower blocks use 256 threads.
@@ -730,10 +775,12 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
 
     // 1. load the tile (pairs (2c, 2c+1) are adjacent in HBM: S[0] == 0)
     const uint32_t npairs = 1u << (T - 1);
+    // |0..0>: only the tile holding index 0 of its state has a non-zero
+    // entry (the bits above n_qubits select the state in a batch); every
+    // other tile of a from-|0> pass stays +0 and skips the register blocks
+    const bool zero_tile = (I.flags & PI_FROM_ZERO) && (gbase & ((1ull << P->n_qubits) - 1ull)) != 0ull;
     if (I.flags & PI_FROM_ZERO) {
-      // |0..0>: only the tile holding index 0 of its state has a non-zero
-      // entry (the bits above n_qubits select the state in a batch)
-      const bool first = (gbase & ((1ull << P->n_qubits) - 1ull)) == 0ull;
+      const bool first = !zero_tile;
       for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
         const uint32_t i = c << 1;
         const float x = (first && i == 0) ? 1.f : 0.f;
@@ -752,7 +799,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
     // 2. register blocks
     const DevBlock* blocks = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off);
     const DevOp* ops = reinterpret_cast<const DevOp*>(reinterpret_cast<const char*>(P) + P->op_off);
-    const int nblocks = P->nblocks;
+    const int nblocks = zero_tile ? 0 : P->nblocks;
     const uint32_t ngroups = 1u << (T - R);
     for (int b = 0; b < nblocks; ++b) {
       const DevBlock blk = blocks[b];
@@ -761,42 +808,7 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
         __syncthreads();
         continue;
       }
-      int pos[R];
-      uint32_t pp[R];
-#pragma unroll
-      for (int k = 0; k < R; ++k) { pos[k] = blk.pos[k]; pp[k] = phys(1u << pos[k]); }
-      const bool need_g = blk.pos[7] != 0;
-      for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
-        uint32_t base = g;
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const uint32_t lo = base & ((1u << pos[k]) - 1u);
-          base = ((base ^ lo) << 1) | lo;
-        }
-        const uint32_t pb = phys(base);
-        const uint64_t gidx = need_g ? (gbase | dep_lo[base & 127] | dep_hi[base >> 7]) : 0ull;
-        float2 v[1 << R];
-        // Gray-code walk: consecutive indices differ in one register bit
-        {
-          uint32_t a = pb;
-#pragma unroll
-          for (int q = 0; q < (1 << R); ++q) {
-            const int j = q ^ (q >> 1);
-            if (q) a ^= pp[__ffs(q) - 1];
-            v[j] = tile[a];
-          }
-        }
-        run_ops<R, TWO>(v, ops, blk.op_begin, blk.op_end, s_coef, gidx);
-        {
-          uint32_t a = pb;
-#pragma unroll
-          for (int q = 0; q < (1 << R); ++q) {
-            const int j = q ^ (q >> 1);
-            if (q) a ^= pp[__ffs(q) - 1];
-            tile[a] = v[j];
-          }
-        }
-      }
+      register_block<R, TWO>(tile, blk, ops, s_coef, ngroups, gbase, dep_lo, dep_hi);
       __syncthreads();
     }
 
@@ -807,6 +819,152 @@ k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restr
       *reinterpret_cast<float4*>(state + g) = *reinterpret_cast<const float4*>(tile + phys(i));
     }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------- persistent batch kernel -
+// Every (state, pass) item of a batch in one launch.  Items are numbered
+// level by level (every state's first pass, then every second pass, ...) and
+// their tiles consecutively; CTAs take tiles one at a time from a device
+// counter in that order.  Before a tile of item i, the CTA waits until item
+// pred(i) (PassItem.pred: the same state's previous pass) has stored all its
+// tiles, counted per item.  Tiles are handed out in order and every CTA that
+// holds one is running, so a wait only depends on tiles already taken by
+// running CTAs.  Each wait is bounded (`limit` ns of %globaltimer): when it
+// runs out the CTA ORs 4 into the status word and takes no further tile.
+// `withhold` names an item whose tiles are not counted (a test hook; ~0u
+// otherwise), so that the waits of its dependents run out.
+constexpr uint32_t kNoPred = 0xffffffffu;
+
+__device__ __forceinline__ uint64_t q_gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ uint32_t q_ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <int R, bool TWO>
+__device__ __forceinline__ void queue_blocks(float2* tile, const DevPass* P, const float2* s_coef, uint64_t gbase,
+                                             const uint64_t* dep_lo, const uint64_t* dep_hi) {
+  const DevBlock* blocks = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off);
+  const DevOp* ops = reinterpret_cast<const DevOp*>(reinterpret_cast<const char*>(P) + P->op_off);
+  const uint32_t ngroups = 1u << (P->T - R);
+  for (int b = 0; b < P->nblocks; ++b) {
+    register_block<R, TWO>(tile, blocks[b], ops, s_coef, ngroups, gbase, dep_lo, dep_hi);
+    __syncthreads();
+  }
+}
+
+template <bool TWO, bool BIG>
+__global__ void __launch_bounds__(BIG ? 256 : 128, BIG ? 1 : 2)
+k_pass_queue(float2* __restrict__ base_state, const PassItem* __restrict__ items, int nitems, uint64_t total_tiles,
+             uint32_t coef_off_bytes, uint32_t dep_off_bytes, uint32_t* __restrict__ counters,
+             uint32_t* __restrict__ status, uint64_t limit, uint32_t withhold) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);
+  float2* s_coef = reinterpret_cast<float2*>(smem_raw + coef_off_bytes);
+  uint64_t* dep_lo = reinterpret_cast<uint64_t*>(smem_raw + dep_off_bytes);
+  uint64_t* dep_hi = dep_lo + 128;
+  int* s_S = reinterpret_cast<int*>(dep_hi + 128);
+  __shared__ unsigned long long s_task;
+  __shared__ int s_fail;
+  unsigned long long* next = reinterpret_cast<unsigned long long*>(counters);  // counters[0..1]
+  uint32_t* done = counters + 2;
+  int cur = -1;
+  const DevPass* P = nullptr;
+  for (;;) {
+    if (threadIdx.x == 0) s_task = atomicAdd(next, 1ull);
+    __syncthreads();
+    const uint64_t t = s_task;
+    if (t >= total_tiles) break;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+    }
+    const int it = lo;
+    const PassItem I = items[it];
+    if (threadIdx.x == 0) {
+      s_fail = 0;
+      if (I.pred != kNoPred) {
+        const uint32_t need = (uint32_t)items[I.pred].ntiles;
+        if (q_ld_acquire(done + I.pred) < need) {
+          const uint64_t t0 = q_gtimer();
+          while (q_ld_acquire(done + I.pred) < need) {
+            if (q_gtimer() - t0 > limit) {
+              s_fail = 1;
+              break;
+            }
+            __nanosleep(256);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (s_fail) {
+      if (threadIdx.x == 0) atomicOr(status, 4u);
+      break;
+    }
+    if (it != cur) {
+      cur = it;
+      P = I.pass;
+      if (threadIdx.x < 16) s_S[threadIdx.x] = P->S[threadIdx.x];
+      const float2* gcoef = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(P) + P->coef_off);
+      for (uint32_t k = threadIdx.x; k < P->ncoef; k += blockDim.x) s_coef[k] = gcoef[k];
+      __syncthreads();
+      for (int e = threadIdx.x; e < 256; e += blockDim.x) {
+        const int part = e >> 7, x = e & 127;
+        uint64_t d = 0;
+        for (int k = 0; k < 7; ++k) {
+          const int kk = part * 7 + k;
+          if (kk < P->T && ((x >> k) & 1)) d |= 1ull << s_S[kk];
+        }
+        if (part == 0) dep_lo[x] = d; else dep_hi[x] = d;
+      }
+      __syncthreads();
+    }
+    const int T = P->T;
+    float2* state = base_state + I.state_off;
+    uint64_t gbase = t - I.tile_begin;
+    for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, s_S[k]);
+    const uint32_t npairs = 1u << (T - 1);
+    const bool zero_tile = (I.flags & PI_FROM_ZERO) && (gbase & ((1ull << P->n_qubits) - 1ull)) != 0ull;
+    if (I.flags & PI_FROM_ZERO) {
+      for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+        const uint32_t i = c << 1;
+        const float x = (!zero_tile && i == 0) ? 1.f : 0.f;
+        *reinterpret_cast<float4*>(tile + phys(i)) = make_float4(x, 0.f, 0.f, 0.f);
+      }
+    } else {
+      for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+        const uint32_t i = c << 1;
+        const uint64_t g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];
+        cp_async16(tile + phys(i), state + g);
+      }
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    if (!zero_tile) {
+      switch (P->R) {
+        case 1: queue_blocks<1, TWO>(tile, P, s_coef, gbase, dep_lo, dep_hi); break;
+        case 2: queue_blocks<2, TWO>(tile, P, s_coef, gbase, dep_lo, dep_hi); break;
+        case 3: queue_blocks<3, TWO>(tile, P, s_coef, gbase, dep_lo, dep_hi); break;
+        case 4: queue_blocks<4, TWO>(tile, P, s_coef, gbase, dep_lo, dep_hi); break;
+        default: queue_blocks<5, TWO>(tile, P, s_coef, gbase, dep_lo, dep_hi); break;
+      }
+    }
+    for (uint32_t c = threadIdx.x; c < npairs; c += blockDim.x) {
+      const uint32_t i = c << 1;
+      const uint64_t g = gbase | dep_lo[i & 127] | dep_hi[i >> 7];
+      *reinterpret_cast<float4*>(state + g) = *reinterpret_cast<const float4*>(tile + phys(i));
+    }
+    __threadfence();   // this thread's stores, before the tile is counted
+    __syncthreads();
+    if (threadIdx.x == 0 && (uint32_t)it != withhold) atomicAdd(done + it, 1u);
   }
 }
 
@@ -906,6 +1064,45 @@ void dispatch(qs_context* h, float2* base, const PassItem& single, const PassIte
   else dispatch_two<false>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
 }
 
+template <bool TWO, bool BIG>
+void launch_queue(qs_context* h, float2* base, const PassItem* d_items, int nitems, uint64_t total, int maxT,
+                  int ncoef, uint32_t* counters, uint32_t withhold, uint64_t limit) {
+  const int threads = BIG ? 256 : 128;
+  const uint32_t tile_bytes = (uint32_t)(sizeof(float2) << maxT);
+  const uint32_t coef_off = tile_bytes;
+  const uint32_t dep_off = coef_off + (uint32_t)coef_bytes_for(ncoef);
+  const int smem = (int)(dep_off + 2 * 128 * sizeof(uint64_t) + 16 * sizeof(int));
+  QS_CHECK_ARG(smem <= kMaxPassSmem, "tile-pass program too large for shared memory (coefficient pool)");
+  int per_sm = 0;
+  {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int>, int> cache;
+    static std::set<int> attr_set;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!attr_set.count(h->device)) {
+      QS_CUDA(cudaFuncSetAttribute(k_pass_queue<TWO, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxPassSmem));
+      attr_set.insert(h->device);
+    }
+    auto key = std::make_tuple(h->device, smem);
+    auto f = cache.find(key);
+    if (f != cache.end()) {
+      per_sm = f->second;
+    } else {
+      QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass_queue<TWO, BIG>, threads, smem));
+      if (per_sm < 1) throw qs_error(QS_ERR_CUDA, "persistent batch kernel does not fit on an SM");
+      cache[key] = per_sm;
+    }
+  }
+  // every CTA is resident at once (grid <= CTAs per SM x SMs): a CTA waiting
+  // on a dependency only waits on tiles that running CTAs hold
+  const uint64_t grid = std::min<uint64_t>(total, (uint64_t)h->sm_count * per_sm);
+  if (grid == 0) return;
+  QS_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (2 + (size_t)nitems), h->stream));
+  k_pass_queue<TWO, BIG><<<(unsigned)grid, threads, smem, h->stream>>>(base, d_items, nitems, total, coef_off, dep_off,
+                                                                      counters, h->dev_status, limit, withhold);
+  qs_after_launch(h, "k_pass_queue");
+}
+
 }  // namespace
 
 // One state, one pass: the item is passed by value (no device table), so the
@@ -928,4 +1125,22 @@ void qs_launch_pass_items(qs_context* h, void* base, const PassItem* d_items, in
   if (n_items <= 0 || total_tiles == 0) return;
   PassItem dummy{};
   dispatch(h, (float2*)base, dummy, d_items, n_items, total_tiles, maxT, R, has2, ncoef, threads);
+}
+
+// The whole batch in one persistent launch (k_pass_queue): d_items holds the
+// items level by level with tile_begin prefix sums and pred links; counters
+// is a device buffer of 2 + n_items words (zeroed here, stream-ordered).
+void qs_launch_pass_queue(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles,
+                          int maxT, int has2, int ncoef, uint32_t* counters, uint32_t withhold, uint64_t limit_ns) {
+  if (n_items <= 0 || total_tiles == 0) return;
+  QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
+  const bool big = maxT >= 14;
+  float2* b = static_cast<float2*>(base);
+  if (has2) {
+    if (big) launch_queue<true, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    else launch_queue<true, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+  } else {
+    if (big) launch_queue<false, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    else launch_queue<false, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+  }
 }

@@ -329,3 +329,39 @@ np.save(sys.argv[1], np.concatenate([e, g.ravel()]))
         subprocess.run([sys.executable, "-c", code, path], env=env, check=True, timeout=300)
         out[flag] = np.load(path)
     np.testing.assert_allclose(out["1"], out["0"], atol=1e-6)
+
+
+def test_batch_is_one_persistent_launch_with_bounded_waits():
+    """A batch plan runs as one persistent launch (tiles taken from a device
+    counter level by level, each state's next pass waiting for its previous
+    one).  With one pass of one state left uncounted (the wait-test hook),
+    the dependent waits run out after 50 ms, the status word reports them,
+    and the next execution is complete and right."""
+    import ctypes as C
+    widths, oo, ops, so = W.qv_batch(24, 14, 18, seed=41)
+    bp = E.BatchPlan(widths, oo, ops, so)
+    assert bp.info["n_launches"] == 1 and bp.info["max_passes"] >= 2
+    st = bp.alloc_states()
+    h = E._h()
+    code = C.c_int(-1)
+    h.call("qs_device_status", C.byref(code))
+    assert code.value == 0
+    l0 = h.launches()
+    bp.execute(st)
+    torch.cuda.synchronize()
+    assert h.launches() - l0 == 1
+    h.call("qs_set_wait_test", 2)
+    bp.execute(st)
+    torch.cuda.synchronize()
+    h.call("qs_device_status", C.byref(code))
+    assert code.value == 4, code.value
+    st.zero_()
+    bp.execute(st)
+    torch.cuda.synchronize()
+    h.call("qs_device_status", C.byref(code))
+    assert code.value == 0
+    allv = st.cpu().numpy()
+    for c in range(len(widths)):
+        n = int(widths[c])
+        got = allv[so[c]: so[c] + (1 << n)]
+        assert abs(1 - O.fidelity(got, O.simulate(n, ops[oo[c]: oo[c + 1]]))) <= 1e-6, c
