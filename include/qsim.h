@@ -186,6 +186,14 @@ int qs_apply_2q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_d
 int qs_apply_diag1_dev(qs_handle_t h, void* state, int n_qubits, const void* diag_dev, int target);
 int qs_apply_mc1q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_dev, const int* controls,
                       int n_controls, int target);
+/* Reference: bwk/csrc/apply_diagonal_sm120.cu:177-208 (apply_diagonal_2q with
+ * a CUDA tensor): as qs_apply_diag2 with the 4 diagonal entries in device
+ * memory (complex64), read by the kernel.                                  */
+int qs_apply_diag2_dev(qs_handle_t h, void* state, int n_qubits, const void* diag_dev, int q0, int q1);
+/* Reference: bwk/csrc/apply_mc2qgate_sm120.cu:127-196 (apply_mc2qgate with a
+ * CUDA tensor): as qs_apply_mc2q with the 4x4 in device memory.           */
+int qs_apply_mc2q_dev(qs_handle_t h, void* state, int n_qubits, const void* gate_dev, const int* controls,
+                      int n_controls, int t0, int t1);
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:64-83,150-175 (apply_diagonal_phase) */
 int qs_apply_phase(qs_handle_t h, void* state, int n_qubits, float phase_re, float phase_im, int target);
 /* Reference: bwk/csrc/apply_diagonal_sm120.cu:88-105,177-208 (apply_diagonal_2q);

@@ -173,7 +173,8 @@ __global__ void k_phase_tn(float2* __restrict__ s, uint64_t nitems, int t, float
   }
 }
 
-__global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G2 D) {
+__global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G2 D0, const float2* __restrict__ gd) {
+  const G2 D = gate2(D0, gd);
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     uint64_t idx = 2 * i;
     float4 v = ld4(s + idx);
@@ -198,7 +199,9 @@ __global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64
   }
 }
 
-__global__ void k_mc2q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int lo, int hi, G4 G) {
+__global__ void k_mc2q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int lo, int hi, G4 G0,
+                       const float2* __restrict__ gd) {
+  const G4 G = gate4(G0, gd, 0);
   const uint64_t sl = 1ull << lo, sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i = insert_zeros(it, P.pos, P.k) | cmask;
@@ -545,7 +548,22 @@ int qs_apply_diag2(qs_handle_t h, void* state, int n, const float* diag, int q0,
   G2 D = load_g2(diag);
   int lo = std::min(q0, q1), hi = std::max(q0, q1);
   uint64_t nvec = (1ull << n) / 2;
-  LAUNCH(h, k_diag2, nvec, (float2*)state, nvec, lo, hi, D);
+  LAUNCH(h, k_diag2, nvec, (float2*)state, nvec, lo, hi, D, nullptr);
+  QS_API_END(h)
+}
+
+int qs_apply_diag2_dev(qs_handle_t h, void* state, int n, const void* diag_dev, int q0, int q1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(n >= 2, "a 2-qubit gate needs n >= 2");
+  qs_check_qubit(q0, n, "qubit0");
+  qs_check_qubit(q1, n, "qubit1");
+  QS_CHECK_ARG(q0 != q1, "qubit0 and qubit1 must differ");
+  check_dev_ptr(h, diag_dev, "diag");
+  const int lo = std::min(q0, q1), hi = std::max(q0, q1);
+  const uint64_t nvec = (1ull << n) / 2;
+  LAUNCH(h, k_diag2, nvec, (float2*)state, nvec, lo, hi, G2{}, static_cast<const float2*>(diag_dev));
   QS_API_END(h)
 }
 
@@ -594,7 +612,34 @@ int qs_apply_mc2q(qs_handle_t h, void* state, int n, const float* gate, const in
   all[nc + 1] = hi;
   Sorted P = make_sorted(all, nc + 2);
   uint64_t items = 1ull << (n - nc - 2);
-  LAUNCH(h, k_mc2q, items, (float2*)state, items, P, cmask, lo, hi, G);
+  LAUNCH(h, k_mc2q, items, (float2*)state, items, P, cmask, lo, hi, G, nullptr);
+  QS_API_END(h)
+}
+
+int qs_apply_mc2q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, const int* controls, int nc, int t0,
+                      int t1) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  qs_check_qubit(t0, n, "target0");
+  qs_check_qubit(t1, n, "target1");
+  QS_CHECK_ARG(t0 != t1, "target0 and target1 must differ");
+  check_controls(controls, nc, n);
+  QS_CHECK_ARG(nc + 2 <= n, "more gate qubits than state qubits");
+  check_dev_ptr(h, gate_dev, "gate");
+  const int lo = std::min(t0, t1), hi = std::max(t0, t1);
+  int all[QS_MAX_CONTROLS + 2];
+  uint64_t cmask = 0;
+  for (int i = 0; i < nc; ++i) {
+    QS_CHECK_ARG(controls[i] != t0 && controls[i] != t1, "target qubits must not appear in controls");
+    all[i] = controls[i];
+    cmask |= 1ull << controls[i];
+  }
+  all[nc] = lo;
+  all[nc + 1] = hi;
+  Sorted P = make_sorted(all, nc + 2);
+  const uint64_t items = 1ull << (n - nc - 2);
+  LAUNCH(h, k_mc2q, items, (float2*)state, items, P, cmask, lo, hi, G4{}, static_cast<const float2*>(gate_dev));
   QS_API_END(h)
 }
 

@@ -140,6 +140,10 @@ def apply_diagonal_phase(state: torch.Tensor, phase: complex, target_qubit: int)
 
 def apply_diagonal_2q(state: torch.Tensor, diag: torch.Tensor, qubit0: int, qubit1: int) -> torch.Tensor:
     n = check_state(state)
+    dd = _gate_dev(diag, (4,), state)
+    if dd is not None:
+        _h(state.get_device()).call("qs_apply_diag2_dev", state.data_ptr(), n, dd.data_ptr(), int(qubit0), int(qubit1))
+        return state
     d = _gate_host(diag, (4,))
     _h(state.device.index).call("qs_apply_diag2", _ptr(state), n, _fp(d), int(qubit0), int(qubit1))
     return state
@@ -181,11 +185,17 @@ def apply_mcgate(state: torch.Tensor, gate: torch.Tensor, controls, target_qubit
 def apply_mc2qgate(state: torch.Tensor, gate: torch.Tensor, controls, target0: int, target1: int) -> torch.Tensor:
     """Multi-controlled 4x4 (cuquantum.py:320-337); bit 0 = min(target0, target1)."""
     n = check_state(state)
-    g = _gate_host(gate, (4, 4))
     c = _ints(controls)
     if c.size > 7:
         raise RuntimeError("controls must have 0-7 elements")
     h = _h(state.device.index)
+    gd = _gate_dev(gate, (4, 4), state)
+    if gd is not None:
+        # read on the device (a SWAP there is still exact: 0/1 products)
+        h.call("qs_apply_mc2q_dev", state.data_ptr(), n, gd.data_ptr(), _ip(c), int(c.size), int(target0),
+               int(target1))
+        return state
+    g = _gate_host(gate, (4, 4))
     if _is_swap(g):
         h.call("qs_apply_mcswap", _ptr(state), n, _ip(c), int(c.size), int(target0), int(target1))
     else:

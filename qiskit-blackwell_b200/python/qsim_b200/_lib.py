@@ -104,6 +104,8 @@ SIGNATURES = {
     "qs_apply_2q_dev": (_i, [_vp, _vp, _i, _vp, _i, _i]),
     "qs_apply_diag1_dev": (_i, [_vp, _vp, _i, _vp, _i]),
     "qs_apply_mc1q_dev": (_i, [_vp, _vp, _i, _vp, _pi, _i, _i]),
+    "qs_apply_diag2_dev": (_i, [_vp, _vp, _i, _vp, _i, _i]),
+    "qs_apply_mc2q_dev": (_i, [_vp, _vp, _i, _vp, _pi, _i, _i, _i]),
     "qs_apply_mc1q": (_i, [_vp, _vp, _i, _pf, _pi, _i, _i]),
     "qs_apply_mc2q": (_i, [_vp, _vp, _i, _pf, _pi, _i, _i, _i]),
     "qs_apply_mcx": (_i, [_vp, _vp, _i, _pi, _i, _i]),

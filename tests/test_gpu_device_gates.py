@@ -69,6 +69,28 @@ def test_mcgate_device_equals_host_and_x_is_exact():
     assert np.array_equal(after, expect)
 
 
+def test_diag2_and_mc2q_device_equal_host_and_swap_is_exact():
+    rng = np.random.default_rng(5)
+    d = torch.from_numpy(np.exp(1j * rng.uniform(0, 6.28, 4)).astype(np.complex64)).cuda()
+    a, b = _state(9, 6), _state(9, 6)
+    bk.apply_diagonal_2q(a, d, 7, 2)
+    bk.apply_diagonal_2q(b, d.cpu(), 7, 2)
+    assert np.array_equal(_bits(a), _bits(b))
+    u = bk.random_unitary_4x4().contiguous()
+    bk.apply_mc2qgate(a, u, [1, 4], 6, 0)
+    bk.apply_mc2qgate(b, u.cpu(), [1, 4], 6, 0)
+    assert np.array_equal(_bits(a), _bits(b))
+    sw = torch.eye(4, dtype=torch.complex64, device="cuda")[[0, 2, 1, 3]].contiguous()
+    before = a.cpu().numpy()
+    bk.apply_mc2qgate(a, sw, [8], 3, 5)              # controlled SWAP on the device: values move exactly
+    after = a.cpu().numpy()
+    idx = np.arange(512)
+    swap = ((idx >> 8) & 1 == 1) & (((idx >> 3) & 1) != ((idx >> 5) & 1))
+    expect = before.copy()
+    expect[swap] = before[idx[swap] ^ ((1 << 3) | (1 << 5))]
+    assert np.array_equal(after, expect)
+
+
 def test_host_pointer_rejected():
     a = _state(4, 4)
     host = np.eye(2, dtype=np.complex64)
