@@ -75,13 +75,44 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             for f in futs:
                 f.result()
     if jobs or not os.path.exists(LIB):
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread", "-ldl"]
+        cmd = [nvcc, *ARCH, "-shared", "-Xlinker", "-soname=libqsim.so", "-o", LIB, *objs, "-lpthread", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 
+PYEXT_SRC = os.path.join(HERE, "pyext", "qs_fast.c")
+
+
+def pyext_path() -> str:
+    import sysconfig
+    return os.path.join(LIBDIR, "_qsfast" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def build_pyext(force: bool = False) -> str | None:
+    """The CPython extension behind blackwell_kernels' per-gate calls
+    (pyext/qs_fast.c, linked against lib/libqsim.so).  Returns its path, or
+    None when no C compiler or Python headers are available (the ctypes path
+    is used then)."""
+    import sysconfig
+    out = pyext_path()
+    inc = sysconfig.get_paths().get("include", "")
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(PYEXT_SRC),
+                                                                           os.path.getmtime(LIB)):
+        return out
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc or not os.path.exists(os.path.join(inc, "Python.h")):
+        return None
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-I", inc, PYEXT_SRC, "-L", LIBDIR, "-lqsim",
+           "-Wl,-rpath,$ORIGIN", "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"extension build failed:\n{r.stdout}\n{r.stderr}")
+    return out
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv)
+    build_pyext()
     print(LIB)

@@ -19,8 +19,30 @@ import math
 import numpy as np
 import torch
 
+from qsim_b200 import _lib
 from qsim_b200 import engine as E
 from qsim_b200.engine import _h, _ptr, check_state
+
+_C64 = torch.complex64
+
+
+def _fast_args(state, gate, shape):
+    """(extension, handle, n, state pointer, gate pointer) for a direct call
+    into libqsim when state and gate are contiguous complex64 CUDA tensors on
+    one device and the gate has `shape`; None otherwise (the general path then
+    checks the arguments and reports what is wrong)."""
+    F = _lib.fast()
+    if F is None or type(state) is not torch.Tensor or type(gate) is not torch.Tensor:
+        return None
+    if not state.is_cuda or state.dtype != _C64 or gate.dtype != _C64 or gate.shape != shape:
+        return None
+    dev = state.get_device()
+    if gate.get_device() != dev or not state.is_contiguous() or not gate.is_contiguous():
+        return None
+    N = state.numel()
+    if N < 2 or N & (N - 1):
+        return None
+    return F, E._hptr(dev), N.bit_length() - 1, state.data_ptr(), gate.data_ptr()
 
 
 def _gate_host(gate, shape) -> np.ndarray:
@@ -63,6 +85,10 @@ def _ints(x) -> np.ndarray:
 # ------------------------------------------------------------------- gates
 def apply_gate(state: torch.Tensor, gate: torch.Tensor, target_qubit: int) -> torch.Tensor:
     """Single-qubit gate in place (cuquantum.py:40-51)."""
+    a = _fast_args(state, gate, (2, 2))
+    if a is not None:
+        a[0].apply_1q_dev(a[1], a[3], a[2], a[4], int(target_qubit))
+        return state
     n = check_state(state)
     gd = _gate_dev(gate, (2, 2), state)
     if gd is not None:
@@ -76,10 +102,14 @@ def apply_gate(state: torch.Tensor, gate: torch.Tensor, target_qubit: int) -> to
 def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: int) -> torch.Tensor:
     """Two-qubit gate in place (cuquantum.py:54-66).  As in the reference
     (apply_gate2q_sm120.cu:244-247) bit 0 of the 4x4 index is min(q0, q1)."""
-    n = check_state(state)
     if qubit0 == qubit1:
         raise RuntimeError("qubit0 and qubit1 must differ")
     lo, hi = min(qubit0, qubit1), max(qubit0, qubit1)
+    a = _fast_args(state, gate, (4, 4))
+    if a is not None:
+        a[0].apply_2q_dev(a[1], a[3], a[2], a[4], int(lo), int(hi))
+        return state
+    n = check_state(state)
     gd = _gate_dev(gate, (4, 4), state)
     if gd is not None:
         _h(state.get_device()).call("qs_apply_2q_dev", state.data_ptr(), n, gd.data_ptr(), int(lo), int(hi))
@@ -119,6 +149,10 @@ def apply_gates_reg_tiled(state: torch.Tensor, gates: torch.Tensor, targets: tor
 
 
 def apply_diagonal(state: torch.Tensor, diag: torch.Tensor, target_qubit: int) -> torch.Tensor:
+    a = _fast_args(state, diag, (2,))
+    if a is not None:
+        a[0].apply_diag1_dev(a[1], a[3], a[2], a[4], int(target_qubit))
+        return state
     n = check_state(state)
     dd = _gate_dev(diag, (2,), state)
     if dd is not None:
@@ -131,14 +165,26 @@ def apply_diagonal(state: torch.Tensor, diag: torch.Tensor, target_qubit: int) -
 
 def apply_diagonal_phase(state: torch.Tensor, phase: complex, target_qubit: int) -> torch.Tensor:
     """Multiply the bit=1 amplitudes of target_qubit by phase (half traffic)."""
-    n = check_state(state)
     phase = complex(phase)
+    F = _lib.fast()
+    if F is not None and type(state) is torch.Tensor and state.is_cuda and state.dtype == _C64 \
+            and state.is_contiguous():
+        N = state.numel()
+        if N >= 2 and not N & (N - 1):
+            F.apply_phase(E._hptr(state.get_device()), state.data_ptr(), N.bit_length() - 1, phase.real, phase.imag,
+                          int(target_qubit))
+            return state
+    n = check_state(state)
     _h(state.device.index).call("qs_apply_phase", _ptr(state), n, C.c_float(phase.real), C.c_float(phase.imag),
                                 int(target_qubit))
     return state
 
 
 def apply_diagonal_2q(state: torch.Tensor, diag: torch.Tensor, qubit0: int, qubit1: int) -> torch.Tensor:
+    a = _fast_args(state, diag, (4,))
+    if a is not None:
+        a[0].apply_diag2_dev(a[1], a[3], a[2], a[4], int(qubit0), int(qubit1))
+        return state
     n = check_state(state)
     dd = _gate_dev(diag, (4,), state)
     if dd is not None:
@@ -163,6 +209,10 @@ def _is_swap(g: np.ndarray) -> bool:
 
 def apply_mcgate(state: torch.Tensor, gate: torch.Tensor, controls, target_qubit: int) -> torch.Tensor:
     """Multi-controlled 2x2 (cuquantum.py:297-317); an exact X moves values."""
+    a = _fast_args(state, gate, (2, 2))
+    if a is not None and isinstance(controls, (list, tuple)):
+        a[0].apply_mc1q_dev(a[1], a[3], a[2], a[4], controls, int(target_qubit))
+        return state
     n = check_state(state)
     c = _ints(controls)
     if c.size > 7:
@@ -184,6 +234,10 @@ def apply_mcgate(state: torch.Tensor, gate: torch.Tensor, controls, target_qubit
 
 def apply_mc2qgate(state: torch.Tensor, gate: torch.Tensor, controls, target0: int, target1: int) -> torch.Tensor:
     """Multi-controlled 4x4 (cuquantum.py:320-337); bit 0 = min(target0, target1)."""
+    a = _fast_args(state, gate, (4, 4))
+    if a is not None and isinstance(controls, (list, tuple)):
+        a[0].apply_mc2q_dev(a[1], a[3], a[2], a[4], controls, int(target0), int(target1))
+        return state
     n = check_state(state)
     c = _ints(controls)
     if c.size > 7:

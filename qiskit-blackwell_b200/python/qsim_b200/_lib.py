@@ -242,6 +242,35 @@ class Handle:
 
 _handles = threading.local()
 
+_fast_mod = False   # not looked up yet
+
+
+def fast():
+    """The _qsfast CPython extension (direct calls into the per-gate entry
+    points, no ctypes marshalling) when it is built and binds the same
+    libqsim.so this process loaded; None otherwise (QSIM_LIB naming another
+    build, or no extension)."""
+    global _fast_mod
+    if _fast_mod is False:
+        _fast_mod = None
+        try:
+            import importlib.machinery
+            import importlib.util
+            import sysconfig
+            lib = load()
+            libdir = os.path.dirname(DEFAULT_LIB)
+            path = os.path.join(libdir, "_qsfast" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+            if lib is not None and os.path.exists(path) and os.path.realpath(lib_path()) == os.path.realpath(DEFAULT_LIB):
+                loader = importlib.machinery.ExtensionFileLoader("_qsfast", path)
+                spec = importlib.util.spec_from_file_location("_qsfast", path, loader=loader)
+                mod = importlib.util.module_from_spec(spec)
+                loader.exec_module(mod)
+                mod.set_error(QsimError)
+                _fast_mod = mod
+        except Exception:
+            _fast_mod = None
+    return _fast_mod
+
 
 def handle(device: int = 0, stream_ptr: int | None = None) -> Handle:
     """Per-thread, per-device handle bound to the given CUDA stream (torch's

@@ -44,6 +44,13 @@ def _h(device: int | None = None) -> _lib.Handle:
     return _lib.handle(dev, sp)
 
 
+def _hptr(device: int) -> int:
+    """Raw qs_handle_t of this thread's handle on `device`, bound to torch's
+    current stream there (for the direct per-gate calls)."""
+    sp = _raw_stream(device) if _raw_stream is not None else torch.cuda.current_stream(device).cuda_stream
+    return _lib.handle(device, sp).h.value
+
+
 def autotune_batch(widths, op_offsets, ops, device: int | None = None) -> dict:
     """Tunes tile and register-block widths per circuit width on the given
     circuits (one sample per width); returns {width: (tile_bits, block_bits)}."""

@@ -51,3 +51,17 @@ def test_version_and_null_handle_errors(lib):
     # calls with a null handle fail cleanly (no GPU needed)
     assert lib.qs_sync(None) == 1
     assert b"null handle" in lib.qs_last_error(None)
+
+
+def test_fast_extension_binds_the_same_library():
+    """blackwell_kernels' per-gate calls go through the _qsfast extension (no
+    ctypes marshalling); it links the in-tree libqsim.so and reports errors
+    as QsimError."""
+    import pytest
+    from qsim_b200 import _lib
+    F = _lib.fast()
+    assert F is not None
+    with pytest.raises(_lib.QsimError, match="null handle"):
+        F.apply_1q_dev(0, 0, 3, 0, 0)
+    with pytest.raises(RuntimeError, match="0-7"):
+        F.apply_mc1q_dev(0, 0, 3, 0, list(range(8)), 0)
