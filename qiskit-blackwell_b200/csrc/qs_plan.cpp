@@ -595,6 +595,70 @@ void qubits_of(const IOp& o, std::vector<int>& qs) {
   for (int c : o.cq) qs.push_back(c);
 }
 
+// Reorders a register block's ops into layers: as many uncontrolled
+// single-qubit rotations / dense 2x2s on distinct qubits as are ready, then
+// every ready diagonal, then the next layer, and so on (two ops keep their
+// order when they share a qubit and are not both diagonal).  The encoder
+// turns each layer into one Kronecker op and each diagonal run into one
+// table, so maximal layers mean fewer table multiplies per amplitude.  Any
+// other op (two-target, controlled) is placed as soon as nothing of the
+// current layer or run is ready.
+void layer_block_ops(const std::vector<IOp>& ops, std::vector<int>& idx) {
+  const int m = (int)idx.size();
+  if (m < 3) return;
+  std::vector<uint64_t> qm(m, 0);
+  std::vector<char> dg(m, 0), kr(m, 0);
+  std::vector<int> qs;
+  for (int i = 0; i < m; ++i) {
+    const IOp& o = ops[idx[i]];
+    qubits_of(o, qs);
+    for (int q : qs) qm[i] |= 1ull << q;
+    dg[i] = is_diag_kind(o.kind);
+    kr[i] = (o.kind == I_RY || o.kind == I_U1) && o.cq.empty();
+  }
+  std::vector<int> indeg(m, 0);
+  std::vector<std::vector<int>> succ(m);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < j; ++i)
+      if ((qm[i] & qm[j]) && !(dg[i] && dg[j])) {
+        succ[i].push_back(j);
+        ++indeg[j];
+      }
+  std::vector<char> done(m, 0);
+  std::vector<int> out;
+  out.reserve(m);
+  auto emit = [&](int i) {
+    done[i] = 1;
+    out.push_back(idx[i]);
+    for (int s2 : succ[i]) --indeg[s2];
+  };
+  while ((int)out.size() < m) {
+    bool any = false;
+    // a layer of ready rotations on distinct qubits (taken in list order)
+    uint64_t used = 0;
+    for (int i = 0; i < m; ++i)
+      if (!done[i] && indeg[i] == 0 && kr[i] && !(qm[i] & used)) {
+        used |= qm[i];
+        emit(i);
+        any = true;
+      }
+    if (any) continue;
+    // every ready diagonal
+    for (int i = 0; i < m; ++i)
+      if (!done[i] && indeg[i] == 0 && dg[i]) {
+        emit(i);
+        any = true;
+      }
+    if (any) continue;
+    for (int i = 0; i < m; ++i)
+      if (!done[i] && indeg[i] == 0) {
+        emit(i);
+        break;
+      }
+  }
+  idx.swap(out);
+}
+
 std::vector<IOp> fuse_1q(int n, const std::vector<IOp>& in, bool decompose) {
   std::vector<IOp> out;
   std::vector<M2> pend(n);
@@ -897,6 +961,11 @@ thread_local int g_last_devops = 0;
 
 void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::vector<char>& blob,
                  uint32_t& pass_off, int& R_out, int& nblocks_out, int& has2_out, int& ncoef_out, int block_bits) {
+  // QSIM_LAYER_BLOCKS=0 keeps each block's ops in the order they were taken
+  static const bool layer_blocks = [] {
+    const char* e = std::getenv("QSIM_LAYER_BLOCKS");
+    return !(e && e[0] == '0');
+  }();
   const int T = pp.T;
   const int R = std::min(block_bits, T);
   std::vector<int> tpos(n, -1);  // global qubit -> tile position
@@ -979,6 +1048,7 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
         }
       }
       if (cur.ops.empty()) throw qs_error(QS_ERR_INVALID, "internal: no op fits an empty register block");
+      if (layer_blocks) layer_block_ops(ops, cur.ops);
       blks.push_back(cur);
     }
     if (blks.empty()) blks.push_back(Blk());
