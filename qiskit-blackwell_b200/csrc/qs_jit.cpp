@@ -940,9 +940,20 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
   s << "  }\n";
   // ---- consumer warps: group grp takes tiles grp, grp + ngrp, ...
   s << "  const u32 grp = tid / " << ncg << "u, lt = tid % " << ncg << "u;\n";
+  // With several groups, a group reaches tile i without having consumed the
+  // stage's previous tile (i - stages, another group's): the stage's "full"
+  // phase for that tile may still be open, and a parity wait would see the
+  // phase before it (same parity) as complete.  So the group first waits for
+  // the "done" phase of tile i - stages (its own arrivals completed the one
+  // before), which also means that tile's "full" phase is over; then the
+  // "full" wait for tile i is unambiguous.
   s << "  for (u64 i = grp; i < mine; i += " << ngrp << "u) {\n";
   s << "    const u32 st = (u32)(i % " << kPipeStages << "u);\n";
-  s << "    if (!mb_wait(bar_full + 8u * st, (u32)((i / " << kPipeStages << "u) & 1u), limit)) *abort_flag = 1u;\n";
+  s << "    bool ok = true;\n";
+  if (ngrp > 1)
+    s << "    if (i >= " << kPipeStages << "u) ok = mb_wait(bar_done + 8u * st, (u32)(((i - " << kPipeStages << "u) / "
+      << kPipeStages << "u) & 1u), limit);\n";
+  s << "    if (!ok || !mb_wait(bar_full + 8u * st, (u32)((i / " << kPipeStages << "u) & 1u), limit)) *abort_flag = 1u;\n";
   s << "    consumers_sync(grp);\n";
   s << "    if (*abort_flag) { if (lt == 0u) atomicOr(status, 2u); return; }\n";
   s << "    const u32 soff = pad + st * " << tile_bytes << "u;\n";
