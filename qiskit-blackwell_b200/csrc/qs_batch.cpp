@@ -151,7 +151,9 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
           last[e.second] = (uint32_t)items.size();
           items.push_back(it);
           B->q_maxT = std::max(B->q_maxT, p.pass_T[L]);
-          B->q_has2 |= p.pass_has2[L];
+          // 2 (dense 4x4 only) survives only if every item has it
+          const int h2 = p.pass_has2[L];
+          B->q_has2 = items.size() == 1 ? h2 : (B->q_has2 == h2 ? h2 : ((B->q_has2 | h2) ? 1 : 0));
           B->q_ncoef = std::max(B->q_ncoef, p.pass_ncoef[L]);
           bytes += ((L == 0 && from_zero) ? 8.0 : 16.0) * std::ldexp(1.0, p.n_qubits);
         }

@@ -160,7 +160,7 @@ struct __align__(16) DevPass {
   uint32_t coef_off;
   uint32_t bytes;     // total bytes of this pass record
   uint32_t ncoef;     // float2 entries in the coefficient pool
-  uint32_t has2;      // 1 if the pass holds a two-target op (U2 / SWAP)
+  uint32_t has2;      // 1 if the pass holds a two-target op (U2 / SWAP), 2 if every op is an uncontrolled U2
   uint32_t pad[2];
 };
 

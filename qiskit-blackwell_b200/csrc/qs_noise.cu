@@ -314,7 +314,7 @@ struct Merger {
         ops.push_back(d);
       }
       coef.insert(coef.end(), pc, pc + 2 * (size_t)hdr.ncoef);
-      has2 |= (int)hdr.has2;
+      has2 |= hdr.has2 ? 1 : 0;  // a merged program is never dense-4x4 only
     }
   }
 

@@ -395,7 +395,7 @@ __device__ __forceinline__ void op_dtab(float2 (&v)[1 << R], const DevOp& op, co
   case 2 * 8 + 4: F<R, 2, 4>(__VA_ARGS__); break;                                \
   case 3 * 8 + 4: F<R, 3, 4>(__VA_ARGS__); break;
 
-template <int R, bool TWO>
+template <int R, int TWO>
 __device__ __forceinline__ void run_ops(float2 (&v)[1 << R], const DevOp* __restrict__ ops, int ob, int oe,
                                         const float2* __restrict__ coef, uint64_t gidx) {
   for (int o = ob; o < oe; ++o) {
@@ -661,10 +661,25 @@ __device__ __noinline__ void noise_block(float2* tile, int T, const DevBlock blk
   }
 }
 
+// Dense-4x4-only programs (TWO == 2: every op of every pass in the launch
+// is an uncontrolled DK_U2, as in Quantum-Volume circuits): the op loop has
+// no kind dispatch, no control predicates and none of the other ops' code,
+// which keeps the register array's allocation across the pair switch
+// simple.  Same arithmetic as run_ops, so the same bits.
+template <int R>
+__device__ __forceinline__ void run_ops_u2(float2 (&v)[1 << R], const DevOp* __restrict__ ops, int ob, int oe,
+                                           const float2* __restrict__ coef) {
+  for (int o = ob; o < oe; ++o) {
+    const uchar4 k = *reinterpret_cast<const uchar4*>(ops + o);  // kind, t0, t1, rc
+    const float2* c = coef + ops[o].coef;
+    switch (k.y * 8 + k.z) { CASES_2(op_u2, v, c) }
+  }
+}
+
 // One register block over the tile: every thread gathers the 2^R amplitudes
 // of each of its groups (Gray-code walk over the swizzled addresses), runs
 // the block's ops in registers and scatters them back.
-template <int R, bool TWO>
+template <int R, int TWO>
 __device__ __forceinline__ void register_block(float2* tile, const DevBlock& blk, const DevOp* __restrict__ ops,
                                                const float2* __restrict__ s_coef, uint32_t ngroups, uint64_t gbase,
                                                const uint64_t* dep_lo, const uint64_t* dep_hi) {
@@ -693,7 +708,8 @@ __device__ __forceinline__ void register_block(float2* tile, const DevBlock& blk
         v[j] = tile[a];
       }
     }
-    run_ops<R, TWO>(v, ops, blk.op_begin, blk.op_end, s_coef, gidx);
+    if constexpr (TWO == 2) run_ops_u2<R>(v, ops, blk.op_begin, blk.op_end, s_coef);
+    else run_ops<R, TWO>(v, ops, blk.op_begin, blk.op_end, s_coef, gidx);
     {
       uint32_t a = pb;
 #pragma unroll
@@ -717,7 +733,7 @@ constexpr int kMinBlocks(int R) { return R == 5 ? 2 : 2; }
 constexpr int kBigThreads(int R) { return 2 * kMaxThreads(R); }
 
 // Dynamic shared memory: [tile 2^maxT float2][coefficient pool][dep tables].
-template <int R, bool TWO, bool BIG>
+template <int R, int TWO, bool BIG>
 __global__ void __launch_bounds__(BIG ? kBigThreads(R) : kMaxThreads(R), BIG ? 1 : kMinBlocks(R))
 k_pass(float2* __restrict__ base_state, PassItem single, const PassItem* __restrict__ items, int nitems,
        uint64_t total_tiles, uint32_t coef_off_bytes, uint32_t dep_off_bytes) {
@@ -847,7 +863,7 @@ __device__ __forceinline__ uint32_t q_ld_acquire(const uint32_t* p) {
   return v;
 }
 
-template <int R, bool TWO>
+template <int R, int TWO>
 __device__ __forceinline__ void queue_blocks(float2* tile, const DevPass* P, const float2* s_coef, uint64_t gbase,
                                              const uint64_t* dep_lo, const uint64_t* dep_hi) {
   const DevBlock* blocks = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off);
@@ -859,7 +875,7 @@ __device__ __forceinline__ void queue_blocks(float2* tile, const DevPass* P, con
   }
 }
 
-template <bool TWO, bool BIG>
+template <int TWO, bool BIG>
 __global__ void __launch_bounds__(BIG ? 256 : 128, BIG ? 1 : 2)
 k_pass_queue(float2* __restrict__ base_state, const PassItem* __restrict__ items, int nitems, uint64_t total_tiles,
              uint32_t coef_off_bytes, uint32_t dep_off_bytes, uint32_t* __restrict__ counters,
@@ -974,7 +990,7 @@ size_t coef_bytes_for(int ncoef) { return (((size_t)ncoef * sizeof(float2)) + 15
 
 // Launch shapes per (device, dynamic shared memory, threads).  Handles on
 // several host threads launch concurrently, so the table is locked.
-template <int R, bool TWO, bool BIG>
+template <int R, int TWO, bool BIG>
 LaunchCfg configure(int device, int smem, int threads) {
   static std::mutex mu;
   static std::map<std::tuple<int, int, int>, LaunchCfg> cache;
@@ -998,7 +1014,7 @@ LaunchCfg configure(int device, int smem, int threads) {
   return c;
 }
 
-template <int R, bool TWO, bool BIG>
+template <int R, int TWO, bool BIG>
 void launch_R(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
               uint64_t total, int maxT, int threads, int ncoef) {
   const uint32_t tile_bytes = (uint32_t)(sizeof(float2) << maxT);
@@ -1031,7 +1047,7 @@ int threads_for(int maxT, int R) {
   return t;
 }
 
-template <bool TWO>
+template <int TWO>
 void dispatch_two(qs_context* h, float2* base, const PassItem& single, const PassItem* d_items, int nitems,
                   uint64_t total, int maxT, int R, int ncoef, int threads_req) {
   int threads = threads_for(maxT, R);
@@ -1060,11 +1076,12 @@ void dispatch(qs_context* h, float2* base, const PassItem& single, const PassIte
               uint64_t total, int maxT, int R, int has2, int ncoef, int threads_req = 0) {
   QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
   QS_CHECK_ARG(threads_req == 0 || (threads_req % 32) == 0, "threads per CTA must be a multiple of 32");
-  if (has2) dispatch_two<true>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
-  else dispatch_two<false>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
+  if (has2 == 2) dispatch_two<2>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
+  else if (has2) dispatch_two<1>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
+  else dispatch_two<0>(h, base, single, d_items, nitems, total, maxT, R, ncoef, threads_req);
 }
 
-template <bool TWO, bool BIG>
+template <int TWO, bool BIG>
 void launch_queue(qs_context* h, float2* base, const PassItem* d_items, int nitems, uint64_t total, int maxT,
                   int ncoef, uint32_t* counters, uint32_t withhold, uint64_t limit) {
   const int threads = BIG ? 256 : 128;
@@ -1136,11 +1153,14 @@ void qs_launch_pass_queue(qs_context* h, void* base, const PassItem* d_items, in
   QS_CHECK_ARG(maxT >= 1 && maxT <= 14, "tile bits out of range");
   const bool big = maxT >= 14;
   float2* b = static_cast<float2*>(base);
-  if (has2) {
-    if (big) launch_queue<true, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
-    else launch_queue<true, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+  if (has2 == 2) {
+    if (big) launch_queue<2, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    else launch_queue<2, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+  } else if (has2) {
+    if (big) launch_queue<1, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    else launch_queue<1, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
   } else {
-    if (big) launch_queue<false, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
-    else launch_queue<false, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    if (big) launch_queue<0, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+    else launch_queue<0, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
   }
 }

@@ -1206,6 +1206,15 @@ void encode_pass(int n, const PassPlan& pp, const std::vector<IOp>& ops, std::ve
   hdr.n_qubits = n;
   for (int k = 0; k < T; ++k) hdr.S[k] = pp.S[k];
   hdr.ncoef = (uint32_t)(coef.size() / 2);
+  // 2: every op is an uncontrolled dense 4x4 (the interpreter then runs a
+  // dispatch-free op loop; QSIM_DENSE_ONLY=0 turns that off)
+  static const bool dense_only_on = [] {
+    const char* e = std::getenv("QSIM_DENSE_ONLY");
+    return !(e && e[0] == '0');
+  }();
+  if (has2 && dense_only_on && !dops.empty() &&
+      std::all_of(dops.begin(), dops.end(), [](const DevOp& d) { return d.kind == DK_U2; }))
+    has2 = 2;
   hdr.has2 = (uint32_t)has2;
   size_t off = align16(sizeof(DevPass));
   hdr.block_off = (uint32_t)off;
