@@ -106,3 +106,18 @@ def test_six_qubit_register_blocks(n, tile_bits):
     ops = np.concatenate([W.layers_ops(n, 6, seed=5), _random_ops(n, 60, rng)])
     psi0 = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
     _check(n, ops, tile_bits, 6, psi0 / np.linalg.norm(psi0), specialised=True)
+
+
+def test_dense_only_passes_are_marked():
+    """Passes whose device ops are all uncontrolled dense 4x4s carry has2 = 2
+    (the interpreter's dispatch-free op loop); any other op kind keeps 1 or 0,
+    and the program still matches the oracle."""
+    ops = W.qv_ops(16, 16, 3)
+    blob = PE.program(16, ops, 13, 4, False)
+    dec = PE.decode(blob)
+    assert all(int(h["has2"]) == 2 for h, _, dops, _ in dec)
+    assert all(int(o["kind"]) == PE.DK_U2 for _, _, dops, _ in dec for o in dops)
+    _check(16, ops, 13, 4)
+    lay = W.layers_ops(16, 4, seed=1)
+    for h, _, dops, _ in PE.decode(PE.program(16, lay, 13, 4, False)):
+        assert int(h["has2"]) in (0, 1)
