@@ -313,6 +313,17 @@ def bench_qv_batch(args, dev):
     per_step = t / args.steps
     peak, src = measured_peaks()
     achieved = bp.info["bytes_moved"] / per_step / 1e9
+    # the same batch as one persistent launch (qs_set_batch_queue)
+    h.call("qs_set_batch_queue", 1)
+    try:
+        bq = E.BatchPlan(widths, oo, ops, so, dev)
+    finally:
+        h.call("qs_set_batch_queue", 0)
+    stepq = lambda: bq.execute(states)
+    for _ in range(args.warmup):
+        stepq()
+    tq = reduce_max(_cuda_time(stepq, stream, args.steps), f"cuda:{dev}") / args.steps
+    del bq
     # plain per-circuit path on a sample of the same circuits
     idx = np.random.default_rng(2).choice(C, size=min(64, C), replace=False)
     plans = [(int(widths[c]), E.Plan(int(widths[c]), ops[oo[c]:oo[c + 1]], dev)) for c in idx]
@@ -374,6 +385,10 @@ def bench_qv_batch(args, dev):
                    "autotuned_tile_block_bits": {str(k): list(v) for k, v in tuned.items()},
                    "autotune_seconds": t_tune, "cuda_graph": "captured at the 2nd execution, replayed",
                    "max_passes": bp.info["max_passes"], "l2": "6.2 GB of states >> L2"},
+        "persistent_launch": {"value": ws * C / tq, "unit": "circuits/s", "ms_per_step": tq * 1e3,
+                              "note": "the same batch plan as one persistent launch (tiles taken from a device "
+                                      "counter level by level); value above: one launch per pass level and tile "
+                                      "shape"},
         "per_circuit_launches": {"value": plain_cps, "unit": "circuits/s",
                                  "sample": f"{len(idx)} random circuits of the batch, one fused plan per circuit"},
         "per_gate_launches": {"value": pergate_cps, "unit": "circuits/s",
@@ -1012,6 +1027,7 @@ def headline_sub_records(args, dev) -> dict:
     batched = {
         "workload": describe("qv_batch", a), "value": qb["value"], "unit": qb["unit"], "steps": a.steps,
         "ms_per_step": qb["ms_per_step"],
+        "persistent_launch": qb["persistent_launch"],
         "per_circuit_launches": qb["per_circuit_launches"], "per_gate_launches": qb["per_gate_launches"],
         "over_per_circuit_launches": qb["value"] / qb["per_circuit_launches"]["value"],
         "over_per_gate_launches": qb["value"] / qb["per_gate_launches"]["value"],

@@ -138,6 +138,14 @@ int64_t qs_launch_count(qs_handle_t h);
  * clears it.  No reference counterpart (the reference has no device-side
  * waits).                                                                   */
 int qs_device_status(qs_handle_t h, int* code);
+/* How batch plans built on this handle run: on = 0 (the default, unless
+ * QSIM_BATCH_QUEUE=1) one launch per (pass level, tile shape), each launch
+ * covering every circuit at that level; on = 1 the whole batch in one
+ * persistent launch whose CTAs take tiles from a device counter level by
+ * level and wait (bounded) for each state's previous pass.  Same results
+ * either way.  No reference counterpart (its batches are fixed-width, one
+ * launch per gate or one CTA per circuit).                                 */
+int qs_set_batch_queue(qs_handle_t h, int on);
 /* Test hook for the above: mode 1 = the next pipelined tile pass this handle
  * launches withholds its first tile's copy; mode 2 = the next persistent
  * batch launch leaves one pass of one state uncounted, so the state's next

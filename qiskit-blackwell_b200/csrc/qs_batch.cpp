@@ -225,15 +225,6 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
 constexpr int kMaxSlices = 8;
 constexpr int kSliceMinCircuits = 256;
 
-// QSIM_BATCH_QUEUE=0 runs batches as one launch per (level, tile shape)
-// instead of one persistent launch.
-static bool batch_queue_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("QSIM_BATCH_QUEUE");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
 
 static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths, const int64_t* op_off,
                                     const qs_op* ops, const int64_t* state_off) {
@@ -247,7 +238,7 @@ static qs_batch_plan_s* build_batch(qs_context* h, int nc, const int32_t* widths
   plan_all(h, nc, widths, op_off, ops, plans);
   std::vector<BatchUnit> units(nc);
   for (int c = 0; c < nc; ++c) units[c] = BatchUnit{c, (uint64_t)state_off[c], 0, nullptr};
-  return qs_batch_build_units(h, plans, units, true, 0, batch_queue_enabled());
+  return qs_batch_build_units(h, plans, units, true, 0, h->batch_queue != 0);
 }
 
 // Bounded dependency waits: 4 s (a tile takes microseconds; the margin

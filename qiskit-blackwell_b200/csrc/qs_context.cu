@@ -98,6 +98,10 @@ int qs_create(int device, qs_handle_t* out) {
   h = new qs_context();
   h->device = device;
   h->jit_mode = qs_jit_env_mode();
+  {
+    const char* e = std::getenv("QSIM_BATCH_QUEUE");
+    h->batch_queue = (e && e[0] == '1') ? 1 : 0;
+  }
   QS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
   QS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
@@ -195,6 +199,14 @@ int qs_device_status(qs_handle_t h, int* code) {
   QS_CUDA(cudaStreamSynchronize(h->stream));
   *code = (int)w;
   if (w) QS_CUDA(cudaMemsetAsync(h->dev_status, 0, sizeof(w), h->stream));
+  QS_API_END(h)
+}
+
+int qs_set_batch_queue(qs_handle_t h, int on) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(on == 0 || on == 1, "batch mode: 0 one launch per pass level and tile shape, 1 one persistent launch");
+  h->batch_queue = on;
   QS_API_END(h)
 }
 

@@ -49,6 +49,9 @@ struct qs_context {
   // 2 every plan.
   int jit_mode = 1;
   int jit_min_qubits = 24;
+  // Batch plans: 0 = one launch per (pass level, tile shape), 1 = one
+  // persistent launch (k_pass_queue).  Default from QSIM_BATCH_QUEUE, else 0.
+  int batch_queue = 0;
   int64_t launches = 0;
   // Device status word of the pipelined tile passes: a kernel whose bounded
   // wait gave up ORs a cause into it (1 producer, 2 consumers); read and

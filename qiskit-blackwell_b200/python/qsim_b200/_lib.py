@@ -88,6 +88,7 @@ SIGNATURES = {
     "qs_counts": (_i, [_vp, _vp, _i64, _pi64, _i64, _pi64]),
     "qs_device_status": (_i, [_vp, _pi]),
     "qs_set_wait_test": (_i, [_vp, _i]),
+    "qs_set_batch_queue": (_i, [_vp, _i]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
     "qs_state_alloc": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
     "qs_state_free": (_i, [_vp, _vp]),

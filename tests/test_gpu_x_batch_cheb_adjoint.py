@@ -339,10 +339,14 @@ def test_batch_is_one_persistent_launch_with_bounded_waits():
     and the next execution is complete and right."""
     import ctypes as C
     widths, oo, ops, so = W.qv_batch(24, 14, 18, seed=41)
-    bp = E.BatchPlan(widths, oo, ops, so)
+    h = E._h()
+    h.call("qs_set_batch_queue", 1)
+    try:
+        bp = E.BatchPlan(widths, oo, ops, so)
+    finally:
+        h.call("qs_set_batch_queue", 0)
     assert bp.info["n_launches"] == 1 and bp.info["max_passes"] >= 2
     st = bp.alloc_states()
-    h = E._h()
     code = C.c_int(-1)
     h.call("qs_device_status", C.byref(code))
     assert code.value == 0
@@ -365,3 +369,10 @@ def test_batch_is_one_persistent_launch_with_bounded_waits():
         n = int(widths[c])
         got = allv[so[c]: so[c] + (1 << n)]
         assert abs(1 - O.fidelity(got, O.simulate(n, ops[oo[c]: oo[c + 1]]))) <= 1e-6, c
+    # the per-level launches give the same bits
+    bl = E.BatchPlan(widths, oo, ops, so)
+    assert bl.info["n_launches"] > 1
+    st2 = bl.alloc_states()
+    bl.execute(st2)
+    torch.cuda.synchronize()
+    assert np.array_equal(st2.cpu().numpy().view(np.uint32), allv.view(np.uint32))
