@@ -78,7 +78,8 @@ def counts_from_samples(samples) -> dict:
     only the distinct outcomes and their counts are copied back (the
     reference copies every shot and loops over them in Python)."""
     if isinstance(samples, torch.Tensor) and samples.is_cuda:
-        return {hex(k): c for k, c in E.counts(samples.to(torch.int64)).items()}
+        keys, cnt = E.counts_arrays(samples.to(torch.int64))
+        return dict(zip(map(hex, keys.tolist()), cnt.tolist()))
     vals, cnt = np.unique(np.asarray(samples, dtype=np.int64), return_counts=True)
     return {hex(int(v)): int(c) for v, c in zip(vals, cnt)}
 

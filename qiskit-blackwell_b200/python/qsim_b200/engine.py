@@ -284,12 +284,19 @@ def counts(shots: torch.Tensor) -> dict:
     """{outcome: count} of int64 shots held on the device (qs_counts: hash
     histogram on the GPU, only the distinct outcomes copied back), in
     ascending outcome order."""
+    keys, cnt = counts_arrays(shots)
+    return dict(zip(keys.tolist(), cnt.tolist()))
+
+
+def counts_arrays(shots: torch.Tensor):
+    """(distinct outcomes ascending, their counts) as int64 numpy arrays, from
+    qs_counts."""
     if not shots.is_cuda or shots.dtype != torch.int64:
         raise RuntimeError("shots must be an int64 CUDA tensor")
     shots = shots.contiguous()
     n = int(shots.numel())
     if n == 0:
-        return {}
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
     h = _h(shots.device.index)
     cap = min(n, 1 << 16)
     nd = C.c_int64(0)
@@ -304,7 +311,7 @@ def counts(shots: torch.Tensor) -> dict:
         _lib.check(rc, h.h)
     pairs = pairs[: nd.value]
     order = np.argsort(pairs[:, 0], kind="stable")
-    return {int(k): int(c) for k, c in pairs[order]}
+    return pairs[order, 0], pairs[order, 1]
 
 
 def seed_uniforms(seed: int, count: int) -> np.ndarray:
