@@ -324,6 +324,19 @@ def bench_qv_batch(args, dev):
         stepq()
     tq = reduce_max(_cuda_time(stepq, stream, args.steps), f"cuda:{dev}") / args.steps
     del bq
+    # the same batch with every pass on the CUDA cores (qs_set_tensor_cores 0)
+    h.call("qs_set_tensor_cores", 0)
+    try:
+        bc = E.BatchPlan(widths, oo, ops, so, dev)
+    finally:
+        h.call("qs_set_tensor_cores", 1)
+    stepc = lambda: bc.execute(states)
+    for _ in range(args.warmup):
+        stepc()
+    tcc = reduce_max(_cuda_time(stepc, stream, args.steps), f"cuda:{dev}") / args.steps
+    del bc
+    for _ in range(2):
+        step()   # leave the states as the headline plan computes them
     # plain per-circuit path on a sample of the same circuits
     idx = np.random.default_rng(2).choice(C, size=min(64, C), replace=False)
     plans = [(int(widths[c]), E.Plan(int(widths[c]), ops[oo[c]:oo[c + 1]], dev)) for c in idx]
@@ -384,11 +397,15 @@ def bench_qv_batch(args, dev):
                    "launches_per_step": bp.info["n_launches"], "items": bp.info["n_items"],
                    "autotuned_tile_block_bits": {str(k): list(v) for k, v in tuned.items()},
                    "autotune_seconds": t_tune, "cuda_graph": "captured at the 2nd execution, replayed",
-                   "max_passes": bp.info["max_passes"], "l2": "6.2 GB of states >> L2"},
+                   "max_passes": bp.info["max_passes"], "tensor_core_launches": bp.info["n_tc_launches"],
+                   "l2": "6.2 GB of states >> L2"},
         "persistent_launch": {"value": ws * C / tq, "unit": "circuits/s", "ms_per_step": tq * 1e3,
                               "note": "the same batch plan as one persistent launch (tiles taken from a device "
                                       "counter level by level); value above: one launch per pass level and tile "
                                       "shape"},
+        "cuda_cores": {"value": ws * C / tcc, "unit": "circuits/s", "ms_per_step": tcc * 1e3,
+                       "note": "the same batch with every pass on the CUDA-core interpreter; value above: dense "
+                               "passes with 5-qubit blocks and 12/13-qubit tiles on tcgen05.mma (TF32 split)"},
         "per_circuit_launches": {"value": plain_cps, "unit": "circuits/s",
                                  "sample": f"{len(idx)} random circuits of the batch, one fused plan per circuit"},
         "per_gate_launches": {"value": pergate_cps, "unit": "circuits/s",

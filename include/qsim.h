@@ -146,6 +146,17 @@ int qs_device_status(qs_handle_t h, int* code);
  * either way.  No reference counterpart (its batches are fixed-width, one
  * launch per gate or one CTA per circuit).                                 */
 int qs_set_batch_queue(qs_handle_t h, int on);
+/* Tensor cores for dense passes: on = 1 (the default, unless QSIM_TC=0)
+ * runs every batch pass whose ops are all dense two-qubit gates, with 5-qubit
+ * register blocks and 12- or 13-qubit tiles, on tcgen05.mma: each register
+ * block is applied as one 32x32 complex matrix (the block's gates multiplied
+ * on the device in FP32) in TF32 with a three-product high/low split and an
+ * FP32 accumulator in tensor memory.  Results agree with the CUDA-core
+ * kernel to about 1e-6 relative per block, not bit for bit.  on = 0 keeps
+ * every pass on the CUDA cores.  Takes effect for batch plans built after
+ * the call.  Replaces the dense per-gate update of the reference's batched
+ * QV kernel (bwk/csrc/qv8_sim_sm120.cu:58-117).                            */
+int qs_set_tensor_cores(qs_handle_t h, int on);
 /* Test hook for the above: mode 1 = the next pipelined tile pass this handle
  * launches withholds its first tile's copy; mode 2 = the next persistent
  * batch launch leaves one pass of one state uncounted, so the state's next
@@ -383,7 +394,7 @@ typedef struct qs_batch_info {
   int32_t n_launches;
   int64_t n_items;        /* (circuit, pass) pairs                           */
   int32_t max_passes;
-  int32_t pad;
+  int32_t n_tc_launches;  /* of n_launches, those on the tensor cores        */
   double  bytes_moved;    /* HBM bytes of all passes (first passes write only) */
   double  flops;          /* FP32 flop estimate                              */
 } qs_batch_info;

@@ -25,7 +25,15 @@ struct qs_batch_plan_s {
   int n_circuits = 0;
   void* d_blob = nullptr;          // all device programs
   void* d_items = nullptr;         // all PassItem tables
-  struct Launch { int T, R, has2, ncoef; size_t item_off; int n_items; uint64_t total_tiles; int threads; };
+  struct Launch {
+    int T, R, has2, ncoef;
+    size_t item_off;
+    int n_items;
+    uint64_t total_tiles;
+    int threads;
+    bool tc;  // tensor-core pass (qs_pass_tc.cu)
+  };
+  float* d_mats = nullptr;         // block matrices of the tensor-core launches' passes
   std::vector<Launch> launches;
   qs_batch_info info{};
   // CUDA graph of the launch sequence, captured at the second execution on
@@ -50,6 +58,7 @@ void free_bplan(qs_batch_plan_s* b) {
   qs_plan_free_device(b->d_blob, b->stream);
   qs_plan_free_device(b->d_items, b->stream);
   qs_plan_free_device(b->d_counters, b->stream);
+  qs_plan_free_device(b->d_mats, b->stream);
   delete b;
 }
 
@@ -67,7 +76,7 @@ void plan_all(const qs_context* h, int nc, const int32_t* widths, const int64_t*
           const int64_t b = op_off[c], e = op_off[c + 1];
           if (b < 0 || e < b) throw qs_error(QS_ERR_INVALID, "op_offsets must be non-decreasing");
           int tb = 0, bb = 0;
-          qs_plan_shape(h, widths[c], false, tb, bb);
+          qs_circuit_shape(h, widths[c], ops + b, (int)(e - b), false, tb, bb);
           qs_build_plan(widths[c], ops + b, (int)(e - b), tb, &plans[c], bb);
         } catch (const std::exception& ex) {
           errs[c] = ex.what();
@@ -162,9 +171,22 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
       B->q_tiles = tb;
       if (!items.empty()) QS_CUDA(cudaMallocAsync(&B->d_counters, sizeof(uint32_t) * (2 + items.size()), us));
     }
+    // Tensor-core launches: every (plan, level) pass they run gets its block
+    // matrices, built on the device after the upload (k_block_mats); an
+    // item's mats field holds the pass's first matrix index until the buffer
+    // exists.
+    std::map<std::pair<int, int>, size_t> mat_first;  // (plan, level) -> matrix index
+    std::vector<std::pair<std::pair<int, int>, size_t>> mat_passes;
+    size_t n_mats = 0;
+    std::vector<size_t> tc_items;
     for (int L = 0; L < (queue ? 0 : maxp); ++L) {
-      // key: (T, R, has2); value: items and the largest coefficient pool
-      std::map<std::tuple<int, int, int>, std::pair<std::vector<PassItem>, int>> groups;
+      // key: (T, R, has2); value: items, their plans and the largest coefficient pool
+      struct Group {
+        std::vector<PassItem> items;
+        std::vector<int> plan;
+        int ncoef = 0;
+      };
+      std::map<std::tuple<int, int, int>, Group> groups;
       for (const BatchUnit& u : units) {
         const qs_plan_s& p = plans[u.plan];
         if (L >= (int)p.pass_offsets.size()) continue;
@@ -178,8 +200,9 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
         it.noise_seed = u.noise_seed;
         it.noise_branch = u.noise_branch;
         auto& g = groups[std::make_tuple(T, p.pass_R[L], p.pass_has2[L])];
-        g.first.push_back(it);
-        g.second = std::max(g.second, p.pass_ncoef[L]);
+        g.items.push_back(it);
+        g.plan.push_back(u.plan);
+        g.ncoef = std::max(g.ncoef, p.pass_ncoef[L]);
         bytes += ((L == 0 && from_zero) ? 8.0 : 16.0) * std::ldexp(1.0, p.n_qubits);
       }
       // larger tiles first: they are the longest-running CTAs
@@ -188,17 +211,57 @@ qs_batch_plan_s* qs_batch_build_units(qs_context* h, const std::vector<qs_plan_s
         Lc.T = std::get<0>(g->first);
         Lc.R = std::get<1>(g->first);
         Lc.has2 = std::get<2>(g->first);
-        Lc.ncoef = g->second.second;
+        Lc.ncoef = g->second.ncoef;
         Lc.item_off = items.size();
-        Lc.n_items = (int)g->second.first.size();
+        Lc.n_items = (int)g->second.items.size();
+        Lc.tc = qs_tc_pass(h, Lc.T, Lc.R, Lc.has2);
         uint64_t tb = 0;
-        for (PassItem& it : g->second.first) { it.tile_begin = tb; tb += it.ntiles; items.push_back(it); }
+        for (size_t k = 0; k < g->second.items.size(); ++k) {
+          PassItem it = g->second.items[k];
+          it.tile_begin = tb;
+          tb += it.ntiles;
+          if (Lc.tc) {
+            const int pl = g->second.plan[k];
+            auto key = std::make_pair(pl, L);
+            auto f = mat_first.find(key);
+            if (f == mat_first.end()) {
+              const auto* P = reinterpret_cast<const DevPass*>(plans[pl].blob.data() + plans[pl].pass_offsets[L]);
+              f = mat_first.emplace(key, n_mats).first;
+              mat_passes.push_back({key, n_mats});
+              n_mats += (size_t)P->nblocks;
+            }
+            it.mats = reinterpret_cast<const float*>((uintptr_t)f->second);
+            tc_items.push_back(items.size());
+          }
+          items.push_back(it);
+        }
         Lc.total_tiles = tb;
         Lc.threads = threads;
         B->launches.push_back(Lc);
+        if (Lc.tc) ++B->info.n_tc_launches;
       }
     }
     for (const BatchUnit& u : units) flops += plans[u.plan].info.flops;
+    std::vector<TcMatJob> jobs;  // host temporary, alive until the synchronisation below
+    if (n_mats) {
+      constexpr size_t kMat = 8192;  // floats per block matrix (TF32 high part + FP32 remainder)
+      QS_CUDA(cudaMallocAsync(&B->d_mats, n_mats * kMat * sizeof(float), us));
+      for (size_t k : tc_items)
+        items[k].mats = B->d_mats + (size_t)(uintptr_t)items[k].mats * kMat;
+      jobs.reserve(n_mats);
+      for (const auto& mp : mat_passes) {
+        const int pl = mp.first.first, L = mp.first.second;
+        const auto* P = reinterpret_cast<const DevPass*>(plans[pl].blob.data() + plans[pl].pass_offsets[L]);
+        const auto* dP = reinterpret_cast<const DevPass*>(static_cast<const char*>(B->d_blob) + boff[pl] +
+                                                          plans[pl].pass_offsets[L]);
+        for (int b = 0; b < P->nblocks; ++b) jobs.push_back(TcMatJob{dP, (uint64_t)b, B->d_mats + (mp.second + b) * kMat});
+      }
+      void* d_jobs = nullptr;
+      QS_CUDA(cudaMallocAsync(&d_jobs, jobs.size() * sizeof(TcMatJob), us));
+      QS_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TcMatJob), cudaMemcpyHostToDevice, us));
+      qs_launch_block_mats(h, us, static_cast<const TcMatJob*>(d_jobs), (int)jobs.size());
+      QS_CUDA(cudaFreeAsync(d_jobs, us));
+    }
     if (!items.empty()) {
       QS_CUDA(cudaMallocAsync(&B->d_items, items.size() * sizeof(PassItem), us));
       QS_CUDA(cudaMemcpyAsync(B->d_items, items.data(), items.size() * sizeof(PassItem), cudaMemcpyHostToDevice,
@@ -264,7 +327,8 @@ void qs_batch_launch(qs_context* h, qs_batch_plan_s* B, void* states) {
   }
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
-    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
+    if (L.tc) qs_launch_pass_tc(h, states, d, L.n_items, L.total_tiles, L.T);
+    else qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
   }
 }
 
@@ -277,7 +341,8 @@ static void run_batch(qs_context* h, qs_batch_plan_s* B, void* states) {
   }
   for (const auto& L : B->launches) {
     const PassItem* d = static_cast<const PassItem*>(B->d_items) + L.item_off;
-    qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
+    if (L.tc) qs_launch_pass_tc(h, states, d, L.n_items, L.total_tiles, L.T);
+    else qs_launch_pass_items(h, states, d, L.n_items, L.total_tiles, L.T, L.R, L.has2, L.ncoef, L.threads);
   }
 }
 

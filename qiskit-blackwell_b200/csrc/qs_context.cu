@@ -101,6 +101,8 @@ int qs_create(int device, qs_handle_t* out) {
   {
     const char* e = std::getenv("QSIM_BATCH_QUEUE");
     h->batch_queue = (e && e[0] == '1') ? 1 : 0;
+    const char* t = std::getenv("QSIM_TC");
+    h->tensor_cores = (t && t[0] == '0') ? 0 : 1;
   }
   QS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device));
   QS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
@@ -207,6 +209,15 @@ int qs_set_batch_queue(qs_handle_t h, int on) {
   QS_API_BEGIN
   QS_CHECK_ARG(on == 0 || on == 1, "batch mode: 0 one launch per pass level and tile shape, 1 one persistent launch");
   h->batch_queue = on;
+  QS_API_END(h)
+}
+
+int qs_set_tensor_cores(qs_handle_t h, int on) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  QS_CHECK_ARG(on == 0 || on == 1, "tensor cores: 0 off, 1 on");
+  if (h->tensor_cores != on) qs_run_cache_clear(h);  // cached plans were built for the other setting
+  h->tensor_cores = on;
   QS_API_END(h)
 }
 

@@ -52,6 +52,10 @@ struct qs_context {
   // Batch plans: 0 = one launch per (pass level, tile shape), 1 = one
   // persistent launch (k_pass_queue).  Default from QSIM_BATCH_QUEUE, else 0.
   int batch_queue = 0;
+  // Dense-4x4-only passes with 5-bit register blocks and 12- or 13-bit tiles
+  // run on the tensor-core pass (qs_pass_tc.cu): 1 on (default), 0 off
+  // (QSIM_TC=0 or qs_set_tensor_cores).
+  int tensor_cores = 1;
   int64_t launches = 0;
   // Device status word of the pipelined tile passes: a kernel whose bounded
   // wait gave up ORs a cause into it (1 producer, 2 consumers); read and
@@ -195,6 +199,11 @@ struct qs_plan_s {
   cudaStream_t stream = nullptr;        // stream of the last upload/execution
   bool jit_tried = false;               // specialisation attempted
   std::vector<JitPass> jit;             // one per pass when specialised
+  // Tensor-core passes (qs_pass_tc.cu): index of each pass's first block
+  // matrix in d_mats, or -1; the matrices follow the program in d_blob's
+  // allocation (built at upload when the handle uses tensor cores).
+  std::vector<int64_t> pass_mats;
+  float* d_mats = nullptr;
   std::shared_ptr<JitJob> jit_job;      // sources awaiting / in background compile
   bool jit_queued = false;              // jit_job handed to the background compiler
   std::string jit_err;                  // why specialisation was not used
@@ -213,6 +222,14 @@ void qs_jit_launch(qs_context* h, const qs_plan_s* p, size_t pass, void* state, 
 // settings win; otherwise the autotuned entry for (device, n) when the plan
 // runs on the generic kernel (qs_tune.cpp); otherwise 13 and 5 / 4.
 void qs_plan_shape(const qs_context* h, int n, bool specialised, int& tile_bits, int& block_bits);
+// Shape of a circuit's plan: qs_plan_shape, except that a circuit of dense
+// two-qubit gates only on >= 12 qubits, planned for the generic kernel with
+// no explicit or autotuned shape, gets 13-bit tiles and 5-bit blocks when the
+// handle uses tensor cores (the tensor-core pass takes exactly those passes)
+// and does not run batches as one persistent launch (which stays on the CUDA
+// cores).
+void qs_circuit_shape(const qs_context* h, int n, const qs_op* ops, int nops, bool specialised, int& tile_bits,
+                      int& block_bits);
 
 // Planner entry (qs_plan.cpp): builds passes for one circuit.
 // `specialised`: the plan will run as specialised passes (enables the Cartan
@@ -241,9 +258,31 @@ struct __align__(16) PassItem {
   uint32_t pred;           // persistent batch launch: index of the same state's previous-pass item (~0u: none)
   uint64_t noise_seed;     // seed of the uniforms of the pass's noise blocks
   uint8_t* noise_branch;   // branch taken by each noise block (by DevOp.coef), or null
-  uint64_t pad1;
+  const float* mats;       // tensor-core pass: block b's matrix operands at mats + 8192 * b (or null)
 };
 static_assert(sizeof(PassItem) == 64, "PassItem layout");
+
+// One 32x32 block matrix to build (k_block_mats): block `block` of `pass`,
+// written as the tensor-core operand pair (TF32 high part, FP32 remainder;
+// 4096 floats each) at `out`.
+struct TcMatJob {
+  const DevPass* pass;
+  uint64_t block;
+  float* out;
+};
+void qs_launch_block_mats(qs_context* h, cudaStream_t stream, const TcMatJob* d_jobs, int n_jobs);
+// Tensor-core tile pass (qs_pass_tc.cu): every item's pass is dense-4x4-only
+// with R = 5 register blocks and T bits (12 or 13), and PassItem.mats holds
+// its block matrices.
+bool qs_tc_enabled(const qs_context* h);
+void qs_launch_pass_tc(qs_context* h, void* base, const PassItem* d_items, int n_items, uint64_t total_tiles, int T);
+// One state (or n equal-width states back to back), one pass, item by value.
+void qs_launch_pass_tc_single(qs_context* h, void* state, const DevPass* d_pass, int T, uint64_t ntiles,
+                              uint32_t flags, const float* mats);
+// Whether a pass (tile bits, block bits, has2) runs on the tensor cores.
+inline bool qs_tc_pass(const qs_context* h, int T, int R, int has2) {
+  return qs_tc_enabled(h) && R == 5 && has2 == 2 && (T == 12 || T == 13);
+}
 // has2: the pass (or any item of the launch) holds a two-target op; ncoef:
 // the largest coefficient pool (float2) of the launch's passes.
 void qs_launch_pass_single(qs_context* h, void* state, const DevPass* d_pass, int T, int R, uint64_t ntiles,

@@ -586,19 +586,20 @@ struct PipeShape {
 
 constexpr int kPipeStages = 3;
 
-// Consumer groups: the compute warps split into groups that take alternate
-// tiles of the ring (group g: tiles g, g + groups, ...), each synchronising
-// on a named barrier of its own, so one group's shared-memory loads overlap
-// the other group's arithmetic instead of every warp waiting in the same
-// phase.  QSIM_PIPE_GROUPS = 1 or 2 (default 1: the 32-qubit circuit measured
-// the same with both, 400 ms vs 402 ms).
-int pipe_groups(int nc) {
+// Consumer groups: each group is a full set of compute warps (one register
+// group per thread per block) and the groups take alternate tiles of the ring
+// (group g: tiles g, g + groups, ...), each synchronising on a named barrier
+// of its own.  Two groups put twice the warps on every scheduler, so one
+// group's shared-memory phases and barrier waits overlap the other group's
+// arithmetic; the price is a 120-register cap (17 warps per SM).
+// QSIM_PIPE_GROUPS = 1 or 2.
+int pipe_groups(int per_group) {
   static const int env = [] {
     const char* e = std::getenv("QSIM_PIPE_GROUPS");
     return e ? std::atoi(e) : 0;
   }();
-  const int g = env == 1 || env == 2 ? env : 1;
-  return (nc / g) % 32 == 0 && nc / g >= 64 ? g : 1;
+  const int g = env == 1 || env == 2 ? env : 2;
+  return per_group % 32 == 0 && per_group >= 64 ? g : 1;
 }
 
 bool pipe_enabled() {
@@ -800,8 +801,8 @@ __device__ __forceinline__ void consumers_sync(u32 grp) { asm volatile("bar.sync
 std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp* ops, const float2* coef,
                           const PipeShape& sh, int min_blocks) {
   const int T = P.T, R = P.R;
-  const int nc = std::min(256, 1 << (T - R));  // consumer threads (a multiple of 32: T - R >= 5)
-  const int ngrp = pipe_groups(nc), ncg = nc / ngrp;
+  const int ncg = std::min(256, 1 << (T - R));  // threads per consumer group (a multiple of 32: T - R >= 5)
+  const int ngrp = pipe_groups(ncg), nc = ngrp * ncg;
   const uint32_t tile_bytes = 8u << T;
   const int nbox = 1 << sh.U.size();
   const uint32_t box_bytes = 8u << sh.box_bits;
@@ -983,7 +984,10 @@ std::string gen_pass_pipe(const DevPass& P, const DevBlock* blocks, const DevOp*
 }
 
 int pipe_smem(int T) { return kPipeStages * (8 << T) + 1024 + 256 * 8 + 2 * kPipeStages * 8 + 16; }
-int pipe_threads(int T, int R) { return std::min(256, 1 << (T - R)) + 32; }
+int pipe_threads(int T, int R) {
+  const int per_group = std::min(256, 1 << (T - R));
+  return pipe_groups(per_group) * per_group + 32;
+}
 
 uint64_t fnv1a(const std::string& s) {
   uint64_t h = 1469598103934665603ull;

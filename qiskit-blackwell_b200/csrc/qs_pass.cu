@@ -1120,6 +1120,48 @@ void launch_queue(qs_context* h, float2* base, const PassItem* d_items, int nite
   qs_after_launch(h, "k_pass_queue");
 }
 
+// ------------------------------------------- dense block matrices (TC) ---
+// The tensor-core pass (qs_pass_tc.cu) applies each register block of a
+// dense-4x4-only pass as one 32x32 complex matrix.  Thread j of a job runs
+// the block's ops on the basis vector e_j with the interpreter's own op loop,
+// which yields column j of the block matrix U; the real form
+//   Bt[2i][2j] = Re U_ij, Bt[2i][2j+1] = -Im U_ij, Bt[2i+1][2j] = Im U_ij,
+//   Bt[2i+1][2j+1] = Re U_ij        (row n = output, column k = input)
+// is written split into its nearest TF32 value and the FP32 remainder, each
+// as a 64 x 64 K-major operand in the no-swizzle canonical layout of
+// tcgen05.mma (8-row groups of 2048 bytes, 16-byte K chunks 128 bytes apart).
+__device__ __forceinline__ uint32_t tc_kmajor(uint32_t r, uint32_t k) {
+  return ((r >> 3) * 2048u + (k >> 2) * 128u + (r & 7u) * 16u + (k & 3u) * 4u) >> 2;
+}
+__device__ __forceinline__ void tc_put(float* hi, float* lo, uint32_t n, uint32_t k, float x) {
+  const float h = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);  // nearest TF32
+  const uint32_t e = tc_kmajor(n, k);
+  hi[e] = h;
+  lo[e] = x - h;
+}
+
+__global__ void __launch_bounds__(32) k_block_mats(const TcMatJob* __restrict__ jobs) {
+  const TcMatJob J = jobs[blockIdx.x];
+  const DevPass* P = J.pass;
+  const DevBlock blk = reinterpret_cast<const DevBlock*>(reinterpret_cast<const char*>(P) + P->block_off)[J.block];
+  const DevOp* ops = reinterpret_cast<const DevOp*>(reinterpret_cast<const char*>(P) + P->op_off);
+  const float2* coef = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(P) + P->coef_off);
+  const uint32_t j = threadIdx.x;
+  float2 v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = make_float2(k == (int)j ? 1.f : 0.f, 0.f);
+  run_ops_u2<5>(v, ops, blk.op_begin, blk.op_end, coef);
+  float* hi = J.out;
+  float* lo = J.out + 4096;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    tc_put(hi, lo, 2 * i, 2 * j, v[i].x);
+    tc_put(hi, lo, 2 * i, 2 * j + 1, -v[i].y);
+    tc_put(hi, lo, 2 * i + 1, 2 * j, v[i].y);
+    tc_put(hi, lo, 2 * i + 1, 2 * j + 1, v[i].x);
+  }
+}
+
 }  // namespace
 
 // One state, one pass: the item is passed by value (no device table), so the
@@ -1162,5 +1204,16 @@ void qs_launch_pass_queue(qs_context* h, void* base, const PassItem* d_items, in
   } else {
     if (big) launch_queue<0, true>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
     else launch_queue<0, false>(h, b, d_items, n_items, total_tiles, maxT, ncoef, counters, withhold, limit_ns);
+  }
+}
+
+// Block matrices of dense-4x4-only R = 5 passes for the tensor-core pass:
+// one 32-thread CTA per job, each writing 32 KiB at job.out.
+void qs_launch_block_mats(qs_context* h, cudaStream_t stream, const TcMatJob* d_jobs, int n_jobs) {
+  if (n_jobs <= 0) return;
+  for (int b = 0; b < n_jobs; b += 65535) {
+    const int n = std::min(65535, n_jobs - b);
+    k_block_mats<<<n, 32, 0, stream>>>(d_jobs + b);
+    qs_after_launch(h, "k_block_mats");
   }
 }

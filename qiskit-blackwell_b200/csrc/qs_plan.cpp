@@ -1312,8 +1312,36 @@ void qs_build_plan(int n, const qs_op* ops, int nops, int tile_bits, qs_plan_s* 
 void qs_plan_upload(qs_context* h, qs_plan_s* p) {
   p->device = h->device;
   if (p->blob.empty()) return;
-  QS_CUDA(cudaMallocAsync(&p->d_blob, p->blob.size(), h->stream));
+  // Passes for the tensor cores get their block matrices (32 KiB each, built
+  // on the device by k_block_mats) after the program, in the same allocation.
+  const size_t np = p->pass_offsets.size();
+  p->pass_mats.assign(np, -1);
+  size_t n_mats = 0;
+  for (size_t i = 0; i < np; ++i)
+    if (qs_tc_pass(h, p->pass_T[i], p->pass_R[i], p->pass_has2[i])) {
+      p->pass_mats[i] = (int64_t)n_mats;
+      n_mats += (size_t)reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i])->nblocks;
+    }
+  constexpr size_t kMat = 8192;  // floats per block matrix
+  const size_t moff = (p->blob.size() + 255) & ~size_t(255);
+  QS_CUDA(cudaMallocAsync(&p->d_blob, moff + n_mats * kMat * sizeof(float), h->stream));
   QS_CUDA(cudaMemcpyAsync(p->d_blob, p->blob.data(), p->blob.size(), cudaMemcpyHostToDevice, h->stream));
+  p->d_mats = n_mats ? reinterpret_cast<float*>(static_cast<char*>(p->d_blob) + moff) : nullptr;
+  std::vector<TcMatJob> jobs;  // host temporary, alive until the synchronisation below
+  if (n_mats) {
+    for (size_t i = 0; i < np; ++i) {
+      if (p->pass_mats[i] < 0) continue;
+      const auto* dP = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
+      const int nb = reinterpret_cast<const DevPass*>(p->blob.data() + p->pass_offsets[i])->nblocks;
+      for (int b = 0; b < nb; ++b)
+        jobs.push_back(TcMatJob{dP, (uint64_t)b, p->d_mats + ((size_t)p->pass_mats[i] + b) * kMat});
+    }
+    void* d_jobs = nullptr;
+    QS_CUDA(cudaMallocAsync(&d_jobs, jobs.size() * sizeof(TcMatJob), h->stream));
+    QS_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(TcMatJob), cudaMemcpyHostToDevice, h->stream));
+    qs_launch_block_mats(h, h->stream, static_cast<const TcMatJob*>(d_jobs), (int)jobs.size());
+    QS_CUDA(cudaFreeAsync(d_jobs, h->stream));
+  }
   // The plan may be executed on another stream: make the program resident
   // before returning (this waits on the handle's stream only).
   QS_CUDA(cudaStreamSynchronize(h->stream));
@@ -1354,6 +1382,11 @@ void qs_plan_run(qs_context* h, qs_plan_s* p, void* state, bool from_zero, uint6
   for (size_t i = 0; i < p->pass_offsets.size(); ++i) {
     const int T = p->pass_T[i];
     const uint32_t flags = (from_zero && i == 0) ? PI_FROM_ZERO : 0u;
+    if (i < p->pass_mats.size() && p->pass_mats[i] >= 0) {  // tensor cores take the pass
+      const DevPass* dp = reinterpret_cast<const DevPass*>(static_cast<const char*>(p->d_blob) + p->pass_offsets[i]);
+      qs_launch_pass_tc_single(h, state, dp, T, n_states << (n - T), flags, p->d_mats + (size_t)p->pass_mats[i] * 8192);
+      continue;
+    }
     if (use_jit) {
       qs_jit_launch(h, p, i, state, n_states << (n - T), flags);
       continue;
@@ -1402,7 +1435,7 @@ int qs_plan_create(qs_handle_t h, int n, const qs_op* ops, int nops, qs_plan_t* 
   *out = nullptr;
   p = new qs_plan_s();
   int tb = 0, bb = 0;
-  qs_plan_shape(h, n, h->jit_mode == 2, tb, bb);
+  qs_circuit_shape(h, n, ops, nops, h->jit_mode == 2, tb, bb);
   qs_build_plan(n, ops, nops, tb, p, bb, h->jit_mode == 2);
   qs_plan_upload(h, p);
   *out = p;
@@ -1505,7 +1538,7 @@ int qs_run_circuit(qs_handle_t h, void* state, int n, const qs_op* ops, int nops
   // call would build, and every run of an entry is on one stream.
   int tb = 0, bb = 0;
   const int spec = h->jit_mode == 2 ? 1 : 0;
-  qs_plan_shape(h, n, spec != 0, tb, bb);
+  qs_circuit_shape(h, n, ops, nops, spec != 0, tb, bb);
   const bool cacheable = nops <= kRunCacheMaxOps;
   const uint64_t key = cacheable ? fnv1a(ops, sizeof(qs_op) * (size_t)nops, (uint64_t)n * 0x100000001b3ull) : 0;
   auto& cache = h->run_cache;

@@ -69,6 +69,24 @@ void qs_plan_shape(const qs_context* h, int n, bool specialised, int& tile_bits,
   if (block_bits == 0) block_bits = specialised ? 5 : 4;
 }
 
+void qs_circuit_shape(const qs_context* h, int n, const qs_op* ops, int nops, bool specialised, int& tile_bits,
+                      int& block_bits) {
+  const bool set = specialised || h->tile_bits != 0 || h->block_bits != 0;
+  bool tuned = false;
+  if (!set) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tuned = tune_table().count({h->device, n}) != 0;
+  }
+  bool dense = !set && !tuned && qs_tc_enabled(h) && !h->batch_queue && n >= 12 && nops > 0;
+  for (int i = 0; dense && i < nops; ++i) dense = ops[i].kind == QS_OP_U2;
+  if (dense) {
+    tile_bits = 13;
+    block_bits = 5;
+    return;
+  }
+  qs_plan_shape(h, n, specialised, tile_bits, block_bits);
+}
+
 extern "C" {
 
 int qs_autotune_batch(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op_off, const qs_op* ops) {

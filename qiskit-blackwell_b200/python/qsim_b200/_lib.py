@@ -40,7 +40,7 @@ class QsPlanInfo(C.Structure):
 
 class QsBatchInfo(C.Structure):
     _fields_ = [("n_circuits", C.c_int32), ("n_launches", C.c_int32), ("n_items", C.c_int64),
-                ("max_passes", C.c_int32), ("pad", C.c_int32), ("bytes_moved", C.c_double), ("flops", C.c_double)]
+                ("max_passes", C.c_int32), ("n_tc_launches", C.c_int32), ("bytes_moved", C.c_double), ("flops", C.c_double)]
 
 
 class QsServerStats(C.Structure):
@@ -89,6 +89,7 @@ SIGNATURES = {
     "qs_device_status": (_i, [_vp, _pi]),
     "qs_set_wait_test": (_i, [_vp, _i]),
     "qs_set_batch_queue": (_i, [_vp, _i]),
+    "qs_set_tensor_cores": (_i, [_vp, _i]),
     "qs_state_init": (_i, [_vp, _vp, _i]),
     "qs_state_alloc": (_i, [_vp, _i, C.POINTER(C.c_void_p)]),
     "qs_state_free": (_i, [_vp, _vp]),

@@ -20,6 +20,7 @@ def _run(n, ops, mode, psi0=None, tile_bits=0, block_bits=0):
     h = E._h()
     h.call("qs_set_tile_bits", tile_bits)
     h.call("qs_set_block_bits", block_bits)
+    h.call("qs_set_tensor_cores", 0)   # every pass on the kernels under comparison
     E.set_jit(mode)
     try:
         plan = E.Plan(n, ops)
@@ -35,6 +36,7 @@ def _run(n, ops, mode, psi0=None, tile_bits=0, block_bits=0):
         E.set_jit(1)
         h.call("qs_set_tile_bits", 0)
         h.call("qs_set_block_bits", 0)
+        h.call("qs_set_tensor_cores", 1)
 
 
 def _same_bits(a, b):
