@@ -273,7 +273,7 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
         pp[k] = tphys(1u << pos[k]);
       }
       for (uint32_t mt = 0; mt < nmt; ++mt) {
-        uint32_t base = mt * 128u + tid;
+        uint32_t base = mt * 128u + tid;  // group bits -> the tile's other positions, ascending
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           const uint32_t lo = base & ((1u << pos[k]) - 1u);
@@ -296,10 +296,14 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
           for (int e = 0; e < 64; ++e) nin = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nin);
         }
 #pragma unroll
-        for (int e = 0; e < 64; ++e) {
-          const float v = __uint_as_float(x[e]), hv = hi_part(v);
-          h[e] = __float_as_uint(hv);
-          x[e] = __float_as_uint(v - hv);
+        for (int e = 0; e < 64; e += 2) {
+          const float2 v = make_float2(__uint_as_float(x[e]), __uint_as_float(x[e + 1]));
+          const float2 hv = make_float2(hi_part(v.x), hi_part(v.y));
+          const float2 lv = __fadd2_rn(v, make_float2(-hv.x, -hv.y));  // exact: v - hv
+          h[e] = __float_as_uint(hv.x);
+          h[e + 1] = __float_as_uint(hv.y);
+          x[e] = __float_as_uint(lv.x);
+          x[e + 1] = __float_as_uint(lv.y);
         }
         tmem_st32(tmem + lane, h);
         tmem_st32(tmem + lane + 32u, h + 32);

@@ -6,9 +6,11 @@
 // memory round trip vs more registers).  qs_autotune_batch times every
 // (T, R) candidate on one sample circuit per distinct width of a batch and
 // records the fastest in a process-wide table per device.  Each candidate runs
-// on enough copies of the sample (2^24 amplitudes in all) to fill the GPU,
-// so the choice reflects batch throughput, not the latency of one small
-// state on a mostly idle GPU.  Every later plan
+// as a batch (the batch engine's own launches, tensor-core passes included)
+// of up to kTuneSamples distinct circuits of the width, repeated to 2^24
+// amplitudes in all, so the choice reflects batch throughput (including the
+// per-circuit program switches inside a launch), not the latency of one
+// small state on a mostly idle GPU.  Every later plan
 // for the generic kernel (batches, single circuits, the adjoint forward pass)
 // on that device and width uses it, so a circuit gives the same bits alone
 // and in a batch.  Specialised plans keep their own defaults.
@@ -30,17 +32,19 @@ std::map<std::pair<int, int>, Shape>& tune_table() {
 constexpr int kTuneMinWidth = 10;
 constexpr int kTuneMaxWidth = 24;  // larger states: tuning runs would take seconds
 
-// Device time of one from-|0> execution of `plan` on `copies` states back to
-// back (best of 3 after 1 warm-up).
-float time_plan(qs_context* h, qs_plan_s* plan, void* scratch, uint64_t copies) {
-  qs_plan_run(h, plan, scratch, true, copies);
+constexpr int kTuneSamples = 8;  // distinct circuits per width in a timing batch
+
+// Device time of one execution of batch B on `scratch` (best of 3 after 1
+// warm-up).
+float time_batch(qs_context* h, qs_batch_plan_s* B, void* scratch) {
+  qs_batch_launch(h, B, scratch);
   cudaEvent_t e0, e1;
   QS_CUDA(cudaEventCreate(&e0));
   QS_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   for (int r = 0; r < 3; ++r) {
     QS_CUDA(cudaEventRecord(e0, h->stream));
-    qs_plan_run(h, plan, scratch, true, copies);
+    qs_batch_launch(h, B, scratch);
     QS_CUDA(cudaEventRecord(e1, h->stream));
     QS_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -95,12 +99,14 @@ int qs_autotune_batch(qs_handle_t h, int nc, const int32_t* widths, const int64_
   const int saved_jit = h->jit_mode;
   QS_API_BEGIN
   QS_CHECK_ARG(nc >= 0 && (nc == 0 || (widths && op_off && ops)), "null batch descriptor");
-  // one sample circuit per distinct width in the tuned range
-  std::map<int, int> sample;
+  // up to kTuneSamples circuits per distinct width in the tuned range
+  std::map<int, std::vector<int>> sample;
   for (int c = 0; c < nc; ++c) {
     QS_CHECK_ARG(widths[c] >= 1 && widths[c] <= QS_MAX_QUBITS, "circuit width out of range");
-    if (widths[c] >= kTuneMinWidth && widths[c] <= kTuneMaxWidth && op_off[c + 1] > op_off[c])
-      sample.emplace(widths[c], c);
+    if (widths[c] >= kTuneMinWidth && widths[c] <= kTuneMaxWidth && op_off[c + 1] > op_off[c]) {
+      auto& v = sample[widths[c]];
+      if ((int)v.size() < kTuneSamples) v.push_back(c);
+    }
   }
   if (sample.empty()) return QS_OK;
   const int wmax = sample.rbegin()->first;
@@ -108,9 +114,12 @@ int qs_autotune_batch(qs_handle_t h, int nc, const int32_t* widths, const int64_
   QS_CUDA(cudaMallocAsync(&scratch, (size_t)8 << std::max(wmax, kFillBits), h->stream));
   h->jit_mode = 0;  // time the generic kernel
   for (const auto& kv : sample) {
-    const int w = kv.first, c = kv.second;
-    const qs_op* cops = ops + op_off[c];
-    const int nops = (int)(op_off[c + 1] - op_off[c]);
+    const int w = kv.first;
+    const std::vector<int>& cs = kv.second;
+    // units: the samples repeated (round robin) to fill 2^24 amplitudes
+    const uint64_t nunits = w >= kFillBits ? 1ull : std::max<uint64_t>(cs.size(), 1ull << (kFillBits - w));
+    std::vector<BatchUnit> units(nunits);
+    for (uint64_t u = 0; u < nunits; ++u) units[u] = BatchUnit{(int)(u % cs.size()), u << w, 0, nullptr};
     std::vector<Shape> cands;
     if (w <= 14) {  // one pass: the whole state is the tile
       for (int bb = 2; bb <= std::min(5, w); ++bb) cands.push_back({13, bb});
@@ -121,17 +130,19 @@ int qs_autotune_batch(qs_handle_t h, int nc, const int32_t* widths, const int64_
     Shape best{13, 4};
     float best_ms = 1e30f;
     for (const Shape& s : cands) {
-      qs_plan_s plan;
-      qs_build_plan(w, cops, nops, s.tile_bits, &plan, s.block_bits, false);
-      qs_plan_upload(h, &plan);
+      std::vector<qs_plan_s> plans(cs.size());
+      for (size_t k = 0; k < cs.size(); ++k)
+        qs_build_plan(w, ops + op_off[cs[k]], (int)(op_off[cs[k] + 1] - op_off[cs[k]]), s.tile_bits, &plans[k],
+                      s.block_bits, false);
+      qs_batch_plan_s* B = qs_batch_build_units(h, plans, units, true, 0, false);
       float ms = 1e30f;
       try {
-        ms = time_plan(h, &plan, scratch, w >= kFillBits ? 1ull : (1ull << (kFillBits - w)));
+        ms = time_batch(h, B, scratch);
       } catch (...) {
-        qs_plan_free_device(plan.d_blob, h->stream);
+        qs_batch_release(B);
         throw;
       }
-      qs_plan_free_device(plan.d_blob, h->stream);
+      qs_batch_release(B);
       if (ms < best_ms) { best_ms = ms; best = s; }
     }
     std::lock_guard<std::mutex> lk(g_tune_mu);
