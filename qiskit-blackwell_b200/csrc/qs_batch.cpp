@@ -471,6 +471,11 @@ int qs_batch_run(qs_handle_t h, int nc, const int32_t* widths, const int64_t* op
     }
     Bs.push_back(build_batch(h, c1 - c0, widths + c0, op_off + c0, ops, state_off + c0));
     run_batch(h, Bs.back(), states);
+    // the slice's buffers are freed in stream order after its launches, so the
+    // next slices reuse the memory (its tensor-core block matrices run to
+    // hundreds of MB) instead of every slice's staying allocated to the end
+    free_bplan(Bs.back());
+    Bs.pop_back();
     c0 = c1;
   }
   release();

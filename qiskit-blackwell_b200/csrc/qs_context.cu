@@ -58,6 +58,14 @@ cudaStream_t qs_upload_stream(qs_context* h) {
   return h->upload_stream;
 }
 
+void qs_pool_keep_at_least(int device, uint64_t keep) {
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess || !pool) return;
+  uint64_t cur = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur >= keep) return;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);  // only ever raised
+}
+
 extern "C" {
 
 const char* qs_version(void) { return "qsim-b200 0.1.0 (sm_100a)"; }
@@ -74,13 +82,10 @@ static void keep_pool_memory(int device) {
   static std::set<int> done;
   std::lock_guard<std::mutex> lk(mu);
   if (!done.insert(device).second) return;
-  cudaMemPool_t pool = nullptr;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess || !pool) return;
   const char* e = std::getenv("QSIM_POOL_KEEP_BYTES");
-  uint64_t keep = e ? std::strtoull(e, nullptr, 10) : (4ull << 30), cur = 0;
-  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur >= keep) return;
-  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);  // only ever raised here
+  qs_pool_keep_at_least(device, e ? std::strtoull(e, nullptr, 10) : (4ull << 30));
 }
+
 
 int qs_create(int device, qs_handle_t* out) {
   qs_context* h = nullptr;

@@ -93,6 +93,9 @@ cudaStream_t qs_upload_stream(qs_context* h);
 void qs_after_launch(qs_context* h, const char* what);
 // Adjusts the launch counters (kernels replayed from, or captured into, a graph).
 void qs_count_launches(qs_context* h, int64_t delta);
+// Raises the release threshold of the device's default memory pool to at
+// least `keep` bytes (freed stream-ordered memory stays mapped up to it).
+void qs_pool_keep_at_least(int device, uint64_t keep);
 
 // ------------------------------------------------------- device program ---
 // A plan is a list of passes.  A pass streams every tile of the state once:

@@ -330,6 +330,11 @@ int qs_server_create(int device, int64_t budget_bytes, int n_workers, qs_server_
     qs_set_tls_error("device index out of range");
     return QS_ERR_INVALID;
   }
+  // The workers allocate and free their items' buffers (states, block
+  // matrices, gradient work) stream-ordered, up to the budget at once; the
+  // pool keeps that much mapped, so a synchronisation does not hand it back
+  // to the driver only for the next item to map it again.
+  qs_pool_keep_at_least(device, (uint64_t)budget_bytes);
   auto* s = new qs_server_s();
   s->device = device;
   s->budget = s->free_bytes = budget_bytes;
