@@ -18,14 +18,15 @@
 // truncation of l leave ~3e-7 relative error per block, of either sign; the
 // CUDA-core interpreter does the same work in FP32 FMAs.
 //
-// Per CTA (128 threads, two CTAs per SM): the tile (2^12 or 2^13 amplitudes)
+// Per CTA (256 threads, two CTAs per SM): the tile (2^12 or 2^13 amplitudes)
 // is staged in shared memory as in qs_pass.cu.  For each block and each 128
-// of the tile's register groups, every thread gathers its group's 32
-// amplitudes from the tile, splits them in registers and stores both halves
-// into its own tensor-memory lane (tcgen05.st: the A operand lives in tensor
-// memory, row m = lane m); one thread issues the 24 MMAs once the block
-// matrix (32 KiB, one bulk copy into shared memory) has landed, and the
-// threads read their group's 32 outputs back (tcgen05.ld) into the tile.
+// of the tile's register groups, two threads per group each gather 16 of
+// its 32 amplitudes from the tile, split them in registers and store both
+// halves into the group's tensor-memory lane (tcgen05.st: the A operand
+// lives in tensor memory, row m = lane m, the two threads on different
+// columns); one thread issues the 24 MMAs once the block matrix (32 KiB, one
+// bulk copy into shared memory) has landed, and the threads read their 16
+// outputs back (tcgen05.ld) into the tile.
 // Tensor memory per CTA: A high part (64 columns), A low part (64), D (64).
 //
 // The pass is unitary on each tile, so it keeps the tile's norm, but the
@@ -52,7 +53,10 @@ using namespace qs;
 
 namespace {
 
-constexpr int kTcThreads = 128;  // one warpgroup: thread m owns tensor-memory lane m
+// Two warpgroups: warp w works on tensor-memory lanes 32 (w % 4) .. + 31
+// (register groups of those rows) and on the amplitudes 16 (w / 4) .. + 15
+// of each group, i.e. on columns 32 (w / 4) .. + 31 of the A and D operands.
+constexpr int kTcThreads = 256;
 // Shared memory (bytes): tile | block matrix (high, low) | dep tables | S |
 // mbarriers + TMEM slot | FP64 partial sums (2 per warp).
 constexpr uint32_t kBOff = 65536;
@@ -102,11 +106,12 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t addr) {
          (1ull << 46);
 }
 // D (+)= A B with A in tensor memory (row m = lane m, K along the columns).
+// The asm statements are volatile (kept in order) but clobber no memory, so
+// the compiler keeps the operands in registers across the issue sequence.
 __device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b, uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}" ::"r"(d),
-      "r"(a), "l"(b), "r"(kIdesc), "r"(acc)
-      : "memory");
+      "r"(a), "l"(b), "r"(kIdesc), "r"(acc));
 }
 // x rounded to the nearest TF32 value (11 significant bits; the carry of a
 // round-up may move into the exponent, which is the correct result).  With
@@ -170,9 +175,12 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
   uint64_t* dep_hi = dep_lo + 128;
   int* s_S = reinterpret_cast<int*>(smem + kSOff);
   double* red = reinterpret_cast<double*>(smem + kRedOff);
-  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, quarter = warp & 3u, half = warp >> 2;
+  const uint32_t row = 32u * quarter + (tid & 31u);  // register group (MMA row) within a 128-group slice
   const uint32_t b_bar = su32(smem + kBarOff), mma_bar = b_bar + 8u, tslot = b_bar + 16u;
-  const uint32_t bhi = su32(smem + kBOff), blo = bhi + 16384u;
+  const uint32_t bhi = su32(smem + kBOff);
+  // B descriptors: K step s starts 256 bytes (16 descriptor units) further
+  const uint64_t bdesc_hi = tc_desc(bhi), bdesc_lo = tc_desc(bhi + 16384u);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tslot), "r"(kTmemCols)
@@ -188,7 +196,7 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + kBarOff + 16);
-  const uint32_t lane = (32u * warp) << 16;  // this warp's 32 lanes
+  const uint32_t lane = ((32u * quarter) << 16) + 32u * half;  // this warp's lanes and column half
 
   uint32_t nb = 0, nm = 0;  // block-matrix loads issued; MMA batches
   int cur = -1;
@@ -273,30 +281,31 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
         pp[k] = tphys(1u << pos[k]);
       }
       for (uint32_t mt = 0; mt < nmt; ++mt) {
-        uint32_t base = mt * 128u + tid;  // group bits -> the tile's other positions, ascending
+        uint32_t base = mt * 128u + row;  // group bits -> the tile's other positions, ascending
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           const uint32_t lo = base & ((1u << pos[k]) - 1u);
           base = ((base ^ lo) << 1) | lo;
         }
-        uint32_t ad[32];
-        ad[0] = tphys(base);
+        // this thread's 16 amplitudes of the group: j = 16 half + j'
+        uint32_t ad[16];
+        ad[0] = tphys(base) ^ (half ? pp[4] : 0u);
 #pragma unroll
-        for (int j = 1; j < 32; ++j) ad[j] = ad[j & (j - 1)] ^ pp[__ffs(j) - 1];
-        // gather this group's amplitudes (re, im interleaved = the K order)
-        uint32_t x[64], h[64];
+        for (int j = 1; j < 16; ++j) ad[j] = ad[j & (j - 1)] ^ pp[__ffs(j) - 1];
+        // gather (re, im interleaved = the K order)
+        uint32_t x[32], h[32];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < 16; ++j) {
           const float2 a = tile[ad[j]];
           x[2 * j] = __float_as_uint(a.x);
           x[2 * j + 1] = __float_as_uint(a.y);
         }
         if (b == 0) {
 #pragma unroll
-          for (int e = 0; e < 64; ++e) nin = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nin);
+          for (int e = 0; e < 32; ++e) nin = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nin);
         }
 #pragma unroll
-        for (int e = 0; e < 64; e += 2) {
+        for (int e = 0; e < 32; e += 2) {
           const float2 v = make_float2(__uint_as_float(x[e]), __uint_as_float(x[e + 1]));
           const float2 hv = make_float2(hi_part(v.x), hi_part(v.y));
           const float2 lv = __fadd2_rn(v, make_float2(-hv.x, -hv.y));  // exact: v - hv
@@ -306,37 +315,40 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
           x[e + 1] = __float_as_uint(lv.y);
         }
         tmem_st32(tmem + lane, h);
-        tmem_st32(tmem + lane + 32u, h + 32);
         tmem_st32(tmem + lane + kColAlo, x);
-        tmem_st32(tmem + lane + kColAlo + 32u, x + 32);
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
           if (mt == 0 && !tc_wait(b_bar, nb & 1u, limit)) atomicOr(status, 8u);
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t dcol = tmem + kColD;
 #pragma unroll
           for (uint32_t s = 0; s < 8; ++s) {
-            const uint64_t bh = tc_desc(bhi + 256u * s), bl = tc_desc(blo + 256u * s);
-            tc_mma(tmem + kColD, tmem + kColAlo + 8u * s, bh, s > 0 ? 1u : 0u);
-            tc_mma(tmem + kColD, tmem + 8u * s, bl, 1u);
-            tc_mma(tmem + kColD, tmem + 8u * s, bh, 1u);
+            const uint64_t bh = bdesc_hi + 16u * s, bl = bdesc_lo + 16u * s;
+            tc_mma(dcol, tmem + kColAlo + 8u * s, bh, s > 0 ? 1u : 0u);
+            tc_mma(dcol, tmem + 8u * s, bl, 1u);
+            tc_mma(dcol, tmem + 8u * s, bh, 1u);
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_bar)
                        : "memory");
+          // the issuing thread alone waits for the MMAs; the others sleep in
+          // the barrier below instead of polling (their issue slots go to
+          // the SM's other CTA)
+          if (!tc_wait(mma_bar, nm & 1u, limit)) atomicOr(status, 8u);
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
-        if (!tc_wait(mma_bar, nm & 1u, limit) && tid == 0) atomicOr(status, 8u);
         ++nm;
+        __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         tmem_ld32(tmem + lane + kColD, x);
-        tmem_ld32(tmem + lane + kColD + 32u, x + 32);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (b + 1 == nblocks) {
 #pragma unroll
-          for (int e = 0; e < 64; ++e) nout = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nout);
+          for (int e = 0; e < 32; ++e) nout = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nout);
         }
 #pragma unroll
-        for (int j = 0; j < 32; ++j) tile[ad[j]] = make_float2(__uint_as_float(x[2 * j]), __uint_as_float(x[2 * j + 1]));
+        for (int j = 0; j < 16; ++j) tile[ad[j]] = make_float2(__uint_as_float(x[2 * j]), __uint_as_float(x[2 * j + 1]));
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
       ++nb;
