@@ -132,8 +132,10 @@ int64_t qs_launch_count(qs_handle_t h);
  * by mbarriers), and a batch plan runs as one persistent launch whose CTAs
  * wait for a state's previous pass before its next; every one of these waits
  * is bounded, and a wait that runs out ORs a cause into this word (1: a
- * pass's copy warp, 2: a pass's compute warps, 4: a batch dependency) and
- * its CTA returns, leaving that part of the state unfinished.  Waits on the
+ * pass's copy warp, 2: a pass's compute warps, 4: a batch dependency, 8: a
+ * tensor-core pass's block-matrix copy or MMA batch) and its CTA returns
+ * (the tensor-core pass finishes its tiles with whatever the wait left),
+ * leaving that part of the state unfinished or wrong.  Waits on the
  * handle's stream, stores the word in *code (0 = no wait ran out) and
  * clears it.  No reference counterpart (the reference has no device-side
  * waits).                                                                   */
