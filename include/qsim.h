@@ -417,6 +417,10 @@ int qs_autotune_batch(qs_handle_t h, int n_circuits, const int32_t* widths, cons
                       const qs_op* ops);
 /* The tuned (tile bits, block bits) for a width; QS_ERR_INVALID if none.    */
 int qs_autotune_get(int device, int width, int* tile_bits, int* block_bits);
+/* Records a (tile bits, block bits) entry for a width as the autotuner would
+ * (a table saved from an earlier process, or a fixed shape for profiling);
+ * QS_ERR_INVALID outside tile bits 10..14, block bits 2..5.                 */
+int qs_autotune_set(int device, int width, int tile_bits, int block_bits);
 /* Forget the tuned entries of a device (device < 0: all devices).           */
 int qs_autotune_clear(int device);
 

@@ -177,6 +177,17 @@ int qs_autotune_get(int device, int width, int* tile_bits, int* block_bits) {
   return QS_OK;
 }
 
+int qs_autotune_set(int device, int width, int tile_bits, int block_bits) {
+  if (device < 0 || width < 1 || width > 40 || tile_bits < 10 || tile_bits > 14 || block_bits < 2 ||
+      block_bits > 5) {
+    qs_set_tls_error("autotune entry out of range (device >= 0, width 1..40, tile bits 10..14, block bits 2..5)");
+    return QS_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_table()[{device, width}] = Shape{tile_bits, block_bits};
+  return QS_OK;
+}
+
 int qs_autotune_clear(int device) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto& t = tune_table();

@@ -125,6 +125,7 @@ SIGNATURES = {
     "qs_plan_jit_check": (_i, [_i, _pop, _i, _i, _i, C.POINTER(C.c_int)]),
     "qs_autotune_batch": (_i, [_vp, _i, _vp, _vp, _pop]),
     "qs_autotune_get": (_i, [_i, _i, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "qs_autotune_set": (_i, [_i, _i, _i, _i]),
     "qs_autotune_clear": (_i, [_i]),
     "qs_server_create": (_i, [_i, C.c_int64, _i, C.POINTER(C.c_void_p)]),
     "qs_server_destroy": (_i, [_vp]),

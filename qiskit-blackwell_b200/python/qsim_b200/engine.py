@@ -69,6 +69,15 @@ def autotune_batch(widths, op_offsets, ops, device: int | None = None) -> dict:
     return out
 
 
+def autotune_set(table: dict, device: int | None = None) -> None:
+    """Records {width: (tile_bits, block_bits)} entries as autotune_batch
+    would (a table saved from an earlier run, or a fixed shape)."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    L = _lib.load()
+    for w, (tb, bb) in table.items():
+        _lib.check(L.qs_autotune_set(dev, int(w), int(tb), int(bb)))
+
+
 def autotune_clear(device: int | None = None) -> None:
     _lib.load().qs_autotune_clear(-1 if device is None else int(device))
 

@@ -65,3 +65,23 @@ def test_fast_extension_binds_the_same_library():
         F.apply_1q_dev(0, 0, 3, 0, 0)
     with pytest.raises(RuntimeError, match="0-7"):
         F.apply_mc1q_dev(0, 0, 3, 0, list(range(8)), 0)
+
+
+def test_autotune_table_set_get_and_range(lib):
+    """A tuned entry set by hand reads back through qs_autotune_get (host-side
+    table, no GPU work); entries outside the kernels' shapes are rejected."""
+    lib.qs_autotune_set.argtypes = [ctypes.c_int] * 4
+    lib.qs_autotune_get.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int)]
+    dev = 7  # a device index no GPU test uses
+    assert lib.qs_autotune_set(dev, 17, 13, 5) == 0
+    tb, bb = ctypes.c_int(0), ctypes.c_int(0)
+    assert lib.qs_autotune_get(dev, 17, ctypes.byref(tb), ctypes.byref(bb)) == 0
+    assert (tb.value, bb.value) == (13, 5)
+    for bad in ((dev, 17, 9, 5), (dev, 17, 15, 5), (dev, 17, 13, 1), (dev, 17, 13, 6), (-1, 17, 13, 5),
+                (dev, 0, 13, 5)):
+        assert lib.qs_autotune_set(*bad) != 0
+    assert lib.qs_autotune_get(dev, 17, ctypes.byref(tb), ctypes.byref(bb)) == 0
+    assert (tb.value, bb.value) == (13, 5)
+    assert lib.qs_autotune_clear(dev) == 0
+    assert lib.qs_autotune_get(dev, 17, ctypes.byref(tb), ctypes.byref(bb)) != 0
