@@ -133,7 +133,8 @@ int64_t qs_launch_count(qs_handle_t h);
  * wait for a state's previous pass before its next; every one of these waits
  * is bounded, and a wait that runs out ORs a cause into this word (1: a
  * pass's copy warp, 2: a pass's compute warps, 4: a batch dependency, 8: a
- * tensor-core pass's block-matrix copy or MMA batch) and its CTA returns
+ * tensor-core pass's block-matrix copy or MMA batch; 16: a target of
+ * qs_apply_gates_fused_dev outside the state) and its CTA returns
  * (the tensor-core pass finishes its tiles with whatever the wait left),
  * leaving that part of the state unfinished or wrong.  Waits on the
  * handle's stream, stores the word in *code (0 = no wait ran out) and
@@ -238,6 +239,18 @@ int qs_apply_mcz(qs_handle_t h, void* state, int n_qubits, const int* qubits, in
  * (apply_gates_fused, apply_gates_reg_tiled): K 1Q gates in one launch.     */
 int qs_apply_gates_fused(qs_handle_t h, void* state, int n_qubits, const float* gates_c64,
                          const int* targets, int n_gates);
+/* The same with the matrices (n_gates x 2x2 complex64, row-major) and the
+ * targets (n_gates int32) in device memory of the handle's GPU: one launch per
+ * 12 gates, no host copy, no stream synchronisation (the reference's
+ * apply_gates_fused also reads device tensors: bwk/python/blackwell_kernels/
+ * cuquantum.py:69-80).  Each launch stages tiles of min(n, 12) qubits that
+ * hold the gates' targets and applies the gates in order in shared memory
+ * (FP32 FMA chains: within ~1e-7 relative per gate of one qs_apply_1q_dev
+ * call per gate, whose compensated products cost 4x the arithmetic).  A target
+ * outside [0, n) is found on the device: that launch leaves the state
+ * unchanged and ORs 16 into the device status word (qs_device_status).      */
+int qs_apply_gates_fused_dev(qs_handle_t h, void* state, int n_qubits, const void* gates_dev,
+                             const void* targets_dev, int n_gates);
 /* Reference: bwk/csrc/batch_sm120.cu:53-102,185-228 (apply_gate_batched):
  * one 2x2 gate on n_states equal-width states stored back to back.          */
 int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n_qubits,

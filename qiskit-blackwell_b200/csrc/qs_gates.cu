@@ -84,6 +84,89 @@ __global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G0, c
   }
 }
 
+// K <= 12 single-qubit gates whose matrices and targets are device arrays,
+// applied in order in one launch (the device-tensor form of
+// apply_gates_fused: no host copy of the gates, no stream synchronisation).
+// Each CTA stages tiles of 2^T amplitudes (T = min(n, 12)) whose qubits are
+// the gates' distinct targets and the lowest other qubits, applies every
+// gate to the tile in shared memory as an FMA chain per output (each FMA
+// rounds once; the single-gate kernels' compensated Dot2 costs four times
+// the arithmetic, which bounds this kernel), and writes the tile back.  A
+// target outside [0, n) makes every CTA return before it writes (bit 16 of
+// the status word).
+constexpr int kFusedMax = 12;
+__global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s, int n, const float2* __restrict__ gates,
+                                                          const int32_t* __restrict__ targets, int K,
+                                                          uint32_t* status) {
+  extern __shared__ float2 tile[];
+  __shared__ G2 sg[kFusedMax];
+  __shared__ int st[kFusedMax];     // targets
+  __shared__ int spos[kFusedMax];   // tile position of gate k's target
+  __shared__ int sq[kFusedMax];     // tile qubits, ascending
+  __shared__ uint64_t dep[2][64];   // tile index bits -> state index bits (6 + 6)
+  __shared__ int s_ok;
+  const int T = n < kFusedMax ? n : kFusedMax;
+  // one round trip for the gates' matrices and targets, then thread 0 picks
+  // the tile qubits from shared memory
+  if ((int)threadIdx.x < K) st[threadIdx.x] = targets[threadIdx.x];
+  if ((int)threadIdx.x < 4 * K) sg[threadIdx.x >> 2].g[threadIdx.x & 3] = gates[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t m = 0;
+    int ok = 1;
+    for (int k = 0; k < K; ++k) {
+      const int t = st[k];
+      if (t < 0 || t >= n) ok = 0; else m |= 1ull << t;
+    }
+    for (int q = 0; q < n && __popcll(m) < T; ++q) m |= 1ull << q;
+    int j = 0;
+    for (int q = 0; q < n; ++q)
+      if ((m >> q) & 1ull) sq[j++] = q;
+    if (ok) {
+      for (int k = 0; k < K; ++k) spos[k] = __popcll(m & ((1ull << st[k]) - 1ull));
+    } else if (blockIdx.x == 0) {
+      atomicOr(status, 16u);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  for (int e = threadIdx.x; e < 128; e += blockDim.x) {
+    const int part = e >> 6, x = e & 63;
+    uint64_t d = 0;
+    for (int b = 0; b < 6; ++b) {
+      const int kk = 6 * part + b;
+      if (kk < T && ((x >> b) & 1)) d |= 1ull << sq[kk];
+    }
+    dep[part][x] = d;
+  }
+  __syncthreads();
+  const uint32_t tsize = 1u << T, half = tsize >> 1;
+  const uint64_t ntiles = 1ull << (n - T);
+  for (uint64_t tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    uint64_t gbase = tl;
+    for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, sq[k]);
+#pragma unroll 8
+    for (uint32_t i = threadIdx.x; i < tsize; i += blockDim.x) tile[i] = s[gbase | dep[0][i & 63] | dep[1][i >> 6]];
+    __syncthreads();
+    for (int k = 0; k < K; ++k) {
+      const int p = spos[k];
+      const G2 G = sg[k];
+#pragma unroll 4
+      for (uint32_t j = threadIdx.x; j < half; j += blockDim.x) {
+        const uint32_t i0 = (uint32_t)insert_zero(j, p), i1 = i0 | (1u << p);
+        const float2 a0 = tile[i0], a1 = tile[i1];
+        tile[i0] = cfma2(G.g[0], a0, G.g[1], a1);
+        tile[i1] = cfma2(G.g[2], a0, G.g[3], a1);
+      }
+      __syncthreads();
+    }
+#pragma unroll 8
+    for (uint32_t i = threadIdx.x; i < tsize; i += blockDim.x) s[gbase | dep[0][i & 63] | dep[1][i >> 6]] = tile[i];
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------- 2Q ---------
 __device__ __forceinline__ void apply4(const G4& G, float2& a0, float2& a1, float2& a2, float2& a3) {
   float2 v[4] = {a0, a1, a2, a3};
@@ -413,14 +496,15 @@ int qs_apply_1q_batched(qs_handle_t h, void* states, int n_states, int n, const 
 // stream.  The pointer must be device memory of the handle's own GPU (or
 // managed memory): a gate on another GPU would be read across the link, or
 // fault when peer access is off.
-// The last pointer that passed is remembered per handle together with the
-// device it was checked for (a gate tensor is usually reused call after
+// The last four pointers that passed are remembered per handle together with
+// the device each was checked for (gate tensors are usually reused call after
 // call).  An address that was freed and handed out again by another
 // allocation of the same GPU is still device memory of that GPU, so the
 // remembered answer stays true for it.
 static void check_dev_ptr(qs_context* h, const void* p, const char* what) {
   QS_CHECK_ARG(p != nullptr && ((uintptr_t)p & 7u) == 0, std::string(what) + " must be 8-byte aligned");
-  if (p == h->dev_ptr_ok && h->dev_ptr_ok_device == h->device) return;
+  for (int k = 0; k < 4; ++k)
+    if (p == h->dev_ptr_ok[k] && h->dev_ptr_ok_device[k] == h->device) return;
   cudaPointerAttributes a;
   const cudaError_t e = cudaPointerGetAttributes(&a, p);
   if (e != cudaSuccess) (void)cudaGetLastError();  // clear the sticky-free error state of the query
@@ -429,8 +513,9 @@ static void check_dev_ptr(qs_context* h, const void* p, const char* what) {
   QS_CHECK_ARG(a.type == cudaMemoryTypeManaged || a.device == h->device,
                std::string(what) + " is device memory of GPU " + std::to_string(a.device) +
                    ", not of the handle's GPU " + std::to_string(h->device));
-  h->dev_ptr_ok = p;
-  h->dev_ptr_ok_device = h->device;
+  h->dev_ptr_ok[h->dev_ptr_next] = p;
+  h->dev_ptr_ok_device[h->dev_ptr_next] = h->device;
+  h->dev_ptr_next = (h->dev_ptr_next + 1) & 3;
 }
 
 int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int t) {
@@ -440,6 +525,31 @@ int qs_apply_1q_dev(qs_handle_t h, void* state, int n, const void* gate_dev, int
   qs_check_qubit(t, n, "target");
   check_dev_ptr(h, gate_dev, "gate");
   qs_launch_1q(h, (float2*)state, 1ull << (n - 1), t, G2{}, static_cast<const float2*>(gate_dev));
+  QS_API_END(h)
+}
+
+int qs_apply_gates_fused_dev(qs_handle_t h, void* state, int n, const void* gates_dev, const void* targets_dev,
+                             int n_gates) {
+  QS_REQUIRE_HANDLE(h);
+  QS_API_BEGIN
+  qs_check_state(state, n);
+  QS_CHECK_ARG(n_gates >= 0, "n_gates must be >= 0");
+  if (n_gates == 0) return QS_OK;
+  check_dev_ptr(h, gates_dev, "gates");
+  QS_CHECK_ARG(((uintptr_t)targets_dev & 3u) == 0, "targets must be 4-byte aligned");
+  check_dev_ptr(h, targets_dev, "targets");
+  const int T = std::min(n, kFusedMax);
+  const size_t smem = sizeof(float2) << T;
+  const uint64_t ntiles = 1ull << (n - T);
+  const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)h->sm_count * 6);
+  const float2* g = static_cast<const float2*>(gates_dev);
+  const int32_t* t = static_cast<const int32_t*>(targets_dev);
+  // at most 12 gates per launch, so their distinct targets always fit a tile
+  for (int k0 = 0; k0 < n_gates; k0 += kFusedMax) {
+    const int K = std::min(kFusedMax, n_gates - k0);
+    k_fused1q_dev<<<grid, kThreads, smem, h->stream>>>((float2*)state, n, g + 4 * k0, t + k0, K, h->dev_status);
+    qs_after_launch(h, "k_fused1q_dev");
+  }
   QS_API_END(h)
 }
 

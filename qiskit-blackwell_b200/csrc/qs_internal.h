@@ -64,8 +64,9 @@ struct qs_context {
   // Test hook (qs_set_wait_test): the next pipelined pass withholds its first
   // tile so that the consumers' bounded wait runs out.
   int wait_test = 0;
-  const void* dev_ptr_ok = nullptr;  // last pointer found to be device memory (qs_apply_*_dev)
-  int dev_ptr_ok_device = -1;        // the device dev_ptr_ok was checked against
+  const void* dev_ptr_ok[4] = {nullptr, nullptr, nullptr, nullptr};  // pointers found to be device memory (qs_apply_*_dev)
+  int dev_ptr_ok_device[4] = {-1, -1, -1, -1};  // the device each was checked against
+  int dev_ptr_next = 0;                          // slot the next new pointer replaces
 
   // grow-only device scratch (reductions, sampling partials, ...)
   void* scratch = nullptr;

@@ -77,6 +77,15 @@ static PyObject* f_apply_1q_dev(PyObject* self, PyObject* const* args, Py_ssize_
   return rc ? fail(h, rc) : Py_NewRef(Py_None);
 }
 
+/* apply_gates_fused_dev(h, state, n, gates, targets, k) */
+static PyObject* f_apply_gates_fused_dev(PyObject* self, PyObject* const* args, Py_ssize_t nargs) {
+  if (!check_n(nargs, 6)) return NULL;
+  void* h = PTR(0);
+  const int rc = qs_apply_gates_fused_dev((qs_handle_t)h, PTR(1), INT(2), PTR(3), PTR(4), INT(5));
+  if (PyErr_Occurred()) return NULL;
+  return rc ? fail(h, rc) : Py_NewRef(Py_None);
+}
+
 /* apply_2q_dev(h, state, n, gate, q0, q1) */
 static PyObject* f_apply_2q_dev(PyObject* self, PyObject* const* args, Py_ssize_t nargs) {
   if (!check_n(nargs, 6)) return NULL;
@@ -140,6 +149,8 @@ static PyMethodDef kMethods[] = {
     {"set_error", (PyCFunction)f_set_error, METH_O, "exception class raised for a non-zero status"},
     {"apply_1q_dev", (PyCFunction)(void (*)(void))f_apply_1q_dev, METH_FASTCALL, "qs_apply_1q_dev"},
     {"apply_2q_dev", (PyCFunction)(void (*)(void))f_apply_2q_dev, METH_FASTCALL, "qs_apply_2q_dev"},
+    {"apply_gates_fused_dev", (PyCFunction)(void (*)(void))f_apply_gates_fused_dev, METH_FASTCALL,
+     "qs_apply_gates_fused_dev"},
     {"apply_diag1_dev", (PyCFunction)(void (*)(void))f_apply_diag1_dev, METH_FASTCALL, "qs_apply_diag1_dev"},
     {"apply_diag2_dev", (PyCFunction)(void (*)(void))f_apply_diag2_dev, METH_FASTCALL, "qs_apply_diag2_dev"},
     {"apply_phase", (PyCFunction)(void (*)(void))f_apply_phase, METH_FASTCALL, "qs_apply_phase"},

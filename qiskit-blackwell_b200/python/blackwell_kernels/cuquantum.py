@@ -122,12 +122,31 @@ def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: 
 def apply_gates_fused(state: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
     """K 1Q gates in one fused program (cuquantum.py:69-80)."""
     n = check_state(state)
-    if (isinstance(gates, torch.Tensor) and isinstance(targets, torch.Tensor)
+    if (isinstance(gates, torch.Tensor) and isinstance(targets, torch.Tensor) and gates.is_cuda
             and gates.device == state.device and targets.device == state.device):
-        # both to pinned host memory on the current stream, one wait for the pair
-        gates = gates.detach().to("cpu", torch.complex64, non_blocking=True)
-        targets = targets.detach().to("cpu", non_blocking=True)
-        torch.cuda.current_stream(state.device).synchronize()
+        # device tensors: the kernel reads matrices and targets itself (no host
+        # copy, no stream synchronisation); one launch per 12 gates
+        g = gates.detach()
+        if g.dtype != _C64:
+            g = g.to(_C64)
+        if g.ndim != 3 or tuple(g.shape[1:]) != (2, 2):
+            raise RuntimeError("gates must be [N, 2, 2]")
+        t = targets.detach().reshape(-1)
+        if t.numel() != g.shape[0]:
+            raise RuntimeError("targets must have N entries")
+        if t.dtype != torch.int32:
+            t = t.to(torch.int32)
+        g = g.contiguous()
+        t = t.contiguous()
+        if t.data_ptr() & 7:
+            t = t.clone()
+        dev = state.get_device()
+        F = _lib.fast()
+        if F is not None:
+            F.apply_gates_fused_dev(E._hptr(dev), state.data_ptr(), n, g.data_ptr(), t.data_ptr(), int(t.numel()))
+        else:
+            _h(dev).call("qs_apply_gates_fused_dev", state.data_ptr(), n, g.data_ptr(), t.data_ptr(), int(t.numel()))
+        return state
     if isinstance(gates, torch.Tensor):
         g = gates.detach().to("cpu", torch.complex64).contiguous().numpy()
     else:

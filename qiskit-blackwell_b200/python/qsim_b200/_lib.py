@@ -103,6 +103,7 @@ SIGNATURES = {
     "qs_apply_phase": (_i, [_vp, _vp, _i, _f, _f, _i]),
     "qs_apply_diag2": (_i, [_vp, _vp, _i, _pf, _i, _i]),
     "qs_apply_1q_dev": (_i, [_vp, _vp, _i, _vp, _i]),
+    "qs_apply_gates_fused_dev": (_i, [_vp, _vp, _i, _vp, _vp, _i]),
     "qs_apply_2q_dev": (_i, [_vp, _vp, _i, _vp, _i, _i]),
     "qs_apply_diag1_dev": (_i, [_vp, _vp, _i, _vp, _i]),
     "qs_apply_mc1q_dev": (_i, [_vp, _vp, _i, _vp, _pi, _i, _i]),
