@@ -129,11 +129,14 @@ __device__ __forceinline__ float2 ry1(float co, float si, float2 a0, float2 a1) 
   return make_float2(fmaf(si, a0.x, __fmul_rn(co, a1.x)), fmaf(si, a0.y, __fmul_rn(co, a1.y)));
 }
 // Scaled rotations (DK_KRY) as packed FP32x2 FMAs: one instruction per
-// output amplitude, lane results identical to the scalar fmaf.
+// output amplitude, lane results identical to the scalar fmaf.  t * a0 - a1
+// is two scalar FMAs instead: the packed form has no negated addend, and the
+// negation of a1 cost two FADDs on the FMA pipe besides the two cycles of the
+// packed FMA (same bits either way: the negation is exact).
 __device__ __forceinline__ float2 rta0(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(-t, -t), a1, a0); }
 __device__ __forceinline__ float2 rta1(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(t, t), a0, a1); }
 __device__ __forceinline__ float2 rtb0(float t, float2 a0, float2 a1) {
-  return __ffma2_rn(make_float2(t, t), a0, make_float2(-a1.x, -a1.y));
+  return make_float2(fmaf(t, a0.x, -a1.x), fmaf(t, a0.y, -a1.y));
 }
 __device__ __forceinline__ float2 rtb1(float t, float2 a0, float2 a1) { return __ffma2_rn(make_float2(t, t), a1, a0); }
 // The same four updates as two scalar FMAs (identical results lane by lane).

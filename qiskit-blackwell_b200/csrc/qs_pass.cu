@@ -242,7 +242,7 @@ __device__ __forceinline__ void kry_stage(float2 (&v)[1 << R], float2 tf) {
       if (j & (1 << K)) continue;
       const int k = j | (1 << K);
       const float2 a0 = v[j], a1 = v[k];
-      v[j] = __ffma2_rn(tt, a0, make_float2(-a1.x, -a1.y));
+      v[j] = make_float2(fmaf(tt.x, a0.x, -a1.x), fmaf(tt.x, a0.y, -a1.y));  // negated addend: scalar FMAs
       v[k] = __ffma2_rn(tt, a1, a0);
     }
   }
@@ -287,7 +287,7 @@ __device__ __forceinline__ void op_xry(float2 (&v)[1 << R], const float2* __rest
         v[j] = __ffma2_rn(nt, a1, a0);
         v[k] = __ffma2_rn(tt, a0, a1);
       } else {
-        v[j] = __ffma2_rn(tt, a0, make_float2(-a1.x, -a1.y));
+        v[j] = make_float2(fmaf(tt.x, a0.x, -a1.x), fmaf(tt.x, a0.y, -a1.y));
         v[k] = __ffma2_rn(tt, a1, a0);
       }
     }
