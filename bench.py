@@ -295,7 +295,11 @@ def bench_qv_batch(args, dev):
     C = args.circuits
     widths, oo, ops, so = W.qv_batch(C, 10, 20, seed=1)
     t_tune = time.perf_counter()
-    tuned = E.autotune_batch(widths, oo, ops, dev)   # shared by the batch and the per-circuit plans
+    if args.tune_table:   # a recorded table (profiling: the tuner's own timings are distorted under a profiler)
+        tuned = {int(k): tuple(v) for k, v in json.loads(args.tune_table).items()}
+        E.autotune_set(tuned, dev)
+    else:
+        tuned = E.autotune_batch(widths, oo, ops, dev)   # shared by the batch and the per-circuit plans
     t_tune = time.perf_counter() - t_tune
     bp = E.BatchPlan(widths, oo, ops, so, dev)
     states = bp.alloc_states()
@@ -1265,6 +1269,8 @@ def main():
                     help="layers32: skip the batched and serving sub-records of the headline metric")
     ap.add_argument("--tile-bits", type=int, default=0, help="planner tile bits (10..14; 0 = library default)")
     ap.add_argument("--block-bits", type=int, default=0, help="register-block qubits (2..5; 0 = default)")
+    ap.add_argument("--tune-table", default="",
+                    help='qv_batch: JSON {width: [tile_bits, block_bits]} recorded instead of autotuning')
     ap.add_argument("--jit", type=int, default=-1,
                     help="pass specialisation: 0 off, 1 tiered (background compile, plans >= 24 qubits), "
                          "2 before first execution (-1 = 2 for layers32, else the library default)")
