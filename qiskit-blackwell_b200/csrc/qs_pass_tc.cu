@@ -280,6 +280,7 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
         pos[k] = blk.pos[k];
         pp[k] = tphys(1u << pos[k]);
       }
+      const bool pair0 = pos[0] == 0;  // register bit 0 on tile bit 0
       for (uint32_t mt = 0; mt < nmt; ++mt) {
         uint32_t base = mt * 128u + row;  // group bits -> the tile's other positions, ascending
 #pragma unroll
@@ -292,13 +293,26 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
         ad[0] = tphys(base) ^ (half ? pp[4] : 0u);
 #pragma unroll
         for (int j = 1; j < 16; ++j) ad[j] = ad[j & (j - 1)] ^ pp[__ffs(j) - 1];
-        // gather (re, im interleaved = the K order)
+        // gather (re, im interleaved = the K order); when register bit 0 is
+        // tile bit 0, amplitudes j and j ^ 1 are neighbours (ad[j] is even:
+        // the swizzle leaves bit 0 alone) and move as one 16-byte access
         uint32_t x[32], h[32];
+        if (pair0) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const float2 a = tile[ad[j]];
-          x[2 * j] = __float_as_uint(a.x);
-          x[2 * j + 1] = __float_as_uint(a.y);
+          for (int j = 0; j < 16; j += 2) {
+            const float4 a = *reinterpret_cast<const float4*>(tile + ad[j]);
+            x[2 * j] = __float_as_uint(a.x);
+            x[2 * j + 1] = __float_as_uint(a.y);
+            x[2 * j + 2] = __float_as_uint(a.z);
+            x[2 * j + 3] = __float_as_uint(a.w);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float2 a = tile[ad[j]];
+            x[2 * j] = __float_as_uint(a.x);
+            x[2 * j + 1] = __float_as_uint(a.y);
+          }
         }
         if (b == 0) {
 #pragma unroll
@@ -348,7 +362,16 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
           for (int e = 0; e < 32; ++e) nout = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nout);
         }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) tile[ad[j]] = make_float2(__uint_as_float(x[2 * j]), __uint_as_float(x[2 * j + 1]));
+        if (pair0) {
+#pragma unroll
+          for (int j = 0; j < 16; j += 2)
+            *reinterpret_cast<float4*>(tile + ad[j]) = make_float4(__uint_as_float(x[2 * j]), __uint_as_float(x[2 * j + 1]),
+                                                                   __uint_as_float(x[2 * j + 2]), __uint_as_float(x[2 * j + 3]));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            tile[ad[j]] = make_float2(__uint_as_float(x[2 * j]), __uint_as_float(x[2 * j + 1]));
+        }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
       ++nb;
