@@ -388,7 +388,7 @@ def bench_qv_batch(args, dev):
     e2e_step()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ne = max(1, args.steps // 2)
+    ne = max(3, args.steps)   # ~0.15 s each: several steps for a stable wall-clock figure
     for _ in range(ne):
         e2e_step()
     torch.cuda.synchronize()
