@@ -361,7 +361,6 @@ k_pass_tc(float2* __restrict__ base_state, PassItem single, const PassItem* __re
 #pragma unroll
           for (int e = 0; e < 32; ++e) nout = fma((double)__uint_as_float(x[e]), (double)__uint_as_float(x[e]), nout);
         }
-#pragma unroll
         if (pair0) {
 #pragma unroll
           for (int j = 0; j < 16; j += 2)
