@@ -59,3 +59,30 @@ def test_tensor_core_pass_is_deterministic():
     _, a = _batch(widths, oo, ops, so, 1)
     _, b = _batch(widths, oo, ops, so, 1)
     assert np.array_equal(a, b)
+
+
+def test_twelve_qubit_tiles_many_tiles_per_circuit():
+    """The tensor-core pass with 12-qubit tiles on circuits of 13-17 qubits
+    (2 to 32 tiles per pass, one 128-group slice per block), the shape the
+    autotuner may record for a width: every circuit against FP64."""
+    widths, oo, ops, so = W.qv_batch(10, 13, 17, seed=91)
+    dev = torch.cuda.current_device()
+    L = E._h().L
+    saved = {}
+    tb, bb = C.c_int(0), C.c_int(0)
+    for w in range(1, 41):
+        if L.qs_autotune_get(dev, w, C.byref(tb), C.byref(bb)) == 0:
+            saved[w] = (tb.value, bb.value)
+    E.autotune_set({w: (12, 5) for w in range(13, 18)})
+    try:
+        info, st = _batch(widths, oo, ops, so, 1)
+    finally:
+        E.autotune_clear(dev)        # the table as it was before the test
+        E.autotune_set(saved, dev)
+    assert info["n_tc_launches"] > 0
+    for c in range(len(widths)):
+        w = int(widths[c])
+        got = st[so[c]: so[c] + (1 << w)]
+        ref = O.simulate(w, ops[oo[c]: oo[c + 1]])
+        assert abs(1 - O.fidelity(got, ref)) <= 1e-6, (c, w)
+        assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max(), (c, w)
