@@ -9,6 +9,7 @@
 #include "qs_api.h"
 #include "qs_common.cuh"
 #include <algorithm>
+#include <cstdlib>
 
 using namespace qs;
 
@@ -20,8 +21,21 @@ struct Sorted { int pos[12]; int k; };
 
 constexpr int kThreads = 256;
 
+// Programmatic dependent launch: the per-gate kernels are launched with the
+// programmatic stream-serialisation attribute, so that the next gate's
+// launch overlaps the end of this one.  Each kernel here first waits for the
+// grid before it in the stream (griddepcontrol.wait: that grid has finished
+// and its writes are visible; a no-op when the kernel was launched without
+// the attribute) and then lets the next grid begin its launch, whose CTAs
+// wait in turn before they touch the state.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------------ init --------
 __global__ void k_state_init(float4* __restrict__ s4, uint64_t nvec, uint64_t index) {
+  pdl_begin();
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if ((index >> 1) == i) { if (index & 1) v.z = 1.f; else v.x = 1.f; }
@@ -31,6 +45,7 @@ __global__ void k_state_init(float4* __restrict__ s4, uint64_t nvec, uint64_t in
 
 // states back to back, each of 2^n amplitudes: amplitude 0 of each is 1.
 __global__ void k_state_init_batched(float4* __restrict__ s4, uint64_t nvec, int n) {
+  pdl_begin();
   uint64_t mask = (1ull << n) - 1ull;
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -60,6 +75,7 @@ __device__ __forceinline__ G2 gate2(const G2& G, const float2* __restrict__ gd) 
 
 // target 0: the pair is one float4.
 __global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G0, const float2* __restrict__ gd) {
+  pdl_begin();
   const G2 G = gate2(G0, gd);
   for (uint64_t p = gtid(); p < npairs; p += gstride()) {
     float4 v = ld4(s + 2 * p);
@@ -71,6 +87,7 @@ __global__ void k_1q_t0(float2* __restrict__ s, uint64_t npairs, G2 G0, const fl
 
 // target t >= 1: two neighbouring pairs per thread, two float4 accesses.
 __global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G0, const float2* __restrict__ gd) {
+  pdl_begin();
   const G2 G = gate2(G0, gd);
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
@@ -98,6 +115,7 @@ constexpr int kFusedMax = 12;
 __global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s, int n, const float2* __restrict__ gates,
                                                           const int32_t* __restrict__ targets, int K,
                                                           uint32_t* status) {
+  pdl_begin();
   extern __shared__ float2 tile[];
   __shared__ G2 sg[kFusedMax];
   __shared__ int st[kFusedMax];     // targets
@@ -196,6 +214,7 @@ __device__ __forceinline__ G4 gate4(const G4& G, const float2* __restrict__ gd, 
 // lo == 0: a00,a01 adjacent and a10,a11 adjacent.
 __global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G0, const float2* __restrict__ gd,
                          int swap) {
+  pdl_begin();
   const G4 G = gate4(G0, gd, swap);
   const uint64_t sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nquads; it += gstride()) {
@@ -211,6 +230,7 @@ __global__ void k_2q_lo0(float2* __restrict__ s, uint64_t nquads, int hi, G4 G0,
 // lo >= 1: two neighbouring quads per thread.
 __global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi, G4 G0,
                          const float2* __restrict__ gd, int swap) {
+  pdl_begin();
   const G4 G = gate4(G0, gd, swap);
   const uint64_t sl = 1ull << lo, sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
@@ -230,6 +250,7 @@ __global__ void k_2q_gen(float2* __restrict__ s, uint64_t nitems, int lo, int hi
 // ----------------------------------------------------------- diagonal -----
 __global__ void k_diag1(float2* __restrict__ s, uint64_t nvec, int t, float2 d0v, float2 d1v,
                         const float2* __restrict__ gd) {
+  pdl_begin();
   const float2 d0 = gd ? gd[0] : d0v, d1 = gd ? gd[1] : d1v;
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     uint64_t idx = 2 * i;
@@ -243,12 +264,14 @@ __global__ void k_diag1(float2* __restrict__ s, uint64_t nvec, int t, float2 d0v
 
 // Only amplitudes with bit t = 1 (half the traffic).
 __global__ void k_phase_t0(float2* __restrict__ s, uint64_t npairs, float2 ph) {
+  pdl_begin();
   for (uint64_t p = gtid(); p < npairs; p += gstride()) {
     uint64_t idx = 2 * p + 1;
     s[idx] = cmul_comp(s[idx], ph);
   }
 }
 __global__ void k_phase_tn(float2* __restrict__ s, uint64_t nitems, int t, float2 ph) {
+  pdl_begin();
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t idx = insert_zero(2 * it, t) | (1ull << t);
     float4 v = ld4(s + idx);
@@ -257,6 +280,7 @@ __global__ void k_phase_tn(float2* __restrict__ s, uint64_t nitems, int t, float
 }
 
 __global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G2 D0, const float2* __restrict__ gd) {
+  pdl_begin();
   const G2 D = gate2(D0, gd);
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     uint64_t idx = 2 * i;
@@ -271,6 +295,7 @@ __global__ void k_diag2(float2* __restrict__ s, uint64_t nvec, int q0, int q1, G
 // ------------------------------------------------- multi-controlled -------
 __global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t, G2 G0,
                        const float2* __restrict__ gd) {
+  pdl_begin();
   const G2 G = gate2(G0, gd);
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
@@ -284,6 +309,7 @@ __global__ void k_mc1q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64
 
 __global__ void k_mc2q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int lo, int hi, G4 G0,
                        const float2* __restrict__ gd) {
+  pdl_begin();
   const G4 G = gate4(G0, gd, 0);
   const uint64_t sl = 1ull << lo, sh = 1ull << hi;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
@@ -296,12 +322,14 @@ __global__ void k_mc2q(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64
 
 // ---------------------------------------------------------- exact ---------
 __global__ void k_x_t0(float2* __restrict__ s, uint64_t npairs) {
+  pdl_begin();
   for (uint64_t p = gtid(); p < npairs; p += gstride()) {
     float4 v = ld4(s + 2 * p);
     st4(s + 2 * p, hi2(v), lo2(v));
   }
 }
 __global__ void k_x_tn(float2* __restrict__ s, uint64_t nitems, int t) {
+  pdl_begin();
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i0 = insert_zero(2 * it, t);
@@ -311,6 +339,7 @@ __global__ void k_x_tn(float2* __restrict__ s, uint64_t nitems, int t) {
   }
 }
 __global__ void k_mcx(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t) {
+  pdl_begin();
   const uint64_t st = 1ull << t;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i0 = insert_zeros(it, P.pos, P.k) | cmask;
@@ -320,6 +349,7 @@ __global__ void k_mcx(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_
   }
 }
 __global__ void k_mcswap(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t cmask, int t0, int t1) {
+  pdl_begin();
   const uint64_t s0 = 1ull << t0, s1 = 1ull << t1;
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i = insert_zeros(it, P.pos, P.k) | cmask;
@@ -329,6 +359,7 @@ __global__ void k_mcswap(float2* __restrict__ s, uint64_t nitems, Sorted P, uint
   }
 }
 __global__ void k_mcz(float2* __restrict__ s, uint64_t nitems, Sorted P, uint64_t mask) {
+  pdl_begin();
   for (uint64_t it = gtid(); it < nitems; it += gstride()) {
     uint64_t i = insert_zeros(it, P.pos, P.k) | mask;
     float2 a = s[i];
@@ -379,11 +410,35 @@ void check_controls(const int* controls, int nc, int n) {
   for (int i = 0; i < nc; ++i) qs_check_qubit(controls[i], n, "control");
 }
 
+// QSIM_PDL=0 launches the per-gate kernels without the attribute.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_PDL");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+void launch_gate(qs_context* h, void (*kern)(KArgs...), unsigned grid, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  QS_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
 #define LAUNCH(h, kern, items, ...)                                              \
   do {                                                                          \
     uint64_t _items = (items);                                                  \
     if (_items) {                                                               \
-      kern<<<qs_blocks_for(h, _items, kThreads), kThreads, 0, h->stream>>>(__VA_ARGS__); \
+      launch_gate(h, kern, (unsigned)qs_blocks_for(h, _items, kThreads), __VA_ARGS__); \
       qs_after_launch(h, #kern);                                                \
     }                                                                           \
   } while (0)
