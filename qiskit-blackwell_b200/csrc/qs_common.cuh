@@ -13,6 +13,16 @@
 
 namespace qs {
 
+// Programmatic dependent launch (kernels launched with qs_launch_pdl): wait
+// for the grid before this one in the stream (griddepcontrol.wait: it has
+// finished and its writes are visible; a no-op for a kernel launched without
+// the attribute), then let the next grid begin its launch, whose CTAs wait in
+// turn before they touch memory.  Called first thing by such a kernel.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------------ indices -----
 // Insert a zero bit at position q: bits >= q move up by one.
 __device__ __forceinline__ uint64_t insert_zero(uint64_t x, int q) {

@@ -21,17 +21,8 @@ struct Sorted { int pos[12]; int k; };
 
 constexpr int kThreads = 256;
 
-// Programmatic dependent launch: the per-gate kernels are launched with the
-// programmatic stream-serialisation attribute, so that the next gate's
-// launch overlaps the end of this one.  Each kernel here first waits for the
-// grid before it in the stream (griddepcontrol.wait: that grid has finished
-// and its writes are visible; a no-op when the kernel was launched without
-// the attribute) and then lets the next grid begin its launch, whose CTAs
-// wait in turn before they touch the state.
-__device__ __forceinline__ void pdl_begin() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// Every kernel here is launched with programmatic dependent launch
+// (qs_launch_pdl) and begins with pdl_begin().
 
 // ------------------------------------------------------------ init --------
 __global__ void k_state_init(float4* __restrict__ s4, uint64_t nvec, uint64_t index) {
@@ -410,35 +401,11 @@ void check_controls(const int* controls, int nc, int n) {
   for (int i = 0; i < nc; ++i) qs_check_qubit(controls[i], n, "control");
 }
 
-// QSIM_PDL=0 launches the per-gate kernels without the attribute.
-bool pdl_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("QSIM_PDL");
-    return !(e && std::atoi(e) == 0);
-  }();
-  return on;
-}
-
-template <typename... KArgs, typename... Args>
-void launch_gate(qs_context* h, void (*kern)(KArgs...), unsigned grid, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = h->stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
-  QS_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
-}
-
 #define LAUNCH(h, kern, items, ...)                                              \
   do {                                                                          \
     uint64_t _items = (items);                                                  \
     if (_items) {                                                               \
-      launch_gate(h, kern, (unsigned)qs_blocks_for(h, _items, kThreads), __VA_ARGS__); \
+      qs_launch_pdl(h, kern, dim3((unsigned)qs_blocks_for(h, _items, kThreads)), dim3(kThreads), 0, __VA_ARGS__); \
       qs_after_launch(h, #kern);                                                \
     }                                                                           \
   } while (0)

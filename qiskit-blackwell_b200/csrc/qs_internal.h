@@ -11,6 +11,7 @@
 #include <vector>
 #include <complex>
 #include <stdexcept>
+#include <cstdlib>
 #include "../../include/qsim.h"
 
 // ---------------------------------------------------------------- errors --
@@ -92,6 +93,19 @@ cudaStream_t qs_upload_stream(qs_context* h);
 
 // Records a launch and checks the launch status.
 void qs_after_launch(qs_context* h, const char* what);
+
+// Launch on the handle's stream with the programmatic stream-serialisation
+// attribute (the kernel must begin with qs::pdl_begin()), so that its launch
+// overlaps the end of the kernel before it; QSIM_PDL=0 launches without it.
+inline bool qs_pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("QSIM_PDL");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+template <typename... KArgs, typename... Args>
+void qs_launch_pdl(qs_context* h, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args);
 // Adjusts the launch counters (kernels replayed from, or captured into, a graph).
 void qs_count_launches(qs_context* h, int64_t delta);
 // Raises the release threshold of the device's default memory pool to at
@@ -351,4 +365,19 @@ inline int qs_blocks_for(qs_context* h, uint64_t items, int threads, int per_sm 
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (int)b;
+}
+
+template <typename... KArgs, typename... Args>
+void qs_launch_pdl(qs_context* h, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = qs_pdl_enabled() ? 1 : 0;
+  QS_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
 }

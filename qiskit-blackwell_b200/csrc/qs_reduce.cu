@@ -88,6 +88,7 @@ struct FZ {  // sum |a_i|^2 (-1)^popc(i & z)
 
 template <class F>
 __global__ void k_reduce(F f, uint64_t items, uint64_t per, double* __restrict__ partial) {
+  pdl_begin();
   const uint64_t b0 = (uint64_t)blockIdx.x * per;
   const uint64_t e = min(b0 + per, items);
   double acc = 0.0;
@@ -98,6 +99,7 @@ __global__ void k_reduce(F f, uint64_t items, uint64_t per, double* __restrict__
 
 // mode 0: out[0] = sum.  mode 1: out[0] = sum, out[1] = 1/sqrt(sum) (renorm).
 __global__ void k_final(const double* __restrict__ partial, int nb, double* __restrict__ out, int mode) {
+  pdl_begin();
   double acc = 0.0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += partial[i];
   acc = block_sum(acc);
@@ -108,6 +110,7 @@ __global__ void k_final(const double* __restrict__ partial, int nb, double* __re
 }
 
 __global__ void k_scale(float4* __restrict__ s, uint64_t nvec, const double* __restrict__ scale) {
+  pdl_begin();
   const float f = (float)scale[1];
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     float4 v = s[i];
@@ -116,6 +119,7 @@ __global__ void k_scale(float4* __restrict__ s, uint64_t nvec, const double* __r
 }
 
 __global__ void k_probs(const float4* __restrict__ s, float2* __restrict__ p, uint64_t nvec) {
+  pdl_begin();
   for (uint64_t i = gtid(); i < nvec; i += gstride()) {
     float4 v = s[i];
     p[i] = make_float2(v.x * v.x + v.y * v.y, v.z * v.z + v.w * v.w);
@@ -126,6 +130,7 @@ __global__ void k_probs(const float4* __restrict__ s, float2* __restrict__ p, ui
 // scaled by 1/sqrt(p_outcome); zero the others.  pr[0] = P(bit = 0).
 __global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double u, const double* __restrict__ pr,
                            int* __restrict__ outcome) {
+  pdl_begin();
   const double p0 = pr[0];
   const int res = (u < p0) ? 0 : 1;
   const double p = res == 0 ? p0 : 1.0 - p0;
@@ -171,6 +176,7 @@ __device__ __forceinline__ double warp_iscan(double v) {
 
 // pass 1: one warp per chunk -> csum[c]
 __global__ void k_chunk_sums(const float2* __restrict__ s, uint64_t n, uint64_t nchunks, double* __restrict__ csum) {
+  pdl_begin();
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -215,6 +221,7 @@ __device__ __forceinline__ void chunk_scan_block(const double* __restrict__ csum
 }
 
 __global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
+  pdl_begin();
   __shared__ double ws[32];
   __shared__ double carry;
   chunk_scan_block(csum, nchunks, cbase, ws, carry);
@@ -260,6 +267,7 @@ __device__ __forceinline__ int64_t sample_one(const float2* __restrict__ s, uint
 
 __global__ void k_sample(const float2* __restrict__ s, uint64_t n, uint64_t nchunks, const double* __restrict__ cbase,
                          const double* __restrict__ u, int64_t nshots, int64_t* __restrict__ out) {
+  pdl_begin();
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -296,6 +304,7 @@ __device__ __forceinline__ int find_desc(const SampleDesc* __restrict__ d, int n
 
 __global__ void k_chunk_sums_b(const float2* __restrict__ base, const SampleDesc* __restrict__ d, int ns,
                                uint64_t total_chunks, double* __restrict__ csum) {
+  pdl_begin();
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -312,6 +321,7 @@ __global__ void k_chunk_sums_b(const float2* __restrict__ base, const SampleDesc
 // one 1024-thread block per state; cbase of state t starts at chunk_off + t
 __global__ void k_chunk_scan_b(const double* __restrict__ csum, const SampleDesc* __restrict__ d,
                                double* __restrict__ cbase) {
+  pdl_begin();
   __shared__ double ws[32];
   __shared__ double carry;
   const SampleDesc D = d[blockIdx.x];
@@ -321,6 +331,7 @@ __global__ void k_chunk_scan_b(const double* __restrict__ csum, const SampleDesc
 
 __global__ void k_sample_b(const float2* __restrict__ base, const SampleDesc* __restrict__ d, int ns,
                            uint64_t total_shots, const double* __restrict__ cbase, int64_t* __restrict__ out) {
+  pdl_begin();
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -350,6 +361,7 @@ __device__ __forceinline__ void term_apply(const Term& T, uint64_t i, const floa
 // <psi|H|psi> partials: sum_i Re(conj(psi_i) (H psi)_i)
 __global__ void k_pauli_expect(const float2* __restrict__ s, uint64_t n, const Term* __restrict__ terms, int nterms,
                                uint64_t per, double* __restrict__ partial) {
+  pdl_begin();
   extern __shared__ Term st[];
   for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
   __syncthreads();
@@ -369,6 +381,7 @@ __global__ void k_pauli_expect(const float2* __restrict__ s, uint64_t n, const T
 // out = H psi (complex64), accumulated in FP64 per amplitude.
 __global__ void k_pauli_apply(const float2* __restrict__ s, float2* __restrict__ out, uint64_t n,
                               const Term* __restrict__ terms, int nterms) {
+  pdl_begin();
   extern __shared__ Term st[];
   for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
   __syncthreads();
@@ -412,9 +425,9 @@ namespace {
 template <class F>
 void reduce_to(qs_context* h, F f, uint64_t items, double* d_out, int mode, double* d_partial) {
   Slicing sl = slice(items);
-  k_reduce<F><<<sl.nb, kThreads, 0, h->stream>>>(f, items, sl.per, d_partial);
+  qs_launch_pdl(h, k_reduce<F>, dim3(sl.nb), dim3(kThreads), 0, f, items, sl.per, d_partial);
   qs_after_launch(h, "k_reduce");
-  k_final<<<1, 1024, 0, h->stream>>>(d_partial, sl.nb, d_out, mode);
+  qs_launch_pdl(h, k_final, dim3(1), dim3(1024), 0, d_partial, sl.nb, d_out, mode);
   qs_after_launch(h, "k_final");
 }
 
@@ -451,7 +464,7 @@ int qs_renorm(qs_handle_t h, void* state, int n) {
   double* o = red_out(h);
   const uint64_t nvec = (1ull << n) / 2;
   reduce_to(h, FNorm{(const float4*)state}, nvec, o, 1, red_part(h));
-  k_scale<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((float4*)state, nvec, o);
+  qs_launch_pdl(h, k_scale, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (float4*)state, nvec, o);
   qs_after_launch(h, "k_scale");
   QS_API_END(h)
 }
@@ -462,7 +475,7 @@ int qs_probs(qs_handle_t h, const void* state, int n, float* probs) {
   qs_check_state(state, n);
   QS_CHECK_ARG(probs != nullptr && ((uintptr_t)probs & 7u) == 0, "probs must be a non-null 8-byte aligned pointer");
   const uint64_t nvec = (1ull << n) / 2;
-  k_probs<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((const float4*)state, (float2*)probs, nvec);
+  qs_launch_pdl(h, k_probs, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (const float4*)state, (float2*)probs, nvec);
   qs_after_launch(h, "k_probs");
   QS_API_END(h)
 }
@@ -475,7 +488,7 @@ int qs_probs_n(qs_handle_t h, const void* states, int64_t n_amps, float* probs) 
   QS_CHECK_ARG(n_amps >= 0 && (n_amps & 1) == 0, "n_amps must be even and >= 0");
   const uint64_t nvec = (uint64_t)n_amps / 2;
   if (nvec) {
-    k_probs<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((const float4*)states, (float2*)probs, nvec);
+    qs_launch_pdl(h, k_probs, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (const float4*)states, (float2*)probs, nvec);
     qs_after_launch(h, "k_probs");
   }
   QS_API_END(h)
@@ -491,7 +504,7 @@ int qs_measure(qs_handle_t h, void* state, int n, int t, double u, int* outcome)
   const uint64_t nvec = (1ull << n) / 2;
   reduce_to(h, FP0{(const float4*)state, t}, nvec, o, 0, red_part(h));
   int* d_out = (int*)(o + 2);
-  k_collapse<<<qs_blocks_for(h, nvec, kThreads), kThreads, 0, h->stream>>>((float4*)state, nvec, t, u, o, d_out);
+  qs_launch_pdl(h, k_collapse, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (float4*)state, nvec, t, u, o, d_out);
   qs_after_launch(h, "k_collapse");
   double* pin = h->pinned_get(64);
   QS_CUDA(cudaMemcpyAsync(pin, d_out, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -524,10 +537,10 @@ int qs_expect_pauli_sum(qs_handle_t h, const void* state, int n, const uint64_t*
   double* part = red_part(h);
   const uint64_t N = 1ull << n;
   Slicing sl = slice(N);
-  k_pauli_expect<<<sl.nb, kThreads, sizeof(Term) * nterms, h->stream>>>((const float2*)state, N, dT, nterms, sl.per,
+  qs_launch_pdl(h, k_pauli_expect, dim3(sl.nb), dim3(kThreads), sizeof(Term) * nterms, (const float2*)state, N, dT, nterms, sl.per,
                                                                         part);
   qs_after_launch(h, "k_pauli_expect");
-  k_final<<<1, 1024, 0, h->stream>>>(part, sl.nb, o, 0);
+  qs_launch_pdl(h, k_final, dim3(1), dim3(1024), 0, part, sl.nb, o, 0);
   qs_after_launch(h, "k_final");
   *out = fetch_scalar(h, o);
   QS_API_END(h)
@@ -543,7 +556,7 @@ int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n, const u
   QS_CHECK_ARG(nterms >= 1 && nterms <= 1024, "n_terms must be in [1, 1024]");
   Term* dT = (Term*)qs_upload_terms(h, 0, n, x, z, c, nterms);
   const uint64_t N = 1ull << n;
-  k_pauli_apply<<<qs_blocks_for(h, N, kThreads), kThreads, sizeof(Term) * nterms, h->stream>>>(
+  qs_launch_pdl(h, k_pauli_apply, dim3(qs_blocks_for(h, N, kThreads)), dim3(kThreads), sizeof(Term) * nterms, 
       (const float2*)psi, (float2*)out, N, dT, nterms);
   qs_after_launch(h, "k_pauli_apply");
   QS_API_END(h)
@@ -584,13 +597,13 @@ int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int
   double* cbase = csum + chunks;
   QS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(SampleDesc), cudaMemcpyHostToDevice, h->stream));
   const int wpb = kThreads / 32;
-  k_chunk_sums_b<<<qs_blocks_for(h, chunks * 32, kThreads), kThreads, 0, h->stream>>>(
+  qs_launch_pdl(h, k_chunk_sums_b, dim3(qs_blocks_for(h, chunks * 32, kThreads)), dim3(kThreads), 0, 
       (const float2*)states, d_desc, n_states, chunks, csum);
   qs_after_launch(h, "k_chunk_sums_b");
-  k_chunk_scan_b<<<(unsigned)n_states, 1024, 0, h->stream>>>(csum, d_desc, cbase);
+  qs_launch_pdl(h, k_chunk_scan_b, dim3((unsigned)n_states), dim3(1024), 0, csum, d_desc, cbase);
   qs_after_launch(h, "k_chunk_scan_b");
   const uint64_t blocks = std::min<uint64_t>((nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
-  k_sample_b<<<(unsigned)blocks, kThreads, 0, h->stream>>>((const float2*)states, d_desc, n_states, nshots, cbase,
+  qs_launch_pdl(h, k_sample_b, dim3((unsigned)blocks), dim3(kThreads), 0, (const float2*)states, d_desc, n_states, nshots, cbase,
                                                            out);
   qs_after_launch(h, "k_sample_b");
   QS_API_END(h)
@@ -609,13 +622,13 @@ int qs_sample(qs_handle_t h, const void* state, int n, const double* u, int64_t 
   double* csum = base;
   double* cbase = base + nchunks;
   const int wpb = kThreads / 32;
-  k_chunk_sums<<<qs_blocks_for(h, nchunks * 32, kThreads), kThreads, 0, h->stream>>>((const float2*)state, N,
+  qs_launch_pdl(h, k_chunk_sums, dim3(qs_blocks_for(h, nchunks * 32, kThreads)), dim3(kThreads), 0, (const float2*)state, N,
                                                                                      nchunks, csum);
   qs_after_launch(h, "k_chunk_sums");
-  k_chunk_scan<<<1, 1024, 0, h->stream>>>(csum, nchunks, cbase);
+  qs_launch_pdl(h, k_chunk_scan, dim3(1), dim3(1024), 0, csum, nchunks, cbase);
   qs_after_launch(h, "k_chunk_scan");
   const uint64_t blocks = std::min<uint64_t>(((uint64_t)nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
-  k_sample<<<(unsigned)blocks, kThreads, 0, h->stream>>>((const float2*)state, N, nchunks, cbase, u, nshots, out);
+  qs_launch_pdl(h, k_sample, dim3((unsigned)blocks), dim3(kThreads), 0, (const float2*)state, N, nchunks, cbase, u, nshots, out);
   qs_after_launch(h, "k_sample");
   QS_API_END(h)
 }
