@@ -10,7 +10,12 @@
 // work items to worker threads.  Every worker owns a libqsim handle on its
 // own CUDA stream, so batches, gradients and evolutions run concurrently on
 // the device; budget is returned when an item completes, which admits more
-// requests.  Results are identical alone and in a mix: batch plans give the
+// requests.  Worker 0 takes the admitted item of most estimated device work
+// (amplitudes x gates for circuits, x passes over the observable for
+// gradients, x degree x terms for evolutions), the others the item of least,
+// so the large items, which fill the GPU one at a time, run back to back
+// while the short ones flow around them instead of queueing behind them.
+// Results are identical alone and in a mix: batch plans give the
 // same bits as single plans, reductions have a fixed order, and each
 // circuit's sampling uniforms come from its own seed.
 //
@@ -21,6 +26,7 @@
 #include "qs_api.h"
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -102,7 +108,11 @@ struct qs_server_s {
   std::mutex mu;
   std::condition_variable cv_sched, cv_work, cv_done;
   std::deque<ReqP> queue;                   // waiting for admission
-  std::deque<std::vector<ReqP>> work;       // admitted items
+  struct Item {
+    std::vector<ReqP> reqs;
+    double cost = 0;  // estimated device work
+  };
+  std::deque<Item> work;                    // admitted items, in admission order
   std::map<int64_t, ReqP> reqs;
   int64_t next_id = 1;
   bool stop = false;
@@ -127,6 +137,29 @@ struct qs_server_s {
       ++failed;
     }
     cv_done.notify_all();
+  }
+
+  // Estimated device work of a request (amplitude updates, arbitrary unit).
+  static double cost_of(const Request& r) {
+    const double amps = std::ldexp(1.0, r.n);
+    if (r.kind == K_CIRCUIT) return amps * (double)(r.ops.size() + 1);
+    if (r.kind == K_GRADIENT) return amps * (double)std::max(1, r.n_batch) * (3.0 * r.ops.size() + r.pc.size());
+    return amps * (double)std::max(1, r.K) * (0.5 * r.px.size() + 2.0);
+  }
+  void push_item(std::vector<ReqP>&& reqs) {
+    Item it;
+    for (const ReqP& r : reqs) it.cost += cost_of(*r);
+    it.reqs = std::move(reqs);
+    work.push_back(std::move(it));
+  }
+  // Worker 0: the largest item; the others: the smallest (ties: the oldest).
+  std::vector<ReqP> take_item(int worker) {
+    auto pick = work.begin();
+    for (auto it = work.begin(); it != work.end(); ++it)
+      if (worker == 0 ? it->cost > pick->cost : it->cost < pick->cost) pick = it;
+    std::vector<ReqP> out = std::move(pick->reqs);
+    work.erase(pick);
+    return out;
   }
 
   void schedule_loop() {
@@ -157,29 +190,29 @@ struct qs_server_s {
           // large fills the GPU by itself and goes alone
           const int64_t amps = int64_t(1) << r->n;
           if (amps >= kBatchAmps) {
-            work.push_back({r});
+            push_item({r});
             continue;
           }
           if (batch_amps + amps > kBatchAmps || (int)circuits.size() == max_batch) {
-            work.push_back(std::move(circuits));
+            push_item(std::move(circuits));
             circuits.clear();
             batch_amps = 0;
           }
           circuits.push_back(r);
           batch_amps += amps;
         } else {
-          work.push_back({r});
+          push_item({r});
         }
       }
       queue.swap(keep);
-      if (!circuits.empty()) work.push_back(std::move(circuits));
+      if (!circuits.empty()) push_item(std::move(circuits));
       cv_work.notify_all();
       // with nothing admissible, wait for a completion (or a new request)
       if (!queue.empty()) cv_sched.wait_for(lk, std::chrono::milliseconds(2));
     }
   }
 
-  void worker_loop() {
+  void worker_loop(int worker) {
     qs_handle_t h = nullptr;
     // This thread's own CUDA calls (buffers, copies) go to the server's device.
     int rc = cudaSetDevice(device) == cudaSuccess ? QS_OK : QS_ERR_CUDA;
@@ -190,8 +223,7 @@ struct qs_server_s {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return stop || !work.empty(); });
         if (work.empty()) break;  // stop requested and nothing left
-        item = std::move(work.front());
-        work.pop_front();
+        item = take_item(worker);
       }
       int status = QS_OK;
       std::string err;
@@ -339,7 +371,7 @@ int qs_server_create(int device, int64_t budget_bytes, int n_workers, qs_server_
   s->device = device;
   s->budget = s->free_bytes = budget_bytes;
   s->scheduler = std::thread([s] { s->schedule_loop(); });
-  for (int w = 0; w < n_workers; ++w) s->workers.emplace_back([s] { s->worker_loop(); });
+  for (int w = 0; w < n_workers; ++w) s->workers.emplace_back([s, w] { s->worker_loop(w); });
   *out = s;
   return QS_OK;
 }
