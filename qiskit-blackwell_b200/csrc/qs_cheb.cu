@@ -84,6 +84,7 @@ template <int V>
 __global__ void k_spmv(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const float2* __restrict__ val,
                        int64_t nrows, const float2* __restrict__ x, float2* __restrict__ y, float2 alpha,
                        float2 beta) {
+  pdl_begin();
   ROW_LOOP(V, {
     const float2 d = row_dot<V>(rp, ci, val, x, live ? r : -1, lane);
     if (live && lane == 0) {
@@ -101,6 +102,7 @@ template <int V>
 __global__ void k_cheb_fused(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                              const float2* __restrict__ val, int64_t nrows, const float2* __restrict__ xk,
                              float2* __restrict__ xprev, float2* __restrict__ out, float two_scale, float2 c) {
+  pdl_begin();
   ROW_LOOP(V, {
     const float2 d = row_dot<V>(rp, ci, val, xk, live ? r : -1, lane);
     if (live && lane == 0) {
@@ -120,6 +122,7 @@ template <int V>
 __global__ void k_cheb_first(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                              const float2* __restrict__ val, int64_t nrows, const float2* __restrict__ x0,
                              float2* __restrict__ x1, float2* __restrict__ out, float scale, float2 c0, float2 c1) {
+  pdl_begin();
   ROW_LOOP(V, {
     const float2 d = row_dot<V>(rp, ci, val, x0, live ? r : -1, lane);
     if (live && lane == 0) {
@@ -138,12 +141,14 @@ __global__ void k_cheb_first(const int32_t* __restrict__ rp, const int32_t* __re
 
 // ---- reference mirrors (chebyshev_sm120.cu:24-91): float4 elementwise ----
 __global__ void k_step(const float4* __restrict__ s, const float4* __restrict__ p, float4* __restrict__ nx, uint64_t nv) {
+  pdl_begin();
   for (uint64_t i = gtid(); i < nv; i += gstride()) {
     float4 a = s[i], b = p[i];
     nx[i] = make_float4(2.f * a.x - b.x, 2.f * a.y - b.y, 2.f * a.z - b.z, 2.f * a.w - b.w);
   }
 }
 __global__ void k_accum(float4* __restrict__ acc, const float4* __restrict__ t, float2 c, uint64_t nv) {
+  pdl_begin();
   for (uint64_t i = gtid(); i < nv; i += gstride()) {
     float4 a = acc[i], x = t[i];
     a.x += c.x * x.x - c.y * x.y;
@@ -155,6 +160,7 @@ __global__ void k_accum(float4* __restrict__ acc, const float4* __restrict__ t, 
 }
 __global__ void k_step_accum(const float4* __restrict__ s, const float4* __restrict__ p, float4* __restrict__ nx,
                              float4* __restrict__ acc, float2 c, uint64_t nv) {
+  pdl_begin();
   for (uint64_t i = gtid(); i < nv; i += gstride()) {
     float4 a = s[i], b = p[i], r = acc[i];
     float4 t = make_float4(2.f * a.x - b.x, 2.f * a.y - b.y, 2.f * a.z - b.z, 2.f * a.w - b.w);
@@ -190,6 +196,7 @@ __device__ __forceinline__ float2 hx_row(const PTerm* __restrict__ st, int nterm
 
 __global__ void k_chebp_first(const PTerm* __restrict__ terms, int nterms, uint64_t n, const float2* __restrict__ x0,
                               float2* __restrict__ x1, float2* __restrict__ out, float scale, float2 c0, float2 c1) {
+  pdl_begin();
   extern __shared__ PTerm st[];
   for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
   __syncthreads();
@@ -209,6 +216,7 @@ __global__ void k_chebp_first(const PTerm* __restrict__ terms, int nterms, uint6
 
 __global__ void k_chebp_fused(const PTerm* __restrict__ terms, int nterms, uint64_t n, const float2* __restrict__ xk,
                               float2* __restrict__ xprev, float2* __restrict__ out, float two_scale, float2 c) {
+  pdl_begin();
   extern __shared__ PTerm st[];
   for (int k = threadIdx.x; k < nterms; k += blockDim.x) st[k] = terms[k];
   __syncthreads();
@@ -237,6 +245,7 @@ struct __align__(16) PPair { uint32_t x, z0, z1, pad; float w0r, w0i, w1r, w1i; 
 struct __align__(16) PDiag { uint64_t z; double c; };
 
 __global__ void k_chebp_diag(const PDiag* __restrict__ terms, int nterms, uint64_t n, float* __restrict__ D) {
+  pdl_begin();
   extern __shared__ PDiag sd[];
   for (int k = threadIdx.x; k < nterms; k += blockDim.x) sd[k] = terms[k];
   __syncthreads();
@@ -275,6 +284,7 @@ __global__ void k_chebp_first_pairs(const PPair* __restrict__ pairs, int npairs,
                                     const float* __restrict__ D, const float2* __restrict__ x0,
                                     float2* __restrict__ x1, float2* __restrict__ out, float scale, float2 c0,
                                     float2 c1) {
+  pdl_begin();
   extern __shared__ PPair sp[];
   for (int k = threadIdx.x; k < npairs; k += blockDim.x) sp[k] = pairs[k];
   __syncthreads();
@@ -296,6 +306,7 @@ __global__ void k_chebp_fused_pairs(const PPair* __restrict__ pairs, int npairs,
                                     const float* __restrict__ D, const float2* __restrict__ xk,
                                     float2* __restrict__ xprev, float2* __restrict__ out, float two_scale,
                                     float2 c) {
+  pdl_begin();
   extern __shared__ PPair sp[];
   for (int k = threadIdx.x; k < npairs; k += blockDim.x) sp[k] = pairs[k];
   __syncthreads();
@@ -326,10 +337,10 @@ int pick_V(int64_t nrows, const int32_t* rp_dev, qs_context* h) {
 
 #define DISPATCH_V(V, KERN, GRID, ...)                                            \
   switch (V) {                                                                   \
-    case 4: KERN<4><<<GRID, kThreads, 0, h->stream>>>(__VA_ARGS__); break;       \
-    case 8: KERN<8><<<GRID, kThreads, 0, h->stream>>>(__VA_ARGS__); break;       \
-    case 16: KERN<16><<<GRID, kThreads, 0, h->stream>>>(__VA_ARGS__); break;     \
-    default: KERN<32><<<GRID, kThreads, 0, h->stream>>>(__VA_ARGS__); break;     \
+    case 4: qs_launch_pdl(h, KERN<4>, dim3(GRID), dim3(kThreads), 0, __VA_ARGS__); break;       \
+    case 8: qs_launch_pdl(h, KERN<8>, dim3(GRID), dim3(kThreads), 0, __VA_ARGS__); break;       \
+    case 16: qs_launch_pdl(h, KERN<16>, dim3(GRID), dim3(kThreads), 0, __VA_ARGS__); break;     \
+    default: qs_launch_pdl(h, KERN<32>, dim3(GRID), dim3(kThreads), 0, __VA_ARGS__); break;     \
   }
 
 inline void check_vec(const void* p, const char* what) {
@@ -363,7 +374,7 @@ int qs_cheb_step(qs_handle_t h, const void* s, const void* p, void* nx, int64_t 
   QS_CHECK_ARG(n >= 0 && (n & 1) == 0, "n must be even and >= 0");
   const uint64_t nv = (uint64_t)n / 2;
   if (nv) {
-    k_step<<<qs_blocks_for(h, nv, kThreads), kThreads, 0, h->stream>>>((const float4*)s, (const float4*)p, (float4*)nx, nv);
+    qs_launch_pdl(h, k_step, dim3(qs_blocks_for(h, nv, kThreads)), dim3(kThreads), 0, (const float4*)s, (const float4*)p, (float4*)nx, nv);
     qs_after_launch(h, "k_step");
   }
   QS_API_END(h)
@@ -376,7 +387,7 @@ int qs_cheb_accum(qs_handle_t h, void* acc, const void* t, double cr, double ci_
   QS_CHECK_ARG(n >= 0 && (n & 1) == 0, "n must be even and >= 0");
   const uint64_t nv = (uint64_t)n / 2;
   if (nv) {
-    k_accum<<<qs_blocks_for(h, nv, kThreads), kThreads, 0, h->stream>>>((float4*)acc, (const float4*)t,
+    qs_launch_pdl(h, k_accum, dim3(qs_blocks_for(h, nv, kThreads)), dim3(kThreads), 0, (float4*)acc, (const float4*)t,
                                                                         make_float2((float)cr, (float)ci_), nv);
     qs_after_launch(h, "k_accum");
   }
@@ -391,7 +402,7 @@ int qs_cheb_step_accum(qs_handle_t h, const void* s, const void* p, void* nx, vo
   QS_CHECK_ARG(n >= 0 && (n & 1) == 0, "n must be even and >= 0");
   const uint64_t nv = (uint64_t)n / 2;
   if (nv) {
-    k_step_accum<<<qs_blocks_for(h, nv, kThreads), kThreads, 0, h->stream>>>(
+    qs_launch_pdl(h, k_step_accum, dim3(qs_blocks_for(h, nv, kThreads)), dim3(kThreads), 0, 
         (const float4*)s, (const float4*)p, (float4*)nx, (float4*)acc, make_float2((float)cr, (float)ci_), nv);
     qs_after_launch(h, "k_step_accum");
   }
@@ -482,18 +493,18 @@ int qs_cheb_evolve_pauli(qs_handle_t h, int n, const void* psi, void* out, const
     float* D = nullptr;
     if (!dg.empty()) {
       QS_CUDA(cudaMallocAsync((void**)&D, sizeof(float) * N, h->stream));
-      k_chebp_diag<<<qs_blocks_for(h, N, kThreads), kThreads, dbytes, h->stream>>>(dD, (int)dg.size(), N, D);
+      qs_launch_pdl(h, k_chebp_diag, dim3(qs_blocks_for(h, N, kThreads)), dim3(kThreads), dbytes, dD, (int)dg.size(), N, D);
       qs_after_launch(h, "k_chebp_diag");
     }
     try {
       QS_CUDA(cudaMemcpyAsync(x0, psi, sizeof(float2) * N, cudaMemcpyDeviceToDevice, h->stream));
       const unsigned grid = (unsigned)qs_blocks_for(h, N, kThreads, 8);
       const int np = (int)pr.size();
-      k_chebp_first_pairs<<<grid, kThreads, pbytes, h->stream>>>(dP, np, N, D, x0, x1, (float2*)out,
+      qs_launch_pdl(h, k_chebp_first_pairs, dim3(grid), dim3(kThreads), pbytes, dP, np, N, D, x0, x1, (float2*)out,
                                                                  (float)scale, C(0), C(1));
       qs_after_launch(h, "k_chebp_first_pairs");
       for (int k = 2; k <= K; ++k) {
-        k_chebp_fused_pairs<<<grid, kThreads, pbytes, h->stream>>>(dP, np, N, D, x1, x0, (float2*)out,
+        qs_launch_pdl(h, k_chebp_fused_pairs, dim3(grid), dim3(kThreads), pbytes, dP, np, N, D, x1, x0, (float2*)out,
                                                                    two_scale, C(k));
         qs_after_launch(h, "k_chebp_fused_pairs");
         std::swap(x0, x1);
@@ -510,10 +521,10 @@ int qs_cheb_evolve_pauli(qs_handle_t h, int n, const void* psi, void* out, const
   QS_CUDA(cudaMemcpyAsync(x0, psi, sizeof(float2) * N, cudaMemcpyDeviceToDevice, h->stream));
   const unsigned grid = (unsigned)qs_blocks_for(h, N, kThreads, 8);
   const size_t smem = sizeof(PTerm) * nterms;
-  k_chebp_first<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x0, x1, (float2*)out, (float)scale, C(0), C(1));
+  qs_launch_pdl(h, k_chebp_first, dim3(grid), dim3(kThreads), smem, dT, nterms, N, x0, x1, (float2*)out, (float)scale, C(0), C(1));
   qs_after_launch(h, "k_chebp_first");
   for (int k = 2; k <= K; ++k) {
-    k_chebp_fused<<<grid, kThreads, smem, h->stream>>>(dT, nterms, N, x1, x0, (float2*)out, two_scale, C(k));
+    qs_launch_pdl(h, k_chebp_fused, dim3(grid), dim3(kThreads), smem, dT, nterms, N, x1, x0, (float2*)out, two_scale, C(k));
     qs_after_launch(h, "k_chebp_fused");
     std::swap(x0, x1);
   }
