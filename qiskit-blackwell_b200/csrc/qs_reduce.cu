@@ -154,11 +154,43 @@ __global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double 
 constexpr int kSeg = 64;
 constexpr int kChunk = 32 * kSeg;
 
+// |a|^2 in FP64, and a segment's running sum: the one expression and order
+// that every pass uses, so the chunk totals and the in-chunk search agree bit
+// for bit.
+__device__ __forceinline__ void seg_add(double& acc, float2 a) { acc += (double)a.x * a.x + (double)a.y * a.y; }
+
 __device__ __forceinline__ double seg_sum(const float2* __restrict__ s, uint64_t start, uint64_t n) {
   double acc = 0.0;
   for (int k = 0; k < kSeg; ++k) {
     uint64_t i = start + k;
-    if (i < n) { float2 a = s[i]; acc += (double)a.x * a.x + (double)a.y * a.y; }
+    if (i < n) seg_add(acc, s[i]);
+  }
+  return acc;
+}
+
+// seg_sum of lane `lane`'s segment of the chunk starting at `c0`, with the
+// chunk read in coalesced 128-byte runs: a segment is 512 contiguous bytes
+// per lane, so loading it lane by lane touches 32 lines per warp access.  The
+// warp stages 16 amplitudes of every segment at a time in `buf` (32 rows of
+// 17: the pad spreads a row walk over the banks) and each lane adds its row
+// in order, giving the same sum as seg_sum.
+__device__ __forceinline__ double seg_sum_staged(const float2* __restrict__ s, uint64_t c0, uint64_t n, int lane,
+                                                 float2 (*buf)[17]) {
+  double acc = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < kSeg / 16; ++q) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int r = 2 * i + (lane >> 4), e = lane & 15;
+      const uint64_t g = c0 + (uint64_t)r * kSeg + 16 * q + e;
+      buf[r][e] = g < n ? s[g] : make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+    const uint64_t start = c0 + (uint64_t)lane * kSeg + 16 * q;
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (start + k < n) seg_add(acc, buf[lane][k]);
+    __syncwarp();
   }
   return acc;
 }
@@ -180,8 +212,9 @@ __global__ void k_chunk_sums(const float2* __restrict__ s, uint64_t n, uint64_t 
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
+  __shared__ float2 stage[kThreads / 32][32][17];
   for (uint64_t c = warp; c < nchunks; c += nwarps) {
-    double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
+    double v = seg_sum_staged(s, c * kChunk, n, lane, stage[threadIdx.x >> 5]);
     v = warp_iscan(v);
     if (lane == 31) csum[c] = v;
   }
@@ -308,11 +341,12 @@ __global__ void k_chunk_sums_b(const float2* __restrict__ base, const SampleDesc
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
+  __shared__ float2 stage[kThreads / 32][32][17];
   for (uint64_t g = warp; g < total_chunks; g += nwarps) {
     const int t = find_desc<&SampleDesc::chunk_off>(d, ns, g);
     const SampleDesc D = d[t];
     const uint64_t c = g - D.chunk_off;
-    double v = seg_sum(base + D.state_off, c * kChunk + (uint64_t)lane * kSeg, D.n);
+    double v = seg_sum_staged(base + D.state_off, c * kChunk, D.n, lane, stage[threadIdx.x >> 5]);
     v = warp_iscan(v);
     if (lane == 31) csum[g] = v;
   }
