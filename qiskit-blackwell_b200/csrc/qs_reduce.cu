@@ -153,6 +153,9 @@ __global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double 
 // and the in-chunk search (pass 3), so both see identical values.
 constexpr int kSeg = 64;
 constexpr int kChunk = 32 * kSeg;
+// the chunk-sum kernels' CTAs that fit on an SM at once (34 KiB of staging
+// each): a grid of one wave, so no second wave runs on a third of the SMs
+constexpr int kChunkBlocksPerSm = 6;
 
 // |a|^2 in FP64, and a segment's running sum: the one expression and order
 // that every pass uses, so the chunk totals and the in-chunk search agree bit
@@ -631,7 +634,7 @@ int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int
   double* cbase = csum + chunks;
   QS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(SampleDesc), cudaMemcpyHostToDevice, h->stream));
   const int wpb = kThreads / 32;
-  qs_launch_pdl(h, k_chunk_sums_b, dim3(qs_blocks_for(h, chunks * 32, kThreads)), dim3(kThreads), 0, 
+  qs_launch_pdl(h, k_chunk_sums_b, dim3(qs_blocks_for(h, chunks * 32, kThreads, kChunkBlocksPerSm)), dim3(kThreads), 0, 
       (const float2*)states, d_desc, n_states, chunks, csum);
   qs_after_launch(h, "k_chunk_sums_b");
   qs_launch_pdl(h, k_chunk_scan_b, dim3((unsigned)n_states), dim3(1024), 0, csum, d_desc, cbase);
@@ -656,7 +659,7 @@ int qs_sample(qs_handle_t h, const void* state, int n, const double* u, int64_t 
   double* csum = base;
   double* cbase = base + nchunks;
   const int wpb = kThreads / 32;
-  qs_launch_pdl(h, k_chunk_sums, dim3(qs_blocks_for(h, nchunks * 32, kThreads)), dim3(kThreads), 0, (const float2*)state, N,
+  qs_launch_pdl(h, k_chunk_sums, dim3(qs_blocks_for(h, nchunks * 32, kThreads, kChunkBlocksPerSm)), dim3(kThreads), 0, (const float2*)state, N,
                                                                                      nchunks, csum);
   qs_after_launch(h, "k_chunk_sums");
   qs_launch_pdl(h, k_chunk_scan, dim3(1), dim3(1024), 0, csum, nchunks, cbase);
