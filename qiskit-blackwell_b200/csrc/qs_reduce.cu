@@ -177,18 +177,40 @@ __device__ __forceinline__ double seg_sum(const float2* __restrict__ s, uint64_t
 // warp stages 16 amplitudes of every segment at a time in `buf` (32 rows of
 // 17: the pad spreads a row walk over the banks) and each lane adds its row
 // in order, giving the same sum as seg_sum.
+__device__ __forceinline__ void seg_stage_load(const float2* __restrict__ s, uint64_t c0, uint64_t n, int lane, int q,
+                                               float4 (&r)[8]) {
+  // lanes 8k..8k+7 cover one 128-byte run (16 amplitudes of one segment),
+  // two amplitudes per lane.  16-byte loads when the state starts on a
+  // 16-byte boundary and has an even length (every state of one or more
+  // qubits): g is even, so the pair is then either inside it or past its end
+  const bool v4 = ((reinterpret_cast<uintptr_t>(s) & 15) == 0) && !(n & 1);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint64_t g = c0 + (uint64_t)(4 * i + (lane >> 3)) * kSeg + 16 * q + 2 * (lane & 7);
+    if (v4 && g < n) {
+      r[i] = *reinterpret_cast<const float4*>(s + g);
+    } else {
+      const float2 lo = g < n ? s[g] : make_float2(0.f, 0.f);
+      const float2 hi = g + 1 < n ? s[g + 1] : make_float2(0.f, 0.f);
+      r[i] = make_float4(lo.x, lo.y, hi.x, hi.y);
+    }
+  }
+}
 __device__ __forceinline__ double seg_sum_staged(const float2* __restrict__ s, uint64_t c0, uint64_t n, int lane,
                                                  float2 (*buf)[17]) {
   double acc = 0.0;
+  float4 r[8];
+  seg_stage_load(s, c0, n, lane, 0, r);
 #pragma unroll 1
   for (int q = 0; q < kSeg / 16; ++q) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int r = 2 * i + (lane >> 4), e = lane & 15;
-      const uint64_t g = c0 + (uint64_t)r * kSeg + 16 * q + e;
-      buf[r][e] = g < n ? s[g] : make_float2(0.f, 0.f);
+    for (int i = 0; i < 8; ++i) {
+      const int row = 4 * i + (lane >> 3), e = 2 * (lane & 7);
+      buf[row][e] = make_float2(r[i].x, r[i].y);
+      buf[row][e + 1] = make_float2(r[i].z, r[i].w);
     }
     __syncwarp();
+    if (q + 1 < kSeg / 16) seg_stage_load(s, c0, n, lane, q + 1, r);  // in flight while this row is summed
     const uint64_t start = c0 + (uint64_t)lane * kSeg + 16 * q;
 #pragma unroll
     for (int k = 0; k < 16; ++k)
