@@ -11,6 +11,8 @@
 #include "qs_common.cuh"
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 using namespace qs;
 
@@ -153,9 +155,6 @@ __global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double 
 // and the in-chunk search (pass 3), so both see identical values.
 constexpr int kSeg = 64;
 constexpr int kChunk = 32 * kSeg;
-// the chunk-sum kernels' CTAs that fit on an SM at once (34 KiB of staging
-// each): a grid of one wave, so no second wave runs on a third of the SMs
-constexpr int kChunkBlocksPerSm = 6;
 
 // |a|^2 in FP64, and a segment's running sum: the one expression and order
 // that every pass uses, so the chunk totals and the in-chunk search agree bit
@@ -248,14 +247,76 @@ __global__ void k_chunk_sums(const float2* __restrict__ s, uint64_t n, uint64_t 
 // pass 2: exclusive scan of the chunk sums, one block, fixed order.
 // cbase[c] = sum_{c' < c} csum[c'];  cbase[nchunks] = total.  The order
 // depends only on nchunks and the block size (1024 threads in every launch).
+// Each thread owns a contiguous run of `per` chunks; the block walks the runs
+// kScanCols columns at a time through a shared tile (one row per thread), so
+// csum is read and cbase written in coalesced 64-byte runs while every thread
+// still adds its own run in order.  The next columns are fetched into
+// registers while the current tile is summed.
+constexpr int kScanThreads = 1024;
+constexpr int kScanCols = 8;
+constexpr size_t kScanSmem = sizeof(double) * kScanThreads * (kScanCols + 1);
+using ScanTile = double (*)[kScanCols + 1];
+
+// element m of this thread's share of a tile is row tid / kScanCols +
+// m * (kScanThreads / kScanCols), column tid % kScanCols: chunk
+// c0 + k0 + m * cstride, with c0 = (tid / kScanCols) * per + tid % kScanCols.
+// A state of at most 34 qubits has at most 2^23 chunks: 32-bit indices.
+struct ScanCols {
+  uint32_t c0, cstride;
+  int col;
+};
+__device__ __forceinline__ ScanCols scan_cols(uint64_t per) {
+  const int col = threadIdx.x % kScanCols;
+  return {(uint32_t)((threadIdx.x / kScanCols) * per + col), (uint32_t)((kScanThreads / kScanCols) * per), col};
+}
+
+__device__ __forceinline__ void scan_tile_fetch(const double* __restrict__ csum, uint64_t nchunks, uint64_t per,
+                                                const ScanCols& sc, uint64_t k0, double (&r)[kScanCols]) {
+  const bool in_run = k0 + sc.col < per;
+#pragma unroll
+  for (int m = 0; m < kScanCols; ++m) {
+    const uint32_t c = sc.c0 + (uint32_t)k0 + m * sc.cstride;
+    r[m] = (in_run && c < nchunks) ? csum[c] : 0.0;
+  }
+}
+
+__device__ __forceinline__ void scan_tile_put(const double (&r)[kScanCols], ScanTile tile) {
+#pragma unroll
+  for (int m = 0; m < kScanCols; ++m) {
+    const int i = threadIdx.x + kScanThreads * m;
+    tile[i / kScanCols][i % kScanCols] = r[m];
+  }
+}
+
+__device__ __forceinline__ void scan_tile_store(double* __restrict__ cbase, uint64_t nchunks, uint64_t per,
+                                                const ScanCols& sc, uint64_t k0, ScanTile tile) {
+  const bool in_run = k0 + sc.col < per;
+#pragma unroll
+  for (int m = 0; m < kScanCols; ++m) {
+    const uint32_t c = sc.c0 + (uint32_t)k0 + m * sc.cstride;
+    const int i = threadIdx.x + kScanThreads * m;
+    if (in_run && c < nchunks) cbase[c] = tile[i / kScanCols][i % kScanCols];
+  }
+}
+
 __device__ __forceinline__ void chunk_scan_block(const double* __restrict__ csum, uint64_t nchunks,
-                                                 double* __restrict__ cbase, double* ws, double& carry) {
+                                                 double* __restrict__ cbase, double* ws, double& carry, ScanTile tile) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  // each thread owns a contiguous run of `per` chunks
-  const uint64_t per = (nchunks + blockDim.x - 1) / blockDim.x;
+  const uint64_t per = (nchunks + kScanThreads - 1) / kScanThreads;
   const uint64_t b = (uint64_t)tid * per, e = min(b + per, nchunks);
+  const ScanCols sc = scan_cols(per);
+  double r[kScanCols];
   double local = 0.0;
-  for (uint64_t c = b; c < e; ++c) local += csum[c];
+  scan_tile_fetch(csum, nchunks, per, sc, 0, r);
+  for (uint64_t k0 = 0; k0 < per; k0 += kScanCols) {
+    scan_tile_put(r, tile);
+    __syncthreads();
+    if (k0 + kScanCols < per) scan_tile_fetch(csum, nchunks, per, sc, k0 + kScanCols, r);
+#pragma unroll
+    for (int j = 0; j < kScanCols; ++j)
+      if (b + k0 + j < e) local += tile[tid][j];
+    __syncthreads();
+  }
   // block exclusive scan of `local`
   double inc = warp_iscan(local);
   double exc = __shfl_up_sync(0xffffffffu, inc, 1);
@@ -263,7 +324,7 @@ __device__ __forceinline__ void chunk_scan_block(const double* __restrict__ csum
   if (lane == 31) ws[w] = inc;
   __syncthreads();
   if (w == 0) {
-    const int nw = blockDim.x >> 5;
+    const int nw = kScanThreads >> 5;
     double x = lane < nw ? ws[lane] : 0.0;
     double xi = warp_iscan(x);
     double xe = __shfl_up_sync(0xffffffffu, xi, 1);
@@ -274,15 +335,33 @@ __device__ __forceinline__ void chunk_scan_block(const double* __restrict__ csum
   }
   __syncthreads();
   double run = ws[w] + exc;
-  for (uint64_t c = b; c < e; ++c) { cbase[c] = run; run += csum[c]; }
+  scan_tile_fetch(csum, nchunks, per, sc, 0, r);
+  for (uint64_t k0 = 0; k0 < per; k0 += kScanCols) {
+    scan_tile_put(r, tile);
+    __syncthreads();
+    if (k0 + kScanCols < per) scan_tile_fetch(csum, nchunks, per, sc, k0 + kScanCols, r);
+#pragma unroll
+    for (int j = 0; j < kScanCols; ++j) {
+      if (b + k0 + j < e) {
+        const double v = tile[tid][j];
+        tile[tid][j] = run;
+        run += v;
+      }
+    }
+    __syncthreads();
+    scan_tile_store(cbase, nchunks, per, sc, k0, tile);
+    __syncthreads();
+  }
   if (tid == 0) cbase[nchunks] = carry;
 }
 
-__global__ void k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
+__global__ void __launch_bounds__(kScanThreads, 1)
+    k_chunk_scan(const double* __restrict__ csum, uint64_t nchunks, double* __restrict__ cbase) {
   pdl_begin();
   __shared__ double ws[32];
   __shared__ double carry;
-  chunk_scan_block(csum, nchunks, cbase, ws, carry);
+  extern __shared__ double scan_smem[];
+  chunk_scan_block(csum, nchunks, cbase, ws, carry, reinterpret_cast<ScanTile>(scan_smem));
 }
 
 // pass 3, one shot by one warp: u -> smallest i with cdf[i] >= u, clamped to
@@ -378,14 +457,16 @@ __global__ void k_chunk_sums_b(const float2* __restrict__ base, const SampleDesc
 }
 
 // one 1024-thread block per state; cbase of state t starts at chunk_off + t
-__global__ void k_chunk_scan_b(const double* __restrict__ csum, const SampleDesc* __restrict__ d,
-                               double* __restrict__ cbase) {
+__global__ void __launch_bounds__(kScanThreads, 1)
+    k_chunk_scan_b(const double* __restrict__ csum, const SampleDesc* __restrict__ d, double* __restrict__ cbase) {
   pdl_begin();
   __shared__ double ws[32];
   __shared__ double carry;
+  extern __shared__ double scan_smem[];
   const SampleDesc D = d[blockIdx.x];
   if (D.shot_off == d[blockIdx.x + 1].shot_off) return;  // no shots: nothing to scan (block-uniform)
-  chunk_scan_block(csum + D.chunk_off, D.nchunks, cbase + D.chunk_off + blockIdx.x, ws, carry);
+  chunk_scan_block(csum + D.chunk_off, D.nchunks, cbase + D.chunk_off + blockIdx.x, ws, carry,
+                   reinterpret_cast<ScanTile>(scan_smem));
 }
 
 __global__ void k_sample_b(const float2* __restrict__ base, const SampleDesc* __restrict__ d, int ns,
@@ -621,6 +702,30 @@ int qs_apply_pauli_sum(qs_handle_t h, const void* psi, void* out, int n, const u
   QS_API_END(h)
 }
 
+
+// Per device, once: the scan kernels' shared-memory limit raised to their
+// tile, and the chunk-sum kernels' grids sized to one wave of the CTAs that
+// fit on an SM at once (registers and 34 KiB of staging each decide how many),
+// so that no second wave runs on part of the SMs while the rest idle.
+struct SampleLaunch {
+  int sums_per_sm, sums_b_per_sm;
+};
+static SampleLaunch sample_launch(qs_context* h) {
+  static std::mutex mu;
+  static std::map<int, SampleLaunch> by_device;
+  std::lock_guard<std::mutex> lk(mu);
+  auto f = by_device.find(h->device);
+  if (f != by_device.end()) return f->second;
+  QS_CUDA(cudaFuncSetAttribute(k_chunk_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
+  QS_CUDA(cudaFuncSetAttribute(k_chunk_scan_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
+  SampleLaunch L{0, 0};
+  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L.sums_per_sm, k_chunk_sums, kThreads, 0));
+  QS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L.sums_b_per_sm, k_chunk_sums_b, kThreads, 0));
+  if (L.sums_per_sm < 1 || L.sums_b_per_sm < 1) throw qs_error(QS_ERR_CUDA, "chunk-sum kernel does not fit on an SM");
+  by_device[h->device] = L;
+  return L;
+}
+
 int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int32_t* widths,
                       const int64_t* state_offsets, const int64_t* shots, const uint64_t* seeds, int64_t* out) {
   QS_REQUIRE_HANDLE(h);
@@ -656,10 +761,11 @@ int qs_sample_batched(qs_handle_t h, const void* states, int n_states, const int
   double* cbase = csum + chunks;
   QS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(SampleDesc), cudaMemcpyHostToDevice, h->stream));
   const int wpb = kThreads / 32;
-  qs_launch_pdl(h, k_chunk_sums_b, dim3(qs_blocks_for(h, chunks * 32, kThreads, kChunkBlocksPerSm)), dim3(kThreads), 0, 
+  const SampleLaunch L = sample_launch(h);
+  qs_launch_pdl(h, k_chunk_sums_b, dim3(qs_blocks_for(h, chunks * 32, kThreads, L.sums_b_per_sm)), dim3(kThreads), 0, 
       (const float2*)states, d_desc, n_states, chunks, csum);
   qs_after_launch(h, "k_chunk_sums_b");
-  qs_launch_pdl(h, k_chunk_scan_b, dim3((unsigned)n_states), dim3(1024), 0, csum, d_desc, cbase);
+  qs_launch_pdl(h, k_chunk_scan_b, dim3((unsigned)n_states), dim3(kScanThreads), kScanSmem, csum, d_desc, cbase);
   qs_after_launch(h, "k_chunk_scan_b");
   const uint64_t blocks = std::min<uint64_t>((nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
   qs_launch_pdl(h, k_sample_b, dim3((unsigned)blocks), dim3(kThreads), 0, (const float2*)states, d_desc, n_states, nshots, cbase,
@@ -681,10 +787,11 @@ int qs_sample(qs_handle_t h, const void* state, int n, const double* u, int64_t 
   double* csum = base;
   double* cbase = base + nchunks;
   const int wpb = kThreads / 32;
-  qs_launch_pdl(h, k_chunk_sums, dim3(qs_blocks_for(h, nchunks * 32, kThreads, kChunkBlocksPerSm)), dim3(kThreads), 0, (const float2*)state, N,
+  const SampleLaunch L = sample_launch(h);
+  qs_launch_pdl(h, k_chunk_sums, dim3(qs_blocks_for(h, nchunks * 32, kThreads, L.sums_per_sm)), dim3(kThreads), 0, (const float2*)state, N,
                                                                                      nchunks, csum);
   qs_after_launch(h, "k_chunk_sums");
-  qs_launch_pdl(h, k_chunk_scan, dim3(1), dim3(1024), 0, csum, nchunks, cbase);
+  qs_launch_pdl(h, k_chunk_scan, dim3(1), dim3(kScanThreads), kScanSmem, csum, nchunks, cbase);
   qs_after_launch(h, "k_chunk_scan");
   const uint64_t blocks = std::min<uint64_t>(((uint64_t)nshots + wpb - 1) / wpb, (uint64_t)h->sm_count * 16);
   qs_launch_pdl(h, k_sample, dim3((unsigned)blocks), dim3(kThreads), 0, (const float2*)state, N, nchunks, cbase, u, nshots, out);
