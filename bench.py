@@ -987,6 +987,30 @@ def bench_micro(args, dev):
         if name == "measure_qubit":
             us -= out["apply_gate"]["b200_us"]  # each call re-mixes qubit 4 with one H first
         out[name] = {"b200_us": us, "reference_rtx5090_us": REF_MICRO_US[name]}
+    # sampling from a state far past L2: 1024 shots from 30 qubits (8 GiB).
+    # One call reads the state once (chunk sums), scans the 2^19 chunk sums
+    # and searches one chunk per shot; its floor is the 8 N-byte read.
+    nw, shots_w = 30, 1024
+    wide = bk.state_init(nw)
+    for q in range(0, nw, 3):
+        bk.apply_gate(wide, H, q)
+    for _ in range(3):
+        bk.sample(wide, shots_w)
+    reps_w = 10
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(reps_w):
+        bk.sample(wide, shots_w)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    us = ev0.elapsed_time(ev1) * 1e3 / reps_w
+    peak, peak_kind = measured_peaks()
+    floor_us = (8 << nw) / (peak * 1e9) * 1e6
+    out["sample_1024_at_30_qubits"] = {"b200_us": us, "hbm_floor_us": floor_us, "frac": floor_us / us,
+                                       "peak": f"{peak} GB/s copy ({peak_kind})"}
+    del wide
+    torch.cuda.empty_cache()
     # QV-20 end to end
     qv = W.qv_ops(n, n, 20)
     qc = Circuit(n, n, name="qv20")

@@ -151,8 +151,9 @@ __global__ void k_collapse(float4* __restrict__ s, uint64_t nvec, int t, double 
 // The CDF is built in chunks of kChunk amplitudes.  A chunk is split into 32
 // contiguous segments of kSeg amplitudes, one per lane; a lane sums its
 // segment sequentially in FP64 and the warp scans the 32 segment sums in a
-// fixed shuffle order.  The same routine produces the chunk totals (pass 1)
-// and the in-chunk search (pass 3), so both see identical values.
+// fixed shuffle order.  The same routine (seg_sum_staged) produces the chunk
+// totals (pass 1) and the in-chunk search (pass 3), so both see identical
+// values.
 constexpr int kSeg = 64;
 constexpr int kChunk = 32 * kSeg;
 
@@ -161,21 +162,12 @@ constexpr int kChunk = 32 * kSeg;
 // for bit.
 __device__ __forceinline__ void seg_add(double& acc, float2 a) { acc += (double)a.x * a.x + (double)a.y * a.y; }
 
-__device__ __forceinline__ double seg_sum(const float2* __restrict__ s, uint64_t start, uint64_t n) {
-  double acc = 0.0;
-  for (int k = 0; k < kSeg; ++k) {
-    uint64_t i = start + k;
-    if (i < n) seg_add(acc, s[i]);
-  }
-  return acc;
-}
-
-// seg_sum of lane `lane`'s segment of the chunk starting at `c0`, with the
-// chunk read in coalesced 128-byte runs: a segment is 512 contiguous bytes
-// per lane, so loading it lane by lane touches 32 lines per warp access.  The
+// Lane `lane`'s segment sum of the chunk starting at `c0`: its amplitudes
+// c0 + lane * kSeg + k, k = 0..kSeg-1, added by seg_add in order.  The chunk
+// is read in coalesced 128-byte runs (a segment is 512 contiguous bytes per
+// lane, so loading it lane by lane would touch 32 lines per warp access): the
 // warp stages 16 amplitudes of every segment at a time in `buf` (32 rows of
-// 17: the pad spreads a row walk over the banks) and each lane adds its row
-// in order, giving the same sum as seg_sum.
+// 17: the pad spreads a row walk over the banks) and each lane adds its row.
 __device__ __forceinline__ void seg_stage_load(const float2* __restrict__ s, uint64_t c0, uint64_t n, int lane, int q,
                                                float4 (&r)[8]) {
   // lanes 8k..8k+7 cover one 128-byte run (16 amplitudes of one segment),
@@ -367,17 +359,29 @@ __global__ void __launch_bounds__(kScanThreads, 1)
 // pass 3, one shot by one warp: u -> smallest i with cdf[i] >= u, clamped to
 // n-1 (reference semantics: sample_sm120.cu:61-68).  Every lane returns it.
 __device__ __forceinline__ int64_t sample_one(const float2* __restrict__ s, uint64_t n, uint64_t nchunks,
-                                              const double* __restrict__ cbase, double x) {
+                                              const double* __restrict__ cbase, double x, float2 (*buf)[17]) {
   const int lane = threadIdx.x & 31;
-  // smallest chunk c with cbase[c+1] >= x
-  uint64_t lo = 0, hi = nchunks;  // search in [0, nchunks)
+  // smallest chunk c with cbase[c+1] >= x (nchunks if none): a 32-way search,
+  // each lane probing one of 32 evenly spaced chunks per round.  cbase is
+  // non-decreasing, so this finds the same chunk as a binary search.
+  // Invariant: the answer is in [lo, hi], and cbase[hi+1] >= x if hi < nchunks.
+  uint64_t lo = 0, hi = nchunks;
   while (lo < hi) {
-    uint64_t mid = (lo + hi) >> 1;
-    if (cbase[mid + 1] >= x) hi = mid; else lo = mid + 1;
+    const uint64_t step = (hi - lo + 31) >> 5;
+    const uint64_t p = lo + (uint64_t)lane * step;
+    const unsigned m = __ballot_sync(0xffffffffu, p < hi && cbase[p + 1] >= x);
+    if (m != 0) {
+      const int j = __ffs(m) - 1;
+      const uint64_t pj = lo + (uint64_t)j * step;
+      lo = j ? pj - step + 1 : pj;
+      hi = pj;
+    } else {
+      lo += (hi - 1 - lo) / step * step + 1;  // past the last probed chunk
+    }
   }
   if (lo >= nchunks) return (int64_t)(n - 1);
   const uint64_t c = lo;
-  double v = seg_sum(s, c * kChunk + (uint64_t)lane * kSeg, n);
+  double v = seg_sum_staged(s, c * kChunk, n, lane, buf);
   double inc = warp_iscan(v);
   const double base = cbase[c];
   const bool hit = base + inc >= x;
@@ -408,8 +412,9 @@ __global__ void k_sample(const float2* __restrict__ s, uint64_t n, uint64_t nchu
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
+  __shared__ float2 stage[kThreads / 32][32][17];
   for (uint64_t k = warp; k < (uint64_t)nshots; k += nwarps) {
-    const int64_t result = sample_one(s, n, nchunks, cbase, u[k]);
+    const int64_t result = sample_one(s, n, nchunks, cbase, u[k], stage[threadIdx.x >> 5]);
     if (lane == 0) out[k] = result;
   }
 }
@@ -475,11 +480,13 @@ __global__ void k_sample_b(const float2* __restrict__ base, const SampleDesc* __
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
+  __shared__ float2 stage[kThreads / 32][32][17];
   for (uint64_t g = warp; g < total_shots; g += nwarps) {
     const int t = find_desc<&SampleDesc::shot_off>(d, ns, g);
     const SampleDesc D = d[t];
     const double x = qs_seed_uniform_at(D.seed, g - D.shot_off);
-    const int64_t result = sample_one(base + D.state_off, D.n, D.nchunks, cbase + D.chunk_off + t, x);
+    const int64_t result =
+        sample_one(base + D.state_off, D.n, D.nchunks, cbase + D.chunk_off + t, x, stage[threadIdx.x >> 5]);
     if (lane == 0) out[g] = result;
   }
 }
