@@ -650,13 +650,14 @@ int qs_measure(qs_handle_t h, void* state, int n, int t, double u, int* outcome)
   double* o = red_out(h);
   const uint64_t nvec = (1ull << n) / 2;
   reduce_to(h, FP0{(const float4*)state, t}, nvec, o, 0, red_part(h));
-  int* d_out = (int*)(o + 2);
-  qs_launch_pdl(h, k_collapse, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (float4*)state, nvec, t, u, o, d_out);
+  // the kernel writes the outcome straight into the handle's pinned buffer
+  // (page-locked host memory is addressable from the device under unified
+  // addressing), so no copy is queued between the kernel and the synchronise
+  int* pin = reinterpret_cast<int*>(h->pinned_get(64));
+  qs_launch_pdl(h, k_collapse, dim3(qs_blocks_for(h, nvec, kThreads)), dim3(kThreads), 0, (float4*)state, nvec, t, u, o, pin);
   qs_after_launch(h, "k_collapse");
-  double* pin = h->pinned_get(64);
-  QS_CUDA(cudaMemcpyAsync(pin, d_out, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   QS_CUDA(cudaStreamSynchronize(h->stream));
-  *outcome = *(int*)pin;
+  *outcome = *pin;
   QS_API_END(h)
 }
 

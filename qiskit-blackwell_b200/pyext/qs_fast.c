@@ -1,6 +1,7 @@
 /*
  * qs_fast.c — a CPython extension that forwards the per-gate calls of the
- * blackwell_kernels API to libqsim's C ABI with no argument marshalling.
+ * blackwell_kernels API (and the measurement and sampling calls) to libqsim's C ABI
+ * with no argument marshalling.
  *
  * The reference binds its kernels with pybind11 (bwk/csrc/apply_gate_sm120.cu:
  * 398-489); through ctypes the same calls spend about 1.5 us each converting
@@ -145,6 +146,27 @@ static PyObject* f_apply_mc2q_dev(PyObject* self, PyObject* const* args, Py_ssiz
   return rc ? fail(h, rc) : Py_NewRef(Py_None);
 }
 
+/* measure(h, state, n, t, u) -> outcome (0 or 1) */
+static PyObject* f_measure(PyObject* self, PyObject* const* args, Py_ssize_t nargs) {
+  if (!check_n(nargs, 5)) return NULL;
+  void* h = PTR(0);
+  const double u = PyFloat_AsDouble(args[4]);
+  int outcome = 0;
+  const int rc = qs_measure((qs_handle_t)h, PTR(1), INT(2), INT(3), u, &outcome);
+  if (PyErr_Occurred()) return NULL;
+  return rc ? fail(h, rc) : PyLong_FromLong(outcome);
+}
+
+/* sample(h, state, n, u, nshots, out) */
+static PyObject* f_sample(PyObject* self, PyObject* const* args, Py_ssize_t nargs) {
+  if (!check_n(nargs, 6)) return NULL;
+  void* h = PTR(0);
+  const long long nshots = PyLong_AsLongLong(args[4]);
+  const int rc = qs_sample((qs_handle_t)h, PTR(1), INT(2), (const double*)PTR(3), (int64_t)nshots, (int64_t*)PTR(5));
+  if (PyErr_Occurred()) return NULL;
+  return rc ? fail(h, rc) : Py_NewRef(Py_None);
+}
+
 static PyMethodDef kMethods[] = {
     {"set_error", (PyCFunction)f_set_error, METH_O, "exception class raised for a non-zero status"},
     {"apply_1q_dev", (PyCFunction)(void (*)(void))f_apply_1q_dev, METH_FASTCALL, "qs_apply_1q_dev"},
@@ -156,6 +178,8 @@ static PyMethodDef kMethods[] = {
     {"apply_phase", (PyCFunction)(void (*)(void))f_apply_phase, METH_FASTCALL, "qs_apply_phase"},
     {"apply_mc1q_dev", (PyCFunction)(void (*)(void))f_apply_mc1q_dev, METH_FASTCALL, "qs_apply_mc1q_dev"},
     {"apply_mc2q_dev", (PyCFunction)(void (*)(void))f_apply_mc2q_dev, METH_FASTCALL, "qs_apply_mc2q_dev"},
+    {"measure", (PyCFunction)(void (*)(void))f_measure, METH_FASTCALL, "qs_measure"},
+    {"sample", (PyCFunction)(void (*)(void))f_sample, METH_FASTCALL, "qs_sample"},
     {NULL, NULL, 0, NULL}};
 
 static struct PyModuleDef kModule = {PyModuleDef_HEAD_INIT, "_qsfast",

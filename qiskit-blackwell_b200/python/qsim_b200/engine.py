@@ -266,6 +266,10 @@ def probs_n(states: torch.Tensor, n_amps: int) -> torch.Tensor:
 
 def measure(state: torch.Tensor, target: int, u: float) -> int:
     n = check_state(state)
+    F = _lib.fast()
+    if F is not None:
+        dev = state.get_device()
+        return F.measure(_hptr(dev), state.data_ptr(), n, int(target), float(u))
     out = C.c_int()
     _h(state.device.index).call("qs_measure", _ptr(state), n, int(target), float(u), C.byref(out))
     return int(out.value)
@@ -277,6 +281,10 @@ def sample_u(state: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
     if u.dtype != torch.float64 or not u.is_cuda or not u.is_contiguous():
         raise RuntimeError("u must be a contiguous float64 CUDA tensor")
     out = torch.empty(u.numel(), dtype=torch.int64, device=state.device)
+    F = _lib.fast()
+    if F is not None and u.device == state.device:
+        F.sample(_hptr(state.get_device()), state.data_ptr(), n, u.data_ptr(), int(u.numel()), out.data_ptr())
+        return out
     _h(state.device.index).call("qs_sample", _ptr(state), n, _ptr(u), int(u.numel()), _ptr(out))
     return out
 
