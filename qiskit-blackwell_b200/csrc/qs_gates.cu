@@ -93,17 +93,73 @@ __global__ void k_1q_tn(float2* __restrict__ s, uint64_t nitems, int t, G2 G0, c
 }
 
 // K <= 12 single-qubit gates whose matrices and targets are device arrays,
-// applied in order in one launch (the device-tensor form of
-// apply_gates_fused: no host copy of the gates, no stream synchronisation).
-// Each CTA stages tiles of 2^T amplitudes (T = min(n, 12)) whose qubits are
-// the gates' distinct targets and the lowest other qubits, applies every
-// gate to the tile in shared memory as an FMA chain per output (each FMA
-// rounds once; the single-gate kernels' compensated Dot2 costs four times
-// the arithmetic, which bounds this kernel), and writes the tile back.  A
-// target outside [0, n) makes every CTA return before it writes (bit 16 of
-// the status word).
+// applied in one launch (the device-tensor form of apply_gates_fused: no host
+// copy of the gates, no stream synchronisation).  Each CTA stages tiles of
+// 2^T amplitudes (T = min(n, 12)) whose qubits are the gates' distinct
+// targets and the lowest other qubits, applies the gates to the tile in
+// shared memory as an FMA chain per output (each FMA rounds once; the
+// single-gate kernels' compensated Dot2 costs four times the arithmetic),
+// and writes the tile back.  Gates on different qubits commute, so the gates
+// are applied in groups of up to four on distinct tile positions, each gate
+// after every earlier gate on its own qubit: a thread holds the 2^G
+// amplitudes that a group mixes in registers and applies the group's gates
+// there, one shared-memory sweep and barrier per group instead of per gate
+// (ten gates on qubits 0, 2, ..., 18: three sweeps).  A group takes at most
+// one position below 5 when the tile has 10 or more qubits, which keeps a
+// warp's shared-memory accesses within two-way bank conflicts.  A target
+// outside [0, n) makes every CTA return before it writes (bit 16 of the
+// status word).
 constexpr int kFusedMax = 12;
-__global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s, int n, const float2* __restrict__ gates,
+constexpr int kFusedGroup = 2;
+constexpr int kFusedThreads = 512;
+
+// One sweep of a group of G gates over the tile: gate b of the group (matrix
+// M[b], tile position pos[b]) acts on register bit b of each thread's 2^G
+// amplitudes; srt = the group's positions ascending.
+template <int G>
+__device__ __forceinline__ void fused_group_sweep(float2* __restrict__ tile, uint32_t tsize, const int* gidx,
+                                                  const int* srt_s, const G2* sg, const int* spos) {
+  int pos[G], srt[G];
+  G2 M[G];
+#pragma unroll
+  for (int b = 0; b < G; ++b) {
+    pos[b] = spos[gidx[b]];
+    M[b] = sg[gidx[b]];
+    srt[b] = srt_s[b];
+  }
+  uint32_t off[1 << G];
+#pragma unroll
+  for (int c = 0; c < (1 << G); ++c) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int b = 0; b < G; ++b)
+      if ((c >> b) & 1) o |= 1u << pos[b];
+    off[c] = o;
+  }
+  const uint32_t nitems = tsize >> G;
+  for (uint32_t j = threadIdx.x; j < nitems; j += blockDim.x) {
+    uint32_t base = j;
+#pragma unroll
+    for (int b = 0; b < G; ++b) base = (uint32_t)insert_zero(base, srt[b]);
+    float2 a[1 << G];
+#pragma unroll
+    for (int c = 0; c < (1 << G); ++c) a[c] = tile[base | off[c]];
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+#pragma unroll
+      for (int c = 0; c < (1 << G); ++c) {
+        if ((c >> b) & 1) continue;
+        const int c1 = c | (1 << b);
+        const float2 x0 = a[c], x1 = a[c1];
+        a[c] = cfma2(M[b].g[0], x0, M[b].g[1], x1);
+        a[c1] = cfma2(M[b].g[2], x0, M[b].g[3], x1);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < (1 << G); ++c) tile[base | off[c]] = a[c];
+  }
+}
+__global__ void __launch_bounds__(kFusedThreads, 2) k_fused1q_dev(float2* __restrict__ s, int n, const float2* __restrict__ gates,
                                                           const int32_t* __restrict__ targets, int K,
                                                           uint32_t* status) {
   pdl_begin();
@@ -113,6 +169,10 @@ __global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s
   __shared__ int spos[kFusedMax];   // tile position of gate k's target
   __shared__ int sq[kFusedMax];     // tile qubits, ascending
   __shared__ uint64_t dep[2][64];   // tile index bits -> state index bits (6 + 6)
+  __shared__ int gidx[kFusedMax][kFusedGroup];  // groups: gate indices, application order
+  __shared__ int gsrt[kFusedMax][kFusedGroup];  // groups: tile positions ascending
+  __shared__ int gsize[kFusedMax];
+  __shared__ int s_ngroups;
   __shared__ int s_ok;
   const int T = n < kFusedMax ? n : kFusedMax;
   // one round trip for the gates' matrices and targets, then thread 0 picks
@@ -121,18 +181,63 @@ __global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s
   if ((int)threadIdx.x < 4 * K) sg[threadIdx.x >> 2].g[threadIdx.x & 3] = gates[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
+    // thread 0 alone, while the CTA waits at the barrier: the targets and
+    // positions live in registers (loops unrolled over kFusedMax), so the
+    // setup costs no shared-memory round trips
+    int tg[kFusedMax];
     uint64_t m = 0;
     int ok = 1;
-    for (int k = 0; k < K; ++k) {
-      const int t = st[k];
-      if (t < 0 || t >= n) ok = 0; else m |= 1ull << t;
+#pragma unroll
+    for (int k = 0; k < kFusedMax; ++k) {
+      tg[k] = k < K ? st[k] : 0;
+      if (k < K) {
+        if (tg[k] < 0 || tg[k] >= n) ok = 0; else m |= 1ull << tg[k];
+      }
     }
     for (int q = 0; q < n && __popcll(m) < T; ++q) m |= 1ull << q;
-    int j = 0;
-    for (int q = 0; q < n; ++q)
-      if ((m >> q) & 1ull) sq[j++] = q;
+    {
+      uint64_t r = m;
+      for (int j = 0; r != 0; ++j, r &= r - 1) sq[j] = __ffsll((long long)r) - 1;
+    }
     if (ok) {
-      for (int k = 0; k < K; ++k) spos[k] = __popcll(m & ((1ull << st[k]) - 1ull));
+      int sp[kFusedMax];
+      uint32_t same[kFusedMax];  // earlier gates on the same position
+#pragma unroll
+      for (int k = 0; k < kFusedMax; ++k) {
+        sp[k] = __popcll(m & ((1ull << tg[k]) - 1ull));
+        spos[k] = sp[k];
+        same[k] = 0;
+#pragma unroll
+        for (int k2 = 0; k2 < k; ++k2)
+          if (sp[k2] == sp[k]) same[k] |= 1u << k2;
+      }
+      // groups: scan the unscheduled gates in order and take gate k unless
+      // an earlier unscheduled gate (in this group or later) has its
+      // position, the group is full, or it would be a second low position
+      const int lowlim = T >= 10 ? 5 : 0;
+      const uint32_t all = (1u << K) - 1u;
+      uint32_t done = 0;
+      int ng = 0;
+      while (done != all) {
+        int cnt = 0;
+        uint32_t used = 0, pick = 0;
+        bool low = false;
+#pragma unroll
+        for (int k = 0; k < kFusedMax; ++k) {
+          const int p = sp[k];
+          if (k < K && cnt < kFusedGroup && !((done >> k) & 1u) && !(same[k] & ~done) && !(p < lowlim && low)) {
+            gidx[ng][cnt++] = k;
+            used |= 1u << p;
+            pick |= 1u << k;
+            if (p < lowlim) low = true;
+          }
+        }
+        done |= pick;
+        uint32_t r = used;
+        for (int j = 0; r != 0; ++j, r &= r - 1) gsrt[ng][j] = __ffs((int)r) - 1;
+        gsize[ng++] = cnt;
+      }
+      s_ngroups = ng;
     } else if (blockIdx.x == 0) {
       atomicOr(status, 16u);
     }
@@ -150,23 +255,18 @@ __global__ void __launch_bounds__(kThreads) k_fused1q_dev(float2* __restrict__ s
     dep[part][x] = d;
   }
   __syncthreads();
-  const uint32_t tsize = 1u << T, half = tsize >> 1;
+  const uint32_t tsize = 1u << T;
   const uint64_t ntiles = 1ull << (n - T);
   for (uint64_t tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
     uint64_t gbase = tl;
     for (int k = 0; k < T; ++k) gbase = insert_zero(gbase, sq[k]);
-#pragma unroll 8
+#pragma unroll 16
     for (uint32_t i = threadIdx.x; i < tsize; i += blockDim.x) tile[i] = s[gbase | dep[0][i & 63] | dep[1][i >> 6]];
     __syncthreads();
-    for (int k = 0; k < K; ++k) {
-      const int p = spos[k];
-      const G2 G = sg[k];
-#pragma unroll 4
-      for (uint32_t j = threadIdx.x; j < half; j += blockDim.x) {
-        const uint32_t i0 = (uint32_t)insert_zero(j, p), i1 = i0 | (1u << p);
-        const float2 a0 = tile[i0], a1 = tile[i1];
-        tile[i0] = cfma2(G.g[0], a0, G.g[1], a1);
-        tile[i1] = cfma2(G.g[2], a0, G.g[3], a1);
+    for (int g = 0; g < s_ngroups; ++g) {
+      switch (gsize[g]) {
+        case 1: fused_group_sweep<1>(tile, tsize, gidx[g], gsrt[g], sg, spos); break;
+        default: fused_group_sweep<2>(tile, tsize, gidx[g], gsrt[g], sg, spos); break;
       }
       __syncthreads();
     }
@@ -569,7 +669,7 @@ int qs_apply_gates_fused_dev(qs_handle_t h, void* state, int n, const void* gate
   // at most 12 gates per launch, so their distinct targets always fit a tile
   for (int k0 = 0; k0 < n_gates; k0 += kFusedMax) {
     const int K = std::min(kFusedMax, n_gates - k0);
-    k_fused1q_dev<<<grid, kThreads, smem, h->stream>>>((float2*)state, n, g + 4 * k0, t + k0, K, h->dev_status);
+    k_fused1q_dev<<<grid, kFusedThreads, smem, h->stream>>>((float2*)state, n, g + 4 * k0, t + k0, K, h->dev_status);
     qs_after_launch(h, "k_fused1q_dev");
   }
   QS_API_END(h)

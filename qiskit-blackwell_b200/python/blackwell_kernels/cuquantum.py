@@ -121,6 +121,23 @@ def apply_gate_2q(state: torch.Tensor, gate: torch.Tensor, qubit0: int, qubit1: 
 
 def apply_gates_fused(state: torch.Tensor, gates: torch.Tensor, targets: torch.Tensor) -> torch.Tensor:
     """K 1Q gates in one fused program (cuquantum.py:69-80)."""
+    F = _lib.fast()
+    if (F is not None and type(state) is torch.Tensor and type(gates) is torch.Tensor
+            and type(targets) is torch.Tensor and state.is_cuda and state.dtype == _C64
+            and gates.dtype == _C64 and targets.dtype == torch.int32 and gates.dim() == 3
+            and targets.dim() == 1 and state.is_contiguous() and gates.is_contiguous()
+            and targets.is_contiguous()):
+        # the common case in the fewest tensor queries: contiguous complex64
+        # gates and int32 targets already on the state's device
+        dev = state.get_device()
+        N = state.numel()
+        K = targets.shape[0]
+        tp = targets.data_ptr()
+        if (gates.get_device() == dev and targets.get_device() == dev and gates.shape[0] == K
+                and gates.shape[1] == 2 and gates.shape[2] == 2 and N >= 2 and not (N & (N - 1))
+                and not (tp & 7)):
+            F.apply_gates_fused_dev(E._hptr(dev), state.data_ptr(), N.bit_length() - 1, gates.data_ptr(), tp, K)
+            return state
     n = check_state(state)
     if (isinstance(gates, torch.Tensor) and isinstance(targets, torch.Tensor) and gates.is_cuda
             and gates.device == state.device and targets.device == state.device):
