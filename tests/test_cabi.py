@@ -65,6 +65,16 @@ def test_fast_extension_binds_the_same_library():
         F.apply_1q_dev(0, 0, 3, 0, 0)
     with pytest.raises(RuntimeError, match="0-7"):
         F.apply_mc1q_dev(0, 0, 3, 0, list(range(8)), 0)
+    # every call the Python layer routes through the extension, each
+    # reaching the library (a null handle is refused before any CUDA call)
+    for name, args in [("apply_2q_dev", (0, 0, 3, 0, 0, 1)), ("apply_gates_fused_dev", (0, 0, 3, 0, 0, 2)),
+                       ("apply_diag1_dev", (0, 0, 3, 0, 0)), ("apply_diag2_dev", (0, 0, 3, 0, 0, 1)),
+                       ("apply_phase", (0, 0, 3, 1.0, 0.0, 0)), ("apply_mc2q_dev", (0, 0, 3, 0, [2], 0, 1)),
+                       ("measure", (0, 0, 3, 0, 0.5)), ("sample", (0, 0, 3, 0, 10, 0))]:
+        with pytest.raises(_lib.QsimError, match="null handle"):
+            getattr(F, name)(*args)
+    with pytest.raises(TypeError, match="expected 5 arguments"):
+        F.measure(0, 0, 3, 0)
 
 
 def test_autotune_table_set_get_and_range(lib):
